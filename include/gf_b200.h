@@ -1,0 +1,221 @@
+/*
+ * gf_b200.h -- C ABI of the B200 filtering library (libgfb200.so).
+ *
+ * Drop-in boundary for GeneralisedFilters' filtering hot path.  Every entry
+ * point is `extern "C"`, takes plain pointers and sizes, and names the Julia
+ * function of TuringLang/SSMProblems.jl it replaces (paths are relative to the
+ * reference project root).  A Julia caller binds these with `ccall`; the
+ * Python host layer (gfb200) binds them with ctypes.
+ *
+ * Conventions
+ *   - Matrices are FP64, column-major (Julia's layout): M[i + j*rows].
+ *   - Particle state buffers are structure-of-arrays: X[d*N + i] (a Julia
+ *     Matrix{T}(N, width)).
+ *   - Ancestor indices crossing the ABI are 1-based, like the reference.
+ *   - `memspace` says where every buffer argument of the call lives:
+ *     GF_MEM_HOST (pageable or pinned host memory; the call copies) or
+ *     GF_MEM_DEVICE (device memory of the context's GPU).
+ *   - A gf_ctx is not thread-safe: use one per host thread.  Calls are
+ *     ordered on the context's stream; calls taking GF_MEM_HOST buffers
+ *     return after the results are in host memory.
+ *   - Errors are returned as gf_status; gf_last_error() gives the message.
+ */
+#ifndef GF_B200_H
+#define GF_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t gf_status;
+enum {
+  GF_OK = 0,
+  GF_ERR_NOT_PD = 1,      /* a covariance lost positive definiteness (PosDefException) */
+  GF_ERR_DIM = 2,         /* unsupported or inconsistent dimensions (DimensionMismatch) */
+  GF_ERR_OOM_BUDGET = 3,  /* request exceeds the context's HBM budget */
+  GF_ERR_TIMEOUT = 4,     /* a bounded device-side wait gave up */
+  GF_ERR_CUDA = 5,        /* CUDA runtime error */
+  GF_ERR_ARG = 6,         /* invalid argument (ArgumentError) */
+  GF_ERR_UNSUPPORTED = 7, /* feature not supported by this build */
+  GF_ERR_BUSY = 8         /* serving queue full */
+};
+
+enum { GF_MEM_HOST = 0, GF_MEM_DEVICE = 1 };
+enum { GF_RS_SYSTEMATIC = 0, GF_RS_STRATIFIED = 1, GF_RS_MULTINOMIAL = 2 };
+/* GF_CONV_CPU: resamplers.jl:214-238 rule a_i = min{k : n*W_k > u_i}, extended
+ * to stratified u_i = (i-1) + U_i and multinomial (first W_k >= U_i*W_n).
+ * GF_CONV_CUDAEXT: the cumulative-offspring rule of ext/CUDAExt.jl:49-78. */
+enum { GF_CONV_CPU = 0, GF_CONV_CUDAEXT = 1 };
+enum { GF_PREC_F32 = 0, GF_PREC_F64 = 1 };
+/* Proposals: BootstrapFilter (particles.jl:197-245); GFTest OptimalProposal
+ * (GFTest/proposals.jl:11-31); GFTest OverdispersedProposal (:33-50). */
+enum { GF_PROP_BOOTSTRAP = 0, GF_PROP_OPTIMAL = 1, GF_PROP_OVERDISPERSED = 2 };
+enum { GF_ALGO_KF = 0, GF_ALGO_SRKF = 1 };
+
+typedef struct gf_ctx gf_ctx;
+
+/* Homogeneous linear-Gaussian SSM: create_homogeneous_linear_gaussian_model
+ * (models/linear_gaussian.jl:125-131). */
+typedef struct {
+  int32_t dx, dy;
+  const double* mu0;    /* dx */
+  const double* Sigma0; /* dx*dx */
+  const double* A;      /* dx*dx */
+  const double* b;      /* dx */
+  const double* Q;      /* dx*dx */
+  const double* H;      /* dy*dx */
+  const double* c;      /* dy */
+  const double* R;      /* dy*dy */
+} gf_lg_model;
+
+/* Conditionally linear-Gaussian HierarchicalSSM (models/hierarchical.jl:4-50):
+ * outer x_t = A_o x_{t-1} + b_o + N(0, Q_o); inner z_t = A_z z_{t-1} + b_z +
+ * C_z x_{t-1} + N(0, Q_z * exp(q_gamma * x_t[q_index])); y_t = H z_t + c + N(0, R).
+ * C_z (dz*dxo) follows GFTest's InnerDynamics (dummy_linear_gaussian.jl:25-46);
+ * the exp(.) scale is the stochastic-volatility shape of the trend-inflation
+ * example (examples/trend-inflation/script.jl:93-165). */
+typedef struct {
+  int32_t dxo, dz, dy;
+  const double *mu_o, *Sigma_o, *A_o, *b_o, *Q_o;
+  const double *mu_z, *Sigma_z, *A_z, *b_z, *C_z, *Q_z;
+  double q_gamma;
+  int32_t q_index;
+  const double *H, *c, *R;
+} gf_rb_model;
+
+/* ParticleFilter(N, proposal; threshold, resampler) (particles.jl:92-108)
+ * wrapped in ESSResampler (resamplers.jl:171-183). */
+typedef struct {
+  int64_t n_particles;
+  int32_t resampler;      /* GF_RS_* */
+  int32_t convention;     /* GF_CONV_* */
+  double threshold;       /* resample iff threshold*N >= ESS (inclusive) */
+  int32_t precision;      /* GF_PREC_F32 (FP32 state, FP64 normaliser) or GF_PREC_F64 */
+  int32_t proposal;       /* GF_PROP_* */
+  double proposal_k;      /* overdispersion factor for GF_PROP_OVERDISPERSED */
+  uint64_t seed;          /* Philox key for in-kernel noise / uniforms */
+  const int8_t* schedule; /* nullable, host [T]: -1 ESS rule, 0 keep, 1 resample
+                             (GFTest AlternatingResampler-style forcing) */
+} gf_pf_config;
+
+/* Outputs of one particle-filter run; every pointer but `ll` is nullable. */
+typedef struct {
+  double* ll;          /* [1]  log-evidence returned by filter() */
+  double* ll_steps;    /* [T]  per-step increments (GeneralisedFilters.jl:76-81) */
+  double* ess_steps;   /* [T]  ESS seen by the resampling decision of step t */
+  int8_t* resampled;   /* [T]  1 if step t resampled */
+  int32_t* ancestors;  /* [T][N] 1-based; identity on steps that did not resample */
+  double* means;       /* [T][dx] weighted filtered means (outer means for RBPF) */
+  void* states;        /* [width][N] final particle states (precision of the run) */
+  double* log_weights; /* [N] final normalised log-weights */
+  int32_t* clamps;     /* [1] slots clamped to N by the ancestor search */
+} gf_pf_out;
+
+/* Outputs of a Kalman batch (per-step arrays are packed filter after filter). */
+typedef struct {
+  double* ll;        /* [B] total log-likelihood per filter */
+  double* ll_steps;  /* [sum_f T_f] */
+  float* means;      /* [sum_f T_f*dx_f] filtered means */
+  float* covs;       /* [sum_f T_f*dx_f*dx_f] filtered covariances, column-major */
+  int32_t* status;   /* [B] per-filter gf_status */
+} gf_kf_out;
+
+/* ------------------------------------------------------------------ context */
+/* Creates a context on `device` with an HBM budget (0 = 90% of free memory). */
+gf_status gf_ctx_create(int32_t device, size_t hbm_budget_bytes, gf_ctx** out);
+gf_status gf_ctx_destroy(gf_ctx* ctx);
+const char* gf_last_error(const gf_ctx* ctx);
+/* Use `stream` (a cudaStream_t) for all work of this context (NULL = own stream). */
+gf_status gf_ctx_set_stream(gf_ctx* ctx, void* stream);
+void* gf_ctx_get_stream(gf_ctx* ctx);
+gf_status gf_ctx_synchronize(gf_ctx* ctx);
+/* Bytes of HBM the context currently holds / may hold. */
+gf_status gf_ctx_memory(const gf_ctx* ctx, size_t* used, size_t* budget);
+/* Per-kernel timing with CUDA events on the context stream (0 = off). */
+gf_status gf_ctx_profile(gf_ctx* ctx, int32_t enable);
+/* Kernel classes: 0 propagate/weight, 1 lookback scan, 2 KF batch, 3 RBPF,
+ * 4 init/prep.  Resolves pending events (synchronises the stream). */
+gf_status gf_ctx_profile_read(gf_ctx* ctx, int32_t kernel_class, double* total_ms,
+                              int64_t* launches);
+int32_t gf_version(void);
+
+/* ---------------------------------------------------------- Kalman filters */
+/* filter(model, KalmanFilter(; jitter), ys) / filter(model, SRKF(; jitter), ys)
+ * for B independent models at once (kalman.jl:23-79, kalman_gradient.jl:12-29,
+ * srkf.jl:41-176).  ys: concatenated [sum_f T_f*dy_f] FP64, step-major.
+ * jitter is applied iff use_jitter != 0 (KalmanFilter(jitter=nothing) default). */
+gf_status gf_kf_batch(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
+                      const int32_t* T, const double* ys, double jitter, int32_t use_jitter,
+                      int32_t memspace, gf_kf_out* out);
+
+/* Batched plan: uploads the models once, buckets filters by dimension,
+ * autotunes the per-bucket group shape and captures one CUDA graph of
+ * persistent launches.  Run with device-resident ys and outputs. */
+typedef struct gf_kf_plan gf_kf_plan;
+gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
+                            const int32_t* T, double jitter, int32_t use_jitter,
+                            int32_t flags, gf_kf_plan** out);
+gf_status gf_kf_plan_run(gf_kf_plan* plan, const double* ys_dev, gf_kf_out* out_dev);
+gf_status gf_kf_plan_destroy(gf_kf_plan* plan);
+/* flags for gf_kf_plan_create */
+enum { GF_PLAN_AUTOTUNE = 1, GF_PLAN_NO_GRAPH = 2, GF_PLAN_PLAIN = 4 };
+
+/* -------------------------------------------------------- particle filters */
+/* filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys)
+ * (GeneralisedFilters.jl:58-84; particles.jl:36-90,147-245; resamplers.jl:
+ * 33-238; containers.jl:140-173).  ys: [T][dy] FP64.
+ * noise: nullable [(T+1)][dx][N] standard normals in the run's precision
+ *   (step 0 = prior draw); NULL draws them in-kernel from Philox(seed).
+ * uniforms: nullable FP64, systematic [T], stratified/multinomial [T][N];
+ *   NULL draws them from Philox(seed). */
+gf_status gf_pf_run(gf_ctx* ctx, const gf_lg_model* model, const gf_pf_config* cfg, int32_t T,
+                    const double* ys, const void* noise, const double* uniforms,
+                    int32_t memspace, gf_pf_out* out);
+
+/* Reusable PF plan: device buffers sized once, the T-step loop captured in a
+ * CUDA graph; gf_pf_plan_run takes device-resident inputs and outputs. */
+typedef struct gf_pf_plan gf_pf_plan;
+gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* model, const gf_pf_config* cfg,
+                            int32_t T, int32_t flags, gf_pf_plan** out);
+gf_status gf_pf_plan_run(gf_pf_plan* plan, const double* ys_dev, const void* noise_dev,
+                         const double* uniforms_dev, gf_pf_out* out_dev);
+gf_status gf_pf_plan_destroy(gf_pf_plan* plan);
+
+/* filter(rng, hier_model, RBPF(PF(N, ...), KalmanFilter()), ys) (rbpf.jl:8-84).
+ * Supports GF_PROP_BOOTSTRAP and GF_PROP_OVERDISPERSED outer proposals.
+ * noise: nullable [(T+1)][dxo][N] FP32.  states out: GF_MEM_HOST gives
+ * [dxo + dz + dz*dz][N] (x, mu, Sigma column-major); GF_MEM_DEVICE gives the
+ * device layout [dxo + dz + dz*(dz+1)/2][N] (Sigma packed upper, row by row).
+ * means / zmeans ([T][dz] weighted inner means) need GF_MEM_HOST. */
+gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* model, const gf_pf_config* cfg, int32_t T,
+                      const double* ys, const void* noise, const double* uniforms,
+                      int32_t memspace, gf_pf_out* out, double* zmeans);
+
+/* ---------------------------------------------------- resampling primitives */
+/* sample_ancestors(rng, resampler, weights) (resamplers.jl:206-238;
+ * ext/CUDAExt.jl:31-78) on device buffers: weights [n] FP64 (need not be
+ * normalised), uniforms [1] (systematic) or [n], ancestors out [n] int64,
+ * 1-based. */
+gf_status gf_sample_ancestors(gf_ctx* ctx, int32_t resampler, int32_t convention, int64_t n,
+                              const double* weights_dev, const double* uniforms_dev,
+                              int64_t* ancestors_dev);
+/* offspring_to_ancestors (ext/CUDAExt.jl:90-117): cumulative offspring ->
+ * 1-based ancestors, device int64 buffers of length n. */
+gf_status gf_offspring_to_ancestors(gf_ctx* ctx, int64_t n, const int64_t* offspring_dev,
+                                    int64_t* ancestors_dev);
+/* ancestors_to_offspring (ext/CUDAExt.jl:119-142): 1-based ancestors ->
+ * offspring counts. */
+gf_status gf_ancestors_to_offspring(gf_ctx* ctx, int64_t n, const int64_t* ancestors_dev,
+                                    int64_t* offspring_dev);
+/* The noise the PF kernels draw in-kernel for step t: out [dx][n] in the given
+ * precision (no reference counterpart: exported so tests can inject it). */
+gf_status gf_rng_normals(gf_ctx* ctx, uint64_t seed, int32_t t, int32_t dx, int64_t n,
+                         int32_t precision, void* out_dev);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* GF_B200_H */

@@ -1,0 +1,395 @@
+"""TEST INFRASTRUCTURE ONLY -- ctypes front end of the FP64 CPU oracle.
+
+The oracle restates GeneralisedFilters' filtering path (KF, SRKF, bootstrap and
+guided PF, systematic/stratified/multinomial resampling, RBPF) in plain C
+(``gf_oracle.c``) plus the numpy pieces below.  Only ``tests/``, the smoke
+check in ``__graft_entry__`` and the CPU-baseline leg of ``bench.py`` import
+this module; the product never does.
+
+numpy helpers restated here:
+* ``compute_joint`` -- the joint-Gaussian construction of
+  GFTest/models/linear_gaussian.jl:171-215 used by test/algorithms/kalman.jl:5-43;
+* ``rand_cov`` -- GFTest/utils.jl:15-36;
+* ``create_linear_gaussian_model`` -- GFTest/models/linear_gaussian.jl:6-38
+  (numpy-seeded: Julia's StableRNG streams cannot be reproduced here);
+* ``sample`` -- SSMProblems/src/utils/forward_simulation.jl:14-26.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+BUILD = os.path.join(HERE, "_build")
+LIB_PATH = os.path.join(BUILD, "libgforacle.so")
+
+SYSTEMATIC, STRATIFIED, MULTINOMIAL = 0, 1, 2
+CONV_CPU, CONV_CUDAEXT = 0, 1
+PROP_BOOTSTRAP, PROP_OPTIMAL, PROP_OVERDISPERSED = 0, 1, 2
+
+
+def build(force: bool = False) -> str:
+    """Compile gf_oracle.c into oracle/_build/libgforacle.so."""
+    src = os.path.join(HERE, "gf_oracle.c")
+    if (not force and os.path.exists(LIB_PATH)
+            and os.path.getmtime(LIB_PATH) >= os.path.getmtime(src)):
+        return LIB_PATH
+    os.makedirs(BUILD, exist_ok=True)
+    subprocess.check_call(["gcc", "-O2", "-fPIC", "-shared", "-fopenmp", "-o",
+                           LIB_PATH, src, "-lm"])
+    return LIB_PATH
+
+
+_lib = None
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        build()
+        _lib = C.CDLL(LIB_PATH)
+        _lib.or_logsumexp.restype = C.c_double
+        _lib.or_philox_uniform.restype = C.c_double
+    return _lib
+
+
+_dp = C.POINTER(C.c_double)
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(_dp)
+
+
+def _f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def _fortran(a):
+    return np.asfortranarray(np.asarray(a, dtype=np.float64))
+
+
+class _LG(C.Structure):
+    _fields_ = [("dx", C.c_int), ("dy", C.c_int)] + [
+        (n, _dp) for n in ("mu0", "Sigma0", "A", "b", "Q", "H", "c", "R")]
+
+
+class _RC(C.Structure):
+    _fields_ = [("kind", C.c_int), ("conv", C.c_int), ("threshold", C.c_double),
+                ("schedule", C.POINTER(C.c_int8))]
+
+
+class _Prop(C.Structure):
+    _fields_ = [("kind", C.c_int), ("k", C.c_double)]
+
+
+class _PFOut(C.Structure):
+    _fields_ = [("ll_steps", _dp), ("ess", _dp), ("resampled", C.POINTER(C.c_int8)),
+                ("ancestors", C.POINTER(C.c_int32)), ("margins", _dp), ("means", _dp),
+                ("x_final", _dp), ("logw_final", _dp), ("clamps", C.POINTER(C.c_long))]
+
+
+class _RB(C.Structure):
+    _fields_ = ([("dxo", C.c_int), ("dz", C.c_int), ("dy", C.c_int)]
+                + [(n, _dp) for n in ("mu_o", "Sigma_o", "A_o", "b_o", "Q_o",
+                                      "mu_z", "Sigma_z", "A_z", "b_z", "C_z", "Q_z")]
+                + [("q_gamma", C.c_double), ("q_index", C.c_int)]
+                + [(n, _dp) for n in ("H", "c", "R")])
+
+
+class LGModel:
+    """Plain FP64 container of a homogeneous linear-Gaussian SSM
+    (models/linear_gaussian.jl:96-131): mu0, Sigma0, A, b, Q, H, c, R."""
+
+    def __init__(self, mu0, Sigma0, A, b, Q, H, c, R):
+        self.mu0, self.b, self.c = _f64(mu0).ravel(), _f64(b).ravel(), _f64(c).ravel()
+        self.Sigma0, self.A, self.Q = _fortran(Sigma0), _fortran(A), _fortran(Q)
+        self.H, self.R = _fortran(np.atleast_2d(H)), _fortran(np.atleast_2d(R))
+        self.dx, self.dy = self.A.shape[0], self.H.shape[0]
+
+    def _struct(self):
+        s = _LG(self.dx, self.dy, *[_p(getattr(self, n)) for n in
+                                    ("mu0", "Sigma0", "A", "b", "Q", "H", "c", "R")])
+        return s
+
+
+def kf_filter(m: LGModel, ys, jitter=None, algo="kf"):
+    """filter(model, KF()/SRKF(), ys) -> (ll, ll_steps, mus[T,dx], Sigmas[T,dx,dx])."""
+    ys = _f64(ys).reshape(-1, m.dy)
+    T = ys.shape[0]
+    ll = C.c_double()
+    lls = np.zeros(T)
+    mus = np.zeros((T, m.dx))
+    sig = np.zeros((T, m.dx, m.dx))
+    f = lib().or_kf_filter if algo == "kf" else lib().or_srkf_filter
+    st = f(C.byref(m._struct()), T, _p(ys), C.c_double(jitter or 0.0),
+           int(jitter is not None), C.byref(ll), _p(lls), _p(mus), _p(sig))
+    if st:
+        raise np.linalg.LinAlgError(f"oracle KF status {st}")
+    # Sigmas are column-major per step; transpose to row-major numpy
+    return ll.value, lls, mus, np.ascontiguousarray(sig.transpose(0, 2, 1))
+
+
+def pf_run(m: LGModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=0.5,
+           schedule=None, noise=None, uniforms=None, seed=0, proposal=PROP_BOOTSTRAP,
+           k=1.0, want_ancestors=False, want_margins=False, threads=1):
+    """filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys).
+
+    noise: [(T+1), dx, N] standard normals (step 0 = prior draw) or None for the
+    shared Philox stream with ``seed``; uniforms: systematic [T], else [T, N].
+    Returns a dict of outputs (ll, ll_steps, ess, resampled, ancestors (1-based),
+    margins, means, x_final [N,dx], logw_final, clamps)."""
+    ys = _f64(ys).reshape(-1, m.dy)
+    T = ys.shape[0]
+    out = dict(ll_steps=np.zeros(T), ess=np.zeros(T), resampled=np.zeros(T, np.int8),
+               means=np.zeros((T, m.dx)), x_final=np.zeros((N, m.dx)),
+               logw_final=np.zeros(N))
+    anc = np.zeros((T, N), np.int32) if want_ancestors else None
+    mar = np.zeros((T, N)) if want_margins else None
+    clamps = C.c_long(0)
+    o = _PFOut(_p(out["ll_steps"]), _p(out["ess"]),
+               out["resampled"].ctypes.data_as(C.POINTER(C.c_int8)),
+               None if anc is None else anc.ctypes.data_as(C.POINTER(C.c_int32)),
+               _p(mar), _p(out["means"]), _p(out["x_final"]), _p(out["logw_final"]),
+               C.pointer(clamps))
+    sched = None if schedule is None else np.ascontiguousarray(schedule, np.int8)
+    rc = _RC(resampler, conv, threshold,
+             None if sched is None else sched.ctypes.data_as(C.POINTER(C.c_int8)))
+    nz = None if noise is None else _f64(noise)
+    un = None if uniforms is None else _f64(uniforms)
+    ll = C.c_double()
+    lib().or_set_threads(int(threads))
+    st = lib().or_pf_run(C.byref(m._struct()), C.byref(_Prop(proposal, k)), C.byref(rc),
+                         C.c_long(N), T, _p(ys), _p(nz), _p(un), C.c_uint64(seed),
+                         C.byref(ll), C.byref(o))
+    lib().or_set_threads(1)
+    if st:
+        raise np.linalg.LinAlgError(f"oracle PF status {st}")
+    out["ll"] = ll.value
+    out["ancestors"] = anc
+    out["margins"] = mar
+    out["clamps"] = clamps.value
+    return out
+
+
+def pf_step(m: LGModel, x, logw, y, noise_t, u, *, uniform=False, resampler=SYSTEMATIC,
+            conv=CONV_CPU, threshold=0.5, decision=-1):
+    """One bootstrap PF step from a given state (teacher forcing).  x: [N, dx]
+    FP64, logw: [N] normalised; noise_t: [dx, N]; u: this step's uniforms."""
+    N = x.shape[0]
+    x = np.ascontiguousarray(x, np.float64).copy()
+    logw = np.ascontiguousarray(logw, np.float64).copy()
+    anc = np.zeros(N, np.int32)
+    mar = np.zeros(N)
+    ess = C.c_double()
+    res = C.c_int8()
+    inc = C.c_double()
+    sched = np.array([decision], np.int8)
+    rc = _RC(resampler, conv, threshold, sched.ctypes.data_as(C.POINTER(C.c_int8)))
+    un = _f64(np.atleast_1d(u))
+    st = lib().or_pf_step(C.byref(m._struct()), C.byref(rc), C.c_long(N), 1,
+                          _p(_f64(y).ravel()), _p(_f64(noise_t)), _p(un), int(uniform),
+                          _p(x), _p(logw), anc.ctypes.data_as(C.POINTER(C.c_int32)),
+                          _p(mar), C.byref(ess), C.byref(res), C.byref(inc))
+    if st:
+        raise np.linalg.LinAlgError(f"oracle PF step status {st}")
+    return dict(x=x, logw=logw, ancestors=anc, margins=mar, ess=ess.value,
+                resampled=bool(res.value), ll_inc=inc.value)
+
+
+def sample_ancestors(kind, weights, u, conv=CONV_CPU):
+    """sample_ancestors(rng, resampler, weights) with injected uniforms.
+    Returns (ancestors 1-based int32, margins, clamps)."""
+    w = _f64(weights)
+    n = w.shape[0]
+    anc = np.zeros(n, np.int32)
+    mar = np.zeros(n)
+    un = _f64(np.atleast_1d(u))
+    cl = lib().or_sample_ancestors(kind, conv, C.c_long(n), _p(w), _p(un),
+                                   anc.ctypes.data_as(C.POINTER(C.c_int32)), _p(mar))
+    return anc, mar, cl
+
+
+def offspring_to_ancestors(offspring):
+    o = np.ascontiguousarray(offspring, np.int64)
+    a = np.zeros_like(o)
+    lib().or_offspring_to_ancestors(C.c_long(o.size), o.ctypes.data_as(C.POINTER(C.c_int64)),
+                                    a.ctypes.data_as(C.POINTER(C.c_int64)))
+    return a
+
+
+def ancestors_to_offspring(ancestors):
+    a = np.ascontiguousarray(ancestors, np.int64)
+    o = np.zeros_like(a)
+    lib().or_ancestors_to_offspring(C.c_long(a.size), a.ctypes.data_as(C.POINTER(C.c_int64)),
+                                    o.ctypes.data_as(C.POINTER(C.c_int64)))
+    return o
+
+
+def philox_normals(seed, N, dx, t):
+    """[dx, N] normals of step t from the shared Philox stream (FP64 Box-Muller)."""
+    out = np.zeros((dx, N))
+    buf = (C.c_double * 4)()
+    for i in range(N):
+        for q in range((dx + 3) // 4):
+            lib().or_philox_normals4(C.c_uint64(seed), i, t, q, buf)
+            for r in range(4):
+                if 4 * q + r < dx:
+                    out[4 * q + r, i] = buf[r]
+    return out
+
+
+def philox_uniform(seed, j, t):
+    return lib().or_philox_uniform(C.c_uint64(seed), j, t)
+
+
+class RBModel:
+    """Conditionally linear-Gaussian HierarchicalSSM (models/hierarchical.jl:4-50):
+    outer LG state x, inner LG state z with b_t = b_z + C_z x_prev and
+    Q_t = Q_z * exp(q_gamma * x_new[q_index]); y = H z + c + N(0, R)."""
+
+    def __init__(self, mu_o, Sigma_o, A_o, b_o, Q_o, mu_z, Sigma_z, A_z, b_z, C_z, Q_z,
+                 H, c, R, q_gamma=0.0, q_index=0):
+        f = _fortran
+        self.mu_o, self.b_o = _f64(mu_o).ravel(), _f64(b_o).ravel()
+        self.Sigma_o, self.A_o, self.Q_o = f(Sigma_o), f(A_o), f(Q_o)
+        self.mu_z, self.b_z = _f64(mu_z).ravel(), _f64(b_z).ravel()
+        self.Sigma_z, self.A_z, self.Q_z = f(Sigma_z), f(A_z), f(Q_z)
+        self.C_z = f(np.atleast_2d(C_z).reshape(self.mu_z.size, self.mu_o.size))
+        self.H, self.c, self.R = f(np.atleast_2d(H)), _f64(c).ravel(), f(np.atleast_2d(R))
+        self.q_gamma, self.q_index = float(q_gamma), int(q_index)
+        self.dxo, self.dz, self.dy = self.mu_o.size, self.mu_z.size, self.H.shape[0]
+
+    def _struct(self):
+        names = ("mu_o", "Sigma_o", "A_o", "b_o", "Q_o", "mu_z", "Sigma_z", "A_z", "b_z",
+                 "C_z", "Q_z")
+        return _RB(self.dxo, self.dz, self.dy, *[_p(getattr(self, n)) for n in names],
+                   self.q_gamma, self.q_index, _p(self.H), _p(self.c), _p(self.R))
+
+
+def rbpf_run(m: RBModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=0.5,
+             schedule=None, noise=None, uniforms=None, seed=0, proposal=PROP_BOOTSTRAP,
+             k=1.0, want_ancestors=False, threads=1):
+    """filter(rng, hier_model, RBPF(PF(N, ...), KalmanFilter()), ys)."""
+    ys = _f64(ys).reshape(-1, m.dy)
+    T = ys.shape[0]
+    width = m.dxo + m.dz + m.dz * m.dz
+    out = dict(ll_steps=np.zeros(T), ess=np.zeros(T), resampled=np.zeros(T, np.int8),
+               means=np.zeros((T, m.dxo)), x_final=np.zeros((N, width)),
+               logw_final=np.zeros(N))
+    zmeans = np.zeros((T, m.dz))
+    anc = np.zeros((T, N), np.int32) if want_ancestors else None
+    clamps = C.c_long(0)
+    o = _PFOut(_p(out["ll_steps"]), _p(out["ess"]),
+               out["resampled"].ctypes.data_as(C.POINTER(C.c_int8)),
+               None if anc is None else anc.ctypes.data_as(C.POINTER(C.c_int32)),
+               None, _p(out["means"]), _p(out["x_final"]), _p(out["logw_final"]),
+               C.pointer(clamps))
+    sched = None if schedule is None else np.ascontiguousarray(schedule, np.int8)
+    rc = _RC(resampler, conv, threshold,
+             None if sched is None else sched.ctypes.data_as(C.POINTER(C.c_int8)))
+    nz = None if noise is None else _f64(noise)
+    un = None if uniforms is None else _f64(uniforms)
+    ll = C.c_double()
+    lib().or_set_threads(int(threads))
+    st = lib().or_rbpf_run(C.byref(m._struct()), C.byref(_Prop(proposal, k)), C.byref(rc),
+                           C.c_long(N), T, _p(ys), _p(nz), _p(un), C.c_uint64(seed),
+                           C.byref(ll), C.byref(o), _p(zmeans))
+    lib().or_set_threads(1)
+    if st:
+        raise np.linalg.LinAlgError(f"oracle RBPF status {st}")
+    out.update(ll=ll.value, ancestors=anc, zmeans=zmeans, clamps=clamps.value)
+    return out
+
+
+# --------------------------------------------------------------------------- #
+# numpy restatements of the reference's test fixtures                          #
+# --------------------------------------------------------------------------- #
+def rand_cov(rng, d, scale=1.0, var_range=(0.8, 1.2)):
+    """GFTest/utils.jl:15-36: random correlation matrix rescaled by variances."""
+    A = rng.random((d, d))
+    S = A @ A.T
+    Dis = np.diag(1.0 / np.sqrt(np.diag(S)))
+    S = Dis @ S @ Dis
+    var = (rng.random(d) * (var_range[1] - var_range[0]) + var_range[0]) * scale
+    Ds = np.diag(np.sqrt(var))
+    S = Ds @ S @ Ds
+    return (S + S.T) / 2
+
+
+def create_linear_gaussian_model(rng, Dx, Dy, process_noise_scale=0.1, obs_noise_scale=1.0):
+    """GFTest/models/linear_gaussian.jl:6-38 (numpy RNG)."""
+    mu0 = rng.random(Dx)
+    S0 = rand_cov(rng, Dx)
+    A = rng.random((Dx, Dx))
+    b = rng.random(Dx)
+    Q = rand_cov(rng, Dx, scale=process_noise_scale)
+    H = rng.random((Dy, Dx))
+    c = rng.random(Dy)
+    R = rand_cov(rng, Dy, scale=obs_noise_scale)
+    return LGModel(mu0, S0, A, b, Q, H, c, R)
+
+
+def sample(rng, m: LGModel, T):
+    """SSMProblems forward simulation (utils/forward_simulation.jl:14-26)."""
+    x = rng.multivariate_normal(m.mu0, m.Sigma0)
+    xs, ys = [], []
+    for _ in range(T):
+        x = m.A @ x + m.b + rng.multivariate_normal(np.zeros(m.dx), m.Q)
+        xs.append(x)
+        ys.append(m.H @ x + m.c + rng.multivariate_normal(np.zeros(m.dy), m.R))
+    return np.array(xs), np.array(ys).reshape(T, m.dy)
+
+
+def compute_joint(m: LGModel, T):
+    """GFTest/models/linear_gaussian.jl:171-215: Z = [X0..XT, Y1..YT] ~ N(mu_Z,
+    Sigma_Z) from (I - P) Z = eps."""
+    Dx, Dy = m.dx, m.dy
+    n = Dx + T * (Dx + Dy)
+    P = np.zeros((n, n))
+    mu_e = np.zeros(n)
+    S_e = np.zeros((n, n))
+    mu_e[:Dx] = m.mu0
+    S_e[:Dx, :Dx] = m.Sigma0
+    for t in range(1, T + 1):
+        iA, jA = t * Dx, (t - 1) * Dx
+        P[iA:iA + Dx, jA:jA + Dx] = m.A
+        iH, jH = Dx * (T + 1) + (t - 1) * Dy, Dx * t
+        P[iH:iH + Dy, jH:jH + Dx] = m.H
+        mu_e[iA:iA + Dx] = m.b
+        mu_e[iH:iH + Dy] = m.c
+        S_e[iA:iA + Dx, iA:iA + Dx] = m.Q
+        S_e[iH:iH + Dy, iH:iH + Dy] = m.R
+    IP = np.eye(n) - P
+    mu_Z = np.linalg.solve(IP, mu_e)
+    Sigma_Z = np.linalg.solve(IP, np.linalg.solve(IP, S_e).T).T
+    return mu_Z, Sigma_Z
+
+
+def joint_filter_truth(m: LGModel, ys):
+    """Exact filtered mean/cov of X_T and log p(y_1:T) by Gaussian conditioning
+    (test/algorithms/kalman.jl:5-43, generalised to T steps)."""
+    ys = np.asarray(ys, np.float64).reshape(-1, m.dy)
+    T = ys.shape[0]
+    mu_Z, S_Z = compute_joint(m, T)
+    Dx, Dy = m.dx, m.dy
+    Ix = slice(T * Dx, (T + 1) * Dx)
+    Iy = slice(Dx * (T + 1), Dx * (T + 1) + T * Dy)
+    y = ys.ravel()
+    Syy = S_Z[Iy, Iy]
+    Syy = (Syy + Syy.T) / 2
+    d = y - mu_Z[Iy]
+    mu_x = mu_Z[Ix] + S_Z[Ix, Iy] @ np.linalg.solve(Syy, d)
+    S_x = S_Z[Ix, Ix] - S_Z[Ix, Iy] @ np.linalg.solve(Syy, S_Z[Iy, Ix])
+    sign, logdet = np.linalg.slogdet(Syy)
+    ll = -0.5 * (d @ np.linalg.solve(Syy, d) + logdet + y.size * np.log(2 * np.pi))
+    return mu_x, S_x, ll
+
+
+def random_orthogonal(rng, d):
+    """Haar-random orthogonal matrix (QR of a Gaussian with sign fix)."""
+    Z = rng.standard_normal((d, d))
+    Qm, Rm = np.linalg.qr(Z)
+    return Qm * np.sign(np.diag(Rm))

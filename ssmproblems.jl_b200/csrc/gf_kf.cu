@@ -1,0 +1,891 @@
+// gf_kf.cu -- batched Kalman and square-root Kalman filters.
+//
+// One thread block per filter; the filter's matrices live in shared memory
+// (row-major, padded stride) for the whole time loop.  FP32 storage and
+// arithmetic for the bulk, FP64 for the innovation covariance S, its Cholesky
+// factor, the gain solve and the log-likelihood.
+//
+// KF step restates kalman.jl:42-66 and kalman_gradient.jl:12-23:
+//   mu^ = A mu + b, Sigma^ = A Sigma A' + Q
+//   z = y - H mu^ - c, S = H Sigma^ H' + R, K = Sigma^ H' S^-1
+//   Sigma = (I - K H) Sigma^ (I - K H)' + K R K'   (Joseph form, upper triangle
+//   mirrored as PDMat(Symmetric(.)) does), mu = mu^ + K z,
+//   ll = -1/2 (z' S^-1 z + log|S| + dy log 2 pi).
+// SRKF step restates srkf.jl:93-176 with Householder QR.
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <numeric>
+#include <string>
+#include <vector>
+
+#include "gf_common.cuh"
+#include "gf_internal.hpp"
+
+namespace gf {
+
+struct KfDesc {
+  int32_t dx, dy, T, pad;
+  int64_t poff;    // float offset into the parameter pool
+  int64_t yoff;    // double offset into ys
+  int64_t soff;    // step offset (ll_steps)
+  int64_t moff;    // float offset of means
+  int64_t coff;    // float offset of covs
+  int32_t index;   // caller's filter index
+  int32_t pad2;
+};
+
+struct KfRun {
+  const KfDesc* desc;
+  const int32_t* order;     // bucket work list (indices into desc)
+  int32_t count;
+  uint32_t* counter;        // persistent work ticket
+  const float* params;
+  const double* ys;
+  double* ll;               // [B]
+  double* ll_steps;
+  float* means;
+  float* covs;
+  int32_t* status;          // [B]
+  double jitter;
+  int32_t use_jitter;
+  int32_t algo;
+};
+
+// parameter pool layout per filter (column-major, unpadded):
+//   A dx*dx | b dx | Q dx*dx | H dy*dx | c dy | R dy*dy | mu0 dx | S0 dx*dx |
+//   UQ dx*dx | UR dy*dy | U0 dx*dx     (upper Cholesky factors, used by the SRKF)
+__host__ __device__ inline int64_t kf_param_len(int dx, int dy) {
+  return (int64_t)3 * dx * dx + 2 * dx + dy * dx + dy + dy * dy + dx + dx * dx + dy * dy + dx * dx;
+}
+
+template <int DXP, int DYP>
+struct KfSmem {
+  static constexpr int LD = DXP + 1;   // row stride of dx-wide matrices
+  static constexpr int LY = DYP + 1;   // row stride of dy-wide matrices
+  float A[DXP * LD], Q[DXP * LD], Sig[DXP * LD], Sp[DXP * LD], T1[DXP * LD], IKH[DXP * LD];
+  float H[DYP * LD], PHt[DXP * LY], K[DXP * LY], KR[DXP * LY], R[DYP * LY];
+  double S[DYP * LY], Li[DYP * LY];
+  float mu[DXP], mup[DXP], b[DXP], c[DYP];
+  double z[DYP], w[DYP];
+  double red[32];
+  int fid, fail;
+};
+
+__device__ __forceinline__ void group_sync() { __syncthreads(); }
+
+// y (m x n, row-major, ld) = op over all elements, strided over the block
+template <int DXP, int DYP>
+__device__ void kf_load(KfSmem<DXP, DYP>& s, const float* P, int dx, int dy) {
+  const int G = blockDim.x;
+  const float* pA = P;
+  const float* pb = pA + dx * dx;
+  const float* pQ = pb + dx;
+  const float* pH = pQ + dx * dx;
+  const float* pc = pH + dy * dx;
+  const float* pR = pc + dy;
+  const float* pm = pR + dy * dy;
+  const float* pS = pm + dx;
+  constexpr int LD = KfSmem<DXP, DYP>::LD, LY = KfSmem<DXP, DYP>::LY;
+  for (int e = threadIdx.x; e < dx * dx; e += G) {
+    int i = e % dx, j = e / dx;  // column-major source
+    s.A[i * LD + j] = pA[e];
+    s.Q[i * LD + j] = pQ[e];
+    s.Sig[i * LD + j] = pS[e];
+  }
+  for (int e = threadIdx.x; e < dy * dx; e += G) {
+    int i = e % dy, j = e / dy;
+    s.H[i * LD + j] = pH[e];
+  }
+  for (int e = threadIdx.x; e < dy * dy; e += G) {
+    int i = e % dy, j = e / dy;
+    s.R[i * LY + j] = pR[e];
+  }
+  for (int e = threadIdx.x; e < dx; e += G) {
+    s.b[e] = pb[e];
+    s.mu[e] = pm[e];
+  }
+  for (int e = threadIdx.x; e < dy; e += G) s.c[e] = pc[e];
+}
+
+// FP64 Cholesky of s.S (dy x dy, lower written in place) by warp 0, then the
+// lower-triangular inverse Li (one column per thread).  Returns 0 if not PD.
+template <int DXP, int DYP>
+__device__ bool kf_chol_inv(KfSmem<DXP, DYP>& s, int dy) {
+  constexpr int LY = KfSmem<DXP, DYP>::LY;
+  if (threadIdx.x < 32) {
+    const int lane = threadIdx.x;
+    for (int j = 0; j < dy; ++j) {
+      double d = s.S[j * LY + j];
+      if (!(d > 0.0)) {
+        if (lane == 0) s.fail = 1;
+        break;
+      }
+      d = sqrt(d);
+      __syncwarp();
+      for (int i = j + 1 + lane; i < dy; i += 32) s.S[i * LY + j] /= d;
+      if (lane == 0) s.S[j * LY + j] = d;
+      __syncwarp();
+      // trailing update of the lower triangle: S[i][k] -= L[i][j] L[k][j], k <= i
+      const int n = dy - j - 1;
+      for (int e = lane; e < n * n; e += 32) {
+        int i = j + 1 + e / n, k = j + 1 + e % n;
+        if (k <= i) s.S[i * LY + k] -= s.S[i * LY + j] * s.S[k * LY + j];
+      }
+      __syncwarp();
+    }
+  }
+  group_sync();
+  if (s.fail) return false;
+  // Li = L^-1, column j by thread j
+  for (int j = threadIdx.x; j < dy; j += blockDim.x) {
+    s.Li[j * LY + j] = 1.0 / s.S[j * LY + j];
+    for (int i = j + 1; i < dy; ++i) {
+      double acc = 0.0;
+      for (int k = j; k < i; ++k) acc += s.S[i * LY + k] * s.Li[k * LY + j];
+      s.Li[i * LY + j] = -acc / s.S[i * LY + i];
+    }
+    for (int i = 0; i < j; ++i) s.Li[i * LY + j] = 0.0;
+  }
+  group_sync();
+  return true;
+}
+
+template <int DXP, int DYP>
+__global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
+  using SM = KfSmem<DXP, DYP>;
+  constexpr int LD = SM::LD, LY = SM::LY;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  SM& s = *reinterpret_cast<SM*>(smraw);
+  const int G = blockDim.x;
+  while (true) {
+    if (threadIdx.x == 0) {
+      unsigned k = atomicAdd(run.counter, 1u);
+      s.fid = k < (unsigned)run.count ? run.order[k] : -1;
+      s.fail = 0;
+    }
+    group_sync();
+    const int f = s.fid;
+    if (f < 0) return;
+    const KfDesc D = run.desc[f];
+    const int dx = D.dx, dy = D.dy;
+    kf_load<DXP, DYP>(s, run.params + D.poff, dx, dy);
+    group_sync();
+    double lltot = 0.0;
+    int status = GF_OK;
+    for (int t = 0; t < D.T; ++t) {
+      const double* y = run.ys + D.yoff + (int64_t)t * dy;
+      // 1. T1 = A Sigma ; mup = A mu + b
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        int i = e / dx, j = e % dx;
+        float acc = 0.f;
+        for (int k = 0; k < dx; ++k) acc = fmaf(s.A[i * LD + k], s.Sig[k * LD + j], acc);
+        s.T1[i * LD + j] = acc;
+      }
+      for (int i = threadIdx.x; i < dx; i += G) {
+        float acc = s.b[i];
+        for (int k = 0; k < dx; ++k) acc = fmaf(s.A[i * LD + k], s.mu[k], acc);
+        s.mup[i] = acc;
+      }
+      group_sync();
+      // 2. Sp = T1 A' + Q (upper triangle, mirrored)
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        int i = e / dx, j = e % dx;
+        if (j < i) continue;
+        float acc = s.Q[i * LD + j];
+        for (int k = 0; k < dx; ++k) acc = fmaf(s.T1[i * LD + k], s.A[j * LD + k], acc);
+        s.Sp[i * LD + j] = acc;
+        s.Sp[j * LD + i] = acc;
+      }
+      group_sync();
+      // 3. PHt = Sp H' ; z = y - H mup - c
+      for (int e = threadIdx.x; e < dx * dy; e += G) {
+        int i = e / dy, j = e % dy;
+        float acc = 0.f;
+        for (int k = 0; k < dx; ++k) acc = fmaf(s.Sp[i * LD + k], s.H[j * LD + k], acc);
+        s.PHt[i * LY + j] = acc;
+      }
+      for (int i = threadIdx.x; i < dy; i += G) {
+        double acc = y[i] - (double)s.c[i];
+        for (int k = 0; k < dx; ++k) acc -= (double)s.H[i * LD + k] * (double)s.mup[k];
+        s.z[i] = acc;
+      }
+      group_sync();
+      // 4. S = H PHt + R in FP64 (lower triangle is all the Cholesky reads)
+      for (int e = threadIdx.x; e < dy * dy; e += G) {
+        int i = e / dy, j = e % dy;
+        if (j > i) continue;
+        double acc = (double)s.R[i * LY + j];
+        for (int k = 0; k < dx; ++k) acc += (double)s.H[i * LD + k] * (double)s.PHt[k * LY + j];
+        s.S[i * LY + j] = acc;
+      }
+      group_sync();
+      // 5. Cholesky + inverse
+      if (!kf_chol_inv<DXP, DYP>(s, dy)) {
+        status = GF_ERR_NOT_PD;
+        break;
+      }
+      // 6. w = Li z ; W = PHt Li' (stored in KR) ; then K = W Li
+      for (int i = threadIdx.x; i < dy; i += G) {
+        double acc = 0.0;
+        for (int k = 0; k <= i; ++k) acc += s.Li[i * LY + k] * s.z[k];
+        s.w[i] = acc;
+      }
+      for (int e = threadIdx.x; e < dx * dy; e += G) {
+        int i = e / dy, j = e % dy;
+        double acc = 0.0;
+        for (int k = 0; k <= j; ++k) acc += (double)s.PHt[i * LY + k] * s.Li[j * LY + k];
+        s.KR[i * LY + j] = (float)acc;
+      }
+      group_sync();
+      for (int e = threadIdx.x; e < dx * dy; e += G) {
+        int i = e / dy, j = e % dy;
+        double acc = 0.0;
+        for (int k = j; k < dy; ++k) acc += (double)s.KR[i * LY + k] * s.Li[k * LY + j];
+        s.K[i * LY + j] = (float)acc;
+      }
+      group_sync();
+      // 7. mu = mup + K z ; IKH = I - K H ; KR = K R
+      for (int i = threadIdx.x; i < dx; i += G) {
+        double acc = (double)s.mup[i];
+        for (int k = 0; k < dy; ++k) acc += (double)s.K[i * LY + k] * s.z[k];
+        s.mu[i] = (float)acc;
+      }
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        int i = e / dx, j = e % dx;
+        float acc = (i == j) ? 1.f : 0.f;
+        for (int k = 0; k < dy; ++k) acc = fmaf(-s.K[i * LY + k], s.H[k * LD + j], acc);
+        s.IKH[i * LD + j] = acc;
+      }
+      for (int e = threadIdx.x; e < dx * dy; e += G) {
+        int i = e / dy, j = e % dy;
+        float acc = 0.f;
+        for (int k = 0; k < dy; ++k) acc = fmaf(s.K[i * LY + k], s.R[k * LY + j], acc);
+        s.KR[i * LY + j] = acc;
+      }
+      group_sync();
+      // 8. T1 = IKH Sp
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        int i = e / dx, j = e % dx;
+        float acc = 0.f;
+        for (int k = 0; k < dx; ++k) acc = fmaf(s.IKH[i * LD + k], s.Sp[k * LD + j], acc);
+        s.T1[i * LD + j] = acc;
+      }
+      group_sync();
+      // 9. Sig = T1 IKH' + KR K' (+ jitter I), upper triangle mirrored
+      float* cov_out = run.covs ? run.covs + D.coff + (int64_t)t * dx * dx : nullptr;
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        int i = e / dx, j = e % dx;
+        if (j < i) continue;
+        float acc = 0.f;
+        for (int k = 0; k < dx; ++k) acc = fmaf(s.T1[i * LD + k], s.IKH[j * LD + k], acc);
+        for (int k = 0; k < dy; ++k) acc = fmaf(s.KR[i * LY + k], s.K[j * LY + k], acc);
+        if (run.use_jitter && i == j) acc += (float)run.jitter;
+        s.Sig[i * LD + j] = acc;
+        s.Sig[j * LD + i] = acc;
+      }
+      group_sync();
+      // 10. outputs
+      if (cov_out)
+        for (int e = threadIdx.x; e < dx * dx; e += G) cov_out[e] = s.Sig[(e % dx) * LD + e / dx];
+      if (run.means)
+        for (int i = threadIdx.x; i < dx; i += G) run.means[D.moff + (int64_t)t * dx + i] = s.mu[i];
+      if (threadIdx.x < 32) {
+        double q = 0.0, ld = 0.0;
+        for (int i = threadIdx.x; i < dy; i += 32) {
+          q += s.w[i] * s.w[i];
+          ld += log(s.S[i * LY + i]);
+        }
+        q = warp_sum(q);
+        ld = warp_sum(ld);
+        double l = -0.5 * (q + 2.0 * ld + dy * GF_LOG2PI);
+        lltot += l;
+        if (threadIdx.x == 0 && run.ll_steps) run.ll_steps[D.soff + t] = l;
+      }
+      group_sync();
+    }
+    if (threadIdx.x == 0) {
+      run.ll[D.index] = lltot;
+      run.status[D.index] = status;
+    }
+    group_sync();
+  }
+}
+
+// ---------------------------------------------------------------- SRKF
+template <int DXP, int DYP>
+struct SrSmem {
+  static constexpr int NN = DXP + DYP;
+  static constexpr int LM = NN + 1;
+  float M[(2 * DXP + DYP) * LM];   // QR work matrix, row-major
+  float A[DXP * (DXP + 1)], H[DYP * (DXP + 1)];
+  float U[DXP * (DXP + 1)], UQ[DXP * (DXP + 1)], UR[DYP * (DYP + 1)];
+  float mu[DXP], b[DXP], c[DYP];
+  double z[DYP], w[DYP], colscale[NN];
+  double red[32];
+  int fid;
+};
+
+// In-place Householder QR of M (m x n, row-major, stride LM); leaves R in the
+// upper triangle with rows sign-corrected so diag(R) >= 0 (srkf.jl:83).
+template <int LM>
+__device__ void householder_qr(float* M, int m, int n, double* colscale, double* red) {
+  for (int k = 0; k < n; ++k) {
+    double part = 0.0;
+    for (int i = k + threadIdx.x; i < m; i += blockDim.x) part += (double)M[i * LM + k] * M[i * LM + k];
+    double nrm2 = block_sum(part, red);
+    double nrm = sqrt(nrm2);
+    double x0 = M[k * LM + k];
+    double alpha = x0 >= 0 ? -nrm : nrm;
+    double v0 = x0 - alpha;
+    double vv = nrm2 - x0 * x0 + v0 * v0;
+    __syncthreads();
+    if (nrm > 0.0 && vv > 0.0) {
+      // column scales s_j = 2 v'M[:,j] / v'v for j > k (v = [v0, M[k+1:,k]])
+      for (int j = k + 1 + threadIdx.x; j < n; j += blockDim.x) {
+        double acc = v0 * M[k * LM + j];
+        for (int i = k + 1; i < m; ++i) acc += (double)M[i * LM + k] * M[i * LM + j];
+        colscale[j] = 2.0 * acc / vv;
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < (m - k) * (n - k - 1); e += blockDim.x) {
+        int i = k + e / (n - k - 1), j = k + 1 + e % (n - k - 1);
+        double vi = i == k ? v0 : (double)M[i * LM + k];
+        M[i * LM + j] = (float)((double)M[i * LM + j] - colscale[j] * vi);
+      }
+      __syncthreads();
+      if (threadIdx.x == 0) M[k * LM + k] = (float)alpha;
+    }
+    __syncthreads();
+  }
+  // sign correction
+  for (int i = threadIdx.x; i < n; i += blockDim.x) {
+    if (M[i * LM + i] < 0.f)
+      for (int j = i; j < n; ++j) M[i * LM + j] = -M[i * LM + j];
+  }
+  __syncthreads();
+}
+
+template <int DXP, int DYP>
+__global__ void __launch_bounds__(256) srkf_batch_kernel(KfRun run) {
+  using SM = SrSmem<DXP, DYP>;
+  constexpr int LM = SM::LM, LD = DXP + 1, LY = DYP + 1;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  SM& s = *reinterpret_cast<SM*>(smraw);
+  const int G = blockDim.x;
+  while (true) {
+    if (threadIdx.x == 0) {
+      unsigned k = atomicAdd(run.counter, 1u);
+      s.fid = k < (unsigned)run.count ? run.order[k] : -1;
+    }
+    __syncthreads();
+    const int f = s.fid;
+    if (f < 0) return;
+    const KfDesc D = run.desc[f];
+    const int dx = D.dx, dy = D.dy;
+    const float* P = run.params + D.poff;
+    const float* pA = P;
+    const float* pb = pA + dx * dx;
+    const float* pH = pb + dx + dx * dx;
+    const float* pc = pH + dy * dx;
+    const float* pm = pc + dy + dy * dy;
+    const float* pUQ = pm + dx + dx * dx;
+    const float* pUR = pUQ + dx * dx;
+    const float* pU0 = pUR + dy * dy;
+    for (int e = threadIdx.x; e < dx * dx; e += G) {
+      int i = e % dx, j = e / dx;
+      s.A[i * LD + j] = pA[e];
+      s.UQ[i * LD + j] = pUQ[e];
+      s.U[i * LD + j] = pU0[e];
+    }
+    for (int e = threadIdx.x; e < dy * dx; e += G) s.H[(e % dy) * LD + e / dy] = pH[e];
+    for (int e = threadIdx.x; e < dy * dy; e += G) s.UR[(e % dy) * LY + e / dy] = pUR[e];
+    for (int e = threadIdx.x; e < dx; e += G) {
+      s.b[e] = pb[e];
+      s.mu[e] = pm[e];
+    }
+    for (int e = threadIdx.x; e < dy; e += G) s.c[e] = pc[e];
+    __syncthreads();
+    double lltot = 0.0;
+    int status = GF_OK;
+    for (int t = 0; t < D.T; ++t) {
+      const double* y = run.ys + D.yoff + (int64_t)t * dy;
+      // predict: mu = A mu + b ; U = R(qr([UQ; U A']))
+      float mnew = 0.f;
+      if (threadIdx.x < dx) {
+        int i = threadIdx.x;
+        float acc = s.b[i];
+        for (int k = 0; k < dx; ++k) acc = fmaf(s.A[i * LD + k], s.mu[k], acc);
+        mnew = acc;
+      }
+      for (int e = threadIdx.x; e < 2 * dx * dx; e += G) {
+        int i = e / dx, j = e % dx;
+        float v;
+        if (i < dx) v = s.UQ[i * LD + j];
+        else {
+          int r = i - dx;
+          float acc = 0.f;
+          for (int k = r; k < dx; ++k) acc = fmaf(s.U[r * LD + k], s.A[j * LD + k], acc);
+          v = acc;
+        }
+        s.M[i * LM + j] = v;
+      }
+      __syncthreads();
+      if (threadIdx.x < dx) s.mu[threadIdx.x] = mnew;
+      householder_qr<LM>(s.M, 2 * dx, dx, s.colscale, s.red);
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        int i = e / dx, j = e % dx;
+        s.U[i * LD + j] = j >= i ? s.M[i * LM + j] : 0.f;
+      }
+      __syncthreads();
+      // update: M = [[UR, 0], [U H', U]]
+      const int nn = dx + dy;
+      for (int e = threadIdx.x; e < nn * nn; e += G) {
+        int i = e / nn, j = e % nn;
+        float v = 0.f;
+        if (i < dy) v = j < dy ? s.UR[i * LY + j] : 0.f;
+        else {
+          int r = i - dy;
+          if (j < dy) {
+            float acc = 0.f;
+            for (int k = r; k < dx; ++k) acc = fmaf(s.U[r * LD + k], s.H[j * LD + k], acc);
+            v = acc;
+          } else {
+            v = s.U[r * LD + (j - dy)];
+          }
+        }
+        s.M[i * LM + j] = v;
+      }
+      for (int i = threadIdx.x; i < dy; i += G) {
+        double acc = y[i] - (double)s.c[i];
+        for (int k = 0; k < dx; ++k) acc -= (double)s.H[i * LD + k] * (double)s.mu[k];
+        s.z[i] = acc;
+      }
+      __syncthreads();
+      householder_qr<LM>(s.M, nn, nn, s.colscale, s.red);
+      // w = U_S' \ z (U_S' lower), FP64, warp 0
+      if (threadIdx.x == 0) {
+        for (int i = 0; i < dy; ++i) {
+          double acc = s.z[i];
+          for (int k = 0; k < i; ++k) acc -= (double)s.M[k * LM + i] * s.w[k];
+          double d = (double)s.M[i * LM + i];
+          if (!(d > 0.0)) {
+            status = GF_ERR_NOT_PD;
+            s.fid = -2;
+            break;
+          }
+          s.w[i] = acc / d;
+        }
+      }
+      __syncthreads();
+      if (s.fid == -2) {
+        status = GF_ERR_NOT_PD;
+        break;
+      }
+      // mu += PHt w (PHt = R[0:dy, dy:]') ; U = R[dy:, dy:] (+ jitter)
+      for (int i = threadIdx.x; i < dx; i += G) {
+        double acc = (double)s.mu[i];
+        for (int k = 0; k < dy; ++k) acc += (double)s.M[k * LM + dy + i] * s.w[k];
+        s.mu[i] = (float)acc;
+      }
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        int i = e / dx, j = e % dx;
+        float v = j >= i ? s.M[(dy + i) * LM + dy + j] : 0.f;
+        if (run.use_jitter && i == j) v += (float)run.jitter;
+        s.U[i * LD + j] = v;
+      }
+      __syncthreads();
+      if (run.covs) {
+        float* co = run.covs + D.coff + (int64_t)t * dx * dx;
+        for (int e = threadIdx.x; e < dx * dx; e += G) {
+          int i = e % dx, j = e / dx;  // column-major output of U'U
+          float acc = 0.f;
+          for (int k = 0; k <= min(i, j); ++k) acc = fmaf(s.U[k * LD + i], s.U[k * LD + j], acc);
+          co[e] = acc;
+        }
+      }
+      if (run.means)
+        for (int i = threadIdx.x; i < dx; i += G) run.means[D.moff + (int64_t)t * dx + i] = s.mu[i];
+      if (threadIdx.x < 32) {
+        double q = 0.0, ld = 0.0;
+        for (int i = threadIdx.x; i < dy; i += 32) {
+          q += s.w[i] * s.w[i];
+          ld += log((double)s.M[i * LM + i]);
+        }
+        q = warp_sum(q);
+        ld = warp_sum(ld);
+        double l = -0.5 * (q + 2.0 * ld + dy * GF_LOG2PI);
+        lltot += l;
+        if (threadIdx.x == 0 && run.ll_steps) run.ll_steps[D.soff + t] = l;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+      run.ll[D.index] = lltot;
+      run.status[D.index] = status;
+    }
+    __syncthreads();
+  }
+}
+
+// ---------------------------------------------------------------- buckets
+struct KfBucketKernels {
+  int dxp, dyp;
+  void (*kf)(KfRun);
+  void (*sr)(KfRun);
+  size_t kf_smem, sr_smem;
+};
+
+template <int DXP, int DYP>
+static KfBucketKernels make_bucket() {
+  return {DXP, DYP, kf_batch_kernel<DXP, DYP>, srkf_batch_kernel<DXP, DYP>, sizeof(KfSmem<DXP, DYP>),
+          sizeof(SrSmem<DXP, DYP>)};
+}
+
+static const std::vector<KfBucketKernels>& kf_buckets() {
+  static std::vector<KfBucketKernels> v = {make_bucket<4, 4>(), make_bucket<8, 8>(),
+                                           make_bucket<16, 16>(), make_bucket<32, 32>()};
+  return v;
+}
+
+}  // namespace gf
+
+using namespace gf;
+
+struct gf_kf_plan {
+  gf_ctx* ctx = nullptr;
+  int algo = 0;
+  int B = 0;
+  double jitter = 0.0;
+  int use_jitter = 0;
+  bool plain = false, use_graph = true;
+  std::vector<DevBuf> bufs;
+  KfDesc* desc = nullptr;
+  int32_t* order = nullptr;
+  uint32_t* counters = nullptr;
+  float* params = nullptr;
+  std::vector<KfDesc> hdesc;
+  struct Bucket {
+    int kidx;
+    int group;  // threads per filter block
+    int grid;
+    int start, count;  // range in `order`
+  };
+  std::vector<Bucket> buckets;
+  std::vector<int32_t> horder;
+  int64_t total_steps = 0, total_means = 0, total_covs = 0;
+  cudaGraphExec_t graph = nullptr;
+  const void* graph_key[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+  std::vector<cudaStream_t> side;
+  std::vector<cudaEvent_t> evs;
+};
+
+static gf_status kf_alloc(gf_kf_plan* p, size_t bytes, void** out) {
+  gf_status st = dev_alloc(p->ctx, bytes, out);
+  if (!st && *out) p->bufs.push_back({*out, bytes});
+  return st;
+}
+
+static void kf_release(gf_kf_plan* p) {
+  if (p->graph) cudaGraphExecDestroy(p->graph);
+  for (auto s : p->side) cudaStreamDestroy(s);
+  for (auto e : p->evs) cudaEventDestroy(e);
+  for (auto& b : p->bufs) dev_free(p->ctx, b.p, b.bytes);
+  p->bufs.clear();
+}
+
+static int default_group(int dxp) { return dxp <= 8 ? 32 : (dxp <= 16 ? 128 : 256); }
+
+static void kf_launch_bucket(gf_kf_plan* p, const gf_kf_plan::Bucket& bk, const KfRun& base,
+                             cudaStream_t s) {
+  const KfBucketKernels& K = kf_buckets()[bk.kidx];
+  KfRun r = base;
+  r.order = p->order + bk.start;
+  r.count = bk.count;
+  r.counter = p->counters + (&bk - p->buckets.data());
+  size_t smem = p->algo == GF_ALGO_KF ? K.kf_smem : K.sr_smem;
+  ProfScope ps(p->ctx, KC_KF);
+  if (p->algo == GF_ALGO_KF) K.kf<<<bk.grid, bk.group, smem, s>>>(r);
+  else K.sr<<<bk.grid, bk.group, smem, s>>>(r);
+}
+
+static gf_status kf_enqueue(gf_kf_plan* p, const double* ys, gf_kf_out* out) {
+  gf_ctx* ctx = p->ctx;
+  cudaStream_t s = ctx->stream;
+  KfRun base{};
+  base.desc = p->desc;
+  base.params = p->params;
+  base.ys = ys;
+  base.ll = out->ll;
+  base.ll_steps = out->ll_steps;
+  base.means = out->means;
+  base.covs = out->covs;
+  base.status = out->status;
+  base.jitter = p->jitter;
+  base.use_jitter = p->use_jitter;
+  base.algo = p->algo;
+  GF_CHECK_CUDA(ctx, cudaMemsetAsync(p->counters, 0, sizeof(uint32_t) * 64, s));
+  if (p->plain) {
+    // plain per-filter form: one launch per filter, one block each
+    for (auto& bk : p->buckets) {
+      for (int q = 0; q < bk.count; ++q) {
+        gf_kf_plan::Bucket one = bk;
+        one.start = bk.start + q;
+        one.count = 1;
+        one.grid = 1;
+        KfRun r = base;
+        r.order = p->order + one.start;
+        r.count = 1;
+        r.counter = p->counters + 63;
+        GF_CHECK_CUDA(ctx, cudaMemsetAsync(p->counters + 63, 0, sizeof(uint32_t), s));
+        const KfBucketKernels& K = kf_buckets()[bk.kidx];
+        size_t smem = p->algo == GF_ALGO_KF ? K.kf_smem : K.sr_smem;
+        ProfScope ps(ctx, KC_KF);
+        if (p->algo == GF_ALGO_KF) K.kf<<<1, bk.group, smem, s>>>(r);
+        else K.sr<<<1, bk.group, smem, s>>>(r);
+      }
+    }
+    return GF_OK;
+  }
+  // fork buckets onto side streams so their persistent launches overlap
+  const int nb = (int)p->buckets.size();
+  if ((int)p->side.size() < nb) {
+    while ((int)p->side.size() < nb) {
+      cudaStream_t ss;
+      cudaStreamCreateWithFlags(&ss, cudaStreamNonBlocking);
+      p->side.push_back(ss);
+    }
+    while ((int)p->evs.size() < nb + 1) {
+      cudaEvent_t e;
+      cudaEventCreateWithFlags(&e, cudaEventDisableTiming);
+      p->evs.push_back(e);
+    }
+  }
+  GF_CHECK_CUDA(ctx, cudaEventRecord(p->evs[nb], s));
+  for (int b = 0; b < nb; ++b) {
+    GF_CHECK_CUDA(ctx, cudaStreamWaitEvent(p->side[b], p->evs[nb], 0));
+    kf_launch_bucket(p, p->buckets[b], base, b == 0 ? s : p->side[b]);
+  }
+  for (int b = 1; b < nb; ++b) {
+    GF_CHECK_CUDA(ctx, cudaEventRecord(p->evs[b], p->side[b]));
+    GF_CHECK_CUDA(ctx, cudaStreamWaitEvent(s, p->evs[b], 0));
+  }
+  return GF_OK;
+}
+
+extern "C" gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_model* models,
+                                       int32_t B, const int32_t* T, double jitter,
+                                       int32_t use_jitter, int32_t flags, gf_kf_plan** out) {
+  if (!ctx || !out || !models || !T || B < 1) return ctx ? set_err(ctx, GF_ERR_ARG, "bad arguments") : GF_ERR_ARG;
+  if (algo != GF_ALGO_KF && algo != GF_ALGO_SRKF) return set_err(ctx, GF_ERR_ARG, "unknown algo");
+  *out = nullptr;
+  cudaSetDevice(ctx->device);
+  auto p = std::make_unique<gf_kf_plan>();
+  p->ctx = ctx;
+  p->algo = algo;
+  p->B = B;
+  p->jitter = jitter;
+  p->use_jitter = use_jitter;
+  p->plain = (flags & GF_PLAN_PLAIN) != 0;
+  p->use_graph = !(flags & GF_PLAN_NO_GRAPH) && !p->plain;
+  const auto& bks = kf_buckets();
+  // descriptors + parameter pool (FP32)
+  std::vector<float> pool;
+  std::vector<std::vector<int32_t>> members(bks.size());
+  p->hdesc.resize(B);
+  int64_t poff = 0, yoff = 0, soff = 0, moff = 0, coff = 0;
+  for (int f = 0; f < B; ++f) {
+    const gf_lg_model& m = models[f];
+    if (m.dx < 1 || m.dy < 1 || T[f] < 1) return set_err(ctx, GF_ERR_DIM, "filter %d: bad dims/T", f);
+    int kidx = -1;
+    for (size_t k = 0; k < bks.size(); ++k)
+      if (bks[k].dxp >= m.dx && bks[k].dyp >= m.dy) {
+        kidx = (int)k;
+        break;
+      }
+    if (kidx < 0) return set_err(ctx, GF_ERR_DIM, "filter %d: dx=%d dy=%d exceeds 32", f, m.dx, m.dy);
+    members[kidx].push_back(f);
+    KfDesc& d = p->hdesc[f];
+    d.dx = m.dx;
+    d.dy = m.dy;
+    d.T = T[f];
+    d.poff = poff;
+    d.yoff = yoff;
+    d.soff = soff;
+    d.moff = moff;
+    d.coff = coff;
+    d.index = f;
+    const int dx = m.dx, dy = m.dy;
+    std::vector<double> LQ(dx * dx), LR(dy * dy), L0(dx * dx);
+    bool bad = chol_lower(dx, m.Q, LQ.data()) || chol_lower(dy, m.R, LR.data()) ||
+               chol_lower(dx, m.Sigma0, L0.data());
+    if (bad && algo == GF_ALGO_SRKF) return set_err(ctx, GF_ERR_NOT_PD, "filter %d: Q, R or Sigma0 not PD", f);
+    auto put = [&](const double* a, int n) {
+      for (int i = 0; i < n; ++i) pool.push_back((float)a[i]);
+    };
+    auto putT = [&](const std::vector<double>& L, int n) {  // upper factor U = L'
+      for (int j = 0; j < n; ++j)
+        for (int i = 0; i < n; ++i) pool.push_back((float)L[j + i * n]);
+    };
+    put(m.A, dx * dx);
+    put(m.b, dx);
+    put(m.Q, dx * dx);
+    put(m.H, dy * dx);
+    put(m.c, dy);
+    put(m.R, dy * dy);
+    put(m.mu0, dx);
+    put(m.Sigma0, dx * dx);
+    putT(LQ, dx);
+    putT(LR, dy);
+    putT(L0, dx);
+    poff += kf_param_len(dx, dy);
+    yoff += (int64_t)T[f] * dy;
+    soff += T[f];
+    moff += (int64_t)T[f] * dx;
+    coff += (int64_t)T[f] * dx * dx;
+  }
+  p->total_steps = soff;
+  p->total_means = moff;
+  p->total_covs = coff;
+  // buckets: longest filters first (largest T*dx^3 first keeps the tail short)
+  for (size_t k = 0; k < bks.size(); ++k) {
+    auto& mem = members[k];
+    if (mem.empty()) continue;
+    std::stable_sort(mem.begin(), mem.end(), [&](int a, int b) {
+      const KfDesc &da = p->hdesc[a], &db = p->hdesc[b];
+      double ca = (double)da.T * da.dx * da.dx * (da.dx + da.dy);
+      double cb = (double)db.T * db.dx * db.dx * (db.dx + db.dy);
+      return ca > cb;
+    });
+    gf_kf_plan::Bucket bk;
+    bk.kidx = (int)k;
+    bk.group = default_group(bks[k].dxp);
+    bk.start = (int)p->horder.size();
+    bk.count = (int)mem.size();
+    p->horder.insert(p->horder.end(), mem.begin(), mem.end());
+    p->buckets.push_back(bk);
+  }
+  gf_status st;
+  void* v;
+  if ((st = kf_alloc(p.get(), sizeof(KfDesc) * B, &v))) { kf_release(p.get()); return st; }
+  p->desc = (KfDesc*)v;
+  if ((st = kf_alloc(p.get(), sizeof(int32_t) * B, &v))) { kf_release(p.get()); return st; }
+  p->order = (int32_t*)v;
+  if ((st = kf_alloc(p.get(), sizeof(uint32_t) * 64, &v))) { kf_release(p.get()); return st; }
+  p->counters = (uint32_t*)v;
+  if ((st = kf_alloc(p.get(), sizeof(float) * pool.size(), &v))) { kf_release(p.get()); return st; }
+  p->params = (float*)v;
+  cudaStream_t s = ctx->stream;
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->desc, p->hdesc.data(), sizeof(KfDesc) * B, cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->order, p->horder.data(), sizeof(int32_t) * B, cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->params, pool.data(), sizeof(float) * pool.size(), cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+  for (auto& bk : p->buckets) {
+    const KfBucketKernels& K = bks[bk.kidx];
+    size_t smem = algo == GF_ALGO_KF ? K.kf_smem : K.sr_smem;
+    const void* fn = algo == GF_ALGO_KF ? (const void*)K.kf : (const void*)K.sr;
+    GF_CHECK_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm = 0;
+    GF_CHECK_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bk.group, smem));
+    bk.grid = std::max(1, std::min(bk.count, per_sm * ctx->num_sms));
+  }
+  *out = p.release();
+  return GF_OK;
+}
+
+extern "C" gf_status gf_kf_plan_run(gf_kf_plan* p, const double* ys_dev, gf_kf_out* out) {
+  if (!p || !ys_dev || !out || !out->ll || !out->status)
+    return p ? set_err(p->ctx, GF_ERR_ARG, "ys, out->ll and out->status are required") : GF_ERR_ARG;
+  gf_ctx* ctx = p->ctx;
+  cudaSetDevice(ctx->device);
+  const void* key[5] = {ys_dev, out->ll, out->ll_steps, out->means, out->covs};
+  if (p->use_graph && !ctx->profiling) {
+    bool same = p->graph && std::equal(key, key + 5, p->graph_key);
+    same = same && out->status == nullptr ? false : same;
+    if (!p->graph || !std::equal(key, key + 5, p->graph_key)) {
+      if (p->graph) {
+        cudaGraphExecDestroy(p->graph);
+        p->graph = nullptr;
+      }
+      cudaGraph_t g;
+      GF_CHECK_CUDA(ctx, cudaStreamBeginCapture(ctx->stream, cudaStreamCaptureModeThreadLocal));
+      gf_status st = kf_enqueue(p, ys_dev, out);
+      cudaError_t e = cudaStreamEndCapture(ctx->stream, &g);
+      if (st) return st;
+      if (e != cudaSuccess) return cuda_err(ctx, e, "cudaStreamEndCapture");
+      e = cudaGraphInstantiate(&p->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return cuda_err(ctx, e, "cudaGraphInstantiate");
+      std::copy(key, key + 5, p->graph_key);
+    }
+    GF_CHECK_CUDA(ctx, cudaGraphLaunch(p->graph, ctx->stream));
+    return GF_OK;
+  }
+  gf_status st = kf_enqueue(p, ys_dev, out);
+  if (st) return st;
+  GF_CHECK_CUDA(ctx, cudaGetLastError());
+  return GF_OK;
+}
+
+extern "C" gf_status gf_kf_plan_destroy(gf_kf_plan* p) {
+  if (!p) return GF_OK;
+  cudaSetDevice(p->ctx->device);
+  cudaStreamSynchronize(p->ctx->stream);
+  kf_release(p);
+  delete p;
+  return GF_OK;
+}
+
+extern "C" gf_status gf_kf_batch(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
+                                 const int32_t* T, const double* ys, double jitter,
+                                 int32_t use_jitter, int32_t memspace, gf_kf_out* out) {
+  if (!ctx || !out || !ys) return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
+  gf_kf_plan* p = nullptr;
+  gf_status st = gf_kf_plan_create(ctx, algo, models, B, T, jitter, use_jitter, GF_PLAN_NO_GRAPH, &p);
+  if (st) return st;
+  std::unique_ptr<gf_kf_plan, gf_status (*)(gf_kf_plan*)> guard(p, gf_kf_plan_destroy);
+  if (memspace == GF_MEM_DEVICE) {
+    if (!out->status) return set_err(ctx, GF_ERR_ARG, "out->status is required");
+    return gf_kf_plan_run(p, ys, out);
+  }
+  // stage host buffers
+  int64_t ny = 0;
+  for (int f = 0; f < B; ++f) ny += (int64_t)T[f] * models[f].dy;
+  cudaStream_t s = ctx->stream;
+  std::vector<DevBuf> tmp;
+  auto get = [&](size_t bytes, void** d) -> gf_status {
+    gf_status s2 = dev_alloc(ctx, bytes, d);
+    if (!s2 && *d) tmp.push_back({*d, bytes});
+    return s2;
+  };
+  struct Cleanup {
+    gf_ctx* c;
+    std::vector<DevBuf>* v;
+    ~Cleanup() {
+      cudaStreamSynchronize(c->stream);
+      for (auto& b : *v) dev_free(c, b.p, b.bytes);
+    }
+  } cleanup{ctx, &tmp};
+  void *d_ys, *d_ll, *d_steps = nullptr, *d_means = nullptr, *d_covs = nullptr, *d_status;
+  if ((st = get(sizeof(double) * ny, &d_ys))) return st;
+  if ((st = get(sizeof(double) * B, &d_ll))) return st;
+  if ((st = get(sizeof(int32_t) * B, &d_status))) return st;
+  if (out->ll_steps && (st = get(sizeof(double) * p->total_steps, &d_steps))) return st;
+  if (out->means && (st = get(sizeof(float) * p->total_means, &d_means))) return st;
+  if (out->covs && (st = get(sizeof(float) * p->total_covs, &d_covs))) return st;
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(d_ys, ys, sizeof(double) * ny, cudaMemcpyHostToDevice, s));
+  gf_kf_out d{(double*)d_ll, (double*)d_steps, (float*)d_means, (float*)d_covs, (int32_t*)d_status};
+  if ((st = gf_kf_plan_run(p, (const double*)d_ys, &d))) return st;
+  if (out->ll) GF_CHECK_CUDA(ctx, cudaMemcpyAsync(out->ll, d_ll, sizeof(double) * B, cudaMemcpyDeviceToHost, s));
+  std::vector<int32_t> hs(B);
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(hs.data(), d_status, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, s));
+  if (d_steps) GF_CHECK_CUDA(ctx, cudaMemcpyAsync(out->ll_steps, d_steps, sizeof(double) * p->total_steps, cudaMemcpyDeviceToHost, s));
+  if (d_means) GF_CHECK_CUDA(ctx, cudaMemcpyAsync(out->means, d_means, sizeof(float) * p->total_means, cudaMemcpyDeviceToHost, s));
+  if (d_covs) GF_CHECK_CUDA(ctx, cudaMemcpyAsync(out->covs, d_covs, sizeof(float) * p->total_covs, cudaMemcpyDeviceToHost, s));
+  GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+  if (out->status) std::memcpy(out->status, hs.data(), sizeof(int32_t) * B);
+  for (int f = 0; f < B; ++f)
+    if (hs[f] != GF_OK) return set_err(ctx, hs[f], "filter %d failed with status %d (S not positive definite)", f, hs[f]);
+  return GF_OK;
+}

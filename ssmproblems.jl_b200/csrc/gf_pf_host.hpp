@@ -1,0 +1,43 @@
+// gf_pf_host.hpp -- host-side pieces of the particle-filter path.
+#pragma once
+#include <cstdint>
+#include <vector>
+
+#include "gf_internal.hpp"
+
+namespace gf {
+
+struct PfJob;
+
+// One compiled (precision, padded dims, proposal) variant of the LG kernels.
+struct PfLgKernels {
+  int dxp = 0, dyp = 0;
+  void (*prop)(const PfJob*, int) = nullptr;
+  void (*init)(const PfJob*, int, int, int) = nullptr;
+  size_t smem = 0;
+  int params_len = 0, off_mu0 = 0, off_L0 = 0;
+};
+
+// FP64 model factors computed once per plan (column-major).
+struct LgFactors {
+  int dx = 0, dy = 0;
+  std::vector<double> A, L, b, Ht, M, Qi, mu0, L0, LRi, c, K, vb;
+  double obs_const = 0.0, prop_const = 0.0;
+};
+
+bool pick_lg_kernels(bool dbl, bool guided, int dx, int dy, PfLgKernels* out);
+gf_status build_lg_factors(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg,
+                           LgFactors* f);
+void pack_params(const LgFactors& f, bool dbl, int dxp, int dyp, std::vector<char>& out);
+double uniform_ess(int64_t n);
+
+void launch_scan(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int njobs, int total_stiles);
+void launch_init_scalars(gf_ctx* ctx, PfJob* jobs_dev, int njobs, const double* ess1,
+                         const int8_t* res1);
+void launch_means(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int njobs, int total_tiles,
+                  double* mpart, int mdim);
+void launch_finish(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int64_t N);
+void launch_prep(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int T, int dx, int dy, int dxp,
+                 int dyp, const double* pp, void* out);
+
+}  // namespace gf

@@ -1,0 +1,227 @@
+// gf_pf_lg.cuh -- linear-Gaussian particle-filter kernel templates.
+//
+// Restates GeneralisedFilters' PF (particles.jl:36-90,147-245) for
+// LinearGaussianStateSpaceModel: state x_t = A x_{t-1} + b + L_Q e (BF) or the
+// linear-Gaussian proposal x_t = M x_{t-1} + v_t + L_q e with weight increment
+// log p(x_t|x_{t-1}) - log q(x_t|x_{t-1},y_t) (GFTest OptimalProposal /
+// OverdispersedProposal).  Observation log-density uses the whitened form
+// -1/2 |L_R^{-1}(y - c) - (L_R^{-1}H) x|^2 + const, the same quantity as
+// logpdf(MvNormal(Hx + c, R), y) (models/linear_gaussian.jl:85-90).
+#pragma once
+#include "gf_pf_host.hpp"
+#include "gf_pf_kernels.cuh"
+
+namespace gf {
+
+// ------------------------------------------------------------------ layout
+// params (Real, column-major, padded to DXP/DYP):
+//   A[DXP*DXP] | L[DXP*DXP] | b[DXP] | Ht[DYP*DXP] | M[DXP*DXP] | Qi[DXP*DXP] |
+//   mu0[DXP] | L0[DXP*DXP]
+// ystep[t] (Real): ytil[DYP] | v[DXP]
+template <int DXP, int DYP>
+struct LgLayout {
+  static constexpr int A = 0, L = DXP * DXP, b = 2 * DXP * DXP, H = 2 * DXP * DXP + DXP;
+  static constexpr int M = H + DYP * DXP, Qi = M + DXP * DXP, mu0 = Qi + DXP * DXP;
+  static constexpr int L0 = mu0 + DXP, total = L0 + DXP * DXP;
+  static constexpr int smem_boot = H + DYP * DXP + DYP + DXP;  // A,L,b,H + ystep
+  static constexpr int smem_guided = smem_boot + 2 * DXP * DXP;
+};
+
+template <typename Real, int DXP>
+__device__ __forceinline__ void draw_noise(const PfJob& J, const Real* noise, int64_t i, int t,
+                                           int dx, int64_t N, Real* e) {
+  if (noise) {
+#pragma unroll
+    for (int d = 0; d < DXP; ++d) e[d] = d < dx ? noise[(size_t)d * N + i] : Real(0);
+  } else {
+#pragma unroll
+    for (int q = 0; q < (DXP + 3) / 4; ++q) {
+      Real tmp[4];
+      philox_normals4<Real>(J.seed, (uint32_t)i, (uint32_t)t, (uint32_t)q, tmp);
+#pragma unroll
+      for (int r = 0; r < 4; ++r)
+        if (4 * q + r < DXP) e[4 * q + r] = tmp[r];
+    }
+  }
+}
+
+template <typename Real, int DXP, int DYP, bool GUIDED>
+__global__ void __launch_bounds__(PF_THREADS) pf_lg_propagate(const PfJob* __restrict__ jobs,
+                                                             int njobs) {
+  using Lay = LgLayout<DXP, DYP>;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  Real* sA = reinterpret_cast<Real*>(smraw);
+  Real* sL = sA + Lay::L;
+  Real* sb = sA + Lay::b;
+  Real* sH = sA + Lay::H;
+  Real* sy = sH + DYP * DXP;  // ytil[DYP] then v[DXP]
+  Real* sv = sy + DYP;
+  Real* sM = sv + DXP;
+  Real* sQi = sM + DXP * DXP;
+  __shared__ double red[32];
+  __shared__ int64_t sbnd[2 * PF_PPT];
+
+  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const PfJob& J = jobs[jb];
+  PfScalars* sc = J.sc;
+  const int t = sc->t + 1;
+  if (t > J.T || sc->status != 0) return;
+  const int tile = blockIdx.x - J.tile0;
+  const bool resamp = sc->resample != 0;
+  const bool fresh = resamp || sc->uniform != 0;
+  const double lse_prev = sc->lse;
+  const bool mono = J.resampler != GF_RS_MULTINOMIAL;
+
+  const Real* P = reinterpret_cast<const Real*>(J.params);
+  for (int k = threadIdx.x; k < Lay::H + DYP * DXP; k += PF_THREADS) sA[k] = P[k];
+  const Real* Y = reinterpret_cast<const Real*>(J.ystep) + (size_t)(t - 1) * J.ystride;
+  for (int k = threadIdx.x; k < DYP + DXP; k += PF_THREADS) sy[k] = Y[k];
+  if constexpr (GUIDED) {
+    for (int k = threadIdx.x; k < 2 * DXP * DXP; k += PF_THREADS) sM[k] = P[Lay::M + k];
+  }
+  if (resamp && mono) chunk_bounds(J, sc, t, tile, sbnd);
+  __syncthreads();
+
+  const int64_t N = J.N;
+  const int dx = J.dx;
+  const Real* Xs = reinterpret_cast<const Real*>(J.X[(t - 1) & 1]);
+  Real* Xd = reinterpret_cast<Real*>(J.X[t & 1]);
+  Real* lw = reinterpret_cast<Real*>(J.lw);
+  const Real* noise = J.noise ? reinterpret_cast<const Real*>(J.noise) + (size_t)t * dx * N : nullptr;
+  LseAcc acc, acc0;
+
+  for (int p = 0; p < PF_PPT; ++p) {
+    const int64_t i = (int64_t)tile * PF_TILE + p * PF_THREADS + threadIdx.x;
+    if (i >= N) break;
+    int64_t a = i;
+    if (resamp) {
+      int64_t lo = 0, hi = N;
+      if (mono) {
+        lo = sbnd[2 * p];
+        hi = sbnd[2 * p + 1] + 1;
+      }
+      a = find_ancestor(J, sc, t, i, lo, hi);
+    }
+    Real x[DXP];
+#pragma unroll
+    for (int d = 0; d < DXP; ++d) x[d] = d < dx ? Xs[(size_t)d * N + a] : Real(0);
+    double lin = 0.0;
+    if (!fresh) {
+      lin = (double)lw[i] - lse_prev;
+      acc0.add(lin);
+    }
+    Real e[DXP];
+    draw_noise<Real, DXP>(J, noise, i, t, dx, N, e);
+
+    Real xn[DXP];
+    double inc = 0.0;
+    if constexpr (!GUIDED) {
+      // x' = A x + b + L_Q e   (simulate(dyn) = rand(MvNormal(A x + b, Q)))
+#pragma unroll
+      for (int r = 0; r < DXP; ++r) xn[r] = sb[r];
+#pragma unroll
+      for (int c = 0; c < DXP; ++c) {
+        const Real xc = x[c], ec = e[c];
+#pragma unroll
+        for (int r = 0; r < DXP; ++r) xn[r] = fma(sA[c * DXP + r], xc, xn[r]);
+#pragma unroll
+        for (int r = c; r < DXP; ++r) xn[r] = fma(sL[c * DXP + r], ec, xn[r]);
+      }
+    } else {
+      // x' = M x + v_t + L_q e ; inc = log N(x'; A x + b, Q) - log N(x'; M x + v_t, L_q L_q')
+      Real ma[DXP];
+#pragma unroll
+      for (int r = 0; r < DXP; ++r) {
+        xn[r] = sv[r];
+        ma[r] = sb[r];
+      }
+#pragma unroll
+      for (int c = 0; c < DXP; ++c) {
+        const Real xc = x[c], ec = e[c];
+#pragma unroll
+        for (int r = 0; r < DXP; ++r) {
+          xn[r] = fma(sM[c * DXP + r], xc, xn[r]);
+          ma[r] = fma(sA[c * DXP + r], xc, ma[r]);
+        }
+#pragma unroll
+        for (int r = c; r < DXP; ++r) xn[r] = fma(sL[c * DXP + r], ec, xn[r]);
+      }
+      Real qz = 0, qe = 0;
+#pragma unroll
+      for (int r = 0; r < DXP; ++r) ma[r] = xn[r] - ma[r];
+#pragma unroll
+      for (int r = 0; r < DXP; ++r) {
+        Real z = 0;
+#pragma unroll
+        for (int c = 0; c <= r; ++c) z = fma(sQi[c * DXP + r], ma[c], z);
+        qz = fma(z, z, qz);
+        qe = fma(e[r], e[r], qe);
+      }
+      inc = -0.5 * (double)qz + 0.5 * (double)qe + J.prop_const;
+    }
+    // observation: -1/2 |ytil - Ht x'|^2 + const
+    Real q = 0;
+#pragma unroll
+    for (int k = 0; k < DYP; ++k) {
+      Real r = sy[k];
+#pragma unroll
+      for (int c = 0; c < DXP; ++c) r = fma(-sH[c * DYP + k], xn[c], r);
+      q = fma(r, r, q);
+    }
+    const double lout = lin + inc + (J.obs_const - 0.5 * (double)q);
+    const Real lst = (Real)lout;
+    lw[i] = lst;
+#pragma unroll
+    for (int d = 0; d < DXP; ++d)
+      if (d < dx) Xd[(size_t)d * N + i] = xn[d];
+    if (J.anc_out) J.anc_out[(size_t)(t - 1) * N + i] = (int32_t)(a + 1);
+    acc.add((double)lst);
+  }
+  block_finish(J, tile, t, fresh, acc, acc0, red);
+}
+
+// x_0 ~ MvNormal(mu0, Sigma0) (particles.jl:36-50, models/linear_gaussian.jl:23-29)
+template <typename Real, int DXP>
+__global__ void __launch_bounds__(PF_THREADS) pf_lg_init(const PfJob* __restrict__ jobs, int njobs,
+                                                        int mu_off, int l0_off) {
+  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const PfJob& J = jobs[jb];
+  const int tile = blockIdx.x - J.tile0;
+  const int64_t N = J.N;
+  const int dx = J.dx;
+  const Real* P = reinterpret_cast<const Real*>(J.params);
+  Real* X = reinterpret_cast<Real*>(J.X[0]);
+  Real* lw = reinterpret_cast<Real*>(J.lw);
+  const Real* noise = reinterpret_cast<const Real*>(J.noise);
+  for (int p = 0; p < PF_PPT; ++p) {
+    const int64_t i = (int64_t)tile * PF_TILE + p * PF_THREADS + threadIdx.x;
+    if (i >= N) break;
+    Real e[DXP];
+    draw_noise<Real, DXP>(J, noise, i, 0, dx, N, e);
+#pragma unroll
+    for (int r = 0; r < DXP; ++r) {
+      if (r >= dx) break;
+      Real v = P[mu_off + r];
+#pragma unroll
+      for (int c = 0; c <= r; ++c) v = fma(P[l0_off + c * DXP + r], e[c], v);
+      X[(size_t)r * N + i] = v;
+    }
+    lw[i] = Real(0);
+  }
+}
+
+template <typename Real, int DXP, int DYP, bool G>
+PfLgKernels make_lg() {
+  PfLgKernels k;
+  k.dxp = DXP;
+  k.dyp = DYP;
+  k.prop = pf_lg_propagate<Real, DXP, DYP, G>;
+  k.init = pf_lg_init<Real, DXP>;
+  k.smem = sizeof(Real) * (G ? LgLayout<DXP, DYP>::smem_guided : LgLayout<DXP, DYP>::smem_boot);
+  k.params_len = LgLayout<DXP, DYP>::total;
+  k.off_mu0 = LgLayout<DXP, DYP>::mu0;
+  k.off_L0 = LgLayout<DXP, DYP>::L0;
+  return k;
+}
+
+}  // namespace gf

@@ -1,0 +1,333 @@
+// gf_pf_plan.cu -- PF plans (device buffers + captured T-step graph) and the
+// particle-filter entry points of the C ABI.
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "gf_internal.hpp"
+#include "gf_pf_host.hpp"
+#include "gf_pf_kernels.cuh"
+
+using namespace gf;
+
+struct gf_pf_plan {
+  gf_ctx* ctx = nullptr;
+  bool dbl = false;
+  int dx = 0, dy = 0, T = 0;
+  int64_t N = 0;
+  gf_pf_config cfg{};
+  std::vector<int8_t> sched;
+  PfLgKernels k;
+  int ntiles = 0, nstiles = 0;
+  size_t rsize = 4;
+  std::vector<DevBuf> bufs;
+  void *params = nullptr, *ystep = nullptr, *X0 = nullptr, *X1 = nullptr, *lw = nullptr;
+  double *pp = nullptr, *key = nullptr, *part = nullptr, *mpart = nullptr, *ess1 = nullptr;
+  unsigned long long* flags = nullptr;
+  PfScalars* sc = nullptr;
+  int8_t *sched_dev = nullptr, *res1 = nullptr;
+  PfJob* job_dev = nullptr;
+  PfJob job{};
+  cudaGraphExec_t graph = nullptr;
+  bool graph_means = false;
+  bool use_graph = true;
+};
+
+static gf_status plan_alloc(gf_pf_plan* p, size_t bytes, void** out) {
+  gf_status st = dev_alloc(p->ctx, bytes, out);
+  if (st == GF_OK && *out) p->bufs.push_back({*out, bytes});
+  return st;
+}
+
+static void plan_release(gf_pf_plan* p) {
+  if (!p) return;
+  if (p->graph) cudaGraphExecDestroy(p->graph);
+  for (auto& b : p->bufs) dev_free(p->ctx, b.p, b.bytes);
+  p->bufs.clear();
+}
+
+static gf_status validate_cfg(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg, int T) {
+  if (!m || !cfg) return set_err(ctx, GF_ERR_ARG, "null model or config");
+  if (m->dx < 1 || m->dy < 1) return set_err(ctx, GF_ERR_DIM, "dx, dy must be >= 1");
+  if (cfg->n_particles < 1 || cfg->n_particles > (int64_t(1) << 31) - 1)
+    return set_err(ctx, GF_ERR_ARG, "n_particles must be in [1, 2^31)");
+  if (T < 1) return set_err(ctx, GF_ERR_ARG, "T must be >= 1");
+  if (cfg->resampler < 0 || cfg->resampler > 2) return set_err(ctx, GF_ERR_ARG, "unknown resampler");
+  if (cfg->convention < 0 || cfg->convention > 1) return set_err(ctx, GF_ERR_ARG, "unknown convention");
+  if (cfg->precision != GF_PREC_F32 && cfg->precision != GF_PREC_F64)
+    return set_err(ctx, GF_ERR_ARG, "unknown precision");
+  if (cfg->convention == GF_CONV_CUDAEXT && cfg->resampler == GF_RS_MULTINOMIAL) return GF_OK;
+  return GF_OK;
+}
+
+extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg,
+                                       int32_t T, int32_t flags, gf_pf_plan** out) {
+  if (!ctx || !out) return GF_ERR_ARG;
+  *out = nullptr;
+  gf_status st = validate_cfg(ctx, m, cfg, T);
+  if (st) return st;
+  cudaSetDevice(ctx->device);
+  auto p = std::make_unique<gf_pf_plan>();
+  p->ctx = ctx;
+  p->dbl = cfg->precision == GF_PREC_F64;
+  p->dx = m->dx;
+  p->dy = m->dy;
+  p->T = T;
+  p->N = cfg->n_particles;
+  p->cfg = *cfg;
+  p->use_graph = !(flags & GF_PLAN_NO_GRAPH);
+  if (cfg->schedule) p->sched.assign(cfg->schedule, cfg->schedule + T);
+  p->cfg.schedule = nullptr;
+  const bool guided = cfg->proposal != GF_PROP_BOOTSTRAP;
+  if (!pick_lg_kernels(p->dbl, guided, m->dx, m->dy, &p->k))
+    return set_err(ctx, GF_ERR_DIM, "no kernel for dx=%d dy=%d in %s", m->dx, m->dy,
+                   p->dbl ? "FP64 (max 16)" : "FP32 (max 64)");
+  LgFactors f;
+  if ((st = build_lg_factors(ctx, m, cfg, &f))) return st;
+  std::vector<char> params;
+  pack_params(f, p->dbl, p->k.dxp, p->k.dyp, params);
+  std::vector<double> pp;
+  pp.insert(pp.end(), f.LRi.begin(), f.LRi.end());
+  pp.insert(pp.end(), f.c.begin(), f.c.end());
+  pp.insert(pp.end(), f.K.begin(), f.K.end());
+  pp.insert(pp.end(), f.vb.begin(), f.vb.end());
+
+  p->rsize = p->dbl ? 8 : 4;
+  const int64_t N = p->N;
+  p->ntiles = (int)((N + PF_TILE - 1) / PF_TILE);
+  p->nstiles = (int)((N + SCAN_TILE - 1) / SCAN_TILE);
+  const int ystride = p->k.dyp + p->k.dxp;
+  void* v;
+#define ALLOC(field, bytes)                                              \
+  if ((st = plan_alloc(p.get(), (bytes), &v))) { plan_release(p.get()); return st; } \
+  p->field = decltype(p->field)(v);
+  ALLOC(params, params.size());
+  ALLOC(pp, sizeof(double) * pp.size());
+  ALLOC(ystep, p->rsize * (size_t)T * ystride);
+  ALLOC(X0, p->rsize * (size_t)N * m->dx);
+  ALLOC(X1, p->rsize * (size_t)N * m->dx);
+  ALLOC(lw, p->rsize * (size_t)N);
+  ALLOC(key, sizeof(double) * (size_t)N);
+  ALLOC(part, sizeof(double) * PF_PW * (size_t)p->ntiles);
+  ALLOC(mpart, sizeof(double) * (size_t)p->ntiles * m->dx);
+  ALLOC(flags, sizeof(unsigned long long) * 2 * (size_t)p->nstiles);
+  ALLOC(sc, sizeof(PfScalars));
+  ALLOC(ess1, sizeof(double));
+  ALLOC(res1, 8);
+  ALLOC(job_dev, sizeof(PfJob));
+  if (!p->sched.empty()) { ALLOC(sched_dev, (size_t)T); }
+#undef ALLOC
+  cudaStream_t s = ctx->stream;
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->params, params.data(), params.size(), cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->pp, pp.data(), sizeof(double) * pp.size(), cudaMemcpyHostToDevice, s));
+  if (p->sched_dev)
+    GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->sched_dev, p->sched.data(), (size_t)T, cudaMemcpyHostToDevice, s));
+  // step-1 decision with the reference's uniform-weight ESS
+  double ess1 = uniform_ess(N);
+  int sch0 = p->sched.empty() ? -1 : p->sched[0];
+  int8_t res1 = (int8_t)(sch0 >= 0 ? (sch0 != 0) : (cfg->threshold * (double)N >= ess1));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->ess1, &ess1, sizeof(double), cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->res1, &res1, 1, cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+  if (p->k.smem > 48 * 1024)
+    GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)p->k.prop,
+                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->k.smem));
+
+  PfJob& J = p->job;
+  std::memset(&J, 0, sizeof J);
+  J.N = N;
+  J.dx = m->dx;
+  J.dy = m->dy;
+  J.T = T;
+  J.width = m->dx;
+  J.tile0 = 0;
+  J.ntiles = p->ntiles;
+  J.stile0 = 0;
+  J.nstiles = p->nstiles;
+  J.resampler = cfg->resampler;
+  J.conv = cfg->convention;
+  J.prop = cfg->proposal;
+  J.threshold = cfg->threshold;
+  J.log_n = std::log((double)N);
+  J.obs_const = f.obs_const;
+  J.prop_const = f.prop_const;
+  J.seed = cfg->seed;
+  J.params = p->params;
+  J.ystep = p->ystep;
+  J.ystride = ystride;
+  J.X[0] = p->X0;
+  J.X[1] = p->X1;
+  J.lw = p->lw;
+  J.key = p->key;
+  J.part = p->part;
+  J.flags = p->flags;
+  J.sc = p->sc;
+  J.schedule = p->sched_dev;
+  *out = p.release();
+  return GF_OK;
+}
+
+// Enqueues one full filter run (prep, init, T steps, outputs) on the stream.
+static void enqueue_run(gf_pf_plan* p, bool means) {
+  gf_ctx* ctx = p->ctx;
+  cudaStream_t s = ctx->stream;
+  launch_prep(ctx, p->dbl, p->job_dev, p->T, p->dx, p->dy, p->k.dxp, p->k.dyp, p->pp, p->ystep);
+  launch_init_scalars(ctx, p->job_dev, 1, p->ess1, p->res1);
+  cudaMemsetAsync(p->flags, 0, sizeof(unsigned long long) * 2 * p->nstiles, s);
+  {
+    ProfScope ps(ctx, KC_PREP);
+    p->k.init<<<p->ntiles, PF_THREADS, 0, s>>>(p->job_dev, 1, p->k.off_mu0, p->k.off_L0);
+  }
+  launch_scan(ctx, p->dbl, p->job_dev, 1, p->nstiles);
+  for (int t = 1; t <= p->T; ++t) {
+    {
+      ProfScope ps(ctx, KC_PROPAGATE);
+      p->k.prop<<<p->ntiles, PF_THREADS, p->k.smem, s>>>(p->job_dev, 1);
+    }
+    if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);
+    if (t < p->T) launch_scan(ctx, p->dbl, p->job_dev, 1, p->nstiles);
+  }
+  launch_finish(ctx, p->dbl, p->job_dev, p->N);
+}
+
+extern "C" gf_status gf_pf_plan_run(gf_pf_plan* p, const double* ys_dev, const void* noise_dev,
+                                    const double* uniforms_dev, gf_pf_out* out) {
+  if (!p || !out || !ys_dev) return GF_ERR_ARG;
+  gf_ctx* ctx = p->ctx;
+  cudaSetDevice(ctx->device);
+  PfJob& J = p->job;
+  J.ys = ys_dev;
+  J.noise = noise_dev;
+  J.unif = uniforms_dev;
+  J.ll_steps = out->ll_steps;
+  J.ess_steps = out->ess_steps;
+  J.res_steps = out->resampled;
+  J.anc_out = out->ancestors;
+  J.ll_out = out->ll;
+  J.logw_out = out->log_weights;
+  J.states_out = out->states;
+  J.clamps_out = out->clamps;
+  J.means_out = out->means;
+  cudaStream_t s = ctx->stream;
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->job_dev, &J, sizeof(PfJob), cudaMemcpyHostToDevice, s));
+  const bool means = out->means != nullptr;
+  if (p->use_graph && !ctx->profiling) {
+    if (!p->graph || p->graph_means != means) {
+      if (p->graph) {
+        cudaGraphExecDestroy(p->graph);
+        p->graph = nullptr;
+      }
+      cudaGraph_t g;
+      GF_CHECK_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
+      enqueue_run(p, means);
+      GF_CHECK_CUDA(ctx, cudaStreamEndCapture(s, &g));
+      cudaError_t e = cudaGraphInstantiate(&p->graph, g, 0);
+      cudaGraphDestroy(g);
+      if (e != cudaSuccess) return cuda_err(ctx, e, "cudaGraphInstantiate");
+      p->graph_means = means;
+    }
+    GF_CHECK_CUDA(ctx, cudaGraphLaunch(p->graph, s));
+  } else {
+    enqueue_run(p, means);
+    GF_CHECK_CUDA(ctx, cudaGetLastError());
+  }
+  return GF_OK;
+}
+
+extern "C" gf_status gf_pf_plan_destroy(gf_pf_plan* p) {
+  if (!p) return GF_OK;
+  cudaSetDevice(p->ctx->device);
+  cudaStreamSynchronize(p->ctx->stream);
+  plan_release(p);
+  delete p;
+  return GF_OK;
+}
+
+// Reads the job status after a run (synchronises the stream).
+static gf_status plan_status(gf_pf_plan* p) {
+  gf_ctx* ctx = p->ctx;
+  PfScalars sc;
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(&sc, p->sc, sizeof sc, cudaMemcpyDeviceToHost, ctx->stream));
+  GF_CHECK_CUDA(ctx, cudaStreamSynchronize(ctx->stream));
+  if (sc.status == GF_ERR_TIMEOUT) return set_err(ctx, GF_ERR_TIMEOUT, "lookback scan wait timed out");
+  if (sc.status != 0)
+    return set_err(ctx, sc.status, "particle weights degenerated at step %d (all zero or NaN)", sc.t + 1);
+  return GF_OK;
+}
+
+// ------------------------------------------------------------- gf_pf_run
+namespace {
+struct TmpDev {
+  gf_ctx* ctx;
+  std::vector<DevBuf> v;
+  explicit TmpDev(gf_ctx* c) : ctx(c) {}
+  ~TmpDev() {
+    for (auto& b : v) dev_free(ctx, b.p, b.bytes);
+  }
+  gf_status get(size_t bytes, void** p) {
+    gf_status st = dev_alloc(ctx, bytes, p);
+    if (!st && *p) v.push_back({*p, bytes});
+    return st;
+  }
+};
+}  // namespace
+
+extern "C" gf_status gf_pf_run(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg,
+                               int32_t T, const double* ys, const void* noise,
+                               const double* uniforms, int32_t memspace, gf_pf_out* out) {
+  if (!ctx || !out || !ys) return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
+  if (!out->ll) return set_err(ctx, GF_ERR_ARG, "out->ll is required");
+  gf_pf_plan* p = nullptr;
+  gf_status st = gf_pf_plan_create(ctx, m, cfg, T, GF_PLAN_NO_GRAPH, &p);
+  if (st) return st;
+  std::unique_ptr<gf_pf_plan, gf_status (*)(gf_pf_plan*)> guard(p, gf_pf_plan_destroy);
+  if (memspace == GF_MEM_DEVICE) {
+    if ((st = gf_pf_plan_run(p, ys, noise, uniforms, out))) return st;
+    return plan_status(p);
+  }
+  // host buffers: stage through device memory
+  TmpDev tmp(ctx);
+  cudaStream_t s = ctx->stream;
+  const int64_t N = p->N;
+  const size_t rs = p->rsize;
+  void *d_ys, *d_noise = nullptr, *d_unif = nullptr;
+  if ((st = tmp.get(sizeof(double) * (size_t)T * m->dy, &d_ys))) return st;
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(d_ys, ys, sizeof(double) * (size_t)T * m->dy, cudaMemcpyHostToDevice, s));
+  if (noise) {
+    size_t nb = rs * (size_t)(T + 1) * m->dx * N;
+    if ((st = tmp.get(nb, &d_noise))) return st;
+    GF_CHECK_CUDA(ctx, cudaMemcpyAsync(d_noise, noise, nb, cudaMemcpyHostToDevice, s));
+  }
+  if (uniforms) {
+    size_t ub = sizeof(double) * (size_t)T * (cfg->resampler == GF_RS_SYSTEMATIC ? 1 : N);
+    if ((st = tmp.get(ub, &d_unif))) return st;
+    GF_CHECK_CUDA(ctx, cudaMemcpyAsync(d_unif, uniforms, ub, cudaMemcpyHostToDevice, s));
+  }
+  gf_pf_out d{};
+  struct Map {
+    void* host;
+    void** dev;
+    size_t bytes;
+  };
+  std::vector<Map> maps;
+  auto mk = [&](void* hptr, void** dptr, size_t bytes) -> gf_status {
+    if (!hptr) return GF_OK;
+    gf_status s2 = tmp.get(bytes, dptr);
+    if (!s2) maps.push_back({hptr, dptr, bytes});
+    return s2;
+  };
+  if ((st = mk(out->ll, (void**)&d.ll, sizeof(double)))) return st;
+  if ((st = mk(out->ll_steps, (void**)&d.ll_steps, sizeof(double) * T))) return st;
+  if ((st = mk(out->ess_steps, (void**)&d.ess_steps, sizeof(double) * T))) return st;
+  if ((st = mk(out->resampled, (void**)&d.resampled, (size_t)T))) return st;
+  if ((st = mk(out->ancestors, (void**)&d.ancestors, sizeof(int32_t) * (size_t)T * N))) return st;
+  if ((st = mk(out->means, (void**)&d.means, sizeof(double) * (size_t)T * m->dx))) return st;
+  if ((st = mk(out->states, (void**)&d.states, rs * (size_t)N * m->dx))) return st;
+  if ((st = mk(out->log_weights, (void**)&d.log_weights, sizeof(double) * (size_t)N))) return st;
+  if ((st = mk(out->clamps, (void**)&d.clamps, sizeof(int32_t)))) return st;
+  if ((st = gf_pf_plan_run(p, (const double*)d_ys, d_noise, (const double*)d_unif, &d))) return st;
+  for (auto& mp : maps)
+    GF_CHECK_CUDA(ctx, cudaMemcpyAsync(mp.host, *mp.dev, mp.bytes, cudaMemcpyDeviceToHost, s));
+  return plan_status(p);
+}

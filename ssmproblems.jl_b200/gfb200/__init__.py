@@ -1,0 +1,20 @@
+"""gfb200 -- host-side mirror of GeneralisedFilters' filtering API over the
+B200 library libgfb200.so (C ABI in include/gf_b200.h).
+
+    from gfb200 import *
+    model = create_homogeneous_linear_gaussian_model(mu0, Sigma0, A, b, Q, H, c, R)
+    state, ll = filter(model, KalmanFilter(), ys)
+    state, ll = filter(model, BF(2**20, threshold=0.5), ys, seed=1)
+"""
+from ._lib import (Context, GFError, PosDefException, default_context, load)  # noqa: F401
+from .algorithms import (BF, KF, PF, RBPF, SRKF, AlternatingResampler, BootstrapFilter,  # noqa: F401
+                         ESSResampler, KalmanFilter, LatentProposal, Multinomial,
+                         OptimalProposal, OverdispersedProposal, ParticleFilter, SRKalmanFilter,
+                         Stratified, Systematic)
+from .filtering import (MvNormal, ParticleDistribution, ancestors_to_offspring, filter,  # noqa: F401
+                        filter_batch, offspring_to_ancestors, rng_normals, sample_ancestors)
+from .models import (HierarchicalSSM, HomogeneousGaussianPrior,  # noqa: F401
+                     HomogeneousLinearGaussianLatentDynamics,
+                     HomogeneousLinearGaussianObservationProcess, InnerDynamics,
+                     LatentDynamics, ObservationProcess, StatePrior, StateSpaceModel,
+                     create_homogeneous_linear_gaussian_model)

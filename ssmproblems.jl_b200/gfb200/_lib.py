@@ -1,0 +1,213 @@
+"""ctypes binding of libgfb200.so (the C ABI declared in include/gf_b200.h).
+
+Loading fails loudly when the shared library is missing: there is no CPU
+fallback anywhere in this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(os.path.dirname(_PKG), "lib", "libgfb200.so")
+
+# status codes
+GF_OK, GF_ERR_NOT_PD, GF_ERR_DIM, GF_ERR_OOM_BUDGET, GF_ERR_TIMEOUT = 0, 1, 2, 3, 4
+GF_ERR_CUDA, GF_ERR_ARG, GF_ERR_UNSUPPORTED, GF_ERR_BUSY = 5, 6, 7, 8
+GF_MEM_HOST, GF_MEM_DEVICE = 0, 1
+GF_RS_SYSTEMATIC, GF_RS_STRATIFIED, GF_RS_MULTINOMIAL = 0, 1, 2
+GF_CONV_CPU, GF_CONV_CUDAEXT = 0, 1
+GF_PREC_F32, GF_PREC_F64 = 0, 1
+GF_PROP_BOOTSTRAP, GF_PROP_OPTIMAL, GF_PROP_OVERDISPERSED = 0, 1, 2
+GF_ALGO_KF, GF_ALGO_SRKF = 0, 1
+GF_PLAN_AUTOTUNE, GF_PLAN_NO_GRAPH, GF_PLAN_PLAIN = 1, 2, 4
+
+EXPORTED = [
+    "gf_ctx_create", "gf_ctx_destroy", "gf_last_error", "gf_ctx_set_stream", "gf_ctx_get_stream",
+    "gf_ctx_synchronize", "gf_ctx_memory", "gf_ctx_profile", "gf_ctx_profile_read", "gf_version",
+    "gf_kf_batch", "gf_kf_plan_create", "gf_kf_plan_run", "gf_kf_plan_destroy",
+    "gf_pf_run", "gf_pf_plan_create", "gf_pf_plan_run", "gf_pf_plan_destroy", "gf_rbpf_run",
+    "gf_sample_ancestors", "gf_offspring_to_ancestors", "gf_ancestors_to_offspring",
+    "gf_rng_normals",
+]
+
+_dp = C.POINTER(C.c_double)
+_vp = C.c_void_p
+
+
+class LGModelC(C.Structure):
+    _fields_ = [("dx", C.c_int32), ("dy", C.c_int32)] + [
+        (n, _dp) for n in ("mu0", "Sigma0", "A", "b", "Q", "H", "c", "R")]
+
+
+class RBModelC(C.Structure):
+    _fields_ = ([("dxo", C.c_int32), ("dz", C.c_int32), ("dy", C.c_int32)]
+                + [(n, _dp) for n in ("mu_o", "Sigma_o", "A_o", "b_o", "Q_o",
+                                      "mu_z", "Sigma_z", "A_z", "b_z", "C_z", "Q_z")]
+                + [("q_gamma", C.c_double), ("q_index", C.c_int32)]
+                + [(n, _dp) for n in ("H", "c", "R")])
+
+
+class PFConfigC(C.Structure):
+    _fields_ = [("n_particles", C.c_int64), ("resampler", C.c_int32), ("convention", C.c_int32),
+                ("threshold", C.c_double), ("precision", C.c_int32), ("proposal", C.c_int32),
+                ("proposal_k", C.c_double), ("seed", C.c_uint64),
+                ("schedule", C.POINTER(C.c_int8))]
+
+
+class PFOutC(C.Structure):
+    _fields_ = [("ll", _vp), ("ll_steps", _vp), ("ess_steps", _vp), ("resampled", _vp),
+                ("ancestors", _vp), ("means", _vp), ("states", _vp), ("log_weights", _vp),
+                ("clamps", _vp)]
+
+
+class KFOutC(C.Structure):
+    _fields_ = [("ll", _vp), ("ll_steps", _vp), ("means", _vp), ("covs", _vp), ("status", _vp)]
+
+
+class GFError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"[gf status {code}] {msg}")
+        self.code = code
+
+
+class PosDefException(GFError):
+    """Raised for GF_ERR_NOT_PD, mirroring LinearAlgebra.PosDefException."""
+
+
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load libgfb200.so (raises if it is not built)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    p = path or LIB_PATH
+    if not os.path.exists(p):
+        raise ImportError(f"libgfb200.so not found at {p}; build it with "
+                          f"`python ssmproblems.jl_b200/build.py`")
+    lib = C.CDLL(p)
+    i32, i64, u64, dbl, sz = C.c_int32, C.c_int64, C.c_uint64, C.c_double, C.c_size_t
+    ctxp = C.c_void_p
+    sig = {
+        "gf_ctx_create": (i32, [i32, sz, C.POINTER(ctxp)]),
+        "gf_ctx_destroy": (i32, [ctxp]),
+        "gf_last_error": (C.c_char_p, [ctxp]),
+        "gf_ctx_set_stream": (i32, [ctxp, _vp]),
+        "gf_ctx_get_stream": (_vp, [ctxp]),
+        "gf_ctx_synchronize": (i32, [ctxp]),
+        "gf_ctx_memory": (i32, [ctxp, C.POINTER(sz), C.POINTER(sz)]),
+        "gf_ctx_profile": (i32, [ctxp, i32]),
+        "gf_ctx_profile_read": (i32, [ctxp, i32, C.POINTER(dbl), C.POINTER(i64)]),
+        "gf_version": (i32, []),
+        "gf_kf_batch": (i32, [ctxp, i32, C.POINTER(LGModelC), i32, C.POINTER(i32), _vp, dbl,
+                              i32, i32, C.POINTER(KFOutC)]),
+        "gf_kf_plan_create": (i32, [ctxp, i32, C.POINTER(LGModelC), i32, C.POINTER(i32), dbl,
+                                    i32, i32, C.POINTER(_vp)]),
+        "gf_kf_plan_run": (i32, [_vp, _vp, C.POINTER(KFOutC)]),
+        "gf_kf_plan_destroy": (i32, [_vp]),
+        "gf_pf_run": (i32, [ctxp, C.POINTER(LGModelC), C.POINTER(PFConfigC), i32, _vp, _vp,
+                            _vp, i32, C.POINTER(PFOutC)]),
+        "gf_pf_plan_create": (i32, [ctxp, C.POINTER(LGModelC), C.POINTER(PFConfigC), i32, i32,
+                                    C.POINTER(_vp)]),
+        "gf_pf_plan_run": (i32, [_vp, _vp, _vp, _vp, C.POINTER(PFOutC)]),
+        "gf_pf_plan_destroy": (i32, [_vp]),
+        "gf_rbpf_run": (i32, [ctxp, C.POINTER(RBModelC), C.POINTER(PFConfigC), i32, _vp, _vp,
+                              _vp, i32, C.POINTER(PFOutC), _vp]),
+        "gf_sample_ancestors": (i32, [ctxp, i32, i32, i64, _vp, _vp, _vp]),
+        "gf_offspring_to_ancestors": (i32, [ctxp, i64, _vp, _vp]),
+        "gf_ancestors_to_offspring": (i32, [ctxp, i64, _vp, _vp]),
+        "gf_rng_normals": (i32, [ctxp, u64, i32, i32, i64, i32, _vp]),
+    }
+    for name, (res, args) in sig.items():
+        f = getattr(lib, name)
+        f.restype = res
+        f.argtypes = args
+    _lib = lib
+    return lib
+
+
+def check(ctx, code):
+    """Raise the Python mirror of the reference's exception for a status."""
+    if code == GF_OK:
+        return
+    msg = load().gf_last_error(ctx).decode() if ctx else ""
+    if code == GF_ERR_NOT_PD:
+        raise PosDefException(code, msg)
+    if code in (GF_ERR_ARG, GF_ERR_DIM):
+        raise GFError(code, "ArgumentError: " + msg)
+    raise GFError(code, msg)
+
+
+def f64(a):
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+def fortran64(a):
+    return np.asfortranarray(np.asarray(a, dtype=np.float64))
+
+
+def ptr(a):
+    """Address of a numpy array or torch tensor (None for None)."""
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor
+
+
+class Context:
+    """Owns a gf_ctx (device, stream, HBM budget)."""
+
+    def __init__(self, device: int = 0, budget_bytes: int = 0):
+        lib = load()
+        h = C.c_void_p()
+        check(None, lib.gf_ctx_create(device, budget_bytes, C.byref(h)))
+        self.h = h
+        self.device = device
+
+    def close(self):
+        if self.h:
+            load().gf_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def set_stream(self, stream_ptr):
+        check(self.h, load().gf_ctx_set_stream(self.h, stream_ptr))
+
+    @property
+    def stream(self):
+        return load().gf_ctx_get_stream(self.h)
+
+    def synchronize(self):
+        check(self.h, load().gf_ctx_synchronize(self.h))
+
+    def memory(self):
+        u, b = C.c_size_t(), C.c_size_t()
+        check(self.h, load().gf_ctx_memory(self.h, C.byref(u), C.byref(b)))
+        return u.value, b.value
+
+    def profile(self, enable: bool):
+        check(self.h, load().gf_ctx_profile(self.h, int(enable)))
+
+    def profile_read(self, cls: int):
+        ms, n = C.c_double(), C.c_int64()
+        check(self.h, load().gf_ctx_profile_read(self.h, cls, C.byref(ms), C.byref(n)))
+        return ms.value, n.value
+
+
+_default_ctx = {}
+
+
+def default_context(device: int = 0) -> Context:
+    if device not in _default_ctx:
+        _default_ctx[device] = Context(device)
+    return _default_ctx[device]

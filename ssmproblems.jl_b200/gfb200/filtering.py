@@ -1,0 +1,258 @@
+"""``filter(model, algo, ys)`` and friends on the B200 library.
+
+Mirrors GeneralisedFilters.filter (GeneralisedFilters.jl:58-84): returns
+``(state, log_likelihood)`` with ``state`` an ``MvNormal`` (KF / SRKF) or a
+``ParticleDistribution`` (PF / RBPF).  Every call goes through the C ABI of
+libgfb200.so; unsupported models or options raise instead of falling back.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib as L
+from .algorithms import (AlternatingResampler, ESSResampler, KalmanFilter, ParticleFilter, RBPF,
+                         SRKalmanFilter)
+from .models import HierarchicalSSM, StateSpaceModel
+
+
+class MvNormal:
+    """Filtered Gaussian N(mu, Sigma) (Distributions.MvNormal stand-in)."""
+
+    def __init__(self, mu, Sigma):
+        self.mu = np.asarray(mu)
+        self.Sigma = np.asarray(Sigma)
+
+    def mean(self):
+        return self.mu
+
+    def cov(self):
+        return self.Sigma
+
+
+class ParticleDistribution:
+    """containers.jl:125-141: particles with normalised log-weights (and the
+    per-step diagnostics of the run)."""
+
+    def __init__(self, particles, log_weights, **info):
+        self.particles = particles
+        self.log_weights = log_weights
+        for k, v in info.items():
+            setattr(self, k, v)
+
+    def weights(self):
+        """StatsBase.weights(state) -> softmax(log_weights) (containers.jl:140-144)."""
+        lw = np.asarray(self.log_weights, dtype=np.float64)
+        w = np.exp(lw - lw.max())
+        return w / w.sum()
+
+    def __len__(self):
+        return len(self.log_weights)
+
+
+def _resolve_ctx(ctx):
+    return ctx if ctx is not None else L.default_context()
+
+
+def _rs_params(algo: ParticleFilter, T: int):
+    rs = algo.resampler
+    sched = None
+    if isinstance(rs, AlternatingResampler):
+        sched = np.asarray(rs.schedule(T), dtype=np.int8)
+        threshold, base = 1.0, rs.resampler
+    elif isinstance(rs, ESSResampler):
+        threshold, base = rs.threshold, rs.resampler
+    else:
+        threshold, base = 1.0, rs
+    return threshold, base.kind, sched
+
+
+def _pf_config(algo: ParticleFilter, T: int, seed: int, schedule=None):
+    threshold, kind, sched = _rs_params(algo, T)
+    if schedule is not None:
+        sched = np.asarray(schedule, dtype=np.int8)
+    prec = L.GF_PREC_F64 if algo.precision in ("f64", np.float64, "float64") else L.GF_PREC_F32
+    conv = L.GF_CONV_CUDAEXT if algo.convention == "cudaext" else L.GF_CONV_CPU
+    cfg = L.PFConfigC(algo.N, kind, conv, threshold, prec, algo.proposal.kind,
+                      float(getattr(algo.proposal, "k", 1.0)), int(seed) & (2**64 - 1),
+                      None if sched is None else sched.ctypes.data_as(C.POINTER(C.c_int8)))
+    return cfg, sched, prec
+
+
+def filter(model, algo, observations, *, seed: int = 0, noise=None, uniforms=None,
+           ctx=None, want_ancestors=False, want_means=False, schedule=None):
+    """filter([rng,] model, algo, observations) -> (state, ll).
+
+    seed     : Philox key of the in-kernel noise and uniforms (the reference's rng)
+    noise    : optional injected standard normals [(T+1), dx, N] (step 0 = prior)
+    uniforms : optional injected resampling uniforms ([T] systematic, else [T, N])
+    """
+    ctx = _resolve_ctx(ctx)
+    ys = L.f64(observations)
+    if isinstance(algo, (KalmanFilter, SRKalmanFilter)):
+        if not isinstance(model, StateSpaceModel):
+            raise TypeError("Kalman filters need a linear-Gaussian StateSpaceModel")
+        res = filter_batch([model], algo, [ys], ctx=ctx)
+        return res[0]
+    if isinstance(algo, RBPF):
+        return _rbpf(model, algo, ys, seed, noise, uniforms, ctx, want_ancestors, want_means,
+                     schedule)
+    if isinstance(algo, ParticleFilter):
+        return _pf(model, algo, ys, seed, noise, uniforms, ctx, want_ancestors, want_means,
+                   schedule)
+    raise TypeError(f"unsupported algorithm {type(algo).__name__}")
+
+
+def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, schedule):
+    if not isinstance(model, StateSpaceModel):
+        raise TypeError("particle filter needs a linear-Gaussian StateSpaceModel")
+    mc = model._c_struct()
+    ys = ys.reshape(-1, model.dy)
+    T = ys.shape[0]
+    cfg, sched, prec = _pf_config(algo, T, seed, schedule)
+    N, dx = algo.N, model.dx
+    rdt = np.float64 if prec == L.GF_PREC_F64 else np.float32
+    out = dict(ll=np.zeros(1), ll_steps=np.zeros(T), ess_steps=np.zeros(T),
+               resampled=np.zeros(T, np.int8), states=np.zeros((dx, N), rdt),
+               log_weights=np.zeros(N), clamps=np.zeros(1, np.int32))
+    out["ancestors"] = np.zeros((T, N), np.int32) if want_anc else None
+    out["means"] = np.zeros((T, dx)) if want_means else None
+    o = L.PFOutC(*[L.ptr(out[k]) for k in ("ll", "ll_steps", "ess_steps", "resampled",
+                                           "ancestors", "means", "states", "log_weights",
+                                           "clamps")])
+    nz = None if noise is None else np.ascontiguousarray(noise, dtype=rdt)
+    un = None if uniforms is None else L.f64(uniforms)
+    L.check(ctx.h, L.load().gf_pf_run(ctx.h, C.byref(mc), C.byref(cfg), T, L.ptr(ys),
+                                      L.ptr(nz), L.ptr(un), L.GF_MEM_HOST, C.byref(o)))
+    state = ParticleDistribution(out["states"].T, out["log_weights"], ll_steps=out["ll_steps"],
+                                 ess_steps=out["ess_steps"], resampled=out["resampled"],
+                                 ancestors=out["ancestors"], means=out["means"],
+                                 clamps=int(out["clamps"][0]))
+    return state, float(out["ll"][0])
+
+
+def _rbpf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, schedule):
+    if not isinstance(model, HierarchicalSSM):
+        raise TypeError("RBPF needs a HierarchicalSSM")
+    mc = model._c_struct()
+    ys = ys.reshape(-1, model.dy)
+    T = ys.shape[0]
+    pf = algo.pf
+    cfg, sched, prec = _pf_config(pf, T, seed, schedule)
+    N, dxo, dz = pf.N, model.dxo, model.dz
+    width = dxo + dz + dz * dz
+    out = dict(ll=np.zeros(1), ll_steps=np.zeros(T), ess_steps=np.zeros(T),
+               resampled=np.zeros(T, np.int8), states=np.zeros((width, N), np.float32),
+               log_weights=np.zeros(N), clamps=np.zeros(1, np.int32))
+    out["ancestors"] = np.zeros((T, N), np.int32) if want_anc else None
+    out["means"] = np.zeros((T, dxo)) if want_means else None
+    zmeans = np.zeros((T, dz)) if want_means else None
+    o = L.PFOutC(*[L.ptr(out[k]) for k in ("ll", "ll_steps", "ess_steps", "resampled",
+                                           "ancestors", "means", "states", "log_weights",
+                                           "clamps")])
+    nz = None if noise is None else np.ascontiguousarray(noise, dtype=np.float32)
+    un = None if uniforms is None else L.f64(uniforms)
+    L.check(ctx.h, L.load().gf_rbpf_run(ctx.h, C.byref(mc), C.byref(cfg), T, L.ptr(ys),
+                                        L.ptr(nz), L.ptr(un), L.GF_MEM_HOST, C.byref(o),
+                                        L.ptr(zmeans)))
+    S = out["states"]
+    x = S[:dxo].T
+    mu = S[dxo:dxo + dz].T
+    Sig = S[dxo + dz:].T.reshape(N, dz, dz).transpose(0, 2, 1)  # column-major per particle
+    state = ParticleDistribution(dict(x=x, mu=mu, Sigma=Sig), out["log_weights"],
+                                 ll_steps=out["ll_steps"], ess_steps=out["ess_steps"],
+                                 resampled=out["resampled"], ancestors=out["ancestors"],
+                                 means=out["means"], zmeans=zmeans,
+                                 clamps=int(out["clamps"][0]))
+    return state, float(out["ll"][0])
+
+
+def filter_batch(models, algo, observations, *, ctx=None, want_steps=True, want_covs=True):
+    """Many independent Kalman / square-root Kalman filters in one batched launch.
+    Returns a list of (MvNormal(final mu, Sigma), ll) with per-step outputs
+    attached as .ll_steps, .means, .covs."""
+    ctx = _resolve_ctx(ctx)
+    if not isinstance(algo, (KalmanFilter, SRKalmanFilter)):
+        raise TypeError("filter_batch supports KalmanFilter / SRKF")
+    B = len(models)
+    mcs = (L.LGModelC * B)(*[m._c_struct() for m in models])
+    ys_list = [L.f64(y).reshape(-1, m.dy) for y, m in zip(observations, models)]
+    T = np.array([y.shape[0] for y in ys_list], dtype=np.int32)
+    ys = np.concatenate([y.ravel() for y in ys_list]) if B else np.zeros(0)
+    dxs = np.array([m.dx for m in models])
+    tot_steps = int(T.sum())
+    out = dict(ll=np.zeros(B), ll_steps=np.zeros(tot_steps) if want_steps else None,
+               means=np.zeros(int((T * dxs).sum()), np.float32),
+               covs=np.zeros(int((T * dxs * dxs).sum()), np.float32) if want_covs else None,
+               status=np.zeros(B, np.int32))
+    o = L.KFOutC(*[L.ptr(out[k]) for k in ("ll", "ll_steps", "means", "covs", "status")])
+    jit = algo.jitter
+    L.check(ctx.h, L.load().gf_kf_batch(ctx.h, algo.algo, mcs,  B,
+                                        T.ctypes.data_as(C.POINTER(C.c_int32)), L.ptr(ys),
+                                        float(jit or 0.0), int(jit is not None), L.GF_MEM_HOST,
+                                        C.byref(o)))
+    res = []
+    so = mo = co = 0
+    for f, m in enumerate(models):
+        dx, t = m.dx, int(T[f])
+        means = out["means"][mo:mo + t * dx].reshape(t, dx)
+        covs = None
+        if want_covs:
+            covs = out["covs"][co:co + t * dx * dx].reshape(t, dx, dx).transpose(0, 2, 1)
+        st = MvNormal(means[-1], covs[-1] if covs is not None else None)
+        st.means, st.covs = means, covs
+        st.ll_steps = out["ll_steps"][so:so + t] if want_steps else None
+        res.append((st, float(out["ll"][f])))
+        so += t
+        mo += t * dx
+        co += t * dx * dx
+    return res
+
+
+# ------------------------------------------------------------ resampling API
+def _dev_i64(n, device):
+    import torch
+    return torch.zeros(n, dtype=torch.int64, device=f"cuda:{device}")
+
+
+def sample_ancestors(resampler, weights, uniforms, *, convention="cpu", ctx=None):
+    """sample_ancestors(rng, resampler, weights) on device tensors (torch CUDA
+    float64 weights and uniforms); returns 1-based int64 ancestors (device)."""
+    ctx = _resolve_ctx(ctx)
+    n = weights.numel()
+    out = _dev_i64(n, ctx.device)
+    conv = L.GF_CONV_CUDAEXT if convention == "cudaext" else L.GF_CONV_CPU
+    L.check(ctx.h, L.load().gf_sample_ancestors(ctx.h, resampler.kind, conv, n, L.ptr(weights),
+                                                L.ptr(uniforms), L.ptr(out)))
+    return out
+
+
+def offspring_to_ancestors(offspring, *, ctx=None):
+    """ext/CUDAExt.jl:105-117 on a device int64 tensor."""
+    ctx = _resolve_ctx(ctx)
+    out = _dev_i64(offspring.numel(), ctx.device)
+    L.check(ctx.h, L.load().gf_offspring_to_ancestors(ctx.h, offspring.numel(), L.ptr(offspring),
+                                                      L.ptr(out)))
+    return out
+
+
+def ancestors_to_offspring(ancestors, *, ctx=None):
+    """ext/CUDAExt.jl:130-142 on a device int64 tensor."""
+    ctx = _resolve_ctx(ctx)
+    out = _dev_i64(ancestors.numel(), ctx.device)
+    L.check(ctx.h, L.load().gf_ancestors_to_offspring(ctx.h, ancestors.numel(), L.ptr(ancestors),
+                                                      L.ptr(out)))
+    return out
+
+
+def rng_normals(seed, t, dx, n, precision="f32", *, ctx=None):
+    """The standard normals the PF kernels draw in-kernel at step t, as [dx, n]."""
+    import torch
+    ctx = _resolve_ctx(ctx)
+    dt = torch.float64 if precision == "f64" else torch.float32
+    out = torch.empty((dx, n), dtype=dt, device=f"cuda:{ctx.device}")
+    prec = L.GF_PREC_F64 if precision == "f64" else L.GF_PREC_F32
+    L.check(ctx.h, L.load().gf_rng_normals(ctx.h, int(seed), int(t), int(dx), int(n), prec,
+                                           L.ptr(out)))
+    return out

@@ -1,0 +1,198 @@
+"""GPU parity of the particle-filter path against the FP64 oracle.
+
+Tolerances: FP64 runs match the oracle's per-step log-likelihood increments to
+1e-9 (absolute) and ancestors bit-exactly except where a slot's threshold lies
+within 1e-9 of a cumulative-weight boundary (counted, expected 0).  FP32 runs
+are checked step by step from the GPU's own state (teacher forcing): ancestors
+exact outside a 1e-8 band, states to 2e-5 relative, ll increments to 1e-4.
+"""
+import numpy as np
+import pytest
+
+import gfb200 as G
+import oracle as O
+from gfb200 import workloads as W
+from helpers import ancestors_match, injected, random_lg, simulate, to_oracle
+
+pytestmark = pytest.mark.gpu
+
+RS = {O.SYSTEMATIC: G.Systematic(), O.STRATIFIED: G.Stratified(), O.MULTINOMIAL: G.Multinomial()}
+
+
+@pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.STRATIFIED, O.MULTINOMIAL])
+@pytest.mark.parametrize("conv", ["cpu", "cudaext"])
+def test_bf_f64_injected_matches_oracle(ctx, kind, conv):
+    """Config-1 model (1-D, N=1024, T=100, ESS < 0.5N, FP64) with injected noise."""
+    m, ys = W.lgssm_1d(seed=3, T=100)
+    N, T = 1024, 100
+    rng = np.random.default_rng(11)
+    noise, unif = injected(rng, T, 1, N, kind)
+    algo = G.BF(N, threshold=0.5, resampler=RS[kind], precision="f64", convention=conv)
+    st, ll = G.filter(m, algo, ys, noise=noise, uniforms=unif, want_ancestors=True, ctx=ctx)
+    ref = O.pf_run(to_oracle(m), N, ys, resampler=kind,
+                   conv=O.CONV_CUDAEXT if conv == "cudaext" else O.CONV_CPU, threshold=0.5,
+                   noise=noise, uniforms=unif, want_ancestors=True, want_margins=True)
+    assert st.resampled.sum() > 3, "workload must exercise resampling"
+    np.testing.assert_array_equal(st.resampled, ref["resampled"])
+    bad, boundary = ancestors_match(st.ancestors, ref["ancestors"], ref["margins"], 1e-9)
+    assert bad == 0 and boundary == 0
+    np.testing.assert_allclose(st.ll_steps, ref["ll_steps"], atol=1e-9, rtol=0)
+    np.testing.assert_allclose(st.ess_steps, ref["ess"], rtol=1e-9)
+    assert abs(ll - ref["ll"]) < 1e-8
+    np.testing.assert_allclose(st.particles[:, 0], ref["x_final"][:, 0], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(st.log_weights, ref["logw_final"], atol=1e-9)
+    assert st.clamps == ref["clamps"] == 0
+
+
+@pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.STRATIFIED, O.MULTINOMIAL])
+def test_bf_f64_in_kernel_philox_matches_oracle(ctx, kind):
+    """In-kernel Philox noise and uniforms: the oracle regenerates the same stream."""
+    rng = np.random.default_rng(5)
+    m = random_lg(rng, 2, 2)
+    _, ys = simulate(rng, m, 30)
+    N = 2048
+    algo = G.BF(N, threshold=0.6, resampler=RS[kind], precision="f64")
+    st, ll = G.filter(m, algo, ys, seed=1234, want_ancestors=True, ctx=ctx)
+    ref = O.pf_run(to_oracle(m), N, ys, resampler=kind, threshold=0.6, seed=1234,
+                   want_ancestors=True, want_margins=True)
+    assert st.resampled.sum() >= 2
+    np.testing.assert_array_equal(st.resampled, ref["resampled"])
+    bad, boundary = ancestors_match(st.ancestors, ref["ancestors"], ref["margins"], 1e-9)
+    assert bad == 0
+    np.testing.assert_allclose(st.ll_steps, ref["ll_steps"], atol=1e-9, rtol=0)
+
+
+@pytest.mark.parametrize("prop", ["optimal", "overdispersed"])
+def test_guided_pf_f64_matches_oracle(ctx, prop):
+    rng = np.random.default_rng(21)
+    m = random_lg(rng, 3, 2)
+    _, ys = simulate(rng, m, 25)
+    N, T = 1024, 25
+    noise, unif = injected(rng, T, 3, N, O.SYSTEMATIC)
+    p = G.OptimalProposal(m.dyn, m.obs) if prop == "optimal" else G.OverdispersedProposal(m.dyn, 1.5)
+    algo = G.PF(N, p, threshold=0.5, precision="f64")
+    st, ll = G.filter(m, algo, ys, noise=noise, uniforms=unif, want_ancestors=True, ctx=ctx)
+    ref = O.pf_run(to_oracle(m), N, ys, threshold=0.5, noise=noise, uniforms=unif,
+                   proposal=O.PROP_OPTIMAL if prop == "optimal" else O.PROP_OVERDISPERSED,
+                   k=1.5, want_ancestors=True, want_margins=True)
+    np.testing.assert_array_equal(st.resampled, ref["resampled"])
+    bad, _ = ancestors_match(st.ancestors, ref["ancestors"], ref["margins"], 1e-9)
+    assert bad == 0
+    np.testing.assert_allclose(st.ll_steps, ref["ll_steps"], atol=1e-8, rtol=0)
+
+
+def test_bf_f32_teacher_forced_steps(ctx):
+    """FP32 state, Dx=16/Dy=8 (large-PF model shape): every step of the GPU run is
+    re-done by the FP64 oracle from the GPU's own previous state."""
+    m, ys = W.lgssm_rot(seed=7, dx=16, dy=8, T=12)
+    N, T = 4096, 12
+    rng = np.random.default_rng(8)
+    noise = rng.standard_normal((T + 1, 16, N)).astype(np.float32)
+    unif = rng.random(T)
+    om = to_oracle(m)
+    runs = {}
+    for t in range(1, T + 1):
+        algo = G.BF(N, threshold=0.9)
+        runs[t] = G.filter(m, algo, ys[:t], noise=noise[:t + 1], uniforms=unif[:t],
+                           want_ancestors=True, ctx=ctx)
+    n_res = 0
+    for t in range(2, T + 1):
+        prev, _ = runs[t - 1]
+        cur, _ = runs[t]
+        ref = O.pf_step(om, prev.particles.astype(np.float64), prev.log_weights, ys[t - 1],
+                        noise[t].astype(np.float64), unif[t - 1], threshold=0.9)
+        assert bool(cur.resampled[t - 1]) == ref["resampled"]
+        n_res += ref["resampled"]
+        bad, _ = ancestors_match(cur.ancestors[t - 1], ref["ancestors"], ref["margins"], 1e-8)
+        assert bad == 0
+        np.testing.assert_allclose(cur.particles, ref["x"], rtol=2e-5, atol=2e-5)
+        assert abs(cur.ll_steps[t - 1] - ref["ll_inc"]) < 1e-4
+    assert n_res >= 3
+
+
+@pytest.mark.parametrize("prec", ["f32", "f64"])
+def test_fused_rng_equals_exported_noise(ctx, prec):
+    """Noise drawn in-kernel == the same stream exported by gf_rng_normals and injected."""
+    m, ys = W.lgssm_rot(seed=2, dx=4, dy=4, T=20)
+    N, T, seed = 3000, 20, 99
+    a, lla = G.filter(m, G.BF(N, threshold=0.7, precision=prec), ys, seed=seed, ctx=ctx,
+                      want_ancestors=True)
+    noise = np.stack([G.rng_normals(seed, t, 4, N, prec, ctx=ctx).cpu().numpy()
+                      for t in range(T + 1)])
+    unif = np.array([O.philox_uniform(seed, 0, t) for t in range(1, T + 1)])
+    b, llb = G.filter(m, G.BF(N, threshold=0.7, precision=prec), ys, noise=noise, uniforms=unif,
+                      ctx=ctx, want_ancestors=True)
+    assert lla == llb
+    np.testing.assert_array_equal(a.ancestors, b.ancestors)
+    np.testing.assert_array_equal(a.particles, b.particles)
+
+
+def test_runs_are_deterministic(ctx):
+    m, ys = W.lgssm_rot(seed=4, dx=16, dy=8, T=40)
+    algo = G.BF(200_000, threshold=0.5)
+    a, lla = G.filter(m, algo, ys, seed=5, ctx=ctx)
+    b, llb = G.filter(m, algo, ys, seed=5, ctx=ctx)
+    assert lla == llb
+    np.testing.assert_array_equal(a.ll_steps, b.ll_steps)
+    np.testing.assert_array_equal(a.particles, b.particles)
+
+
+def _kf_ll(m, ys):
+    ll, _, mus, _ = O.kf_filter(to_oracle(m), ys)
+    return ll, mus
+
+
+def test_bf_converges_to_kf(ctx):
+    """test/algorithms/particles.jl:5-27 shape: 1-D random model, T=4, N=10^6,
+    AlternatingResampler: |ll_BF - ll_KF| <= 1e-3, filtered mean rtol 1e-3."""
+    rng = np.random.default_rng(1234)
+    m = random_lg(rng, 1, 1)
+    _, ys = simulate(rng, m, 4)
+    algo = G.BF(10**6, resampler=G.AlternatingResampler())
+    st, ll = G.filter(m, algo, ys, seed=77, ctx=ctx)
+    llkf, mus = _kf_ll(m, ys)
+    w = st.weights()
+    assert abs(ll - llkf) <= 1e-3
+    assert abs(np.sum(st.particles[:, 0] * w) - mus[-1, 0]) <= 1e-3 * abs(mus[-1, 0])
+
+
+def test_guided_converges_to_kf(ctx):
+    """test/algorithms/particles.jl:31-53 shape with OptimalProposal."""
+    rng = np.random.default_rng(1234)
+    m = random_lg(rng, 1, 1)
+    _, ys = simulate(rng, m, 4)
+    algo = G.PF(10**6, G.OptimalProposal(m.dyn, m.obs), resampler=G.AlternatingResampler())
+    st, ll = G.filter(m, algo, ys, seed=78, ctx=ctx)
+    llkf, mus = _kf_ll(m, ys)
+    assert abs(ll - llkf) <= 1e-3
+    assert abs(np.sum(st.particles[:, 0] * st.weights()) - mus[-1, 0]) <= 1e-3 * abs(mus[-1, 0])
+
+
+@pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.STRATIFIED, O.MULTINOMIAL])
+def test_large_pf_properties(ctx, kind):
+    """N = 2^20, Dx=16, Dy=8: size-independent invariants of the full-size run."""
+    m, ys = W.lgssm_rot(seed=1, dx=16, dy=8, T=30)
+    N = 2**20
+    st, ll = G.filter(m, G.BF(N, threshold=0.5, resampler=RS[kind]), ys, seed=3,
+                      want_ancestors=True, ctx=ctx)
+    assert np.isfinite(ll) and abs(ll - st.ll_steps.sum()) < 1e-6 * max(1, abs(ll))
+    assert st.clamps == 0
+    assert st.resampled[1:].sum() >= 1
+    for t in range(30):
+        a = st.ancestors[t]
+        assert a.min() >= 1 and a.max() <= N
+        if not st.resampled[t]:
+            np.testing.assert_array_equal(a, np.arange(1, N + 1))
+        else:
+            assert st.ess_steps[t] <= 0.5 * N + 1e-6 or t == 0
+            if kind != O.MULTINOMIAL:
+                assert np.all(np.diff(a) >= 0)
+    np.testing.assert_allclose(st.weights().sum(), 1.0, rtol=1e-12)
+
+
+def test_large_pf_converges_to_kf_ll(ctx):
+    """The PF log-likelihood estimate at N = 2^20 is close to the exact KF value."""
+    m, ys = W.lgssm_rot(seed=9, dx=16, dy=8, T=50)
+    st, ll = G.filter(m, G.BF(2**20, threshold=0.5), ys, seed=1, ctx=ctx)
+    llkf, _ = _kf_ll(m, ys)
+    assert abs(ll - llkf) < 0.5 + 1e-3 * abs(llkf)

@@ -1,0 +1,75 @@
+"""GPU parity of the Rao-Blackwellised PF (per-particle Kalman banks).
+
+FP32 bank with FP64 innovation Cholesky: per-step ll increments within 1e-4
+relative of the FP64 oracle fed the same injected noise and uniforms (one
+resample at step 1, as GFTest's AlternatingResampler does); convergence to the
+exact KF of the joint model within the reference's 1e-3 (test/algorithms/rbpf.jl:5-34)."""
+import numpy as np
+import pytest
+
+import gfb200 as G
+import oracle as O
+from gfb200 import workloads as W
+from helpers import dummy_rb_model, simulate, to_oracle, to_oracle_rb
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.mark.parametrize("dims", [(1, 1, 1), (2, 4, 2), (2, 8, 4)])
+def test_rbpf_matches_oracle(ctx, dims):
+    rng = np.random.default_rng(sum(dims))
+    full, hier = dummy_rb_model(rng, *dims)
+    _, ys = simulate(rng, full, 10)
+    N, T = 2048, 10
+    noise = rng.standard_normal((T + 1, dims[0], N)).astype(np.float32)
+    unif = rng.random(T)
+    algo = G.RBPF(G.BF(N, resampler=G.AlternatingResampler()), G.KalmanFilter())
+    st, ll = G.filter(hier, algo, ys, noise=noise, uniforms=unif, want_ancestors=True,
+                      want_means=True, ctx=ctx)
+    ref = O.rbpf_run(to_oracle_rb(hier), N, ys, schedule=[1] + [0] * (T - 1),
+                     noise=noise.astype(np.float64), uniforms=unif, want_ancestors=True)
+    np.testing.assert_array_equal(st.ancestors, ref["ancestors"])
+    np.testing.assert_allclose(st.ll_steps, ref["ll_steps"], rtol=1e-4, atol=1e-4)
+    np.testing.assert_allclose(st.means, ref["means"], rtol=1e-3, atol=1e-4)
+    np.testing.assert_allclose(st.zmeans, ref["zmeans"], rtol=1e-3, atol=1e-4)
+
+
+def test_rbpf_converges_to_kf(ctx):
+    rng = np.random.default_rng(1234)
+    full, hier = dummy_rb_model(rng, 1, 1, 1)
+    _, ys = simulate(rng, full, 4)
+    algo = G.RBPF(G.BF(10**6, resampler=G.AlternatingResampler()), G.KalmanFilter())
+    st, ll = G.filter(hier, algo, ys, seed=31, ctx=ctx)
+    llkf, _, mus, _ = O.kf_filter(to_oracle(full), ys)
+    w = st.weights()
+    assert abs(ll - llkf) <= 1e-3
+    assert abs(np.sum(st.particles["x"][:, 0] * w) - mus[-1, 0]) <= 1e-3 * abs(mus[-1, 0])
+    assert abs(np.sum(st.particles["mu"][:, 0] * w) - mus[-1, 1]) <= 1e-3 * abs(mus[-1, 1])
+
+
+def test_guided_rbpf_matches_oracle(ctx):
+    rng = np.random.default_rng(77)
+    full, hier = dummy_rb_model(rng, 1, 1, 1)
+    _, ys = simulate(rng, full, 8)
+    N, T = 1024, 8
+    noise = rng.standard_normal((T + 1, 1, N)).astype(np.float32)
+    unif = rng.random(T)
+    prop = G.OverdispersedProposal(hier.outer_dyn, 1.5)
+    algo = G.RBPF(G.PF(N, prop, resampler=G.AlternatingResampler()), G.KalmanFilter())
+    st, ll = G.filter(hier, algo, ys, noise=noise, uniforms=unif, ctx=ctx)
+    ref = O.rbpf_run(to_oracle_rb(hier), N, ys, schedule=[1] + [0] * (T - 1),
+                     noise=noise.astype(np.float64), uniforms=unif,
+                     proposal=O.PROP_OVERDISPERSED, k=1.5)
+    np.testing.assert_allclose(st.ll_steps, ref["ll_steps"], rtol=1e-4, atol=1e-4)
+
+
+def test_trend_model_full_size(ctx):
+    """N = 65536, T = 500 stochastic-volatility RBPF: invariants of the full run."""
+    model, ys = W.rb_trend(seed=1)
+    algo = G.RBPF(G.BF(65536, threshold=0.5), G.KalmanFilter())
+    st, ll = G.filter(model, algo, ys, seed=2, ctx=ctx)
+    assert np.isfinite(ll)
+    assert st.resampled.sum() > 0 and st.clamps == 0
+    assert np.all(st.ess_steps > 0) and np.all(st.ess_steps <= 65536 * (1 + 1e-9))
+    S = st.particles["Sigma"]
+    assert np.all(np.linalg.eigvalsh(S[:1000].astype(np.float64)) > 0)

@@ -1,0 +1,140 @@
+"""CPU pins of the FP64 oracle: analytic truths, the reference's known answers,
+the committed golden fixtures and Monte-Carlo convergence (no GPU needed)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+GOLD = json.load(open(os.path.join(os.path.dirname(__file__), "golden", "golden.json")))
+
+
+@pytest.mark.parametrize("Dy", [2, 3, 4])
+@pytest.mark.parametrize("T", [1, 5])
+def test_kf_matches_joint_gaussian(Dy, T):
+    """test/algorithms/kalman.jl:5-43 (the reference's analytic oracle)."""
+    rng = np.random.default_rng(1234 + Dy + 10 * T)
+    m = O.create_linear_gaussian_model(rng, 3, Dy)
+    _, ys = O.sample(rng, m, T)
+    ll, _, mus, S = O.kf_filter(m, ys)
+    mu, St, lt = O.joint_filter_truth(m, ys)
+    assert abs(ll - lt) <= 1e-10 * abs(lt)
+    np.testing.assert_allclose(mus[-1], mu, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(S[-1], St, rtol=1e-8, atol=1e-12)
+
+
+@pytest.mark.parametrize("Dy", [2, 3, 4])
+def test_srkf_equals_kf(Dy):
+    """test/algorithms/srkf.jl:3-26."""
+    rng = np.random.default_rng(99 + Dy)
+    m = O.create_linear_gaussian_model(rng, 3, Dy)
+    _, ys = O.sample(rng, m, 5)
+    a = O.kf_filter(m, ys)
+    b = O.kf_filter(m, ys, algo="srkf")
+    assert abs(a[0] - b[0]) <= 1e-10 * abs(a[0])
+    np.testing.assert_allclose(a[2], b[2], rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(a[3], b[3], rtol=1e-9, atol=1e-12)
+
+
+def test_known_answer_offspring_ancestors():
+    g = GOLD["offspring_to_ancestors"]
+    assert O.offspring_to_ancestors(g["offspring"]).tolist() == g["ancestors"]
+    g = GOLD["ancestors_to_offspring"]
+    assert O.ancestors_to_offspring(g["ancestors"]).tolist() == g["offspring"]
+
+
+def test_golden_kalman():
+    for case in GOLD["kalman"]:
+        m = O.LGModel(*[np.array(case["model"][k]) for k in
+                        ("mu0", "Sigma0", "A", "b", "Q", "H", "c", "R")])
+        ys = np.array(case["ys"])
+        ll, lls, mus, S = O.kf_filter(m, ys)
+        assert ll == pytest.approx(case["ll"], rel=1e-13)
+        np.testing.assert_allclose(lls, case["ll_steps"], rtol=1e-12)
+        np.testing.assert_allclose(S[-1], case["Sigma_T"], rtol=1e-12)
+        ll2 = O.kf_filter(m, ys, algo="srkf")[0]
+        assert ll2 == pytest.approx(case["ll_srkf"], rel=1e-13)
+
+
+def test_golden_bootstrap_pf():
+    m = O.LGModel([0.0], [[1.0]], [[1.0]], [0.0], [[0.01]], [[1.0]], [0.0], [[0.04]])
+    for case in GOLD["bootstrap_pf"]:
+        N = case["N"]
+        ys = np.array(case["ys"]).reshape(-1, 1)
+        T = ys.shape[0]
+        noise = np.array(case["noise"]).reshape(T + 1, 1, N)
+        unif = np.array(case["uniforms"])
+        if case["kind"] != O.SYSTEMATIC:
+            unif = unif.reshape(T, N)
+        r = O.pf_run(m, N, ys, resampler=case["kind"], threshold=0.5, noise=noise, uniforms=unif,
+                     want_ancestors=True)
+        assert r["ll"] == pytest.approx(case["ll"], rel=1e-12)
+        np.testing.assert_array_equal(r["ancestors"], np.array(case["ancestors"]))
+        np.testing.assert_array_equal(r["resampled"], case["resampled"])
+
+
+def test_systematic_rule_small_case():
+    """resamplers.jl:216-238 by hand: vs = n*cumsum(w), a_i = min{k : vs_k > u0 + i - 1}."""
+    w = np.array([0.1, 0.4, 0.0, 0.3, 0.2])
+    a, mar, cl = O.sample_ancestors(O.SYSTEMATIC, w, [0.5])
+    # vs = [0.5, 2.5, 2.5, 4.0, 5.0]; thresholds 0.5,1.5,2.5,3.5,4.5
+    assert a.tolist() == [2, 2, 4, 4, 5]
+    assert cl == 0
+
+
+def test_cudaext_systematic_rule_small_case():
+    """CUDAExt.jl:49-58 + offspring_to_ancestors: O_k = min(n, floor(n W_k/W_n + u0))."""
+    w = np.array([0.1, 0.4, 0.0, 0.3, 0.2])
+    a, _, _ = O.sample_ancestors(O.SYSTEMATIC, w, [0.5], conv=O.CONV_CUDAEXT)
+    # r = [0.5, 2.5, 2.5, 4, 5] -> O = [1, 3, 3, 4, 5]
+    assert a.tolist() == [1, 2, 2, 4, 5]
+
+
+@pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.STRATIFIED, O.MULTINOMIAL])
+def test_resampled_mean(kind):
+    """test/components/resamplers.jl:5-34: N = 10^6 importance weights, rtol 0.1."""
+    rng = np.random.default_rng(1234)
+    n = 10**6
+    xs = rng.standard_normal(n)
+    ws = np.exp(-0.5 * (xs - 1) ** 2 + 0.5 * xs ** 2)
+    ws /= ws.sum()
+    u = rng.random(1 if kind == O.SYSTEMATIC else n)
+    a, _, cl = O.sample_ancestors(kind, ws, u)
+    mu0 = np.sum(ws * xs)
+    assert abs(xs[a - 1].mean() - mu0) <= 0.1 * abs(mu0)
+
+
+def test_pf_converges_to_kf():
+    """test/algorithms/particles.jl:5-27 shape (N = 10^6, T = 4, resample at step 1)."""
+    rng = np.random.default_rng(1234)
+    m = O.create_linear_gaussian_model(rng, 1, 1)
+    _, ys = O.sample(rng, m, 4)
+    ll, _, mus, _ = O.kf_filter(m, ys)
+    r = O.pf_run(m, 10**6, ys, schedule=[1, 0, 0, 0], seed=3, threads=os.cpu_count())
+    assert abs(r["ll"] - ll) <= 1e-3
+    w = np.exp(r["logw_final"])
+    assert abs(np.sum(w * r["x_final"][:, 0]) - mus[-1, 0]) <= 1e-3 * abs(mus[-1, 0])
+
+
+def test_philox_known_answer():
+    """Philox4x32-10 against the published Random123 known-answer vectors; the CUDA
+    kernels use the same round function (checked on the GPU by the fused-RNG tests)."""
+    import ctypes as C
+    lib = O.lib()
+
+    def ph(ctr, k):
+        c = (C.c_uint32 * 4)(*ctr)
+        o = (C.c_uint32 * 4)()
+        lib.or_philox4x32_10(c, C.c_uint32(k[0]), C.c_uint32(k[1]), o)
+        return [int(v) for v in o]
+
+    assert ph([0, 0, 0, 0], [0, 0]) == [0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8]
+    assert ph([0xffffffff] * 4, [0xffffffff] * 2) == [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd]
+    assert ph([0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344], [0xa4093822, 0x299f31d0]) == \
+        [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]
+    vals = np.array([O.philox_uniform(12345, j, 3) for j in range(20000)])
+    assert abs(vals.mean() - 0.5) < 0.01 and abs(vals.var() - 1 / 12) < 0.005
+    z = O.philox_normals(7, 4000, 4, 1)
+    assert abs(z.mean()) < 0.03 and abs(z.var() - 1) < 0.05
