@@ -183,7 +183,7 @@ double or_logsumexp(const double* x, long n) {
   double m = x[0], r = 0.0;
   for (long i = 1; i < n; ++i) {
     if (x[i] <= m) r += exp(x[i] - m);
-    else { r = r * exp(m - x[i]) + 1.0; m = x[i]; }
+    else { r = (r + 1.0) * exp(m - x[i]); m = x[i]; }
   }
   return m + log1p(r);
 }

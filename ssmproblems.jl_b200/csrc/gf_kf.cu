@@ -57,7 +57,7 @@ struct KfRun {
 //   A dx*dx | b dx | Q dx*dx | H dy*dx | c dy | R dy*dy | mu0 dx | S0 dx*dx |
 //   UQ dx*dx | UR dy*dy | U0 dx*dx     (upper Cholesky factors, used by the SRKF)
 __host__ __device__ inline int64_t kf_param_len(int dx, int dy) {
-  return (int64_t)3 * dx * dx + 2 * dx + dy * dx + dy + dy * dy + dx + dx * dx + dy * dy + dx * dx;
+  return (int64_t)5 * dx * dx + 2 * dx + dy * dx + dy + 2 * dy * dy;
 }
 
 template <int DXP, int DYP>

@@ -190,6 +190,12 @@ void launch_scan(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int njobs, int to
   else pf_scan_kernel<float><<<total_stiles, SCAN_THREADS, 0, ctx->stream>>>(jobs_dev, njobs);
 }
 
+void launch_resample(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int njobs, int total_tiles) {
+  ProfScope ps(ctx, KC_SCAN);
+  if (dbl) pf_resample_kernel<double><<<total_tiles, PF_THREADS, 0, ctx->stream>>>(jobs_dev, njobs);
+  else pf_resample_kernel<float><<<total_tiles, PF_THREADS, 0, ctx->stream>>>(jobs_dev, njobs);
+}
+
 void launch_init_scalars(gf_ctx* ctx, PfJob* jobs_dev, int njobs, const double* ess1,
                          const int8_t* res1) {
   pf_init_scalars<<<(njobs + 127) / 128, 128, 0, ctx->stream>>>(jobs_dev, njobs, ess1, res1);

@@ -32,6 +32,7 @@ void pack_params(const LgFactors& f, bool dbl, int dxp, int dyp, std::vector<cha
 double uniform_ess(int64_t n);
 
 void launch_scan(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int njobs, int total_stiles);
+void launch_resample(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int njobs, int total_tiles);
 void launch_init_scalars(gf_ctx* ctx, PfJob* jobs_dev, int njobs, const double* ess1,
                          const int8_t* res1);
 void launch_means(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int njobs, int total_tiles,

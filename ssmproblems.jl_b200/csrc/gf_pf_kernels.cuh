@@ -31,7 +31,7 @@ struct PfJob {
   int64_t N;
   int32_t dx, dy, T, width;
   int32_t tile0, ntiles, stile0, nstiles;
-  int32_t resampler, conv, prop, pad0;
+  int32_t resampler, conv, prop, diag_l;  // diag_l: proposal noise factor is diagonal
   double threshold, log_n, obs_const, prop_const;
   uint64_t seed;
   const void* params;        // model parameters in the run's precision
@@ -57,6 +57,8 @@ struct PfJob {
   int32_t* clamps_out;       // nullable [1]
   double* means_out;         // nullable [T][mdim]
   const double* wraw;        // nullable: scan raw weights wraw[k] / sc->wtotal instead of exp(lw - LSE)
+  double* tprefix;           // [ntiles + 1] cumulative normalised weight at each tile start
+  int32_t* anc;              // [N] 0-based ancestors of the pending resample
 };
 
 __device__ __forceinline__ int find_job(const PfJob* jobs, int njobs, int block, bool scan) {
@@ -144,23 +146,39 @@ __device__ __forceinline__ int64_t find_ancestor(const PfJob& J, PfScalars* sc, 
   return a;
 }
 
-// Boundary ancestors of the block's slot chunks (monotone resamplers): thread
-// 2p / 2p+1 searches the first / last slot of chunk p over the whole range.
-__device__ __forceinline__ void chunk_bounds(const PfJob& J, PfScalars* sc, int t, int tile,
-                                             int64_t* sb) {
-  if (threadIdx.x < 2 * PF_PPT) {
-    int p = threadIdx.x >> 1;
-    int64_t first = (int64_t)tile * PF_TILE + (int64_t)p * PF_THREADS;
-    int64_t j = (threadIdx.x & 1) ? first + PF_THREADS - 1 : first;
-    if (j > J.N - 1) j = J.N - 1;
-    if (first > J.N - 1) {
-      sb[threadIdx.x] = 0;
-    } else {
-      SlotSearch s = make_search(J, sc, t, j);
-      int64_t a = s.first(0, J.N);
-      sb[threadIdx.x] = a >= J.N ? J.N - 1 : a;
+// Offspring count: the number of slots j in [0, N) assigned to particles whose
+// cumulative normalised weight is <= W, i.e. O_k for W = W_k.  Exact and O(1):
+//  CPU rule (resamplers.jl:220-235) with thresholds t_j = u0 + j (systematic)
+//  or j + U_j (stratified), both in [j, j+1]: every j < floor(n W) - 1 counts,
+//  the two candidates at floor(n W) - 1 and floor(n W) are compared exactly.
+//  CUDAExt rule (CUDAExt.jl:55-57,74-76): O = min(n, floor(n W / W_n + u)).
+__device__ __forceinline__ int64_t offspring_count(const PfJob& J, const PfScalars* sc, int t,
+                                                   double W) {
+  const int64_t N = J.N;
+  const double dn = (double)N;
+  if (J.conv == GF_CONV_CPU) {
+    const double vs = dn * W;
+    double f = floor(vs) - 1.0;
+    int64_t g = f <= 0.0 ? 0 : (f >= dn ? N : (int64_t)f);
+    int64_t cnt = g;
+    for (int64_t j = g; j <= g + 1 && j < N; ++j) {
+      const double thr = J.resampler == GF_RS_SYSTEMATIC ? sc->u0 + (double)j
+                                                         : (double)j + slot_uniform(J, j, t);
+      if (thr < vs) cnt = j + 1;
     }
+    return cnt;
   }
+  const double r = (dn * W) / sc->wn;
+  double u;
+  if (J.resampler == GF_RS_SYSTEMATIC) {
+    u = sc->u0;
+  } else {
+    const double kk = floor(r + 1.0);
+    const int64_t ki = kk < dn ? (kk < 1.0 ? 1 : (int64_t)kk) : N;
+    u = slot_uniform(J, ki - 1, t);
+  }
+  const double f = floor(r + u);
+  return f < dn ? (f < 0.0 ? 0 : (int64_t)f) : N;
 }
 
 // Per-thread online accumulation of (max, sum exp, sum exp^2) in FP64.
@@ -184,27 +202,22 @@ struct LseAcc {
 // Folds the block's accumulators into part[tile] and lets the last block of
 // the job finalise the step (containers.jl:160-173 marginalise!,
 // particles.jl:70-73 baseline, resamplers.jl:179-183 ESS decision).
-static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh, LseAcc a, LseAcc b0,
-                             double* red) {
+// Baseline: log N after a resample or for the initial TypelessZero weights;
+// otherwise logsumexp of the normalised log-weights, which is 0 up to the
+// rounding of the normalisation (below 1e-15), so it is taken as 0.
+static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh, LseAcc a,
+                                    double* red) {
   PfScalars* sc = J.sc;
   __shared__ int s_last;
   double M = block_max(a.m, red);
   double f = a.m > -INFINITY ? exp(a.m - M) : 0.0;
   double S1 = block_sum(a.s1 * f, red);
   double S2 = block_sum(a.s2 * f * f, red);
-  double M0 = -INFINITY, S0 = 0.0;
-  if (!fresh) {
-    M0 = block_max(b0.m, red);
-    double f0 = b0.m > -INFINITY ? exp(b0.m - M0) : 0.0;
-    S0 = block_sum(b0.s1 * f0, red);
-  }
   if (threadIdx.x == 0) {
     double* p = J.part + (size_t)tile * PF_PW;
     p[0] = M;
     p[1] = S1;
     p[2] = S2;
-    p[3] = M0;
-    p[4] = S0;
     __threadfence();
     unsigned prev = atomicAdd(&sc->counter, 1u);
     s_last = (prev == (unsigned)(J.ntiles - 1));
@@ -216,7 +229,7 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
   double m = -INFINITY;
   for (int bb = threadIdx.x; bb < J.ntiles; bb += blockDim.x) m = fmax(m, __ldcg(J.part + (size_t)bb * PF_PW));
   double GM = block_max(m, red);
-  double s1 = 0.0, s2 = 0.0, m0 = -INFINITY;
+  double s1 = 0.0, s2 = 0.0;
   for (int bb = threadIdx.x; bb < J.ntiles; bb += blockDim.x) {
     const double* p = J.part + (size_t)bb * PF_PW;
     double mb = __ldcg(p);
@@ -225,26 +238,13 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
       s1 += __ldcg(p + 1) * ff;
       s2 += __ldcg(p + 2) * ff * ff;
     }
-    if (!fresh) m0 = fmax(m0, __ldcg(p + 3));
   }
   double GS1 = block_sum(s1, red);
   double GS2 = block_sum(s2, red);
-  double base = J.log_n;
-  if (!fresh) {
-    double GM0 = block_max(m0, red);
-    double s0 = 0.0;
-    for (int bb = threadIdx.x; bb < J.ntiles; bb += blockDim.x) {
-      const double* p = J.part + (size_t)bb * PF_PW;
-      double mb = __ldcg(p + 3);
-      if (mb > -INFINITY) s0 += __ldcg(p + 4) * exp(mb - GM0);
-    }
-    double GS0 = block_sum(s0, red);
-    base = GM0 + log(GS0);
-  }
-  // clear the lookback flags for the scan that may follow
-  for (int bb = threadIdx.x; bb < 2 * J.nstiles; bb += blockDim.x) J.flags[bb] = 0ull;
+  const double base = fresh ? J.log_n : 0.0;
+  __shared__ int s_res;
+  const double lse = GM + log(GS1);
   if (threadIdx.x == 0) {
-    double lse = GM + log(GS1);
     double inc = lse - base;
     double ess = GS1 * GS1 / GS2;
     if (!(lse > -INFINITY) || isnan(lse)) sc->status = GF_ERR_ARG;  // all weights vanished
@@ -261,11 +261,135 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
     sc->lse = lse;
     sc->ess = ess;
     sc->resample = res;
+    s_res = res;
+  }
+  __syncthreads();
+  if (s_res && threadIdx.x < 32) {
+    // Cumulative normalised weight at every tile start, P_{b+1} = P_b + S1_b e^{M_b - LSE}:
+    // each lane sums a contiguous run of tiles, lane 0 chains the lane totals, so
+    // every P is an exact running sum (monotone, deterministic).
+    const int lane = threadIdx.x;
+    const int per = (J.ntiles + 31) / 32;
+    const int b0 = min(lane * per, J.ntiles), b1 = min(b0 + per, J.ntiles);
+    double tot = 0.0;
+    for (int bb = b0; bb < b1; ++bb) {
+      const double* p = J.part + (size_t)bb * PF_PW;
+      const double mb = __ldcg(p);
+      if (mb > -INFINITY) tot += __ldcg(p + 1) * exp(mb - lse);
+    }
+    double off = 0.0;
+    for (int l = 0; l < 32; ++l) {
+      const double tl = __shfl_sync(0xffffffffu, tot, l);
+      if (l < lane) off += tl;
+    }
+    double run = off;
+    for (int bb = b0; bb < b1; ++bb) {
+      J.tprefix[bb] = run;
+      const double* p = J.part + (size_t)bb * PF_PW;
+      const double mb = __ldcg(p);
+      if (mb > -INFINITY) run += __ldcg(p + 1) * exp(mb - lse);
+    }
+    if (lane == 31) {
+      J.tprefix[J.ntiles] = run;
+      sc->wn = run;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
     sc->uniform = 0;
     sc->scan_tile = 0u;
     sc->counter = 0u;
     __threadfence();
     sc->t = t;
+  }
+}
+
+// ---------------------------------------------------------- resample kernel
+// Runs after a propagate whose finalise decided to resample: per propagate
+// tile, the cumulative normalised weights W_k = P_b + (running sum inside the
+// tile), then each particle's offspring slot range [O(W_{k-1}), O(W_k)) gets
+// ancestor k (the cumulative-offspring form of CUDAExt.jl:90-117, with the
+// counts computed exactly per rule).  Multinomial ancestors (unsorted
+// uniforms) instead take W_k to the per-slot search of the next propagate.
+constexpr int RS_LONG = 32;  // offspring runs longer than this are filled by the whole block
+template <typename Real>
+__global__ void __launch_bounds__(PF_THREADS) pf_resample_kernel(const PfJob* __restrict__ jobs,
+                                                                int njobs) {
+  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const PfJob& J = jobs[jb];
+  PfScalars* sc = J.sc;
+  if (!sc->resample || sc->status != 0 || sc->t >= J.T) return;
+  __shared__ double sw[PF_TILE];
+  __shared__ int32_t sO[PF_TILE];
+  __shared__ int32_t sq[PF_TILE][3];
+  __shared__ int s_qn;
+  __shared__ int32_t s_O0;
+  const int tstep = sc->t + 1;
+  const int tile = blockIdx.x - J.tile0;
+  const int64_t N = J.N, i0 = (int64_t)tile * PF_TILE;
+  const int nloc = (int)min((int64_t)PF_TILE, N - i0);
+  const double lse = sc->lse;
+  const Real* lw = reinterpret_cast<const Real*>(J.lw);
+  const double P0 = J.tprefix[tile], P1 = J.tprefix[tile + 1];
+#pragma unroll
+  for (int p = 0; p < PF_PPT; ++p) {
+    const int l = p * PF_THREADS + threadIdx.x;
+    sw[l] = l < nloc ? exp((double)lw[i0 + l] - lse) : 0.0;
+  }
+  if (threadIdx.x == 0) s_qn = 0;
+  __syncthreads();
+  if (threadIdx.x < 32) {
+    // 32 lanes x 32 contiguous particles: lane-serial sums chained by lane
+    // order, so W is an exact running sum, then clamped to the tile's end value.
+    const int lane = threadIdx.x;
+    constexpr int PER = PF_TILE / 32;
+    double tot = 0.0;
+#pragma unroll 8
+    for (int q = 0; q < PER; ++q) tot += sw[lane * PER + q];
+    double off = P0;
+    for (int l = 0; l < 32; ++l) {
+      const double tl = __shfl_sync(0xffffffffu, tot, l);
+      if (l < lane) off += tl;
+    }
+    double run = 0.0;
+    for (int q = 0; q < PER; ++q) {
+      const int l = lane * PER + q;
+      run += sw[l];
+      double W = off + run;
+      W = W < P1 ? W : P1;
+      if (l == nloc - 1) W = P1;
+      sw[l] = W;
+    }
+  }
+  __syncthreads();
+  if (J.resampler == GF_RS_MULTINOMIAL) {
+    for (int l = threadIdx.x; l < nloc; l += PF_THREADS) J.key[i0 + l] = sw[l];
+    return;
+  }
+  for (int l = threadIdx.x; l < nloc; l += PF_THREADS) sO[l] = (int32_t)offspring_count(J, sc, tstep, sw[l]);
+  if (threadIdx.x == 0) s_O0 = (int32_t)offspring_count(J, sc, tstep, P0);
+  __syncthreads();
+  for (int l = threadIdx.x; l < nloc; l += PF_THREADS) {
+    const int32_t lo = l == 0 ? s_O0 : sO[l - 1], hi = sO[l];
+    if (hi - lo > RS_LONG) {
+      const int q = atomicAdd(&s_qn, 1);
+      sq[q][0] = l;
+      sq[q][1] = lo;
+      sq[q][2] = hi;
+    } else {
+      for (int32_t j = lo; j < hi; ++j) J.anc[j] = (int32_t)(i0 + l);
+    }
+  }
+  __syncthreads();
+  for (int q = 0; q < s_qn; ++q) {
+    const int32_t k = (int32_t)(i0 + sq[q][0]);
+    for (int32_t j = sq[q][1] + threadIdx.x; j < sq[q][2]; j += PF_THREADS) J.anc[j] = k;
+  }
+  if (i0 + nloc == N && threadIdx.x == 0) {
+    // slots beyond the last threshold below W_N (rounding): last particle, counted
+    const int32_t last = sO[nloc - 1];
+    if (last < N) atomicAdd(&sc->clamps, (int32_t)(N - last));
+    for (int64_t j = last; j < N; ++j) J.anc[j] = (int32_t)(N - 1);
   }
 }
 

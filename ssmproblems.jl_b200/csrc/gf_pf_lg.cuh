@@ -46,7 +46,7 @@ __device__ __forceinline__ void draw_noise(const PfJob& J, const Real* noise, in
 }
 
 template <typename Real, int DXP, int DYP, bool GUIDED>
-__global__ void __launch_bounds__(PF_THREADS) pf_lg_propagate(const PfJob* __restrict__ jobs,
+__global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __restrict__ jobs,
                                                              int njobs) {
   using Lay = LgLayout<DXP, DYP>;
   extern __shared__ __align__(16) unsigned char smraw[];
@@ -59,7 +59,6 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_propagate(const PfJob* __res
   Real* sM = sv + DXP;
   Real* sQi = sM + DXP * DXP;
   __shared__ double red[32];
-  __shared__ int64_t sbnd[2 * PF_PPT];
 
   const int jb = find_job(jobs, njobs, blockIdx.x, false);
   const PfJob& J = jobs[jb];
@@ -70,7 +69,7 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_propagate(const PfJob* __res
   const bool resamp = sc->resample != 0;
   const bool fresh = resamp || sc->uniform != 0;
   const double lse_prev = sc->lse;
-  const bool mono = J.resampler != GF_RS_MULTINOMIAL;
+  const bool searched = J.resampler == GF_RS_MULTINOMIAL;
 
   const Real* P = reinterpret_cast<const Real*>(J.params);
   for (int k = threadIdx.x; k < Lay::H + DYP * DXP; k += PF_THREADS) sA[k] = P[k];
@@ -79,7 +78,6 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_propagate(const PfJob* __res
   if constexpr (GUIDED) {
     for (int k = threadIdx.x; k < 2 * DXP * DXP; k += PF_THREADS) sM[k] = P[Lay::M + k];
   }
-  if (resamp && mono) chunk_bounds(J, sc, t, tile, sbnd);
   __syncthreads();
 
   const int64_t N = J.N;
@@ -88,65 +86,73 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_propagate(const PfJob* __res
   Real* Xd = reinterpret_cast<Real*>(J.X[t & 1]);
   Real* lw = reinterpret_cast<Real*>(J.lw);
   const Real* noise = J.noise ? reinterpret_cast<const Real*>(J.noise) + (size_t)t * dx * N : nullptr;
-  LseAcc acc, acc0;
+  LseAcc acc;
 
   for (int p = 0; p < PF_PPT; ++p) {
     const int64_t i = (int64_t)tile * PF_TILE + p * PF_THREADS + threadIdx.x;
     if (i >= N) break;
     int64_t a = i;
-    if (resamp) {
-      int64_t lo = 0, hi = N;
-      if (mono) {
-        lo = sbnd[2 * p];
-        hi = sbnd[2 * p + 1] + 1;
-      }
-      a = find_ancestor(J, sc, t, i, lo, hi);
-    }
+    if (resamp) a = searched ? find_ancestor(J, sc, t, i, 0, N) : (int64_t)J.anc[i];
     Real x[DXP];
 #pragma unroll
     for (int d = 0; d < DXP; ++d) x[d] = d < dx ? Xs[(size_t)d * N + a] : Real(0);
-    double lin = 0.0;
-    if (!fresh) {
-      lin = (double)lw[i] - lse_prev;
-      acc0.add(lin);
-    }
-    Real e[DXP];
-    draw_noise<Real, DXP>(J, noise, i, t, dx, N, e);
-
+    const double lin = fresh ? 0.0 : (double)lw[i] - lse_prev;
+    // mean part: x' = A x + b (bootstrap, simulate(dyn) = rand(MvNormal(A x + b, Q)))
+    // or M x + v_t (guided), with ma = A x + b kept for log p(x'|x)
     Real xn[DXP];
-    double inc = 0.0;
-    if constexpr (!GUIDED) {
-      // x' = A x + b + L_Q e   (simulate(dyn) = rand(MvNormal(A x + b, Q)))
+    Real ma[GUIDED ? DXP : 1];
 #pragma unroll
-      for (int r = 0; r < DXP; ++r) xn[r] = sb[r];
+    for (int r = 0; r < DXP; ++r) xn[r] = GUIDED ? sv[r] : sb[r];
+    if constexpr (GUIDED) {
 #pragma unroll
-      for (int c = 0; c < DXP; ++c) {
-        const Real xc = x[c], ec = e[c];
+      for (int r = 0; r < DXP; ++r) ma[r] = sb[r];
+    }
 #pragma unroll
-        for (int r = 0; r < DXP; ++r) xn[r] = fma(sA[c * DXP + r], xc, xn[r]);
-#pragma unroll
-        for (int r = c; r < DXP; ++r) xn[r] = fma(sL[c * DXP + r], ec, xn[r]);
-      }
-    } else {
-      // x' = M x + v_t + L_q e ; inc = log N(x'; A x + b, Q) - log N(x'; M x + v_t, L_q L_q')
-      Real ma[DXP];
+    for (int c = 0; c < DXP; ++c) {
+      const Real xc = x[c];
 #pragma unroll
       for (int r = 0; r < DXP; ++r) {
-        xn[r] = sv[r];
-        ma[r] = sb[r];
-      }
-#pragma unroll
-      for (int c = 0; c < DXP; ++c) {
-        const Real xc = x[c], ec = e[c];
-#pragma unroll
-        for (int r = 0; r < DXP; ++r) {
+        if constexpr (GUIDED) {
           xn[r] = fma(sM[c * DXP + r], xc, xn[r]);
           ma[r] = fma(sA[c * DXP + r], xc, ma[r]);
+        } else {
+          xn[r] = fma(sA[c * DXP + r], xc, xn[r]);
         }
-#pragma unroll
-        for (int r = c; r < DXP; ++r) xn[r] = fma(sL[c * DXP + r], ec, xn[r]);
       }
-      Real qz = 0, qe = 0;
+    }
+    // noise part: + L e, with e drawn four at a time and consumed at once
+    Real qe = 0;
+#pragma unroll
+    for (int q = 0; q < (DXP + 3) / 4; ++q) {
+      Real e4[4];
+      if (noise) {
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+          const int c = 4 * q + cc;
+          e4[cc] = (c < DXP && c < dx) ? noise[(size_t)c * N + i] : Real(0);
+        }
+      } else {
+        philox_normals4<Real>(J.seed, (uint32_t)i, (uint32_t)t, (uint32_t)q, e4);
+      }
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) {
+        const int c = 4 * q + cc;
+        if (c < DXP) {
+          const Real ec = e4[cc];
+          if constexpr (GUIDED) qe = fma(ec, ec, qe);
+          if (J.diag_l) {
+            xn[c] = fma(sL[c * DXP + c], ec, xn[c]);
+          } else {
+#pragma unroll
+            for (int r = c; r < DXP; ++r) xn[r] = fma(sL[c * DXP + r], ec, xn[r]);
+          }
+        }
+      }
+    }
+    double inc = 0.0;
+    if constexpr (GUIDED) {
+      // inc = log N(x'; A x + b, Q) - log N(x'; M x + v_t, Lq Lq')
+      Real qz = 0;
 #pragma unroll
       for (int r = 0; r < DXP; ++r) ma[r] = xn[r] - ma[r];
 #pragma unroll
@@ -155,7 +161,6 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_propagate(const PfJob* __res
 #pragma unroll
         for (int c = 0; c <= r; ++c) z = fma(sQi[c * DXP + r], ma[c], z);
         qz = fma(z, z, qz);
-        qe = fma(e[r], e[r], qe);
       }
       inc = -0.5 * (double)qz + 0.5 * (double)qe + J.prop_const;
     }
@@ -177,7 +182,7 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_propagate(const PfJob* __res
     if (J.anc_out) J.anc_out[(size_t)(t - 1) * N + i] = (int32_t)(a + 1);
     acc.add((double)lst);
   }
-  block_finish(J, tile, t, fresh, acc, acc0, red);
+  block_finish(J, tile, t, fresh, acc, red);
 }
 
 // x_0 ~ MvNormal(mu0, Sigma0) (particles.jl:36-50, models/linear_gaussian.jl:23-29)
@@ -207,6 +212,11 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_init(const PfJob* __restrict
       X[(size_t)r * N + i] = v;
     }
     lw[i] = Real(0);
+  }
+  // cumulative weight at each tile start for the uniform initial weights
+  if (threadIdx.x == 0) {
+    J.tprefix[tile] = (double)((int64_t)tile * PF_TILE) / (double)N;
+    if (tile == J.ntiles - 1) J.tprefix[J.ntiles] = 1.0;
   }
 }
 

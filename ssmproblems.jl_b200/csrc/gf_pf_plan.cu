@@ -24,6 +24,8 @@ struct gf_pf_plan {
   std::vector<DevBuf> bufs;
   void *params = nullptr, *ystep = nullptr, *X0 = nullptr, *X1 = nullptr, *lw = nullptr;
   double *pp = nullptr, *key = nullptr, *part = nullptr, *mpart = nullptr, *ess1 = nullptr;
+  double* tprefix = nullptr;
+  int32_t* anc = nullptr;
   unsigned long long* flags = nullptr;
   PfScalars* sc = nullptr;
   int8_t *sched_dev = nullptr, *res1 = nullptr;
@@ -109,6 +111,8 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   ALLOC(X1, p->rsize * (size_t)N * m->dx);
   ALLOC(lw, p->rsize * (size_t)N);
   ALLOC(key, sizeof(double) * (size_t)N);
+  ALLOC(anc, sizeof(int32_t) * (size_t)N);
+  ALLOC(tprefix, sizeof(double) * (size_t)(p->ntiles + 1));
   ALLOC(part, sizeof(double) * PF_PW * (size_t)p->ntiles);
   ALLOC(mpart, sizeof(double) * (size_t)p->ntiles * m->dx);
   ALLOC(flags, sizeof(unsigned long long) * 2 * (size_t)p->nstiles);
@@ -148,6 +152,13 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   J.resampler = cfg->resampler;
   J.conv = cfg->convention;
   J.prop = cfg->proposal;
+  {
+    bool diag = true;
+    for (int j = 0; j < m->dx; ++j)
+      for (int i = 0; i < m->dx; ++i)
+        if (i != j && f.L[i + j * m->dx] != 0.0) diag = false;
+    J.diag_l = diag ? 1 : 0;
+  }
   J.threshold = cfg->threshold;
   J.log_n = std::log((double)N);
   J.obs_const = f.obs_const;
@@ -163,6 +174,8 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   J.part = p->part;
   J.flags = p->flags;
   J.sc = p->sc;
+  J.anc = p->anc;
+  J.tprefix = p->tprefix;
   J.schedule = p->sched_dev;
   *out = p.release();
   return GF_OK;
@@ -179,14 +192,14 @@ static void enqueue_run(gf_pf_plan* p, bool means) {
     ProfScope ps(ctx, KC_PREP);
     p->k.init<<<p->ntiles, PF_THREADS, 0, s>>>(p->job_dev, 1, p->k.off_mu0, p->k.off_L0);
   }
-  launch_scan(ctx, p->dbl, p->job_dev, 1, p->nstiles);
+  launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
   for (int t = 1; t <= p->T; ++t) {
     {
       ProfScope ps(ctx, KC_PROPAGATE);
       p->k.prop<<<p->ntiles, PF_THREADS, p->k.smem, s>>>(p->job_dev, 1);
     }
     if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);
-    if (t < p->T) launch_scan(ctx, p->dbl, p->job_dev, 1, p->nstiles);
+    if (t < p->T) launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
   }
   launch_finish(ctx, p->dbl, p->job_dev, p->N);
 }

@@ -43,7 +43,6 @@ __global__ void __launch_bounds__(PF_THREADS) rbpf_propagate(const PfJob* __rest
   __shared__ float sp[L::total];
   __shared__ double sy[DY];
   __shared__ double red[32];
-  __shared__ int64_t sbnd[2 * PF_PPT];
   const int jb = find_job(jobs, njobs, blockIdx.x, false);
   const PfJob& J = jobs[jb];
   PfScalars* sc = J.sc;
@@ -53,31 +52,23 @@ __global__ void __launch_bounds__(PF_THREADS) rbpf_propagate(const PfJob* __rest
   const bool resamp = sc->resample != 0;
   const bool fresh = resamp || sc->uniform != 0;
   const double lse_prev = sc->lse;
-  const bool mono = J.resampler != GF_RS_MULTINOMIAL;
+  const bool searched = J.resampler == GF_RS_MULTINOMIAL;
   const float* P = reinterpret_cast<const float*>(J.params);
   for (int k = threadIdx.x; k < L::total; k += PF_THREADS) sp[k] = P[k];
   if (threadIdx.x < DY) sy[threadIdx.x] = J.ys[(size_t)(t - 1) * DY + threadIdx.x];
-  if (resamp && mono) chunk_bounds(J, sc, t, tile, sbnd);
   __syncthreads();
   const int64_t N = J.N;
   const float* Xs = reinterpret_cast<const float*>(J.X[(t - 1) & 1]);
   float* Xd = reinterpret_cast<float*>(J.X[t & 1]);
   float* lw = reinterpret_cast<float*>(J.lw);
   const float* noise = J.noise ? reinterpret_cast<const float*>(J.noise) + (size_t)t * DXO * N : nullptr;
-  LseAcc acc, acc0;
+  LseAcc acc;
   int fail = 0;
   for (int p = 0; p < PF_PPT; ++p) {
     const int64_t i = (int64_t)tile * PF_TILE + p * PF_THREADS + threadIdx.x;
     if (i >= N) break;
     int64_t a = i;
-    if (resamp) {
-      int64_t lo = 0, hi = N;
-      if (mono) {
-        lo = sbnd[2 * p];
-        hi = sbnd[2 * p + 1] + 1;
-      }
-      a = find_ancestor(J, sc, t, i, lo, hi);
-    }
+    if (resamp) a = searched ? find_ancestor(J, sc, t, i, 0, N) : (int64_t)J.anc[i];
     float x[DXO], mu[DZ], S[NS];
 #pragma unroll
     for (int d = 0; d < DXO; ++d) x[d] = Xs[(size_t)d * N + a];
@@ -85,11 +76,7 @@ __global__ void __launch_bounds__(PF_THREADS) rbpf_propagate(const PfJob* __rest
     for (int d = 0; d < DZ; ++d) mu[d] = Xs[(size_t)(DXO + d) * N + a];
 #pragma unroll
     for (int d = 0; d < NS; ++d) S[d] = Xs[(size_t)(DXO + DZ + d) * N + a];
-    double lin = 0.0;
-    if (!fresh) {
-      lin = (double)lw[i] - lse_prev;
-      acc0.add(lin);
-    }
+    const double lin = fresh ? 0.0 : (double)lw[i] - lse_prev;
     // ---- outer propagate
     float e[DXO];
     if (noise) {
@@ -322,7 +309,7 @@ __global__ void __launch_bounds__(PF_THREADS) rbpf_propagate(const PfJob* __rest
     acc.add((double)lst);
   }
   if (fail) sc->status = GF_ERR_NOT_PD;
-  block_finish(J, tile, t, fresh, acc, acc0, red);
+  block_finish(J, tile, t, fresh, acc, red);
 }
 
 template <int DXO, int DZ, int DY>
@@ -358,6 +345,10 @@ __global__ void __launch_bounds__(PF_THREADS) rbpf_init(const PfJob* __restrict_
     for (int d = 0; d < DZ; ++d) X[(size_t)(DXO + d) * N + i] = P[L::muz + d];
     for (int d = 0; d < L::NS; ++d) X[(size_t)(DXO + DZ + d) * N + i] = P[L::S0z + d];
     lw[i] = 0.f;
+  }
+  if (threadIdx.x == 0) {
+    J.tprefix[tile] = (double)((int64_t)tile * PF_TILE) / (double)N;
+    if (tile == J.ntiles - 1) J.tprefix[J.ntiles] = 1.0;
   }
 }
 
@@ -458,11 +449,14 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
     return s2;
   };
   void *d_params, *X0, *X1, *lw, *key, *part, *mpart, *flags, *scv, *ess1, *res1, *jobv, *schedv = nullptr;
+  void *ancv, *tprev;
   if ((st = get(sizeof(float) * P.size(), &d_params))) return st;
   if ((st = get(sizeof(float) * (size_t)N * width, &X0))) return st;
   if ((st = get(sizeof(float) * (size_t)N * width, &X1))) return st;
   if ((st = get(sizeof(float) * (size_t)N, &lw))) return st;
   if ((st = get(sizeof(double) * (size_t)N, &key))) return st;
+  if ((st = get(sizeof(int32_t) * (size_t)N, &ancv))) return st;
+  if ((st = get(sizeof(double) * (size_t)(ntiles + 1), &tprev))) return st;
   if ((st = get(sizeof(double) * PF_PW * ntiles, &part))) return st;
   if ((st = get(sizeof(double) * ntiles * (dxo + dz), &mpart))) return st;
   if ((st = get(sizeof(unsigned long long) * 2 * nstiles, &flags))) return st;
@@ -551,6 +545,8 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   J.part = (double*)part;
   J.flags = (unsigned long long*)flags;
   J.sc = (PfScalars*)scv;
+  J.anc = (int32_t*)ancv;
+  J.tprefix = (double*)tprev;
   J.noise = d_noise;
   J.unif = d_unif;
   J.schedule = (const int8_t*)schedv;
@@ -569,7 +565,7 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   launch_init_scalars(ctx, jd, 1, (const double*)ess1, (const int8_t*)res1);
   GF_CHECK_CUDA(ctx, cudaMemsetAsync(flags, 0, sizeof(unsigned long long) * 2 * nstiles, s));
   K.init<<<ntiles, PF_THREADS, 0, s>>>(jd, 1);
-  launch_scan(ctx, false, jd, 1, nstiles);
+  launch_resample(ctx, false, jd, 1, ntiles);
   const int guided = cfg->proposal == GF_PROP_OVERDISPERSED;
   for (int t = 1; t <= T; ++t) {
     {
@@ -577,7 +573,7 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
       K.prop<<<ntiles, PF_THREADS, 0, s>>>(jd, 1, (float)m->q_gamma, m->q_index, guided);
     }
     if (want_means) launch_means(ctx, false, jd, 1, ntiles, (double*)mpart, dxo + dz);
-    if (t < T) launch_scan(ctx, false, jd, 1, nstiles);
+    if (t < T) launch_resample(ctx, false, jd, 1, ntiles);
   }
   launch_finish(ctx, false, jd, N);
   GF_CHECK_CUDA(ctx, cudaGetLastError());

@@ -41,6 +41,9 @@ def dummy_rb_model(rng, d_outer=1, d_inner=1, dy=1):
     A[:d_outer, :d_outer] = rng.random((d_outer, d_outer))
     A[d_outer:, :d_outer] = rng.random((d_inner, d_outer))
     A[d_outer:, d_outer:] = rng.random((d_inner, d_inner))
+    rho = np.max(np.abs(np.linalg.eigvals(A)))
+    if D > 2 and rho > 0.9:  # GFTest draws U(0,1) entries; keep the larger test models stable
+        A *= 0.9 / rho
     b = rng.random(D)
     Q = np.zeros((D, D))
     Q[:d_outer, :d_outer] = O.rand_cov(rng, d_outer, scale=0.1)

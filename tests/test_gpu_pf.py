@@ -191,8 +191,12 @@ def test_large_pf_properties(ctx, kind):
 
 
 def test_large_pf_converges_to_kf_ll(ctx):
-    """The PF log-likelihood estimate at N = 2^20 is close to the exact KF value."""
+    """The PF log-likelihood estimate at N = 2^20 (Dx=16, T=50) agrees with the exact
+    KF value within its Monte-Carlo spread (6 independent seeds)."""
     m, ys = W.lgssm_rot(seed=9, dx=16, dy=8, T=50)
-    st, ll = G.filter(m, G.BF(2**20, threshold=0.5), ys, seed=1, ctx=ctx)
+    lls = np.array([G.filter(m, G.BF(2**20, threshold=0.5), ys, seed=s, ctx=ctx)[1]
+                    for s in range(6)])
     llkf, _ = _kf_ll(m, ys)
-    assert abs(ll - llkf) < 0.5 + 1e-3 * abs(llkf)
+    sd = lls.std(ddof=1)
+    assert sd < 2.0
+    assert abs(np.median(lls) - llkf) < 2.0 + 3 * sd

@@ -35,10 +35,11 @@ def test_rbpf_matches_oracle(ctx, dims):
 
 
 def test_rbpf_converges_to_kf(ctx):
+    """Reference tolerances (ll 1e-3 absolute, means 1e-3 relative) at N = 2^22."""
     rng = np.random.default_rng(1234)
     full, hier = dummy_rb_model(rng, 1, 1, 1)
     _, ys = simulate(rng, full, 4)
-    algo = G.RBPF(G.BF(10**6, resampler=G.AlternatingResampler()), G.KalmanFilter())
+    algo = G.RBPF(G.BF(2**22, resampler=G.AlternatingResampler()), G.KalmanFilter())
     st, ll = G.filter(hier, algo, ys, seed=31, ctx=ctx)
     llkf, _, mus, _ = O.kf_filter(to_oracle(full), ys)
     w = st.weights()
