@@ -210,6 +210,25 @@ gf_status gf_offspring_to_ancestors(gf_ctx* ctx, int64_t n, const int64_t* offsp
  * offspring counts. */
 gf_status gf_ancestors_to_offspring(gf_ctx* ctx, int64_t n, const int64_t* ancestors_dev,
                                     int64_t* offspring_dev);
+/* gf_sample_ancestors without any device allocation.  No counterpart in the
+ * reference: it exists for callers that cannot call cudaMalloc where they
+ * resample (a memory-pool-managed host framework that forbids foreign
+ * allocations, a real-time loop that must not take the allocator's locks or
+ * synchronise the device, code sized up front that must not fail with
+ * out-of-memory mid-run).  Same arguments and results as gf_sample_ancestors,
+ * on the caller's `stream` (a cudaStream_t, NULL = default stream) of the
+ * current device; returns once the ancestors are written.
+ * Limit: n <= gf_sample_ancestors_noalloc_max_n() (2^18); larger n returns
+ * GF_ERR_DIM.  All scratch lives in one fixed device array (about 2.1 MB) that
+ * every device loading the library holds until the process exits.  The first
+ * call on a device resolves that array's address (cudaGetSymbolAddress), so
+ * make the first call before any stream capture.  Calls share the array:
+ * calls that overlap on the GPU (other streams, other host threads on the
+ * same device) race and must be serialised by the caller. */
+gf_status gf_sample_ancestors_noalloc(int32_t resampler, int32_t convention, int64_t n,
+                                      const double* weights_dev, const double* uniforms_dev,
+                                      int64_t* ancestors_dev, void* stream);
+int64_t gf_sample_ancestors_noalloc_max_n(void);
 /* The noise the PF kernels draw in-kernel for step t: out [dx][n] in the given
  * precision (no reference counterpart: exported so tests can inject it). */
 gf_status gf_rng_normals(gf_ctx* ctx, uint64_t seed, int32_t t, int32_t dx, int64_t n,

@@ -30,7 +30,7 @@ EXPORTED = [
     "gf_kf_batch", "gf_kf_plan_create", "gf_kf_plan_run", "gf_kf_plan_destroy",
     "gf_pf_run", "gf_pf_plan_create", "gf_pf_plan_run", "gf_pf_plan_destroy", "gf_rbpf_run",
     "gf_sample_ancestors", "gf_offspring_to_ancestors", "gf_ancestors_to_offspring",
-    "gf_rng_normals",
+    "gf_rng_normals", "gf_sample_ancestors_noalloc", "gf_sample_ancestors_noalloc_max_n",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -121,6 +121,8 @@ def load(path: str | None = None):
         "gf_offspring_to_ancestors": (i32, [ctxp, i64, _vp, _vp]),
         "gf_ancestors_to_offspring": (i32, [ctxp, i64, _vp, _vp]),
         "gf_rng_normals": (i32, [ctxp, u64, i32, i32, i64, i32, _vp]),
+        "gf_sample_ancestors_noalloc": (i32, [i32, i32, i64, _vp, _vp, _vp, _vp]),
+        "gf_sample_ancestors_noalloc_max_n": (i64, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
