@@ -264,34 +264,50 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
     s_res = res;
   }
   __syncthreads();
-  if (s_res && threadIdx.x < 32) {
+  if (s_res) {
     // Cumulative normalised weight at every tile start, P_{b+1} = P_b + S1_b e^{M_b - LSE}:
-    // each lane sums a contiguous run of tiles, lane 0 chains the lane totals, so
-    // every P is an exact running sum (monotone, deterministic).
-    const int lane = threadIdx.x;
-    const int per = (J.ntiles + 31) / 32;
-    const int b0 = min(lane * per, J.ntiles), b1 = min(b0 + per, J.ntiles);
-    double tot = 0.0;
-    for (int bb = b0; bb < b1; ++bb) {
-      const double* p = J.part + (size_t)bb * PF_PW;
-      const double mb = __ldcg(p);
-      if (mb > -INFINITY) tot += __ldcg(p + 1) * exp(mb - lse);
+    // tile masses in parallel, then each lane of warp 0 sums a contiguous run
+    // and the lane totals are chained in order, so every P is an exact running
+    // sum (monotone, deterministic).  Chunks of 32 * 32 tiles at a time.
+    __shared__ double stw[32 * 33];
+    __shared__ double s_carry;
+    if (threadIdx.x == 0) s_carry = 0.0;
+    for (int c0 = 0; c0 < J.ntiles; c0 += 32 * 32) {
+      __syncthreads();
+      for (int q = threadIdx.x; q < 32 * 32; q += blockDim.x) {
+        const int bb = c0 + q;
+        double v = 0.0;
+        if (bb < J.ntiles) {
+          const double* p = J.part + (size_t)bb * PF_PW;
+          const double mb = __ldcg(p);
+          if (mb > -INFINITY) v = __ldcg(p + 1) * exp(mb - lse);
+        }
+        stw[q + (q >> 5)] = v;
+      }
+      __syncthreads();
+      if (threadIdx.x < 32) {
+        const int lane = threadIdx.x;
+        double tot = 0.0;
+        for (int q = 0; q < 32; ++q) tot += stw[lane * 33 + q];
+        double off = s_carry;
+        for (int l = 0; l < 32; ++l) {
+          const double tl = __shfl_sync(0xffffffffu, tot, l);
+          if (l < lane) off += tl;
+        }
+        double run = 0.0;  // same serial order as `tot`, so the lane's end equals the next lane's start
+        for (int q = 0; q < 32; ++q) {
+          const int bb = c0 + lane * 32 + q;
+          if (bb < J.ntiles) J.tprefix[bb] = off + run;
+          run += stw[lane * 33 + q];
+        }
+        const double last = __shfl_sync(0xffffffffu, off + tot, 31);
+        if (lane == 0) s_carry = last;
+      }
     }
-    double off = 0.0;
-    for (int l = 0; l < 32; ++l) {
-      const double tl = __shfl_sync(0xffffffffu, tot, l);
-      if (l < lane) off += tl;
-    }
-    double run = off;
-    for (int bb = b0; bb < b1; ++bb) {
-      J.tprefix[bb] = run;
-      const double* p = J.part + (size_t)bb * PF_PW;
-      const double mb = __ldcg(p);
-      if (mb > -INFINITY) run += __ldcg(p + 1) * exp(mb - lse);
-    }
-    if (lane == 31) {
-      J.tprefix[J.ntiles] = run;
-      sc->wn = run;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      J.tprefix[J.ntiles] = s_carry;
+      sc->wn = s_carry;
     }
   }
   __syncthreads();
@@ -319,7 +335,7 @@ __global__ void __launch_bounds__(PF_THREADS) pf_resample_kernel(const PfJob* __
   const PfJob& J = jobs[jb];
   PfScalars* sc = J.sc;
   if (!sc->resample || sc->status != 0 || sc->t >= J.T) return;
-  __shared__ double sw[PF_TILE];
+  __shared__ double sw[PF_TILE + PF_TILE / 32];  // index l + l/32 (conflict-free lane runs)
   __shared__ int32_t sO[PF_TILE];
   __shared__ int32_t sq[PF_TILE][3];
   __shared__ int s_qn;
@@ -334,7 +350,7 @@ __global__ void __launch_bounds__(PF_THREADS) pf_resample_kernel(const PfJob* __
 #pragma unroll
   for (int p = 0; p < PF_PPT; ++p) {
     const int l = p * PF_THREADS + threadIdx.x;
-    sw[l] = l < nloc ? exp((double)lw[i0 + l] - lse) : 0.0;
+    sw[l + (l >> 5)] = l < nloc ? exp((double)lw[i0 + l] - lse) : 0.0;
   }
   if (threadIdx.x == 0) s_qn = 0;
   __syncthreads();
@@ -345,7 +361,7 @@ __global__ void __launch_bounds__(PF_THREADS) pf_resample_kernel(const PfJob* __
     constexpr int PER = PF_TILE / 32;
     double tot = 0.0;
 #pragma unroll 8
-    for (int q = 0; q < PER; ++q) tot += sw[lane * PER + q];
+    for (int q = 0; q < PER; ++q) tot += sw[lane * (PER + 1) + q];
     double off = P0;
     for (int l = 0; l < 32; ++l) {
       const double tl = __shfl_sync(0xffffffffu, tot, l);
@@ -354,19 +370,20 @@ __global__ void __launch_bounds__(PF_THREADS) pf_resample_kernel(const PfJob* __
     double run = 0.0;
     for (int q = 0; q < PER; ++q) {
       const int l = lane * PER + q;
-      run += sw[l];
+      run += sw[l + lane];
       double W = off + run;
       W = W < P1 ? W : P1;
       if (l == nloc - 1) W = P1;
-      sw[l] = W;
+      sw[l + lane] = W;
     }
   }
   __syncthreads();
   if (J.resampler == GF_RS_MULTINOMIAL) {
-    for (int l = threadIdx.x; l < nloc; l += PF_THREADS) J.key[i0 + l] = sw[l];
+    for (int l = threadIdx.x; l < nloc; l += PF_THREADS) J.key[i0 + l] = sw[l + (l >> 5)];
     return;
   }
-  for (int l = threadIdx.x; l < nloc; l += PF_THREADS) sO[l] = (int32_t)offspring_count(J, sc, tstep, sw[l]);
+  for (int l = threadIdx.x; l < nloc; l += PF_THREADS)
+    sO[l] = (int32_t)offspring_count(J, sc, tstep, sw[l + (l >> 5)]);
   if (threadIdx.x == 0) s_O0 = (int32_t)offspring_count(J, sc, tstep, P0);
   __syncthreads();
   for (int l = threadIdx.x; l < nloc; l += PF_THREADS) {
