@@ -136,8 +136,9 @@ gf_status gf_ctx_synchronize(gf_ctx* ctx);
 gf_status gf_ctx_memory(const gf_ctx* ctx, size_t* used, size_t* budget);
 /* Per-kernel timing with CUDA events on the context stream (0 = off). */
 gf_status gf_ctx_profile(gf_ctx* ctx, int32_t enable);
-/* Kernel classes: 0 propagate/weight, 1 lookback scan, 2 KF batch, 3 RBPF,
- * 4 init/prep.  Resolves pending events (synchronises the stream). */
+/* Kernel classes: 0 propagate/weight, 1 resample (cumulative weights and
+ * offspring counts), 2 KF batch, 3 RBPF, 4 init/prep, 5 ancestor fill.
+ * Resolves pending events (synchronises the stream). */
 gf_status gf_ctx_profile_read(gf_ctx* ctx, int32_t kernel_class, double* total_ms,
                               int64_t* launches);
 int32_t gf_version(void);
@@ -160,8 +161,11 @@ gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_model* models
                             int32_t flags, gf_kf_plan** out);
 gf_status gf_kf_plan_run(gf_kf_plan* plan, const double* ys_dev, gf_kf_out* out_dev);
 gf_status gf_kf_plan_destroy(gf_kf_plan* plan);
-/* flags for gf_kf_plan_create */
-enum { GF_PLAN_AUTOTUNE = 1, GF_PLAN_NO_GRAPH = 2, GF_PLAN_PLAIN = 4 };
+/* plan flags: AUTOTUNE (KF: time each bucket's block shapes and keep the
+ * fastest), NO_GRAPH (launch eagerly instead of replaying a CUDA graph), PLAIN
+ * (KF: one launch per filter, the unbatched baseline form), SIMT (PF: keep the
+ * CUDA-core propagation even where the tensor-core path applies). */
+enum { GF_PLAN_AUTOTUNE = 1, GF_PLAN_NO_GRAPH = 2, GF_PLAN_PLAIN = 4, GF_PLAN_SIMT = 8 };
 
 /* -------------------------------------------------------- particle filters */
 /* filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys)

@@ -31,7 +31,7 @@ struct gf_ctx {
 
 namespace gf {
 
-enum KernelClass { KC_PROPAGATE = 0, KC_SCAN = 1, KC_KF = 2, KC_RBPF = 3, KC_PREP = 4 };
+enum KernelClass { KC_PROPAGATE = 0, KC_SCAN = 1, KC_KF = 2, KC_RBPF = 3, KC_PREP = 4, KC_FILL = 5 };
 
 gf_status set_err(gf_ctx* ctx, gf_status code, const char* fmt, ...);
 gf_status cuda_err(gf_ctx* ctx, cudaError_t e, const char* where);

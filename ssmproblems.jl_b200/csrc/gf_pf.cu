@@ -191,9 +191,13 @@ void launch_scan(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int njobs, int to
 }
 
 void launch_resample(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int njobs, int total_tiles) {
-  ProfScope ps(ctx, KC_SCAN);
-  if (dbl) pf_resample_kernel<double><<<total_tiles, PF_THREADS, 0, ctx->stream>>>(jobs_dev, njobs);
-  else pf_resample_kernel<float><<<total_tiles, PF_THREADS, 0, ctx->stream>>>(jobs_dev, njobs);
+  {
+    ProfScope ps(ctx, KC_SCAN);
+    if (dbl) pf_resample_kernel<double><<<total_tiles, PF_THREADS, 0, ctx->stream>>>(jobs_dev, njobs);
+    else pf_resample_kernel<float><<<total_tiles, PF_THREADS, 0, ctx->stream>>>(jobs_dev, njobs);
+  }
+  ProfScope ps(ctx, KC_FILL);
+  pf_fill_ancestors_kernel<<<total_tiles, PF_THREADS, 0, ctx->stream>>>(jobs_dev, njobs);
 }
 
 void launch_init_scalars(gf_ctx* ctx, PfJob* jobs_dev, int njobs, const double* ess1,
@@ -361,7 +365,33 @@ static void pack_lg_params(const LgFactors& f, int DXP, int DYP, std::vector<cha
   }
   for (int j = 0; j < dx; ++j)
     for (int k = 0; k < dy; ++k) v[oH + j * DYP + k] = (Real)f.Ht[k + j * dy];
-  out.resize(sizeof(Real) * tot);
+  if (sizeof(Real) == 4 && DXP >= 16) {
+    // tensor-core appendix: B = [[A, L], [H~A, H~L]] (NM x 2DXP, row-major), H~b
+    const int K = 2 * DXP, NM = ((DXP + DYP + 15) / 16) * 16;
+    std::vector<Real> B((size_t)NM * K, Real(0)), Hb(DYP, Real(0));
+    for (int n = 0; n < dx; ++n)
+      for (int k = 0; k < dx; ++k) {
+        B[(size_t)n * K + k] = (Real)f.A[n + k * dx];
+        B[(size_t)n * K + DXP + k] = (Real)f.L[n + k * dx];
+      }
+    for (int j = 0; j < dy; ++j) {
+      double hb = 0.0;
+      for (int p = 0; p < dx; ++p) hb += f.Ht[j + p * dy] * f.b[p];
+      Hb[j] = (Real)hb;
+      for (int k = 0; k < dx; ++k) {
+        double ha = 0.0, hl = 0.0;
+        for (int p = 0; p < dx; ++p) {
+          ha += f.Ht[j + p * dy] * f.A[p + k * dx];
+          hl += f.Ht[j + p * dy] * f.L[p + k * dx];
+        }
+        B[(size_t)(DXP + j) * K + k] = (Real)ha;
+        B[(size_t)(DXP + j) * K + DXP + k] = (Real)hl;
+      }
+    }
+    v.insert(v.end(), B.begin(), B.end());
+    v.insert(v.end(), Hb.begin(), Hb.end());
+  }
+  out.resize(sizeof(Real) * v.size());
   std::memcpy(out.data(), v.data(), out.size());
 }
 

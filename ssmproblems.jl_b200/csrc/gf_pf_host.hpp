@@ -16,6 +16,10 @@ struct PfLgKernels {
   void (*init)(const PfJob*, int, int, int) = nullptr;
   size_t smem = 0;
   int params_len = 0, off_mu0 = 0, off_L0 = 0;
+  // tensor-core bootstrap propagation (FP32, state dim >= 16), null if none
+  void (*prop_tc)(const PfJob*, int) = nullptr;
+  size_t tc_smem = 0;
+  int tc_nm = 0;
 };
 
 // FP64 model factors computed once per plan (column-major).

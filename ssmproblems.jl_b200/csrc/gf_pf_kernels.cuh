@@ -58,6 +58,8 @@ struct PfJob {
   double* means_out;         // nullable [T][mdim]
   const double* wraw;        // nullable: scan raw weights wraw[k] / sc->wtotal instead of exp(lw - LSE)
   double* tprefix;           // [ntiles + 1] cumulative normalised weight at each tile start
+  int32_t* ocum;             // [N] cumulative offspring counts of the pending resample
+  int32_t* tocum;            // [ntiles + 1] particle whose offspring run covers slot b * PF_TILE
   int32_t* anc;              // [N] 0-based ancestors of the pending resample
 };
 
@@ -152,33 +154,80 @@ __device__ __forceinline__ int64_t find_ancestor(const PfJob& J, PfScalars* sc, 
 //  or j + U_j (stratified), both in [j, j+1]: every j < floor(n W) - 1 counts,
 //  the two candidates at floor(n W) - 1 and floor(n W) are compared exactly.
 //  CUDAExt rule (CUDAExt.jl:55-57,74-76): O = min(n, floor(n W / W_n + u)).
-__device__ __forceinline__ int64_t offspring_count(const PfJob& J, const PfScalars* sc, int t,
-                                                   double W) {
-  const int64_t N = J.N;
-  const double dn = (double)N;
-  if (J.conv == GF_CONV_CPU) {
-    const double vs = dn * W;
-    double f = floor(vs) - 1.0;
-    int64_t g = f <= 0.0 ? 0 : (f >= dn ? N : (int64_t)f);
-    int64_t cnt = g;
-    for (int64_t j = g; j <= g + 1 && j < N; ++j) {
-      const double thr = J.resampler == GF_RS_SYSTEMATIC ? sc->u0 + (double)j
-                                                         : (double)j + slot_uniform(J, j, t);
-      if (thr < vs) cnt = j + 1;
+// The rule's inputs are copied into registers once per block.
+struct OffspringRule {
+  int64_t N;
+  double dn, u0, wn;
+  const double* unif;  // injected uniforms of this step (nullable)
+  uint64_t seed;
+  int kind, conv, t;
+  __device__ __forceinline__ double uniform(int64_t j) const {
+    return unif ? unif[j] : philox_uniform(seed, (uint32_t)j, (uint32_t)t);
+  }
+  __device__ __forceinline__ int64_t count(double W) const {
+    if (conv == GF_CONV_CPU) {
+      const double vs = dn * W;
+      const double f = floor(vs) - 1.0;
+      const int64_t g = f <= 0.0 ? 0 : (f >= dn ? N : (int64_t)f);
+      int64_t cnt = g;
+      for (int64_t j = g; j <= g + 1 && j < N; ++j) {
+        const double thr = kind == GF_RS_SYSTEMATIC ? u0 + (double)j : (double)j + uniform(j);
+        if (thr < vs) cnt = j + 1;
+      }
+      return cnt;
     }
-    return cnt;
+    const double r = (dn * W) / wn;
+    double u;
+    if (kind == GF_RS_SYSTEMATIC) {
+      u = u0;
+    } else {
+      const double kk = floor(r + 1.0);
+      const int64_t ki = kk < dn ? (kk < 1.0 ? 1 : (int64_t)kk) : N;
+      u = uniform(ki - 1);
+    }
+    const double f = floor(r + u);
+    return f < dn ? (f < 0.0 ? 0 : (int64_t)f) : N;
   }
-  const double r = (dn * W) / sc->wn;
-  double u;
-  if (J.resampler == GF_RS_SYSTEMATIC) {
-    u = sc->u0;
-  } else {
-    const double kk = floor(r + 1.0);
-    const int64_t ki = kk < dn ? (kk < 1.0 ? 1 : (int64_t)kk) : N;
-    u = slot_uniform(J, ki - 1, t);
+};
+
+__device__ __forceinline__ OffspringRule make_rule(const PfJob& J, const PfScalars* sc, int t) {
+  OffspringRule R;
+  R.N = J.N;
+  R.dn = (double)J.N;
+  R.u0 = sc->u0;
+  R.wn = sc->wn;
+  R.unif = (J.unif && J.resampler != GF_RS_SYSTEMATIC) ? J.unif + (size_t)(t - 1) * J.N : nullptr;
+  R.seed = J.seed;
+  R.kind = J.resampler;
+  R.conv = J.conv;
+  R.t = t;
+  return R;
+}
+
+
+// Block-wide exclusive scan of unsigned 64-bit values (exact, associative);
+// returns the exclusive prefix of this thread's value, *total gets the sum.
+__device__ __forceinline__ unsigned long long block_excl_scan_u64(unsigned long long v,
+                                                                  unsigned long long* sh,
+                                                                  unsigned long long* total) {
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  unsigned long long x = v;
+#pragma unroll
+  for (int o = 1; o < 32; o <<= 1) {
+    const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
+    if (lane >= o) x += y;
   }
-  const double f = floor(r + u);
-  return f < dn ? (f < 0.0 ? 0 : (int64_t)f) : N;
+  __syncthreads();
+  if (lane == 31) sh[wid] = x;
+  __syncthreads();
+  unsigned long long pre = 0ull, tot = 0ull;
+  for (int w = 0; w < nw; ++w) {
+    const unsigned long long tw = sh[w];
+    if (w < wid) pre += tw;
+    tot += tw;
+  }
+  *total = tot;
+  return pre + x - v;
 }
 
 // Per-thread online accumulation of (max, sum exp, sum exp^2) in FP64.
@@ -265,49 +314,29 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
   }
   __syncthreads();
   if (s_res) {
-    // Cumulative normalised weight at every tile start, P_{b+1} = P_b + S1_b e^{M_b - LSE}:
-    // tile masses in parallel, then each lane of warp 0 sums a contiguous run
-    // and the lane totals are chained in order, so every P is an exact running
-    // sum (monotone, deterministic).  Chunks of 32 * 32 tiles at a time.
-    __shared__ double stw[32 * 33];
-    __shared__ double s_carry;
-    if (threadIdx.x == 0) s_carry = 0.0;
-    for (int c0 = 0; c0 < J.ntiles; c0 += 32 * 32) {
-      __syncthreads();
-      for (int q = threadIdx.x; q < 32 * 32; q += blockDim.x) {
-        const int bb = c0 + q;
-        double v = 0.0;
-        if (bb < J.ntiles) {
-          const double* p = J.part + (size_t)bb * PF_PW;
-          const double mb = __ldcg(p);
-          if (mb > -INFINITY) v = __ldcg(p + 1) * exp(mb - lse);
-        }
-        stw[q + (q >> 5)] = v;
-      }
-      __syncthreads();
-      if (threadIdx.x < 32) {
-        const int lane = threadIdx.x;
-        double tot = 0.0;
-        for (int q = 0; q < 32; ++q) tot += stw[lane * 33 + q];
-        double off = s_carry;
-        for (int l = 0; l < 32; ++l) {
-          const double tl = __shfl_sync(0xffffffffu, tot, l);
-          if (l < lane) off += tl;
-        }
-        double run = 0.0;  // same serial order as `tot`, so the lane's end equals the next lane's start
-        for (int q = 0; q < 32; ++q) {
-          const int bb = c0 + lane * 32 + q;
-          if (bb < J.ntiles) J.tprefix[bb] = off + run;
-          run += stw[lane * 33 + q];
-        }
-        const double last = __shfl_sync(0xffffffffu, off + tot, 31);
-        if (lane == 0) s_carry = last;
-      }
+    // Cumulative normalised weight at every tile start, P_b = sum_{b'<b} S1_b' e^{M_b' - LSE},
+    // summed in 64-bit fixed point (2^-62 units): integer sums are exact, so the
+    // parallel scan gives the same monotone prefixes in any order.
+    __shared__ unsigned long long s_wsum[32];
+    const int per = (J.ntiles + blockDim.x - 1) / blockDim.x;
+    const int b0 = min((int)threadIdx.x * per, J.ntiles), b1 = min(b0 + per, J.ntiles);
+    unsigned long long tot = 0ull;
+    for (int bb = b0; bb < b1; ++bb) {
+      const double* p = J.part + (size_t)bb * PF_PW;
+      const double mb = __ldcg(p);
+      if (mb > -INFINITY) tot += __double2ull_rn(__ldcg(p + 1) * exp(mb - lse) * kFix);
     }
-    __syncthreads();
+    unsigned long long all = 0ull;
+    unsigned long long run = block_excl_scan_u64(tot, s_wsum, &all);
+    for (int bb = b0; bb < b1; ++bb) {
+      J.tprefix[bb] = (double)run * kInvFix;
+      const double* p = J.part + (size_t)bb * PF_PW;
+      const double mb = __ldcg(p);
+      if (mb > -INFINITY) run += __double2ull_rn(__ldcg(p + 1) * exp(mb - lse) * kFix);
+    }
     if (threadIdx.x == 0) {
-      J.tprefix[J.ntiles] = s_carry;
-      sc->wn = s_carry;
+      J.tprefix[J.ntiles] = (double)all * kInvFix;
+      sc->wn = (double)all * kInvFix;
     }
   }
   __syncthreads();
@@ -323,11 +352,10 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
 // ---------------------------------------------------------- resample kernel
 // Runs after a propagate whose finalise decided to resample: per propagate
 // tile, the cumulative normalised weights W_k = P_b + (running sum inside the
-// tile), then each particle's offspring slot range [O(W_{k-1}), O(W_k)) gets
-// ancestor k (the cumulative-offspring form of CUDAExt.jl:90-117, with the
-// counts computed exactly per rule).  Multinomial ancestors (unsorted
-// uniforms) instead take W_k to the per-slot search of the next propagate.
-constexpr int RS_LONG = 32;  // offspring runs longer than this are filled by the whole block
+// tile) and each particle's cumulative offspring count O(W_k) (exact per
+// rule); the next propagate turns the counts into ancestors (tile_ancestors).
+// Multinomial ancestors (unsorted uniforms) instead take W_k to the per-slot
+// search of the next propagate.
 template <typename Real>
 __global__ void __launch_bounds__(PF_THREADS) pf_resample_kernel(const PfJob* __restrict__ jobs,
                                                                 int njobs) {
@@ -335,11 +363,10 @@ __global__ void __launch_bounds__(PF_THREADS) pf_resample_kernel(const PfJob* __
   const PfJob& J = jobs[jb];
   PfScalars* sc = J.sc;
   if (!sc->resample || sc->status != 0 || sc->t >= J.T) return;
-  __shared__ double sw[PF_TILE + PF_TILE / 32];  // index l + l/32 (conflict-free lane runs)
-  __shared__ int32_t sO[PF_TILE];
-  __shared__ int32_t sq[PF_TILE][3];
-  __shared__ int s_qn;
-  __shared__ int32_t s_O0;
+  // shared layouts padded one slot per 4 (thread-contiguous runs of 4 with few bank conflicts)
+  __shared__ unsigned long long sq64[PF_TILE + PF_TILE / 4];
+  __shared__ double sw[PF_TILE + PF_TILE / 4];
+  __shared__ unsigned long long s_wsum[32];
   const int tstep = sc->t + 1;
   const int tile = blockIdx.x - J.tile0;
   const int64_t N = J.N, i0 = (int64_t)tile * PF_TILE;
@@ -350,64 +377,131 @@ __global__ void __launch_bounds__(PF_THREADS) pf_resample_kernel(const PfJob* __
 #pragma unroll
   for (int p = 0; p < PF_PPT; ++p) {
     const int l = p * PF_THREADS + threadIdx.x;
-    sw[l + (l >> 5)] = l < nloc ? exp((double)lw[i0 + l] - lse) : 0.0;
+    sq64[l + (l >> 2)] = l < nloc ? __double2ull_rn(exp((double)lw[i0 + l] - lse) * kFix) : 0ull;
   }
-  if (threadIdx.x == 0) s_qn = 0;
   __syncthreads();
-  if (threadIdx.x < 32) {
-    // 32 lanes x 32 contiguous particles: lane-serial sums chained by lane
-    // order, so W is an exact running sum, then clamped to the tile's end value.
-    const int lane = threadIdx.x;
-    constexpr int PER = PF_TILE / 32;
-    double tot = 0.0;
-#pragma unroll 8
-    for (int q = 0; q < PER; ++q) tot += sw[lane * (PER + 1) + q];
-    double off = P0;
-    for (int l = 0; l < 32; ++l) {
-      const double tl = __shfl_sync(0xffffffffu, tot, l);
-      if (l < lane) off += tl;
+  {
+    // W_k = P0 + (fixed-point running sum inside the tile), clamped to the tile's end
+    const int l0 = PF_PPT * threadIdx.x;
+    unsigned long long loc[PF_PPT], acc = 0ull;
+#pragma unroll
+    for (int q = 0; q < PF_PPT; ++q) {
+      const int l = l0 + q;
+      acc += sq64[l + (l >> 2)];
+      loc[q] = acc;
     }
-    double run = 0.0;
-    for (int q = 0; q < PER; ++q) {
-      const int l = lane * PER + q;
-      run += sw[l + lane];
-      double W = off + run;
+    unsigned long long all;
+    const unsigned long long excl = block_excl_scan_u64(acc, s_wsum, &all);
+#pragma unroll
+    for (int q = 0; q < PF_PPT; ++q) {
+      const int l = l0 + q;
+      double W = P0 + (double)(excl + loc[q]) * kInvFix;
       W = W < P1 ? W : P1;
       if (l == nloc - 1) W = P1;
-      sw[l + lane] = W;
+      sw[l + (l >> 2)] = W;
     }
   }
   __syncthreads();
   if (J.resampler == GF_RS_MULTINOMIAL) {
-    for (int l = threadIdx.x; l < nloc; l += PF_THREADS) J.key[i0 + l] = sw[l + (l >> 5)];
+    double* __restrict__ key = J.key;
+    for (int l = threadIdx.x; l < nloc; l += PF_THREADS) key[i0 + l] = sw[l + (l >> 2)];
     return;
   }
-  for (int l = threadIdx.x; l < nloc; l += PF_THREADS)
-    sO[l] = (int32_t)offspring_count(J, sc, tstep, sw[l + (l >> 5)]);
-  if (threadIdx.x == 0) s_O0 = (int32_t)offspring_count(J, sc, tstep, P0);
+  const OffspringRule rule = make_rule(J, sc, tstep);
+  int32_t* __restrict__ ocum = J.ocum;
+  int32_t* __restrict__ sOc = reinterpret_cast<int32_t*>(sq64);  // counts, reusing the scan buffer
   __syncthreads();
   for (int l = threadIdx.x; l < nloc; l += PF_THREADS) {
-    const int32_t lo = l == 0 ? s_O0 : sO[l - 1], hi = sO[l];
-    if (hi - lo > RS_LONG) {
-      const int q = atomicAdd(&s_qn, 1);
-      sq[q][0] = l;
-      sq[q][1] = lo;
-      sq[q][2] = hi;
-    } else {
-      for (int32_t j = lo; j < hi; ++j) J.anc[j] = (int32_t)(i0 + l);
+    int32_t c = (int32_t)rule.count(sw[l + (l >> 2)]);
+    if (i0 + l == N - 1) {
+      // slots past the last threshold below W_N (rounding) go to the last
+      // particle; the reference's walk has no clamp, so they are counted
+      if (c < N) atomicAdd(&sc->clamps, (int32_t)(N - c));
+      c = (int32_t)N;
+    }
+    sOc[l] = c;
+    ocum[i0 + l] = c;
+  }
+  __shared__ int32_t s_O0;
+  if (threadIdx.x == 0) s_O0 = (int32_t)rule.count(P0);
+  __syncthreads();
+  // the particle whose slot run [O_{k-1}, O_k) covers a chunk start c * PF_TILE
+  for (int l = threadIdx.x; l < nloc; l += PF_THREADS) {
+    const int32_t lo = l == 0 ? s_O0 : sOc[l - 1], hi = sOc[l];
+    for (int64_t c0 = ((int64_t)lo + PF_TILE - 1) / PF_TILE * PF_TILE; c0 < hi; c0 += PF_TILE)
+      J.tocum[c0 / PF_TILE] = (int32_t)(i0 + l);
+  }
+}
+
+// Ancestors (0-based) of the block's PF_TILE slots from the cumulative
+// offspring counts: slot j's ancestor is the first k with ocum[k] > j (the
+// cumulative-offspring form of CUDAExt.jl:90-103).  The particles covering the
+// block's first slot and the next block's first slot bound the search; the
+// range is staged in shared memory when it is short, and every slot then
+// binary-searches it -- balanced however the offspring are distributed.
+constexpr int ANC_STAGE = 4096;
+static __device__ void tile_ancestors(const PfJob& J, int tile, int32_t* s_anc, int32_t* s_oc);
+
+// Fill kernel: per block of PF_TILE slots, ancestors from the cumulative counts
+// (tile_ancestors) written to J.anc, which the next propagate reads coalesced.
+template <int DUMMY = 0>
+__global__ void __launch_bounds__(PF_THREADS) pf_fill_ancestors_kernel(const PfJob* __restrict__ jobs,
+                                                                      int njobs) {
+  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const PfJob& J = jobs[jb];
+  const PfScalars* sc = J.sc;
+  if (!sc->resample || sc->status != 0 || sc->t >= J.T || J.resampler == GF_RS_MULTINOMIAL) return;
+  __shared__ int32_t s_anc[PF_TILE];
+  __shared__ int32_t s_oc[ANC_STAGE];
+  const int tile = blockIdx.x - J.tile0;
+  tile_ancestors(J, tile, s_anc, s_oc);
+  const int64_t i0 = (int64_t)tile * PF_TILE;
+  const int nloc = (int)min((int64_t)PF_TILE, J.N - i0);
+  int32_t* __restrict__ anc = J.anc;
+  for (int l = threadIdx.x; l < nloc; l += PF_THREADS) anc[i0 + l] = s_anc[l];
+}
+
+static __device__ void tile_ancestors(const PfJob& J, int tile, int32_t* s_anc, int32_t* s_oc) {
+  __shared__ int64_t s_k[2];
+  const int64_t N = J.N;
+  const int64_t j0 = (int64_t)tile * PF_TILE;
+  const int64_t jl = min(j0 + PF_TILE, N) - 1;
+  const int32_t* __restrict__ oc = J.ocum;
+  if (threadIdx.x == 0) {
+    s_k[0] = J.tocum[tile];
+    s_k[1] = tile + 1 < J.ntiles ? (int64_t)J.tocum[tile + 1] : N - 1;
+  }
+  __syncthreads();
+  const int64_t kf = s_k[0], kl = s_k[1];
+  const int64_t R = kl - kf + 1;
+  if (R <= ANC_STAGE) {
+    for (int q = threadIdx.x; q < (int)R; q += blockDim.x) s_oc[q] = oc[kf + q];
+    __syncthreads();
+    for (int l = threadIdx.x; l < PF_TILE; l += blockDim.x) {
+      const int64_t j = j0 + l;
+      if (j > jl) break;
+      int lo = 0, hi = (int)R - 1;
+      while (lo < hi) {
+        const int mid = (lo + hi) >> 1;
+        if (s_oc[mid] > j) hi = mid;
+        else lo = mid + 1;
+      }
+      s_anc[l] = (int32_t)(kf + lo);
+    }
+  } else {
+    for (int l = threadIdx.x; l < PF_TILE; l += blockDim.x) {
+      const int64_t j = j0 + l;
+      if (j > jl) break;
+      int64_t lo = kf, hi = kl;
+      while (lo < hi) {
+        const int64_t mid = (lo + hi) >> 1;
+        if (oc[mid] > j) hi = mid;
+        else lo = mid + 1;
+      }
+      s_anc[l] = (int32_t)lo;
     }
   }
   __syncthreads();
-  for (int q = 0; q < s_qn; ++q) {
-    const int32_t k = (int32_t)(i0 + sq[q][0]);
-    for (int32_t j = sq[q][1] + threadIdx.x; j < sq[q][2]; j += PF_THREADS) J.anc[j] = k;
-  }
-  if (i0 + nloc == N && threadIdx.x == 0) {
-    // slots beyond the last threshold below W_N (rounding): last particle, counted
-    const int32_t last = sO[nloc - 1];
-    if (last < N) atomicAdd(&sc->clamps, (int32_t)(N - last));
-    for (int64_t j = last; j < N; ++j) J.anc[j] = (int32_t)(N - 1);
-  }
 }
 
 // ------------------------------------------------------------ lookback scan

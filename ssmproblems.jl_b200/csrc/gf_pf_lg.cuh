@@ -8,8 +8,10 @@
 // -1/2 |L_R^{-1}(y - c) - (L_R^{-1}H) x|^2 + const, the same quantity as
 // logpdf(MvNormal(Hx + c, R), y) (models/linear_gaussian.jl:85-90).
 #pragma once
+#include <type_traits>
 #include "gf_pf_host.hpp"
 #include "gf_pf_kernels.cuh"
+#include "gf_umma.cuh"
 
 namespace gf {
 
@@ -86,13 +88,18 @@ __global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __
   Real* Xd = reinterpret_cast<Real*>(J.X[t & 1]);
   Real* lw = reinterpret_cast<Real*>(J.lw);
   const Real* noise = J.noise ? reinterpret_cast<const Real*>(J.noise) + (size_t)t * dx * N : nullptr;
+  const int32_t* __restrict__ ancv = J.anc;
+  int32_t* __restrict__ anc_out = J.anc_out;
+  const uint64_t seed = J.seed;
+  const bool diag = J.diag_l != 0;
+  const double obs_const = J.obs_const, prop_const = J.prop_const;
   LseAcc acc;
 
   for (int p = 0; p < PF_PPT; ++p) {
     const int64_t i = (int64_t)tile * PF_TILE + p * PF_THREADS + threadIdx.x;
     if (i >= N) break;
     int64_t a = i;
-    if (resamp) a = searched ? find_ancestor(J, sc, t, i, 0, N) : (int64_t)J.anc[i];
+    if (resamp) a = searched ? find_ancestor(J, sc, t, i, 0, N) : (int64_t)ancv[i];
     Real x[DXP];
 #pragma unroll
     for (int d = 0; d < DXP; ++d) x[d] = d < dx ? Xs[(size_t)d * N + a] : Real(0);
@@ -132,7 +139,7 @@ __global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __
           e4[cc] = (c < DXP && c < dx) ? noise[(size_t)c * N + i] : Real(0);
         }
       } else {
-        philox_normals4<Real>(J.seed, (uint32_t)i, (uint32_t)t, (uint32_t)q, e4);
+        philox_normals4<Real>(seed, (uint32_t)i, (uint32_t)t, (uint32_t)q, e4);
       }
 #pragma unroll
       for (int cc = 0; cc < 4; ++cc) {
@@ -140,7 +147,7 @@ __global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __
         if (c < DXP) {
           const Real ec = e4[cc];
           if constexpr (GUIDED) qe = fma(ec, ec, qe);
-          if (J.diag_l) {
+          if (diag) {
             xn[c] = fma(sL[c * DXP + c], ec, xn[c]);
           } else {
 #pragma unroll
@@ -162,7 +169,7 @@ __global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __
         for (int c = 0; c <= r; ++c) z = fma(sQi[c * DXP + r], ma[c], z);
         qz = fma(z, z, qz);
       }
-      inc = -0.5 * (double)qz + 0.5 * (double)qe + J.prop_const;
+      inc = -0.5 * (double)qz + 0.5 * (double)qe + prop_const;
     }
     // observation: -1/2 |ytil - Ht x'|^2 + const
     Real q = 0;
@@ -173,13 +180,13 @@ __global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __
       for (int c = 0; c < DXP; ++c) r = fma(-sH[c * DYP + k], xn[c], r);
       q = fma(r, r, q);
     }
-    const double lout = lin + inc + (J.obs_const - 0.5 * (double)q);
+    const double lout = lin + inc + (obs_const - 0.5 * (double)q);
     const Real lst = (Real)lout;
     lw[i] = lst;
 #pragma unroll
     for (int d = 0; d < DXP; ++d)
       if (d < dx) Xd[(size_t)d * N + i] = xn[d];
-    if (J.anc_out) J.anc_out[(size_t)(t - 1) * N + i] = (int32_t)(a + 1);
+    if (anc_out) anc_out[(size_t)(t - 1) * N + i] = (int32_t)(a + 1);
     acc.add((double)lst);
   }
   block_finish(J, tile, t, fresh, acc, red);
@@ -220,6 +227,184 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_init(const PfJob* __restrict
   }
 }
 
+
+// ------------------------------------------------- tensor-core propagation
+// Bootstrap propagation + observation for state dimension >= 16 on the tcgen05
+// tensor cores.  Per 128-particle sub-tile, one MMA chain computes
+//   [x' - b | H~x' - H~b] = [x | e] * [[A, L], [H~A, H~L]]^T
+// in kind::tf32 with the 3xTF32 split (A_hi B_hi + A_hi B_lo + A_lo B_hi), so
+// the result carries FP32-level accuracy; the FP32 accumulator lives in TMEM
+// (one lane per particle) and is read back for the weight and the state store.
+constexpr int TC_THREADS = 128;
+constexpr int TC_SUB = PF_TILE / TC_THREADS;
+constexpr uint32_t TC_WAIT = 1u << 22;  // bounded mbarrier polls
+
+template <int DXP, int DYP>
+struct TcLayout {
+  static constexpr int K = 2 * DXP;
+  static constexpr int NM = ((DXP + DYP + 15) / 16) * 16;
+  static constexpr uint32_t NCOLS = NM <= 32 ? 32 : (NM <= 64 ? 64 : 128);
+  // params appendix (float): B [NM][K] row-major, H~b [DYP]
+  static constexpr int B_off = LgLayout<DXP, DYP>::total;
+  static constexpr int Hb_off = B_off + NM * K;
+  static constexpr int total = Hb_off + DYP;
+  static constexpr size_t smem_bytes = sizeof(float) * (2 * 128 * K + 2 * NM * K + DXP + 2 * DYP);
+};
+
+template <int DXP, int DYP>
+__global__ void __launch_bounds__(TC_THREADS) pf_lg_propagate_tc(const PfJob* __restrict__ jobs,
+                                                               int njobs) {
+  using Lay = LgLayout<DXP, DYP>;
+  using TL = TcLayout<DXP, DYP>;
+  constexpr int K = TL::K, NM = TL::NM;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float* sAh = reinterpret_cast<float*>(smraw);
+  float* sAl = sAh + 128 * K;
+  float* sBh = sAl + 128 * K;
+  float* sBl = sBh + NM * K;
+  float* sb = sBl + NM * K;
+  float* sHb = sb + DXP;
+  float* sy = sHb + DYP;
+  __shared__ double red[32];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+
+  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const PfJob& J = jobs[jb];
+  PfScalars* sc = J.sc;
+  const int t = sc->t + 1;
+  if (t > J.T || sc->status != 0) return;
+  const int tile = blockIdx.x - J.tile0;
+  const int tid = threadIdx.x;
+  const bool resamp = sc->resample != 0;
+  const bool fresh = resamp || sc->uniform != 0;
+  const double lse_prev = sc->lse;
+  const bool searched = J.resampler == GF_RS_MULTINOMIAL;
+
+  const float* P = reinterpret_cast<const float*>(J.params);
+  for (int e = tid; e < NM * K; e += TC_THREADS) {
+    const int n = e / K, k = e - n * K;
+    const float v = P[TL::B_off + e];
+    const float h = umma::to_tf32(v);
+    const uint32_t off = umma::kmajor_offset(n, k, K) >> 2;
+    sBh[off] = h;
+    sBl[off] = umma::to_tf32(v - h);
+  }
+  for (int e = tid; e < DXP; e += TC_THREADS) sb[e] = P[Lay::b + e];
+  const float* Y = reinterpret_cast<const float*>(J.ystep) + (size_t)(t - 1) * J.ystride;
+  for (int e = tid; e < DYP; e += TC_THREADS) {
+    sHb[e] = P[TL::Hb_off + e];
+    sy[e] = Y[e];
+  }
+  if (tid == 0) {
+    umma::mbar_init(&mbar, 1);
+    umma::fence_mbar_init();
+  }
+  if (tid < 32) umma::tmem_alloc(&tmem_slot, TL::NCOLS);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tbase = tmem_slot;
+  const uint32_t tlane = tbase + ((uint32_t)(32 * (tid >> 5)) << 16);
+
+  const int64_t N = J.N;
+  const int dx = J.dx;
+  const float* Xs = reinterpret_cast<const float*>(J.X[(t - 1) & 1]);
+  float* Xd = reinterpret_cast<float*>(J.X[t & 1]);
+  float* lw = reinterpret_cast<float*>(J.lw);
+  const float* noise = J.noise ? reinterpret_cast<const float*>(J.noise) + (size_t)t * dx * N : nullptr;
+  const int32_t* __restrict__ ancv = J.anc;
+  int32_t* __restrict__ anc_out = J.anc_out;
+  const uint64_t seed = J.seed;
+  const double obs_const = J.obs_const;
+  const uint32_t idesc = umma::idesc_tf32(128, NM);
+  const uint32_t kstride = 128, mstride = (uint32_t)(K / 4) * 128;
+  LseAcc acc;
+  bool ok = true;
+
+  for (int s = 0; s < TC_SUB; ++s) {
+    const int64_t i = (int64_t)tile * PF_TILE + s * TC_THREADS + tid;
+    const bool valid = i < N;
+    int64_t a = i;
+    if (valid && resamp) a = searched ? find_ancestor(J, sc, t, i, 0, N) : (int64_t)ancv[i];
+    float xe[K];
+#pragma unroll
+    for (int d = 0; d < DXP; ++d) xe[d] = (valid && d < dx) ? Xs[(size_t)d * N + a] : 0.f;
+#pragma unroll
+    for (int q = 0; q < DXP / 4; ++q) {
+      float e4[4];
+      if (noise) {
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+          const int c = 4 * q + cc;
+          e4[cc] = (valid && c < dx) ? noise[(size_t)c * N + i] : 0.f;
+        }
+      } else {
+        philox_normals4<float>(seed, (uint32_t)i, (uint32_t)t, (uint32_t)q, e4);
+      }
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) xe[DXP + 4 * q + cc] = e4[cc];
+    }
+    const double lin = (fresh || !valid) ? 0.0 : (double)lw[i] - lse_prev;
+    // this particle's row of the A operand, split hi / lo, 16-byte chunks
+#pragma unroll
+    for (int k4 = 0; k4 < K / 4; ++k4) {
+      float4 h, l;
+      umma::split_tf32(xe[4 * k4 + 0], h.x, l.x);
+      umma::split_tf32(xe[4 * k4 + 1], h.y, l.y);
+      umma::split_tf32(xe[4 * k4 + 2], h.z, l.z);
+      umma::split_tf32(xe[4 * k4 + 3], h.w, l.w);
+      const uint32_t off = umma::kmajor_offset(tid, 4 * k4, K) >> 2;
+      *reinterpret_cast<float4*>(sAh + off) = h;
+      *reinterpret_cast<float4*>(sAl + off) = l;
+    }
+    umma::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+#pragma unroll
+      for (int ks = 0; ks < K / 8; ++ks) {
+        const uint32_t koff = (uint32_t)ks * 2 * kstride;
+        const uint64_t ah = umma::desc(umma::smem_u32(sAh) + koff, kstride, mstride);
+        const uint64_t al = umma::desc(umma::smem_u32(sAl) + koff, kstride, mstride);
+        const uint64_t bh = umma::desc(umma::smem_u32(sBh) + koff, kstride, mstride);
+        const uint64_t bl = umma::desc(umma::smem_u32(sBl) + koff, kstride, mstride);
+        umma::mma_tf32(tbase, ah, bh, idesc, ks > 0 ? 1u : 0u);
+        umma::mma_tf32(tbase, ah, bl, idesc, 1u);
+        umma::mma_tf32(tbase, al, bh, idesc, 1u);
+      }
+      umma::mma_commit(&mbar);
+    }
+    ok = umma::mbar_wait(&mbar, (uint32_t)(s & 1), TC_WAIT) && ok;
+    umma::fence_after_sync();
+    float accv[NM];
+#pragma unroll
+    for (int c = 0; c < NM; c += 16) umma::tmem_ld16(tlane + (uint32_t)c, accv + c);
+    umma::tmem_wait_ld();
+    if (valid) {
+      float q = 0.f;
+#pragma unroll
+      for (int k = 0; k < DYP; ++k) {
+        const float r = sy[k] - accv[DXP + k] - sHb[k];
+        q = fmaf(r, r, q);
+      }
+      const double lout = lin + (obs_const - 0.5 * (double)q);
+      const float lst = (float)lout;
+      lw[i] = lst;
+#pragma unroll
+      for (int d = 0; d < DXP; ++d)
+        if (d < dx) Xd[(size_t)d * N + i] = accv[d] + sb[d];
+      if (anc_out) anc_out[(size_t)(t - 1) * N + i] = (int32_t)(a + 1);
+      acc.add((double)lst);
+    }
+    umma::fence_before_sync();
+    __syncthreads();
+  }
+  if (!ok && tid == 0) sc->status = GF_ERR_TIMEOUT;
+  if (tid < 32) umma::tmem_dealloc(tbase, TL::NCOLS);
+  block_finish(J, tile, t, fresh, acc, red);
+}
+
 template <typename Real, int DXP, int DYP, bool G>
 PfLgKernels make_lg() {
   PfLgKernels k;
@@ -231,6 +416,11 @@ PfLgKernels make_lg() {
   k.params_len = LgLayout<DXP, DYP>::total;
   k.off_mu0 = LgLayout<DXP, DYP>::mu0;
   k.off_L0 = LgLayout<DXP, DYP>::L0;
+  if constexpr (std::is_same<Real, float>::value && !G && DXP >= 16) {
+    k.prop_tc = pf_lg_propagate_tc<DXP, DYP>;
+    k.tc_smem = TcLayout<DXP, DYP>::smem_bytes;
+    k.tc_nm = TcLayout<DXP, DYP>::NM;
+  }
   return k;
 }
 

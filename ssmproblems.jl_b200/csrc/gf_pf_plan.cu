@@ -25,12 +25,15 @@ struct gf_pf_plan {
   void *params = nullptr, *ystep = nullptr, *X0 = nullptr, *X1 = nullptr, *lw = nullptr;
   double *pp = nullptr, *key = nullptr, *part = nullptr, *mpart = nullptr, *ess1 = nullptr;
   double* tprefix = nullptr;
-  int32_t* anc = nullptr;
+  int32_t *ocum = nullptr, *tocum = nullptr, *anc = nullptr;
   unsigned long long* flags = nullptr;
   PfScalars* sc = nullptr;
   int8_t *sched_dev = nullptr, *res1 = nullptr;
   PfJob* job_dev = nullptr;
   PfJob job{};
+  void (*prop_fn)(const PfJob*, int) = nullptr;  // chosen propagate kernel
+  int prop_threads = 0;
+  size_t prop_smem = 0;
   cudaGraphExec_t graph = nullptr;
   bool graph_means = false;
   bool use_graph = true;
@@ -111,6 +114,8 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   ALLOC(X1, p->rsize * (size_t)N * m->dx);
   ALLOC(lw, p->rsize * (size_t)N);
   ALLOC(key, sizeof(double) * (size_t)N);
+  ALLOC(ocum, sizeof(int32_t) * (size_t)N);
+  ALLOC(tocum, sizeof(int32_t) * (size_t)(p->ntiles + 1));
   ALLOC(anc, sizeof(int32_t) * (size_t)N);
   ALLOC(tprefix, sizeof(double) * (size_t)(p->ntiles + 1));
   ALLOC(part, sizeof(double) * PF_PW * (size_t)p->ntiles);
@@ -134,9 +139,17 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->ess1, &ess1, sizeof(double), cudaMemcpyHostToDevice, s));
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->res1, &res1, 1, cudaMemcpyHostToDevice, s));
   GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
-  if (p->k.smem > 48 * 1024)
-    GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)p->k.prop,
-                                            cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->k.smem));
+  if (p->k.prop_tc && !(flags & GF_PLAN_SIMT)) {
+    p->prop_fn = p->k.prop_tc;
+    p->prop_threads = 128;
+    p->prop_smem = p->k.tc_smem;
+  } else {
+    p->prop_fn = p->k.prop;
+    p->prop_threads = PF_THREADS;
+    p->prop_smem = p->k.smem;
+  }
+  GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)p->prop_fn,
+                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->prop_smem));
 
   PfJob& J = p->job;
   std::memset(&J, 0, sizeof J);
@@ -174,6 +187,8 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   J.part = p->part;
   J.flags = p->flags;
   J.sc = p->sc;
+  J.ocum = p->ocum;
+  J.tocum = p->tocum;
   J.anc = p->anc;
   J.tprefix = p->tprefix;
   J.schedule = p->sched_dev;
@@ -196,7 +211,7 @@ static void enqueue_run(gf_pf_plan* p, bool means) {
   for (int t = 1; t <= p->T; ++t) {
     {
       ProfScope ps(ctx, KC_PROPAGATE);
-      p->k.prop<<<p->ntiles, PF_THREADS, p->k.smem, s>>>(p->job_dev, 1);
+      p->prop_fn<<<p->ntiles, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
     }
     if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);
     if (t < p->T) launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);

@@ -44,6 +44,14 @@ __device__ __forceinline__ float to_tf32(float x) {
   asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(x));
   return __uint_as_float(r);
 }
+// Split x into hi + lo for the 3xTF32 product: hi is x rounded to the 10-bit
+// TF32 mantissa by integer rounding of the magnitude (finite inputs), lo = x -
+// hi is exact in FP32 and the tensor core keeps its leading 10 mantissa bits,
+// leaving an error below 2^-21 |x|.
+__device__ __forceinline__ void split_tf32(float x, float& hi, float& lo) {
+  hi = __uint_as_float((__float_as_uint(x) + 0x1000u) & 0xFFFFE000u);
+  lo = x - hi;
+}
 
 // ---- TMEM allocation (whole warp) -----------------------------------------
 __device__ __forceinline__ void tmem_alloc(uint32_t* smem_dst, uint32_t ncols) {

@@ -22,7 +22,7 @@ GF_CONV_CPU, GF_CONV_CUDAEXT = 0, 1
 GF_PREC_F32, GF_PREC_F64 = 0, 1
 GF_PROP_BOOTSTRAP, GF_PROP_OPTIMAL, GF_PROP_OVERDISPERSED = 0, 1, 2
 GF_ALGO_KF, GF_ALGO_SRKF = 0, 1
-GF_PLAN_AUTOTUNE, GF_PLAN_NO_GRAPH, GF_PLAN_PLAIN = 1, 2, 4
+GF_PLAN_AUTOTUNE, GF_PLAN_NO_GRAPH, GF_PLAN_PLAIN, GF_PLAN_SIMT = 1, 2, 4, 8
 
 EXPORTED = [
     "gf_ctx_create", "gf_ctx_destroy", "gf_last_error", "gf_ctx_set_stream", "gf_ctx_get_stream",

@@ -200,3 +200,33 @@ def test_large_pf_converges_to_kf_ll(ctx):
     sd = lls.std(ddof=1)
     assert sd < 5.0
     assert abs(np.median(lls) - llkf) < 2.0 + 3 * sd
+
+
+@pytest.mark.parametrize("dims", [(16, 8), (32, 16), (20, 5)])
+def test_tensor_core_path_matches_simt(ctx, dims):
+    """The tcgen05 propagation (3xTF32) and the CUDA-core propagation agree to FP32
+    accuracy on the same injected noise (no resampling, so particles stay aligned)."""
+    import torch
+    from gfb200.plans import PfPlan
+    dx, dy = dims
+    m, ys = W.lgssm_rot(seed=dx, dx=dx, dy=dy, T=4)
+    N, T = 5000, 4
+    rng = np.random.default_rng(3)
+    noise = torch.tensor(rng.standard_normal((T + 1, dx, N)).astype(np.float32), device="cuda:0")
+    ysd = torch.tensor(ys, device="cuda:0")
+    algo = G.BF(N, resampler=G.AlternatingResampler())
+    out = {}
+    for simt in (False, True):
+        plan = PfPlan(m, algo, T, ctx=ctx, graph=False, simt=simt)
+        plan._cfg.schedule = None
+        states = torch.zeros((dx, N), dtype=torch.float32, device="cuda:0")
+        lw = torch.zeros(N, dtype=torch.float64, device="cuda:0")
+        plan.run(ysd, noise_dev=noise, unif_dev=torch.zeros(T, dtype=torch.float64, device="cuda:0"),
+                 states=states, log_weights=lw)
+        ctx.synchronize()
+        out[simt] = (states.cpu().numpy(), lw.cpu().numpy(), plan.ll_steps.cpu().numpy())
+        plan.close()
+    (s0, w0, l0), (s1, w1, l1) = out[False], out[True]
+    np.testing.assert_allclose(s0, s1, rtol=2e-5, atol=2e-5)
+    np.testing.assert_allclose(w0, w1, rtol=1e-5, atol=2e-4)
+    np.testing.assert_allclose(l0, l1, rtol=1e-6, atol=1e-5)
