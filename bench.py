@@ -160,7 +160,6 @@ def bench_pf(args, world, rank, local):
     ctx.profile(True)
     _barrier(world)
     torch.cuda.synchronize()
-    s = torch.cuda.Stream(device=dev)  # events on the library's stream
     stream_ptr = ctx.stream
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
@@ -177,6 +176,7 @@ def bench_pf(args, world, rank, local):
     prop_ms, prop_n = ctx.profile_read(0)
     scan_ms, scan_n = ctx.profile_read(1)
     prep_ms, prep_n = ctx.profile_read(4)
+    fill_ms, fill_n = ctx.profile_read(5)
     ctx.profile(False)
     ms_max = _max_over_ranks(ms, world, dev)
     n_res = int(plan.resampled.sum().item())
@@ -247,19 +247,102 @@ def bench_pf(args, world, rank, local):
         "e2e": {"value": units / e2e_s, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": int(ys.nbytes), "d2h_bytes_per_step": int(8 + 8 * T),
                 "call": "gf_pf_run(GF_MEM_HOST) from pinned host buffers"},
-        "gpu_launches": int(prop_n + scan_n + prep_n + 3 * args.steps),
+        "gpu_launches": int(prop_n + scan_n + fill_n + prep_n + 3 * args.steps),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
                      "kernel": "pf_lg_propagate<float,16,8>", "peak_source": peak_kind,
                      "avg_launch_ms": prop_avg_ms, "launches": prop_n,
                      "bytes_per_launch": bytes_total / launches},
-        "kernels_ms": {"propagate": prop_ms, "scan": scan_ms, "prep_init": prep_ms},
+        "kernels_ms": {"propagate": prop_ms, "resample": scan_ms, "ancestor_fill": fill_ms,
+                       "prep_init": prep_ms},
         "graph_ms_per_step": graph_ms,
         "clocks": clk.summary(),
     }
     plan.close()
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_pf(model, ys, N, seconds=args.cpu_seconds)
+    ctx.close()
+    return line
+
+
+def bench_kf(args, world, rank, local):
+    """Batched Kalman filters: 65536 uneven LGSSMs (Dx 2..32, Dy 1..Dx, T 64..2048),
+    per-step ll / mean / covariance outputs, one graph-captured persistent plan
+    with autotuned block sizes; the plain one-launch-per-filter form is timed on a
+    sample for comparison."""
+    import torch
+    import gfb200 as G
+    from gfb200 import _lib as L
+    from gfb200 import workloads as W
+    from gfb200.plans import KfPlan
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    ctx = G.Context(local)
+    B = args.kf_filters
+    algo = G.SRKF() if args.kf_algo == "srkf" else G.KalmanFilter()
+    models, Ts, _ = W.kf_bank(B, seed=7 + rank, make_ys=False)
+    plan = KfPlan(models, algo, Ts, ctx=ctx, flags=L.GF_PLAN_AUTOTUNE)
+    ys = torch.randn(plan.n_y, dtype=torch.float64, device=dev)
+    steps = torch.empty(plan.n_steps, dtype=torch.float64, device=dev)
+    means = torch.empty(plan.n_means, dtype=torch.float32, device=dev)
+    covs = torch.empty(plan.n_covs, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        plan.run(ys, steps, means, covs)
+    ctx.synchronize()
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    _barrier(world)
+    with ClockSampler(local) as clk:
+        e0.record(ext)
+        for _ in range(args.steps):
+            plan.run(ys, steps, means, covs)
+        e1.record(ext)
+        e1.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1), world, dev)
+    assert int(plan.status.abs().sum().item()) == 0
+    n_steps = plan.n_steps
+    value = n_steps * args.steps * world / (ms / 1e3)
+    dxs = np.array([m.dx for m in models], dtype=np.float64)
+    dys = np.array([m.dy for m in models], dtype=np.float64)
+    Tarr = np.array(Ts, dtype=np.float64)
+    bytes_run = float(np.sum(Tarr * (8 * dys + 8 + 4 * dxs + 4 * dxs * dxs)))
+    flops_run = float(np.sum(Tarr * 2 * (4 * dxs**3 + 4 * dys * dxs**2 + 4 * dys**2 * dxs + dys**3 / 3)))
+    run_s = ms / 1e3 / args.steps
+    peak, peak_kind = _peaks()
+    # plain form: one launch per filter on a sample, extrapolated per KF step
+    sample = min(256, B)
+    idx = np.random.default_rng(0).choice(B, sample, replace=False)
+    pm = [models[i] for i in idx]
+    pT = [Ts[i] for i in idx]
+    pplan = KfPlan(pm, algo, pT, ctx=ctx, flags=L.GF_PLAN_PLAIN | L.GF_PLAN_NO_GRAPH)
+    pys = torch.randn(pplan.n_y, dtype=torch.float64, device=dev)
+    pplan.run(pys)
+    ctx.synchronize()
+    p0, p1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    p0.record(ext)
+    pplan.run(pys)
+    p1.record(ext)
+    p1.synchronize()
+    plain_value = pplan.n_steps / (p0.elapsed_time(p1) / 1e3)
+    pplan.close()
+    line = {
+        "metric": "KF-steps/s", "value": value, "unit": "KF-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"{B} uneven LGSSMs, Dx~U{{2..32}}, Dy~U{{1..Dx}}, T~U{{64..2048}}, "
+                               f"{'SRKF' if args.kf_algo == 'srkf' else 'KF'} with per-step ll/mean/cov",
+                   "filters": B, "kf_steps": n_steps, "form": "one graph of persistent per-bucket launches, autotuned",
+                   "l2": "outputs ~100 GB per run > L2 (no flush)"},
+        "roofline": {"bound": "hbm", "achieved": bytes_run / run_s / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": bytes_run / run_s / 1e9 / peak, "traffic": None,
+                     "fp32_tflops": flops_run / run_s / 1e12, "fp32_nominal_tflops": 74.4,
+                     "peak_source": peak_kind},
+        "plain_form_kf_steps_per_s": plain_value,
+        "batched_over_plain": value / world / plain_value,
+        "clocks": clk.summary(),
+    }
+    plan.close()
     ctx.close()
     return line
 
@@ -297,7 +380,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pf", choices=["pf"])
+    ap.add_argument("--workload", default="pf", choices=["pf", "kf"])
+    ap.add_argument("--kf-filters", type=int, default=65536)
+    ap.add_argument("--kf-algo", default="kf", choices=["kf", "srkf"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
@@ -312,6 +397,8 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     if args.impl == "reference":
         line = bench_reference(args, world, rank, local)
+    elif args.workload == "kf":
+        line = bench_kf(args, world, rank, local)
     else:
         line = bench_pf(args, world, rank, local)
     if rank == 0 and line is not None:

@@ -13,8 +13,11 @@
 //   ll = -1/2 (z' S^-1 z + log|S| + dy log 2 pi).
 // SRKF step restates srkf.jl:93-176 with Householder QR.
 #include <algorithm>
+#include <cstddef>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
+#include <fstream>
 #include <memory>
 #include <numeric>
 #include <string>
@@ -66,7 +69,8 @@ struct KfSmem {
   static constexpr int LY = DYP + 1;   // row stride of dy-wide matrices
   float A[DXP * LD], Q[DXP * LD], Sig[DXP * LD], Sp[DXP * LD], T1[DXP * LD], IKH[DXP * LD];
   float H[DYP * LD], PHt[DXP * LY], K[DXP * LY], KR[DXP * LY], R[DYP * LY];
-  double S[DYP * LY], Li[DYP * LY];
+  static constexpr int LW = DXP + 2;  // row stride of the solve buffer (dx RHS + z)
+  double S[DYP * LY], Wm[DYP * LW], dinv[DYP];
   float mu[DXP], mup[DXP], b[DXP], c[DYP];
   double z[DYP], w[DYP];
   double red[32];
@@ -109,47 +113,68 @@ __device__ void kf_load(KfSmem<DXP, DYP>& s, const float* P, int dx, int dy) {
   for (int e = threadIdx.x; e < dy; e += G) s.c[e] = pc[e];
 }
 
-// FP64 Cholesky of s.S (dy x dy, lower written in place) by warp 0, then the
-// lower-triangular inverse Li (one column per thread).  Returns 0 if not PD.
+// FP64 Cholesky of s.S (dy x dy, lower triangle, in place) by warp 0 with one
+// lane per row (right-looking; dy <= 32), plus the reciprocal diagonal.
+// Returns false if S is not positive definite.
 template <int DXP, int DYP>
-__device__ bool kf_chol_inv(KfSmem<DXP, DYP>& s, int dy) {
+__device__ bool kf_chol(KfSmem<DXP, DYP>& s, int dy) {
   constexpr int LY = KfSmem<DXP, DYP>::LY;
   if (threadIdx.x < 32) {
-    const int lane = threadIdx.x;
+    const int r = threadIdx.x;
     for (int j = 0; j < dy; ++j) {
-      double d = s.S[j * LY + j];
-      if (!(d > 0.0)) {
-        if (lane == 0) s.fail = 1;
+      const double djj = s.S[j * LY + j];
+      if (!(djj > 0.0)) {
+        if (r == 0) s.fail = 1;
         break;
       }
-      d = sqrt(d);
-      __syncwarp();
-      for (int i = j + 1 + lane; i < dy; i += 32) s.S[i * LY + j] /= d;
-      if (lane == 0) s.S[j * LY + j] = d;
-      __syncwarp();
-      // trailing update of the lower triangle: S[i][k] -= L[i][j] L[k][j], k <= i
-      const int n = dy - j - 1;
-      for (int e = lane; e < n * n; e += 32) {
-        int i = j + 1 + e / n, k = j + 1 + e % n;
-        if (k <= i) s.S[i * LY + k] -= s.S[i * LY + j] * s.S[k * LY + j];
+      const double d = sqrt(djj), inv = 1.0 / d;
+      double lrj = 0.0;
+      if (r > j && r < dy) {
+        lrj = s.S[r * LY + j] * inv;
+        s.S[r * LY + j] = lrj;
+      }
+      if (r == j) {
+        s.S[j * LY + j] = d;
+        s.dinv[j] = inv;
       }
       __syncwarp();
+      if (r > j && r < dy)
+        for (int k = j + 1; k <= r; ++k) s.S[r * LY + k] -= lrj * s.S[k * LY + j];
+      __syncwarp();
     }
   }
-  group_sync();
-  if (s.fail) return false;
-  // Li = L^-1, column j by thread j
-  for (int j = threadIdx.x; j < dy; j += blockDim.x) {
-    s.Li[j * LY + j] = 1.0 / s.S[j * LY + j];
-    for (int i = j + 1; i < dy; ++i) {
-      double acc = 0.0;
-      for (int k = j; k < i; ++k) acc += s.S[i * LY + k] * s.Li[k * LY + j];
-      s.Li[i * LY + j] = -acc / s.S[i * LY + i];
+  __syncthreads();
+  return !s.fail;
+}
+
+// Triangular solves on the RHS buffer Wm (dy rows): forward L Y = Wm over
+// columns [0, nf), then back L' X = Y over columns [0, nb).  Lane = row, warps
+// take interleaved column sets; dy <= 32.
+template <int DXP, int DYP>
+__device__ void kf_solves(KfSmem<DXP, DYP>& s, int dy, int nf, int nb) {
+  constexpr int LY = KfSmem<DXP, DYP>::LY, LW = KfSmem<DXP, DYP>::LW;
+  const int r = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  for (int i = 0; i < dy; ++i) {
+    if (r == i)
+      for (int c = w; c < nf; c += nw) s.Wm[i * LW + c] *= s.dinv[i];
+    __syncwarp();
+    if (r > i && r < dy) {
+      const double l = s.S[r * LY + i];
+      for (int c = w; c < nf; c += nw) s.Wm[r * LW + c] -= l * s.Wm[i * LW + c];
     }
-    for (int i = 0; i < j; ++i) s.Li[i * LY + j] = 0.0;
+    __syncwarp();
   }
-  group_sync();
-  return true;
+  for (int i = dy - 1; i >= 0; --i) {
+    if (r == i)
+      for (int c = w; c < nb; c += nw) s.Wm[i * LW + c] *= s.dinv[i];
+    __syncwarp();
+    if (r < i) {
+      const double l = s.S[i * LY + r];
+      for (int c = w; c < nb; c += nw) s.Wm[r * LW + c] -= l * s.Wm[i * LW + c];
+    }
+    __syncwarp();
+  }
+  __syncthreads();
 }
 
 template <int DXP, int DYP>
@@ -172,13 +197,19 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
     const int dx = D.dx, dy = D.dy;
     kf_load<DXP, DYP>(s, run.params + D.poff, dx, dy);
     group_sync();
+    // 2-D thread maps without integer division: rows of width dx / dy are
+    // covered by 2^lx / 2^ly lanes, the remaining threads step over rows
+    const int lx = dx <= 4 ? 2 : (dx <= 8 ? 3 : (dx <= 16 ? 4 : 5));
+    const int ly = dy <= 4 ? 2 : (dy <= 8 ? 3 : (dy <= 16 ? 4 : 5));
+    const int tx = threadIdx.x & ((1 << lx) - 1), ty = threadIdx.x >> lx, nx = 1 << lx, ny = G >> lx;
+    const int ux = threadIdx.x & ((1 << ly) - 1), uy = threadIdx.x >> ly, mx = 1 << ly, my = G >> ly;
     double lltot = 0.0;
     int status = GF_OK;
     for (int t = 0; t < D.T; ++t) {
       const double* y = run.ys + D.yoff + (int64_t)t * dy;
       // 1. T1 = A Sigma ; mup = A mu + b
-      for (int e = threadIdx.x; e < dx * dx; e += G) {
-        int i = e / dx, j = e % dx;
+      for (int i = ty; i < dx; i += ny)
+      for (int j = tx; j < dx; j += nx) {
         float acc = 0.f;
         for (int k = 0; k < dx; ++k) acc = fmaf(s.A[i * LD + k], s.Sig[k * LD + j], acc);
         s.T1[i * LD + j] = acc;
@@ -190,8 +221,8 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       }
       group_sync();
       // 2. Sp = T1 A' + Q (upper triangle, mirrored)
-      for (int e = threadIdx.x; e < dx * dx; e += G) {
-        int i = e / dx, j = e % dx;
+      for (int i = ty; i < dx; i += ny)
+      for (int j = tx; j < dx; j += nx) {
         if (j < i) continue;
         float acc = s.Q[i * LD + j];
         for (int k = 0; k < dx; ++k) acc = fmaf(s.T1[i * LD + k], s.A[j * LD + k], acc);
@@ -200,8 +231,8 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       }
       group_sync();
       // 3. PHt = Sp H' ; z = y - H mup - c
-      for (int e = threadIdx.x; e < dx * dy; e += G) {
-        int i = e / dy, j = e % dy;
+      for (int i = uy; i < dx; i += my)
+      for (int j = ux; j < dy; j += mx) {
         float acc = 0.f;
         for (int k = 0; k < dx; ++k) acc = fmaf(s.Sp[i * LD + k], s.H[j * LD + k], acc);
         s.PHt[i * LY + j] = acc;
@@ -213,38 +244,28 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       }
       group_sync();
       // 4. S = H PHt + R in FP64 (lower triangle is all the Cholesky reads)
-      for (int e = threadIdx.x; e < dy * dy; e += G) {
-        int i = e / dy, j = e % dy;
-        if (j > i) continue;
+      for (int i = uy; i < dy; i += my)
+      for (int j = ux; j <= i; j += mx) {
         double acc = (double)s.R[i * LY + j];
         for (int k = 0; k < dx; ++k) acc += (double)s.H[i * LD + k] * (double)s.PHt[k * LY + j];
         s.S[i * LY + j] = acc;
       }
       group_sync();
-      // 5. Cholesky + inverse
-      if (!kf_chol_inv<DXP, DYP>(s, dy)) {
+      // 5. Cholesky of S (FP64)
+      if (!kf_chol<DXP, DYP>(s, dy)) {
         status = GF_ERR_NOT_PD;
         break;
       }
-      // 6. w = Li z ; W = PHt Li' (stored in KR) ; then K = W Li
-      for (int i = threadIdx.x; i < dy; i += G) {
-        double acc = 0.0;
-        for (int k = 0; k <= i; ++k) acc += s.Li[i * LY + k] * s.z[k];
-        s.w[i] = acc;
-      }
-      for (int e = threadIdx.x; e < dx * dy; e += G) {
-        int i = e / dy, j = e % dy;
-        double acc = 0.0;
-        for (int k = 0; k <= j; ++k) acc += (double)s.PHt[i * LY + k] * s.Li[j * LY + k];
-        s.KR[i * LY + j] = (float)acc;
-      }
-      group_sync();
-      for (int e = threadIdx.x; e < dx * dy; e += G) {
-        int i = e / dy, j = e % dy;
-        double acc = 0.0;
-        for (int k = j; k < dy; ++k) acc += (double)s.KR[i * LY + k] * s.Li[k * LY + j];
-        s.K[i * LY + j] = (float)acc;
-      }
+      // 6. RHS = [PHt' | z]; forward solve gives w = L^-1 z (last column),
+      //    back solve of the first dx columns gives K' = S^-1 PHt'
+      constexpr int LW = SM::LW;
+      for (int c = ty; c <= dx; c += ny)
+        for (int i = tx; i < dy; i += nx) s.Wm[i * LW + c] = c < dx ? (double)s.PHt[c * LY + i] : s.z[i];
+      __syncthreads();
+      kf_solves<DXP, DYP>(s, dy, dx + 1, dx);
+      for (int i = threadIdx.x; i < dy; i += G) s.w[i] = s.Wm[i * LW + dx];
+      for (int i = uy; i < dx; i += my)
+        for (int j = ux; j < dy; j += mx) s.K[i * LY + j] = (float)s.Wm[j * LW + i];
       group_sync();
       // 7. mu = mup + K z ; IKH = I - K H ; KR = K R
       for (int i = threadIdx.x; i < dx; i += G) {
@@ -252,22 +273,22 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
         for (int k = 0; k < dy; ++k) acc += (double)s.K[i * LY + k] * s.z[k];
         s.mu[i] = (float)acc;
       }
-      for (int e = threadIdx.x; e < dx * dx; e += G) {
-        int i = e / dx, j = e % dx;
+      for (int i = ty; i < dx; i += ny)
+      for (int j = tx; j < dx; j += nx) {
         float acc = (i == j) ? 1.f : 0.f;
         for (int k = 0; k < dy; ++k) acc = fmaf(-s.K[i * LY + k], s.H[k * LD + j], acc);
         s.IKH[i * LD + j] = acc;
       }
-      for (int e = threadIdx.x; e < dx * dy; e += G) {
-        int i = e / dy, j = e % dy;
+      for (int i = uy; i < dx; i += my)
+      for (int j = ux; j < dy; j += mx) {
         float acc = 0.f;
         for (int k = 0; k < dy; ++k) acc = fmaf(s.K[i * LY + k], s.R[k * LY + j], acc);
         s.KR[i * LY + j] = acc;
       }
       group_sync();
       // 8. T1 = IKH Sp
-      for (int e = threadIdx.x; e < dx * dx; e += G) {
-        int i = e / dx, j = e % dx;
+      for (int i = ty; i < dx; i += ny)
+      for (int j = tx; j < dx; j += nx) {
         float acc = 0.f;
         for (int k = 0; k < dx; ++k) acc = fmaf(s.IKH[i * LD + k], s.Sp[k * LD + j], acc);
         s.T1[i * LD + j] = acc;
@@ -275,8 +296,8 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       group_sync();
       // 9. Sig = T1 IKH' + KR K' (+ jitter I), upper triangle mirrored
       float* cov_out = run.covs ? run.covs + D.coff + (int64_t)t * dx * dx : nullptr;
-      for (int e = threadIdx.x; e < dx * dx; e += G) {
-        int i = e / dx, j = e % dx;
+      for (int i = ty; i < dx; i += ny)
+      for (int j = tx; j < dx; j += nx) {
         if (j < i) continue;
         float acc = 0.f;
         for (int k = 0; k < dx; ++k) acc = fmaf(s.T1[i * LD + k], s.IKH[j * LD + k], acc);
@@ -288,7 +309,8 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       group_sync();
       // 10. outputs
       if (cov_out)
-        for (int e = threadIdx.x; e < dx * dx; e += G) cov_out[e] = s.Sig[(e % dx) * LD + e / dx];
+        for (int j = ty; j < dx; j += ny)
+          for (int i = tx; i < dx; i += nx) cov_out[i + j * dx] = s.Sig[i * LD + j];
       if (run.means)
         for (int i = threadIdx.x; i < dx; i += G) run.means[D.moff + (int64_t)t * dx + i] = s.mu[i];
       if (threadIdx.x < 32) {
@@ -349,10 +371,10 @@ __device__ void householder_qr(float* M, int m, int n, double* colscale, double*
         colscale[j] = 2.0 * acc / vv;
       }
       __syncthreads();
-      for (int e = threadIdx.x; e < (m - k) * (n - k - 1); e += blockDim.x) {
-        int i = k + e / (n - k - 1), j = k + 1 + e % (n - k - 1);
-        double vi = i == k ? v0 : (double)M[i * LM + k];
-        M[i * LM + j] = (float)((double)M[i * LM + j] - colscale[j] * vi);
+      for (int i = k + (threadIdx.x >> 5); i < m; i += (blockDim.x >> 5)) {
+        const double vi = i == k ? v0 : (double)M[i * LM + k];
+        for (int j = k + 1 + (threadIdx.x & 31); j < n; j += 32)
+          M[i * LM + j] = (float)((double)M[i * LM + j] - colscale[j] * vi);
       }
       __syncthreads();
       if (threadIdx.x == 0) M[k * LM + k] = (float)alpha;
@@ -674,6 +696,127 @@ static gf_status kf_enqueue(gf_kf_plan* p, const double* ys, gf_kf_out* out) {
   return GF_OK;
 }
 
+// ------------------------------------------------------------- autotuner
+// Picks the block size (threads per filter) of each dimension bucket by timing
+// the candidates on a sample of the bucket (its longest filters, T clipped to
+// 64 steps, outputs off); results are cached per (GPU, algorithm, bucket) in
+// the file named by GF_AUTOTUNE_CACHE (default ~/.cache/gfb200/kf_autotune.txt).
+static std::string autotune_path() {
+  const char* e = std::getenv("GF_AUTOTUNE_CACHE");
+  if (e && *e) return e;
+  const char* h = std::getenv("HOME");
+  return std::string(h ? h : "/tmp") + "/.cache/gfb200/kf_autotune.txt";
+}
+static std::string autotune_key(gf_ctx* ctx, int algo, int dxp) {
+  cudaDeviceProp prop;
+  cudaGetDeviceProperties(&prop, ctx->device);
+  std::string name = prop.name;
+  for (auto& c : name)
+    if (c == ' ') c = '_';
+  return name + "|" + (algo == GF_ALGO_KF ? "kf" : "srkf") + "|" + std::to_string(dxp);
+}
+static int autotune_lookup(gf_ctx* ctx, int algo, int dxp) {
+  std::ifstream f(autotune_path());
+  std::string k, want = autotune_key(ctx, algo, dxp);
+  int g;
+  int found = 0;
+  while (f >> k >> g)
+    if (k == want && (g == 32 || g == 64 || g == 128 || g == 256)) found = g;
+  return found;
+}
+static void autotune_store(gf_ctx* ctx, int algo, int dxp, int group) {
+  std::string path = autotune_path();
+  std::string dir = path.substr(0, path.find_last_of('/'));
+  std::string cmd = "mkdir -p '" + dir + "'";
+  if (std::system(cmd.c_str()) != 0) return;
+  std::ofstream f(path, std::ios::app);
+  if (f) f << autotune_key(ctx, algo, dxp) << " " << group << "\n";
+}
+
+static gf_status kf_autotune_bucket(gf_kf_plan* p, gf_kf_plan::Bucket& bk) {
+  gf_ctx* ctx = p->ctx;
+  const KfBucketKernels& K = kf_buckets()[bk.kidx];
+  const size_t smem = p->algo == GF_ALGO_KF ? K.kf_smem : K.sr_smem;
+  const void* fn = p->algo == GF_ALGO_KF ? (const void*)K.kf : (const void*)K.sr;
+  const int sample = std::min(bk.count, 2 * ctx->num_sms * 4);
+  std::vector<KfDesc> td(sample);
+  std::vector<int32_t> ord(sample);
+  int maxdy = 1;
+  for (int q = 0; q < sample; ++q) {
+    td[q] = p->hdesc[p->horder[bk.start + q]];
+    td[q].T = std::min(td[q].T, 64);
+    td[q].yoff = 0;
+    td[q].soff = td[q].moff = td[q].coff = 0;
+    td[q].index = q;
+    ord[q] = q;
+    maxdy = std::max(maxdy, td[q].dy);
+  }
+  void *ddesc = nullptr, *dord = nullptr, *dys = nullptr, *dll = nullptr, *dst = nullptr, *dcnt = nullptr;
+  std::vector<DevBuf> tmp;
+  auto get = [&](size_t b, void** d) -> gf_status {
+    gf_status s2 = dev_alloc(ctx, b, d);
+    if (!s2 && *d) tmp.push_back({*d, b});
+    return s2;
+  };
+  struct Free {
+    gf_ctx* c;
+    std::vector<DevBuf>* v;
+    ~Free() {
+      cudaStreamSynchronize(c->stream);
+      for (auto& b : *v) dev_free(c, b.p, b.bytes);
+    }
+  } fr{ctx, &tmp};
+  gf_status st;
+  if ((st = get(sizeof(KfDesc) * sample, &ddesc)) || (st = get(sizeof(int32_t) * sample, &dord)) ||
+      (st = get(sizeof(double) * 64 * maxdy, &dys)) || (st = get(sizeof(double) * sample, &dll)) ||
+      (st = get(sizeof(int32_t) * sample, &dst)) || (st = get(sizeof(uint32_t), &dcnt)))
+    return st;
+  cudaStream_t s = ctx->stream;
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(ddesc, td.data(), sizeof(KfDesc) * sample, cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(dord, ord.data(), sizeof(int32_t) * sample, cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemsetAsync(dys, 0, sizeof(double) * 64 * maxdy, s));
+  KfRun r{};
+  r.desc = (const KfDesc*)ddesc;
+  r.order = (const int32_t*)dord;
+  r.count = sample;
+  r.counter = (uint32_t*)dcnt;
+  r.params = p->params;
+  r.ys = (const double*)dys;
+  r.ll = (double*)dll;
+  r.status = (int32_t*)dst;
+  r.algo = p->algo;
+  cudaEvent_t e0, e1;
+  cudaEventCreate(&e0);
+  cudaEventCreate(&e1);
+  float best = 1e30f;
+  int best_g = bk.group;
+  for (int g : {32, 64, 128, 256}) {
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, g, smem);
+    if (per_sm < 1) continue;
+    const int grid = std::max(1, std::min(sample, per_sm * ctx->num_sms));
+    float ms = 0.f;
+    for (int rep = 0; rep < 2; ++rep) {
+      cudaMemsetAsync(dcnt, 0, sizeof(uint32_t), s);
+      cudaEventRecord(e0, s);
+      if (p->algo == GF_ALGO_KF) K.kf<<<grid, g, smem, s>>>(r);
+      else K.sr<<<grid, g, smem, s>>>(r);
+      cudaEventRecord(e1, s);
+      cudaEventSynchronize(e1);
+      cudaEventElapsedTime(&ms, e0, e1);
+    }
+    if (cudaGetLastError() != cudaSuccess) continue;
+    if (ms < best) {
+      best = ms;
+      best_g = g;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  bk.group = best_g;
+  return GF_OK;
+}
+
 extern "C" gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_model* models,
                                        int32_t B, const int32_t* T, double jitter,
                                        int32_t use_jitter, int32_t flags, gf_kf_plan** out) {
@@ -786,6 +929,15 @@ extern "C" gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_mo
     size_t smem = algo == GF_ALGO_KF ? K.kf_smem : K.sr_smem;
     const void* fn = algo == GF_ALGO_KF ? (const void*)K.kf : (const void*)K.sr;
     GF_CHECK_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int cached = (flags & GF_PLAN_AUTOTUNE) ? autotune_lookup(ctx, algo, bks[bk.kidx].dxp) : 0;
+    if (cached) bk.group = cached;
+    else if (flags & GF_PLAN_AUTOTUNE) {
+      if ((st = kf_autotune_bucket(p.get(), bk))) {
+        kf_release(p.get());
+        return st;
+      }
+      autotune_store(ctx, algo, bks[bk.kidx].dxp, bk.group);
+    }
     int per_sm = 0;
     GF_CHECK_CUDA(ctx, cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, bk.group, smem));
     bk.grid = std::max(1, std::min(bk.count, per_sm * ctx->num_sms));

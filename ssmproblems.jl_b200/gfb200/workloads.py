@@ -69,32 +69,44 @@ def lgssm_rot(seed=0, dx=16, dy=8, T=1000, rho=0.95, q=0.1, r=0.2):
     return m, ys
 
 
-def kf_bank(B, seed=0, dx_range=(2, 32), T_range=(64, 2048), simulate=False):
+def kf_bank(B, seed=0, dx_range=(2, 32), T_range=(64, 2048), simulate=False, make_ys=True):
     """Returns (models, T list, ys list).  With simulate=False the observations are
     N(0,1) draws: the KF's arithmetic does not depend on their values, and the
-    bank stays cheap to build at B = 65536."""
+    bank stays cheap to build at B = 65536 (parameters are drawn in batches per
+    state dimension)."""
     rng = np.random.default_rng(seed)
-    models, Ts, yss = [], [], []
-    for _ in range(B):
-        dx = int(rng.integers(dx_range[0], dx_range[1] + 1))
-        dy = int(rng.integers(1, dx + 1))
-        rho = rng.uniform(0.8, 0.99)
-        q = float(np.exp(rng.uniform(np.log(1e-3), np.log(1.0))))
-        r = float(np.exp(rng.uniform(np.log(1e-2), np.log(1.0))))
-        A = random_orthogonal(rng, dx) * rho
+    dxs = rng.integers(dx_range[0], dx_range[1] + 1, size=B)
+    dys = np.array([rng.integers(1, d + 1) for d in dxs])
+    rhos = rng.uniform(0.8, 0.99, size=B)
+    qs = np.exp(rng.uniform(np.log(1e-3), np.log(1.0), size=B))
+    rs = np.exp(rng.uniform(np.log(1e-2), np.log(1.0), size=B))
+    Ts = rng.integers(T_range[0], T_range[1] + 1, size=B)
+    As = [None] * B
+    for d in np.unique(dxs):
+        idx = np.nonzero(dxs == d)[0]
+        Z = rng.standard_normal((idx.size, d, d))
+        Qm, Rm = np.linalg.qr(Z)
+        sgn = np.sign(np.diagonal(Rm, axis1=1, axis2=2))
+        Orth = Qm * sgn[:, None, :]
+        for j, f in enumerate(idx):
+            As[f] = Orth[j] * rhos[f]
+    models, yss = [], []
+    for f in range(B):
+        dx, dy = int(dxs[f]), int(dys[f])
         H = rng.standard_normal((dy, dx)) / np.sqrt(dx)
-        T = int(rng.integers(T_range[0], T_range[1] + 1))
-        m = create_homogeneous_linear_gaussian_model(np.zeros(dx), np.eye(dx), A, np.zeros(dx),
-                                                     q * np.eye(dx), H, np.zeros(dy),
-                                                     r * np.eye(dy))
+        m = create_homogeneous_linear_gaussian_model(np.zeros(dx), np.eye(dx), As[f], np.zeros(dx),
+                                                     qs[f] * np.eye(dx), H, np.zeros(dy),
+                                                     rs[f] * np.eye(dy))
+        T = int(Ts[f])
         if simulate:
             _, ys = simulate_lg(rng, m, T)
-        else:
+        elif make_ys:
             ys = rng.standard_normal((T, dy))
+        else:
+            ys = None
         models.append(m)
-        Ts.append(T)
         yss.append(ys)
-    return models, Ts, yss
+    return models, [int(t) for t in Ts], yss
 
 
 def rb_trend(seed=0, T=500, dz=8, dy=4, q_gamma=1.0):
