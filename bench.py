@@ -7,7 +7,7 @@ ESS < 0.5 N, FP64 normaliser and cumulative weights, in-kernel Philox noise.
 One step = one full filter run (N * T particle-steps).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload pf|kf|rbpf]
+                    [--workload pf|kf|serve]
 
 Under torchrun each rank runs an independent replica (the filters shard by
 filter; no data-path collective).  Rank 0 prints one JSON line.
@@ -347,6 +347,101 @@ def bench_kf(args, world, rank, local):
     return line
 
 
+def _serve_stream(rng, mix, ypool, m1, y1, hm, yr):
+    """Models, algorithms and observations of a request stream (serving_mix)."""
+    import gfb200 as G
+    from gfb200 import workloads as W
+    out = []
+    for t, kind, p in mix:
+        if kind == "kf":
+            dx, dy, T = p["dx"], p["dy"], p["T"]
+            A = W.random_orthogonal(rng, dx) * rng.uniform(0.8, 0.99)
+            H = rng.standard_normal((dy, dx)) / np.sqrt(dx)
+            q = float(np.exp(rng.uniform(np.log(1e-3), 0.0)))
+            r = float(np.exp(rng.uniform(np.log(1e-2), 0.0)))
+            m = G.create_homogeneous_linear_gaussian_model(
+                np.zeros(dx), np.eye(dx), A, np.zeros(dx), q * np.eye(dx), H, np.zeros(dy),
+                r * np.eye(dy))
+            out.append((t, m, G.KF(), ypool[:T * dy].reshape(T, dy), 0, T, 0))
+        elif kind == "bf":
+            out.append((t, m1, G.BF(p["N"], threshold=0.5), y1[:p["T"]], p["seed"], p["T"], p["N"]))
+        else:
+            algo = G.RBPF(G.BF(p["N"], threshold=0.5), G.KalmanFilter())
+            out.append((t, hm, algo, yr[:p["T"]], p["seed"], p["T"], p["N"]))
+    return out
+
+
+def bench_serve(args, world, rank, local):
+    """Served filtering (Poisson arrivals of a 70% KF / 25% BF / 5% RBPF mix):
+    requests are submitted from host memory at their arrival times through the
+    serving C ABI and each result returns to host memory; the line reports
+    completed requests per second and the submit-to-result latency quantiles."""
+    import gfb200 as G
+    from gfb200 import workloads as W
+    rate, M = args.serve_rate, args.serve_requests
+    rng = np.random.default_rng(5 + rank)
+    ypool = rng.standard_normal(5000 * 32)
+    m1, y1 = W.lgssm_1d(seed=3, T=2000)
+    hm, yr = W.rb_trend(seed=4, T=500)
+    warm = _serve_stream(rng, W.serving_mix(60, rate, seed=99 + rank), ypool, m1, y1, hm, yr)
+    streams = [_serve_stream(rng, W.serving_mix(M, rate, seed=11 + 100 * k + rank), ypool, m1, y1,
+                             hm, yr) for k in range(args.steps)]
+    srv = G.Server(device=local, hbm_budget_bytes=args.serve_hbm_gb << 30,
+                   host_budget_bytes=4 << 30)
+
+    def play(stream):
+        t0 = time.perf_counter()
+        h2d = 0
+        for t, m, algo, ys, seed, T, N in stream:
+            d = t0 + t - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            while True:
+                try:
+                    srv.submit(m, algo, ys, seed=seed, want_mean=True)
+                    break
+                except G.GFError as e:
+                    if e.code != 8:  # GF_ERR_BUSY: back off and retry
+                        raise
+                    time.sleep(1e-4)
+            h2d += ys.nbytes
+        srv.drain()
+        srv.poll(max_results=1 << 16)
+        return h2d
+
+    for _ in range(args.warmup):
+        play(warm)
+    srv.reset_stats()
+    s0 = srv.stats()
+    with ClockSampler(local) as clk:
+        h2d = sum(play(st) for st in streams)
+    st = srv.stats()
+    srv.close()
+    el = st["elapsed_ms"] / 1e3
+    served = st["completed"] / el
+    offered = M * args.steps / sum(s[-1][0] for s in streams)
+    line = {
+        "metric": "served requests/s", "value": served, "unit": "req/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": st["elapsed_ms"] / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"Poisson request stream at {rate:g} req/s: 70% KF (Dx 2..32, "
+                               f"T 100..5000), 25% BF on the 1-D LGSSM (N 4096..262144, T 100..2000), "
+                               f"5% RBPF (N 4096..32768, T 500)", "requests_per_step": M,
+                   "offered_req_s": offered, "hbm_budget_gb": args.serve_hbm_gb},
+        "latency_ms": {"p50": st["p50_ms"], "p99": st["p99_ms"], "mean": st["mean_ms"],
+                       "max": st["max_ms"]},
+        "completed": st["completed"], "failed": st["failed"], "rejected": st["rejected"],
+        "kf_steps_per_s": st["kf_steps"] / el, "particle_steps_per_s": st["particle_steps"] / el,
+        "gpu_launches": st["launches"] - s0["launches"],
+        "e2e": {"value": served, "unit": "req/s", "h2d_bytes_per_step": h2d // args.steps,
+                "d2h_bytes_per_step": None},
+        "hbm_peak_gb": st["hbm_peak"] / 2**30,
+        "clocks": clk.summary(),
+    }
+    return line
+
+
 def bench_reference(args, world, rank, local):
     """The reference arm: the FP64 oracle port of the reference algorithm on the
     host cores (the reference is Julia and cannot run on this image)."""
@@ -380,7 +475,10 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pf", choices=["pf", "kf"])
+    ap.add_argument("--workload", default="pf", choices=["pf", "kf", "serve"])
+    ap.add_argument("--serve-rate", type=float, default=1000.0)
+    ap.add_argument("--serve-requests", type=int, default=2000)
+    ap.add_argument("--serve-hbm-gb", type=int, default=64)
     ap.add_argument("--kf-filters", type=int, default=65536)
     ap.add_argument("--kf-algo", default="kf", choices=["kf", "srkf"])
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -399,6 +497,8 @@ def main():
         line = bench_reference(args, world, rank, local)
     elif args.workload == "kf":
         line = bench_kf(args, world, rank, local)
+    elif args.workload == "serve":
+        line = bench_serve(args, world, rank, local)
     else:
         line = bench_pf(args, world, rank, local)
     if rank == 0 and line is not None:

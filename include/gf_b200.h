@@ -238,6 +238,76 @@ int64_t gf_sample_ancestors_noalloc_max_n(void);
 gf_status gf_rng_normals(gf_ctx* ctx, uint64_t seed, int32_t t, int32_t dx, int64_t n,
                          int32_t precision, void* out_dev);
 
+/* ------------------------------------------------------------------ serving */
+/* No reference counterpart: the reference runs one synchronous filter() call
+ * at a time (GeneralisedFilters.jl:58-84).  A server owns one GPU through a
+ * worker thread and runs many independent requests at once: Kalman requests
+ * as persistent batched launches, particle-filter requests continuously
+ * batched into shared per-step launches.  Admission is first-come-first-served
+ * against a fixed HBM arena (hbm_budget_bytes) and a pinned host arena.
+ * Submitting, polling and statistics are thread-safe.  A served request
+ * returns exactly what gf_kf_batch / gf_pf_run / gf_rbpf_run return for the
+ * same inputs (with in-kernel Philox draws). */
+typedef struct gf_srv gf_srv;
+enum { GF_REQ_KF = 0, GF_REQ_SRKF = 1, GF_REQ_PF = 2, GF_REQ_RBPF = 3 };
+typedef struct {
+  int32_t device;
+  size_t hbm_budget_bytes;  /* device arena (0 = half of the free memory) */
+  size_t host_budget_bytes; /* pinned host arena for staging and results (0 = 1 GiB) */
+  int32_t max_pending;      /* submitted, not yet admitted requests before GF_ERR_BUSY (0 = 65536) */
+  int32_t pf_chunk;         /* steps per particle-filter batch iteration (0 = 16) */
+  int32_t kf_streams;       /* streams for concurrent Kalman batches (0 = 64) */
+  int32_t max_active_pf;    /* particle-filter jobs running at once (0 = 4096) */
+} gf_srv_config;
+typedef struct {
+  int32_t kind;             /* GF_REQ_* */
+  int32_t T;
+  const gf_lg_model* lg;    /* KF, SRKF, PF */
+  const gf_rb_model* rb;    /* RBPF */
+  const gf_pf_config* pf;   /* PF, RBPF (noise and uniforms are drawn in-kernel) */
+  const double* ys;         /* host [T][dy]; copied by gf_srv_submit */
+  double jitter;            /* KF, SRKF */
+  int32_t use_jitter;
+  int32_t reserved;
+  /* Optional host destinations, written before the result is reported; they
+   * must stay valid until then. */
+  double* ll_steps;         /* [T] per-step log-likelihood increments */
+  double* mean;             /* KF/SRKF/PF: final filtered (weighted) mean [dx];
+                               RBPF: [dxo + dz] weighted outer then inner means */
+  double* cov;              /* KF/SRKF: final filtered covariance [dx*dx], column-major */
+  uint64_t tag;             /* returned in the result */
+} gf_srv_request;
+typedef struct {
+  uint64_t id, tag;
+  gf_status status;
+  int32_t kind;
+  double ll;                /* log-evidence (filter()'s second return value) */
+  double submit_ms, start_ms, done_ms; /* since gf_srv_create; start = admission (-1 if never) */
+} gf_srv_result;
+typedef struct {
+  int64_t submitted, completed, failed, rejected, pending, running;
+  double p50_ms, p99_ms, mean_ms, max_ms; /* submit -> result latency of completed requests */
+  double kf_steps, particle_steps;        /* work of completed requests */
+  double elapsed_ms;                      /* first submit -> last result */
+  size_t hbm_budget, hbm_used, hbm_peak;
+  int64_t pf_iterations, kf_batches, launches;
+} gf_srv_metrics;
+gf_status gf_srv_create(const gf_srv_config* cfg, gf_srv** out);
+/* Validates and copies the request (inputs need not outlive the call); returns
+ * GF_ERR_BUSY when max_pending requests wait for admission. */
+gf_status gf_srv_submit(gf_srv* srv, const gf_srv_request* req, uint64_t* id);
+/* Moves up to `max` finished results to `out`, waiting up to wait_ms for the
+ * first; returns how many were written. */
+int32_t gf_srv_poll(gf_srv* srv, gf_srv_result* out, int32_t max, int32_t wait_ms);
+/* Waits until every submitted request has a result (timeout_ms < 0: forever). */
+gf_status gf_srv_drain(gf_srv* srv, int32_t timeout_ms);
+gf_status gf_srv_stats(gf_srv* srv, gf_srv_metrics* out);
+/* Forgets finished requests' latencies and work (for a fresh measurement window). */
+gf_status gf_srv_reset_stats(gf_srv* srv);
+const char* gf_srv_last_error(gf_srv* srv);
+/* Cancels requests not yet admitted, waits for the running ones, frees the arenas. */
+gf_status gf_srv_destroy(gf_srv* srv);
+
 #ifdef __cplusplus
 }
 #endif

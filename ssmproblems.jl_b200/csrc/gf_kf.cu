@@ -25,43 +25,9 @@
 
 #include "gf_common.cuh"
 #include "gf_internal.hpp"
+#include "gf_kf_host.hpp"
 
 namespace gf {
-
-struct KfDesc {
-  int32_t dx, dy, T, pad;
-  int64_t poff;    // float offset into the parameter pool
-  int64_t yoff;    // double offset into ys
-  int64_t soff;    // step offset (ll_steps)
-  int64_t moff;    // float offset of means
-  int64_t coff;    // float offset of covs
-  int32_t index;   // caller's filter index
-  int32_t pad2;
-};
-
-struct KfRun {
-  const KfDesc* desc;
-  const int32_t* order;     // bucket work list (indices into desc)
-  int32_t count;
-  uint32_t* counter;        // persistent work ticket
-  const float* params;
-  const double* ys;
-  double* ll;               // [B]
-  double* ll_steps;
-  float* means;
-  float* covs;
-  int32_t* status;          // [B]
-  double jitter;
-  int32_t use_jitter;
-  int32_t algo;
-};
-
-// parameter pool layout per filter (column-major, unpadded):
-//   A dx*dx | b dx | Q dx*dx | H dy*dx | c dy | R dy*dy | mu0 dx | S0 dx*dx |
-//   UQ dx*dx | UR dy*dy | U0 dx*dx     (upper Cholesky factors, used by the SRKF)
-__host__ __device__ inline int64_t kf_param_len(int dx, int dy) {
-  return (int64_t)5 * dx * dx + 2 * dx + dy * dx + dy + 2 * dy * dy;
-}
 
 template <int DXP, int DYP>
 struct KfSmem {
@@ -175,6 +141,23 @@ __device__ void kf_solves(KfSmem<DXP, DYP>& s, int dy, int nf, int nb) {
     __syncwarp();
   }
   __syncthreads();
+}
+
+// Serving: publishes the final mean, covariance (cov(i, j)), ll and status of a
+// filter to its host-mapped record; `done` is written after a system-scope fence.
+template <typename CovF>
+__device__ void kf_srv_publish(const KfDesc& D, const float* mu, CovF cov, double ll, int status) {
+  const int dx = D.dx;
+  for (int i = threadIdx.x; i < dx; i += blockDim.x) D.srv_mu[i] = mu[i];
+  for (int e = threadIdx.x; e < dx * dx; e += blockDim.x) D.srv_cov[e] = cov(e % dx, e / dx);
+  __threadfence_system();
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    D.srv->ll = ll;
+    D.srv->status = status;
+    __threadfence_system();
+    D.srv->done = 1;
+  }
 }
 
 template <int DXP, int DYP>
@@ -324,10 +307,13 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
         double l = -0.5 * (q + 2.0 * ld + dy * GF_LOG2PI);
         lltot += l;
         if (threadIdx.x == 0 && run.ll_steps) run.ll_steps[D.soff + t] = l;
+        if (threadIdx.x == 0 && D.srv_steps) D.srv_steps[t] = l;
       }
       group_sync();
     }
-    if (threadIdx.x == 0) {
+    if (D.srv)
+      kf_srv_publish(D, s.mu, [&](int i, int j) { return s.Sig[i * LD + j]; }, lltot, status);
+    if (threadIdx.x == 0 && run.ll) {
       run.ll[D.index] = lltot;
       run.status[D.index] = status;
     }
@@ -540,10 +526,17 @@ __global__ void __launch_bounds__(256) srkf_batch_kernel(KfRun run) {
         double l = -0.5 * (q + 2.0 * ld + dy * GF_LOG2PI);
         lltot += l;
         if (threadIdx.x == 0 && run.ll_steps) run.ll_steps[D.soff + t] = l;
+        if (threadIdx.x == 0 && D.srv_steps) D.srv_steps[t] = l;
       }
       __syncthreads();
     }
-    if (threadIdx.x == 0) {
+    if (D.srv)
+      kf_srv_publish(D, s.mu, [&](int i, int j) {
+        float acc = 0.f;
+        for (int k = 0; k <= min(i, j); ++k) acc = fmaf(s.U[k * LD + i], s.U[k * LD + j], acc);
+        return acc;
+      }, lltot, status);
+    if (threadIdx.x == 0 && run.ll) {
       run.ll[D.index] = lltot;
       run.status[D.index] = status;
     }
@@ -569,6 +562,75 @@ static const std::vector<KfBucketKernels>& kf_buckets() {
   static std::vector<KfBucketKernels> v = {make_bucket<4, 4>(), make_bucket<8, 8>(),
                                            make_bucket<16, 16>(), make_bucket<32, 32>()};
   return v;
+}
+
+int kf_bucket_count() { return (int)kf_buckets().size(); }
+int kf_bucket_dxp(int kidx) { return kf_buckets()[kidx].dxp; }
+
+int kf_bucket_for(int dx, int dy) {
+  const auto& b = kf_buckets();
+  for (size_t k = 0; k < b.size(); ++k)
+    if (b[k].dxp >= dx && b[k].dyp >= dy) return (int)k;
+  return -1;
+}
+
+int kf_default_group(int kidx) {
+  const int dxp = kf_buckets()[kidx].dxp;
+  return dxp <= 8 ? 32 : (dxp <= 16 ? 128 : 256);
+}
+
+static const void* kf_fn(int algo, int kidx, size_t* smem) {
+  const KfBucketKernels& K = kf_buckets()[kidx];
+  *smem = algo == GF_ALGO_KF ? K.kf_smem : K.sr_smem;
+  return algo == GF_ALGO_KF ? (const void*)K.kf : (const void*)K.sr;
+}
+
+gf_status kf_prepare_bucket(gf_ctx* ctx, int algo, int kidx) {
+  size_t smem;
+  const void* fn = kf_fn(algo, kidx, &smem);
+  GF_CHECK_CUDA(ctx, cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  return GF_OK;
+}
+
+int kf_blocks_per_sm(int algo, int kidx, int group) {
+  size_t smem;
+  const void* fn = kf_fn(algo, kidx, &smem);
+  int per_sm = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fn, group, smem) != cudaSuccess) per_sm = 1;
+  return std::max(1, per_sm);
+}
+
+void kf_launch(int algo, int kidx, int group, int grid, const KfRun& r, cudaStream_t s) {
+  const KfBucketKernels& K = kf_buckets()[kidx];
+  if (algo == GF_ALGO_KF) K.kf<<<grid, group, K.kf_smem, s>>>(r);
+  else K.sr<<<grid, group, K.sr_smem, s>>>(r);
+}
+
+gf_status kf_pack_model(gf_ctx* ctx, int algo, const gf_lg_model& m, int f, std::vector<float>& pool) {
+  const int dx = m.dx, dy = m.dy;
+  std::vector<double> LQ(dx * dx), LR(dy * dy), L0(dx * dx);
+  bool bad = chol_lower(dx, m.Q, LQ.data()) || chol_lower(dy, m.R, LR.data()) ||
+             chol_lower(dx, m.Sigma0, L0.data());
+  if (bad && algo == GF_ALGO_SRKF) return set_err(ctx, GF_ERR_NOT_PD, "filter %d: Q, R or Sigma0 not PD", f);
+  auto put = [&](const double* a, int n) {
+    for (int i = 0; i < n; ++i) pool.push_back((float)a[i]);
+  };
+  auto putT = [&](const std::vector<double>& L, int n) {  // upper factor U = L'
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) pool.push_back((float)L[j + i * n]);
+  };
+  put(m.A, dx * dx);
+  put(m.b, dx);
+  put(m.Q, dx * dx);
+  put(m.H, dy * dx);
+  put(m.c, dy);
+  put(m.R, dy * dy);
+  put(m.mu0, dx);
+  put(m.Sigma0, dx * dx);
+  putT(LQ, dx);
+  putT(LR, dy);
+  putT(L0, dx);
+  return GF_OK;
 }
 
 }  // namespace gf
@@ -617,7 +679,6 @@ static void kf_release(gf_kf_plan* p) {
   p->bufs.clear();
 }
 
-static int default_group(int dxp) { return dxp <= 8 ? 32 : (dxp <= 16 ? 128 : 256); }
 
 static void kf_launch_bucket(gf_kf_plan* p, const gf_kf_plan::Bucket& bk, const KfRun& base,
                              cudaStream_t s) {
@@ -841,15 +902,11 @@ extern "C" gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_mo
   for (int f = 0; f < B; ++f) {
     const gf_lg_model& m = models[f];
     if (m.dx < 1 || m.dy < 1 || T[f] < 1) return set_err(ctx, GF_ERR_DIM, "filter %d: bad dims/T", f);
-    int kidx = -1;
-    for (size_t k = 0; k < bks.size(); ++k)
-      if (bks[k].dxp >= m.dx && bks[k].dyp >= m.dy) {
-        kidx = (int)k;
-        break;
-      }
+    const int kidx = kf_bucket_for(m.dx, m.dy);
     if (kidx < 0) return set_err(ctx, GF_ERR_DIM, "filter %d: dx=%d dy=%d exceeds 32", f, m.dx, m.dy);
     members[kidx].push_back(f);
     KfDesc& d = p->hdesc[f];
+    std::memset(&d, 0, sizeof d);
     d.dx = m.dx;
     d.dy = m.dy;
     d.T = T[f];
@@ -860,28 +917,8 @@ extern "C" gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_mo
     d.coff = coff;
     d.index = f;
     const int dx = m.dx, dy = m.dy;
-    std::vector<double> LQ(dx * dx), LR(dy * dy), L0(dx * dx);
-    bool bad = chol_lower(dx, m.Q, LQ.data()) || chol_lower(dy, m.R, LR.data()) ||
-               chol_lower(dx, m.Sigma0, L0.data());
-    if (bad && algo == GF_ALGO_SRKF) return set_err(ctx, GF_ERR_NOT_PD, "filter %d: Q, R or Sigma0 not PD", f);
-    auto put = [&](const double* a, int n) {
-      for (int i = 0; i < n; ++i) pool.push_back((float)a[i]);
-    };
-    auto putT = [&](const std::vector<double>& L, int n) {  // upper factor U = L'
-      for (int j = 0; j < n; ++j)
-        for (int i = 0; i < n; ++i) pool.push_back((float)L[j + i * n]);
-    };
-    put(m.A, dx * dx);
-    put(m.b, dx);
-    put(m.Q, dx * dx);
-    put(m.H, dy * dx);
-    put(m.c, dy);
-    put(m.R, dy * dy);
-    put(m.mu0, dx);
-    put(m.Sigma0, dx * dx);
-    putT(LQ, dx);
-    putT(LR, dy);
-    putT(L0, dx);
+    gf_status pst = kf_pack_model(ctx, algo, m, f, pool);
+    if (pst) return pst;
     poff += kf_param_len(dx, dy);
     yoff += (int64_t)T[f] * dy;
     soff += T[f];
@@ -903,7 +940,7 @@ extern "C" gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_mo
     });
     gf_kf_plan::Bucket bk;
     bk.kidx = (int)k;
-    bk.group = default_group(bks[k].dxp);
+    bk.group = kf_default_group((int)k);
     bk.start = (int)p->horder.size();
     bk.count = (int)mem.size();
     p->horder.insert(p->horder.end(), mem.begin(), mem.end());

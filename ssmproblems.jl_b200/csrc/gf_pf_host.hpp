@@ -46,3 +46,43 @@ void launch_prep(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int T, int dx, int
                  int dyp, const double* pp, void* out);
 
 }  // namespace gf
+
+namespace gf {
+
+// Rao-Blackwellised PF kernels of one compiled (dxo, dz, dy).
+struct RbKernels {
+  int dxo, dz, dy;
+  void (*prop)(const PfJob*, int, float, int, int);
+  void (*init)(const PfJob*, int);
+};
+bool pick_rb(int dxo, int dz, int dy, RbKernels* out);
+gf_status rb_pack_params(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_config* cfg,
+                         std::vector<float>& P, double* prop_const);
+
+}  // namespace gf
+
+#include "gf_pf_kernels.cuh"
+
+namespace gf {
+
+// Everything of one linear-Gaussian PF job that does not depend on its device
+// buffers: kernels (the propagate variant a plan picks for `flags`), packed
+// parameters, the observation-prep block, the step-1 decision and the job
+// descriptor's scalar fields.  Plans and the serving loop share it, so a
+// served filter computes exactly what a standalone run computes.
+struct LgJobSetup {
+  bool dbl = false;
+  PfLgKernels k;
+  void (*prop)(const PfJob*, int) = nullptr;
+  int threads = 0;
+  size_t smem = 0;
+  std::vector<char> params;
+  std::vector<double> pp;
+  double ess1 = 0.0;
+  int8_t res1 = 0;
+  PfJob J;
+};
+gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg, int32_t T,
+                       int32_t flags, LgJobSetup* out);
+
+}  // namespace gf

@@ -66,16 +66,79 @@ static gf_status validate_cfg(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_con
   return GF_OK;
 }
 
+namespace gf {
+
+gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg, int32_t T,
+                       int32_t flags, LgJobSetup* o) {
+  gf_status st = validate_cfg(ctx, m, cfg, T);
+  if (st) return st;
+  o->dbl = cfg->precision == GF_PREC_F64;
+  const bool guided = cfg->proposal != GF_PROP_BOOTSTRAP;
+  if (!pick_lg_kernels(o->dbl, guided, m->dx, m->dy, &o->k))
+    return set_err(ctx, GF_ERR_DIM, "no kernel for dx=%d dy=%d in %s", m->dx, m->dy,
+                   o->dbl ? "FP64 (max 16)" : "FP32 (max 64)");
+  LgFactors f;
+  if ((st = build_lg_factors(ctx, m, cfg, &f))) return st;
+  o->params.clear();
+  pack_params(f, o->dbl, o->k.dxp, o->k.dyp, o->params);
+  o->pp.clear();
+  o->pp.insert(o->pp.end(), f.LRi.begin(), f.LRi.end());
+  o->pp.insert(o->pp.end(), f.c.begin(), f.c.end());
+  o->pp.insert(o->pp.end(), f.K.begin(), f.K.end());
+  o->pp.insert(o->pp.end(), f.vb.begin(), f.vb.end());
+  if (o->k.prop_tc && !(flags & GF_PLAN_SIMT)) {
+    o->prop = o->k.prop_tc;
+    o->threads = 128;
+    o->smem = o->k.tc_smem;
+  } else {
+    o->prop = o->k.prop;
+    o->threads = PF_THREADS;
+    o->smem = o->k.smem;
+  }
+  const int64_t N = cfg->n_particles;
+  // step-1 decision with the reference's uniform-weight ESS
+  o->ess1 = uniform_ess(N);
+  const int sch0 = cfg->schedule ? cfg->schedule[0] : -1;
+  o->res1 = (int8_t)(sch0 >= 0 ? (sch0 != 0) : (cfg->threshold * (double)N >= o->ess1));
+  PfJob& J = o->J;
+  std::memset(&J, 0, sizeof J);
+  J.N = N;
+  J.dx = m->dx;
+  J.dy = m->dy;
+  J.T = T;
+  J.width = m->dx;
+  J.ntiles = (int)((N + PF_TILE - 1) / PF_TILE);
+  J.nstiles = (int)((N + SCAN_TILE - 1) / SCAN_TILE);
+  J.resampler = cfg->resampler;
+  J.conv = cfg->convention;
+  J.prop = cfg->proposal;
+  bool diag = true;
+  for (int j = 0; j < m->dx; ++j)
+    for (int i = 0; i < m->dx; ++i)
+      if (i != j && f.L[i + j * m->dx] != 0.0) diag = false;
+  J.diag_l = diag ? 1 : 0;
+  J.threshold = cfg->threshold;
+  J.log_n = std::log((double)N);
+  J.obs_const = f.obs_const;
+  J.prop_const = f.prop_const;
+  J.seed = cfg->seed;
+  J.ystride = o->k.dyp + o->k.dxp;
+  return GF_OK;
+}
+
+}  // namespace gf
+
 extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg,
                                        int32_t T, int32_t flags, gf_pf_plan** out) {
   if (!ctx || !out) return GF_ERR_ARG;
   *out = nullptr;
-  gf_status st = validate_cfg(ctx, m, cfg, T);
+  LgJobSetup L;
+  gf_status st = lg_job_setup(ctx, m, cfg, T, flags, &L);
   if (st) return st;
   cudaSetDevice(ctx->device);
   auto p = std::make_unique<gf_pf_plan>();
   p->ctx = ctx;
-  p->dbl = cfg->precision == GF_PREC_F64;
+  p->dbl = L.dbl;
   p->dx = m->dx;
   p->dy = m->dy;
   p->T = T;
@@ -84,31 +147,18 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   p->use_graph = !(flags & GF_PLAN_NO_GRAPH);
   if (cfg->schedule) p->sched.assign(cfg->schedule, cfg->schedule + T);
   p->cfg.schedule = nullptr;
-  const bool guided = cfg->proposal != GF_PROP_BOOTSTRAP;
-  if (!pick_lg_kernels(p->dbl, guided, m->dx, m->dy, &p->k))
-    return set_err(ctx, GF_ERR_DIM, "no kernel for dx=%d dy=%d in %s", m->dx, m->dy,
-                   p->dbl ? "FP64 (max 16)" : "FP32 (max 64)");
-  LgFactors f;
-  if ((st = build_lg_factors(ctx, m, cfg, &f))) return st;
-  std::vector<char> params;
-  pack_params(f, p->dbl, p->k.dxp, p->k.dyp, params);
-  std::vector<double> pp;
-  pp.insert(pp.end(), f.LRi.begin(), f.LRi.end());
-  pp.insert(pp.end(), f.c.begin(), f.c.end());
-  pp.insert(pp.end(), f.K.begin(), f.K.end());
-  pp.insert(pp.end(), f.vb.begin(), f.vb.end());
-
+  p->k = L.k;
   p->rsize = p->dbl ? 8 : 4;
   const int64_t N = p->N;
-  p->ntiles = (int)((N + PF_TILE - 1) / PF_TILE);
-  p->nstiles = (int)((N + SCAN_TILE - 1) / SCAN_TILE);
-  const int ystride = p->k.dyp + p->k.dxp;
+  p->ntiles = L.J.ntiles;
+  p->nstiles = L.J.nstiles;
+  const int ystride = L.J.ystride;
   void* v;
 #define ALLOC(field, bytes)                                              \
   if ((st = plan_alloc(p.get(), (bytes), &v))) { plan_release(p.get()); return st; } \
   p->field = decltype(p->field)(v);
-  ALLOC(params, params.size());
-  ALLOC(pp, sizeof(double) * pp.size());
+  ALLOC(params, L.params.size());
+  ALLOC(pp, sizeof(double) * L.pp.size());
   ALLOC(ystep, p->rsize * (size_t)T * ystride);
   ALLOC(X0, p->rsize * (size_t)N * m->dx);
   ALLOC(X1, p->rsize * (size_t)N * m->dx);
@@ -128,58 +178,22 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   if (!p->sched.empty()) { ALLOC(sched_dev, (size_t)T); }
 #undef ALLOC
   cudaStream_t s = ctx->stream;
-  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->params, params.data(), params.size(), cudaMemcpyHostToDevice, s));
-  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->pp, pp.data(), sizeof(double) * pp.size(), cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->params, L.params.data(), L.params.size(), cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->pp, L.pp.data(), sizeof(double) * L.pp.size(), cudaMemcpyHostToDevice, s));
   if (p->sched_dev)
     GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->sched_dev, p->sched.data(), (size_t)T, cudaMemcpyHostToDevice, s));
-  // step-1 decision with the reference's uniform-weight ESS
-  double ess1 = uniform_ess(N);
-  int sch0 = p->sched.empty() ? -1 : p->sched[0];
-  int8_t res1 = (int8_t)(sch0 >= 0 ? (sch0 != 0) : (cfg->threshold * (double)N >= ess1));
-  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->ess1, &ess1, sizeof(double), cudaMemcpyHostToDevice, s));
-  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->res1, &res1, 1, cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->ess1, &L.ess1, sizeof(double), cudaMemcpyHostToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->res1, &L.res1, 1, cudaMemcpyHostToDevice, s));
   GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
-  if (p->k.prop_tc && !(flags & GF_PLAN_SIMT)) {
-    p->prop_fn = p->k.prop_tc;
-    p->prop_threads = 128;
-    p->prop_smem = p->k.tc_smem;
-  } else {
-    p->prop_fn = p->k.prop;
-    p->prop_threads = PF_THREADS;
-    p->prop_smem = p->k.smem;
-  }
+  p->prop_fn = L.prop;
+  p->prop_threads = L.threads;
+  p->prop_smem = L.smem;
   GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)p->prop_fn,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->prop_smem));
-
   PfJob& J = p->job;
-  std::memset(&J, 0, sizeof J);
-  J.N = N;
-  J.dx = m->dx;
-  J.dy = m->dy;
-  J.T = T;
-  J.width = m->dx;
-  J.tile0 = 0;
-  J.ntiles = p->ntiles;
-  J.stile0 = 0;
-  J.nstiles = p->nstiles;
-  J.resampler = cfg->resampler;
-  J.conv = cfg->convention;
-  J.prop = cfg->proposal;
-  {
-    bool diag = true;
-    for (int j = 0; j < m->dx; ++j)
-      for (int i = 0; i < m->dx; ++i)
-        if (i != j && f.L[i + j * m->dx] != 0.0) diag = false;
-    J.diag_l = diag ? 1 : 0;
-  }
-  J.threshold = cfg->threshold;
-  J.log_n = std::log((double)N);
-  J.obs_const = f.obs_const;
-  J.prop_const = f.prop_const;
-  J.seed = cfg->seed;
+  J = L.J;
   J.params = p->params;
   J.ystep = p->ystep;
-  J.ystride = ystride;
   J.X[0] = p->X0;
   J.X[1] = p->X1;
   J.lw = p->lw;

@@ -352,18 +352,12 @@ __global__ void __launch_bounds__(PF_THREADS) rbpf_init(const PfJob* __restrict_
   }
 }
 
-struct RbKernels {
-  int dxo, dz, dy;
-  void (*prop)(const PfJob*, int, float, int, int);
-  void (*init)(const PfJob*, int);
-};
-
 template <int A, int B, int C>
 static RbKernels make_rb() {
   return {A, B, C, rbpf_propagate<A, B, C>, rbpf_init<A, B, C>};
 }
 
-static bool pick_rb(int dxo, int dz, int dy, RbKernels* out) {
+bool pick_rb(int dxo, int dz, int dy, RbKernels* out) {
   static const RbKernels tab[] = {make_rb<1, 1, 1>(), make_rb<1, 2, 1>(), make_rb<2, 2, 2>(),
                                   make_rb<2, 4, 2>(), make_rb<2, 8, 4>()};
   for (const auto& k : tab)
@@ -374,27 +368,12 @@ static bool pick_rb(int dxo, int dz, int dy, RbKernels* out) {
   return false;
 }
 
-}  // namespace gf
 
-using namespace gf;
-
-extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_config* cfg,
-                                 int32_t T, const double* ys, const void* noise,
-                                 const double* uniforms, int32_t memspace, gf_pf_out* out,
-                                 double* zmeans) {
-  if (!ctx || !m || !cfg || !out || !ys || !out->ll)
-    return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
-  if (cfg->precision != GF_PREC_F32) return set_err(ctx, GF_ERR_UNSUPPORTED, "RBPF runs in FP32 only");
-  if (cfg->proposal == GF_PROP_OPTIMAL)
-    return set_err(ctx, GF_ERR_UNSUPPORTED, "RBPF supports bootstrap and overdispersed outer proposals");
-  if (cfg->n_particles < 1 || T < 1) return set_err(ctx, GF_ERR_ARG, "bad N or T");
-  RbKernels K;
-  if (!pick_rb(m->dxo, m->dz, m->dy, &K))
-    return set_err(ctx, GF_ERR_DIM, "no RBPF kernel for (dxo, dz, dy) = (%d, %d, %d)", m->dxo, m->dz, m->dy);
-  cudaSetDevice(ctx->device);
+// Parameters (float) in RbLayout order, with the outer Cholesky factors and the
+// proposal's log-normaliser difference.
+gf_status rb_pack_params(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_config* cfg,
+                         std::vector<float>& P, double* prop_const_out) {
   const int dxo = m->dxo, dz = m->dz, dy = m->dy;
-  const int NS = dz * (dz + 1) / 2, width = dxo + dz + NS;
-  // ---- parameters (float), same order as RbLayout
   std::vector<double> Lo(dxo * dxo), L0o(dxo * dxo), LQi(dxo * dxo), Lq(dxo * dxo);
   if (chol_lower(dxo, m->Q_o, Lo.data()) || chol_lower(dxo, m->Sigma_o, L0o.data()))
     return set_err(ctx, GF_ERR_NOT_PD, "outer Q or Sigma not positive definite");
@@ -403,7 +382,6 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   for (int i = 0; i < dxo * dxo; ++i) Lq[i] = std::sqrt(kk) * Lo[i];
   double prop_const = 0.0;
   for (int i = 0; i < dxo; ++i) prop_const += std::log(Lq[i + i * dxo]) - std::log(Lo[i + i * dxo]);
-  std::vector<float> P;
   auto put = [&](const double* a, int n) {
     for (int i = 0; i < n; ++i) P.push_back((float)a[i]);
   };
@@ -430,6 +408,34 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   put(m->mu_z, dz);
   put_packed(m->Sigma_z, dz);
 
+  *prop_const_out = prop_const;
+  return GF_OK;
+}
+
+}  // namespace gf
+
+using namespace gf;
+
+extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_config* cfg,
+                                 int32_t T, const double* ys, const void* noise,
+                                 const double* uniforms, int32_t memspace, gf_pf_out* out,
+                                 double* zmeans) {
+  if (!ctx || !m || !cfg || !out || !ys || !out->ll)
+    return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
+  if (cfg->precision != GF_PREC_F32) return set_err(ctx, GF_ERR_UNSUPPORTED, "RBPF runs in FP32 only");
+  if (cfg->proposal == GF_PROP_OPTIMAL)
+    return set_err(ctx, GF_ERR_UNSUPPORTED, "RBPF supports bootstrap and overdispersed outer proposals");
+  if (cfg->n_particles < 1 || T < 1) return set_err(ctx, GF_ERR_ARG, "bad N or T");
+  RbKernels K;
+  if (!pick_rb(m->dxo, m->dz, m->dy, &K))
+    return set_err(ctx, GF_ERR_DIM, "no RBPF kernel for (dxo, dz, dy) = (%d, %d, %d)", m->dxo, m->dz, m->dy);
+  cudaSetDevice(ctx->device);
+  const int dxo = m->dxo, dz = m->dz, dy = m->dy;
+  const int NS = dz * (dz + 1) / 2, width = dxo + dz + NS;
+  std::vector<float> P;
+  double prop_const = 0.0;
+  gf_status st;
+  if ((st = rb_pack_params(ctx, m, cfg, P, &prop_const))) return st;
   const int64_t N = cfg->n_particles;
   const int ntiles = (int)((N + PF_TILE - 1) / PF_TILE);
   const int nstiles = (int)((N + SCAN_TILE - 1) / SCAN_TILE);
@@ -442,7 +448,6 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
       for (auto& b : *v) dev_free(c, b.p, b.bytes);
     }
   } cleanup{ctx, &bufs};
-  gf_status st;
   auto get = [&](size_t bytes, void** d) -> gf_status {
     gf_status s2 = dev_alloc(ctx, bytes, d);
     if (!s2 && *d) bufs.push_back({*d, bytes});

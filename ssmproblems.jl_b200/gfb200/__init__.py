@@ -18,3 +18,4 @@ from .models import (HierarchicalSSM, HomogeneousGaussianPrior,  # noqa: F401
                      HomogeneousLinearGaussianObservationProcess, InnerDynamics,
                      LatentDynamics, ObservationProcess, StatePrior, StateSpaceModel,
                      create_homogeneous_linear_gaussian_model)
+from .serving import Server  # noqa: F401,E402

@@ -23,6 +23,7 @@ GF_PREC_F32, GF_PREC_F64 = 0, 1
 GF_PROP_BOOTSTRAP, GF_PROP_OPTIMAL, GF_PROP_OVERDISPERSED = 0, 1, 2
 GF_ALGO_KF, GF_ALGO_SRKF = 0, 1
 GF_PLAN_AUTOTUNE, GF_PLAN_NO_GRAPH, GF_PLAN_PLAIN, GF_PLAN_SIMT = 1, 2, 4, 8
+GF_REQ_KF, GF_REQ_SRKF, GF_REQ_PF, GF_REQ_RBPF = 0, 1, 2, 3
 
 EXPORTED = [
     "gf_ctx_create", "gf_ctx_destroy", "gf_last_error", "gf_ctx_set_stream", "gf_ctx_get_stream",
@@ -31,6 +32,8 @@ EXPORTED = [
     "gf_pf_run", "gf_pf_plan_create", "gf_pf_plan_run", "gf_pf_plan_destroy", "gf_rbpf_run",
     "gf_sample_ancestors", "gf_offspring_to_ancestors", "gf_ancestors_to_offspring",
     "gf_rng_normals", "gf_sample_ancestors_noalloc", "gf_sample_ancestors_noalloc_max_n",
+    "gf_srv_create", "gf_srv_submit", "gf_srv_poll", "gf_srv_drain", "gf_srv_stats",
+    "gf_srv_reset_stats", "gf_srv_last_error", "gf_srv_destroy",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -65,6 +68,34 @@ class PFOutC(C.Structure):
 
 class KFOutC(C.Structure):
     _fields_ = [("ll", _vp), ("ll_steps", _vp), ("means", _vp), ("covs", _vp), ("status", _vp)]
+
+
+class SrvConfigC(C.Structure):
+    _fields_ = [("device", C.c_int32), ("hbm_budget_bytes", C.c_size_t),
+                ("host_budget_bytes", C.c_size_t), ("max_pending", C.c_int32),
+                ("pf_chunk", C.c_int32), ("kf_streams", C.c_int32), ("max_active_pf", C.c_int32)]
+
+
+class SrvRequestC(C.Structure):
+    _fields_ = [("kind", C.c_int32), ("T", C.c_int32), ("lg", C.POINTER(LGModelC)),
+                ("rb", C.POINTER(RBModelC)), ("pf", C.POINTER(PFConfigC)), ("ys", _dp),
+                ("jitter", C.c_double), ("use_jitter", C.c_int32), ("reserved", C.c_int32),
+                ("ll_steps", _dp), ("mean", _dp), ("cov", _dp), ("tag", C.c_uint64)]
+
+
+class SrvResultC(C.Structure):
+    _fields_ = [("id", C.c_uint64), ("tag", C.c_uint64), ("status", C.c_int32),
+                ("kind", C.c_int32), ("ll", C.c_double), ("submit_ms", C.c_double),
+                ("start_ms", C.c_double), ("done_ms", C.c_double)]
+
+
+class SrvMetricsC(C.Structure):
+    _fields_ = ([(n, C.c_int64) for n in ("submitted", "completed", "failed", "rejected",
+                                          "pending", "running")]
+                + [(n, C.c_double) for n in ("p50_ms", "p99_ms", "mean_ms", "max_ms", "kf_steps",
+                                             "particle_steps", "elapsed_ms")]
+                + [(n, C.c_size_t) for n in ("hbm_budget", "hbm_used", "hbm_peak")]
+                + [(n, C.c_int64) for n in ("pf_iterations", "kf_batches", "launches")])
 
 
 class GFError(RuntimeError):
@@ -123,6 +154,14 @@ def load(path: str | None = None):
         "gf_rng_normals": (i32, [ctxp, u64, i32, i32, i64, i32, _vp]),
         "gf_sample_ancestors_noalloc": (i32, [i32, i32, i64, _vp, _vp, _vp, _vp]),
         "gf_sample_ancestors_noalloc_max_n": (i64, []),
+        "gf_srv_create": (i32, [C.POINTER(SrvConfigC), C.POINTER(_vp)]),
+        "gf_srv_submit": (i32, [_vp, C.POINTER(SrvRequestC), C.POINTER(u64)]),
+        "gf_srv_poll": (i32, [_vp, C.POINTER(SrvResultC), i32, i32]),
+        "gf_srv_drain": (i32, [_vp, i32]),
+        "gf_srv_stats": (i32, [_vp, C.POINTER(SrvMetricsC)]),
+        "gf_srv_reset_stats": (i32, [_vp]),
+        "gf_srv_last_error": (C.c_char_p, [_vp]),
+        "gf_srv_destroy": (i32, [_vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)
