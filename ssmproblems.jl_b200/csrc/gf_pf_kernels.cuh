@@ -22,6 +22,8 @@ constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_IPT = 16;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_IPT;
 constexpr int PF_PW = 6;                       // doubles per block partial
+constexpr int FILL_D = 2 * PF_TILE;            // merge items (particles + slots) per fill block
+constexpr int FILL_IPT = FILL_D / PF_THREADS;  // merge items per fill thread
 constexpr unsigned long long kReady = 1ull << 63;
 constexpr double kFix = 4611686018427387904.0; // 2^62
 constexpr double kInvFix = 1.0 / 4611686018427387904.0;
@@ -59,7 +61,7 @@ struct PfJob {
   const double* wraw;        // nullable: scan raw weights wraw[k] / sc->wtotal instead of exp(lw - LSE)
   double* tprefix;           // [ntiles + 1] cumulative normalised weight at each tile start
   int32_t* ocum;             // [N] cumulative offspring counts of the pending resample
-  int32_t* tocum;            // [ntiles + 1] particle whose offspring run covers slot b * PF_TILE
+  int32_t* mpk;              // [ntiles + 1] merge-path start particle of each fill block
   int32_t* anc;              // [N] 0-based ancestors of the pending resample
 };
 
@@ -353,155 +355,158 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
 // Runs after a propagate whose finalise decided to resample: per propagate
 // tile, the cumulative normalised weights W_k = P_b + (running sum inside the
 // tile) and each particle's cumulative offspring count O(W_k) (exact per
-// rule); the next propagate turns the counts into ancestors (tile_ancestors).
+// rule) and the merge-path start points of the fill kernel, which turns the
+// counts into ancestors.
 // Multinomial ancestors (unsorted uniforms) instead take W_k to the per-slot
 // search of the next propagate.
 template <typename Real>
-__global__ void __launch_bounds__(PF_THREADS) pf_resample_kernel(const PfJob* __restrict__ jobs,
-                                                                int njobs) {
+__global__ void __launch_bounds__(PF_THREADS, 6) pf_resample_kernel(const PfJob* __restrict__ jobs,
+                                                                   int njobs) {
   const int jb = find_job(jobs, njobs, blockIdx.x, false);
   const PfJob& J = jobs[jb];
   PfScalars* sc = J.sc;
   if (!sc->resample || sc->status != 0 || sc->t >= J.T) return;
-  // shared layouts padded one slot per 4 (thread-contiguous runs of 4 with few bank conflicts)
-  __shared__ unsigned long long sq64[PF_TILE + PF_TILE / 4];
-  __shared__ double sw[PF_TILE + PF_TILE / 4];
   __shared__ unsigned long long s_wsum[32];
+  __shared__ int32_t s_last[PF_THREADS / 32];
+  __shared__ int32_t s_O0;
   const int tstep = sc->t + 1;
   const int tile = blockIdx.x - J.tile0;
   const int64_t N = J.N, i0 = (int64_t)tile * PF_TILE;
   const int nloc = (int)min((int64_t)PF_TILE, N - i0);
   const double lse = sc->lse;
-  const Real* lw = reinterpret_cast<const Real*>(J.lw);
   const double P0 = J.tprefix[tile], P1 = J.tprefix[tile + 1];
-#pragma unroll
-  for (int p = 0; p < PF_PPT; ++p) {
-    const int l = p * PF_THREADS + threadIdx.x;
-    sq64[l + (l >> 2)] = l < nloc ? __double2ull_rn(exp((double)lw[i0 + l] - lse) * kFix) : 0ull;
-  }
-  __syncthreads();
-  {
-    // W_k = P0 + (fixed-point running sum inside the tile), clamped to the tile's end
-    const int l0 = PF_PPT * threadIdx.x;
-    unsigned long long loc[PF_PPT], acc = 0ull;
-#pragma unroll
-    for (int q = 0; q < PF_PPT; ++q) {
-      const int l = l0 + q;
-      acc += sq64[l + (l >> 2)];
-      loc[q] = acc;
+  // this thread's PF_PPT consecutive particles (vector loads; tiles start 16-byte aligned)
+  const int l0 = PF_PPT * threadIdx.x;
+  const Real* lw = reinterpret_cast<const Real*>(J.lw) + i0 + l0;
+  Real x[PF_PPT];
+  if (l0 + PF_PPT <= nloc) {
+    if constexpr (sizeof(Real) == 4) {
+      const float4 v = *reinterpret_cast<const float4*>(lw);
+      x[0] = v.x, x[1] = v.y, x[2] = v.z, x[3] = v.w;
+    } else {
+      const double2 a = reinterpret_cast<const double2*>(lw)[0], b = reinterpret_cast<const double2*>(lw)[1];
+      x[0] = a.x, x[1] = a.y, x[2] = b.x, x[3] = b.y;
     }
-    unsigned long long all;
-    const unsigned long long excl = block_excl_scan_u64(acc, s_wsum, &all);
+  } else {
 #pragma unroll
-    for (int q = 0; q < PF_PPT; ++q) {
-      const int l = l0 + q;
-      double W = P0 + (double)(excl + loc[q]) * kInvFix;
-      W = W < P1 ? W : P1;
-      if (l == nloc - 1) W = P1;
-      sw[l + (l >> 2)] = W;
-    }
+    for (int q = 0; q < PF_PPT; ++q) x[q] = l0 + q < nloc ? lw[q] : (Real)0;
   }
-  __syncthreads();
+  // W_k = P0 + (fixed-point running sum inside the tile), clamped to the tile's end
+  unsigned long long loc[PF_PPT], acc = 0ull;
+#pragma unroll
+  for (int q = 0; q < PF_PPT; ++q) {
+    if (l0 + q < nloc) acc += __double2ull_rn(exp((double)x[q] - lse) * kFix);
+    loc[q] = acc;
+  }
+  unsigned long long all;
+  const unsigned long long excl = block_excl_scan_u64(acc, s_wsum, &all);
+  auto cumw = [&](int q) {
+    const double W = P0 + (double)(excl + loc[q]) * kInvFix;
+    return (l0 + q == nloc - 1) ? P1 : (W < P1 ? W : P1);
+  };
   if (J.resampler == GF_RS_MULTINOMIAL) {
-    double* __restrict__ key = J.key;
-    for (int l = threadIdx.x; l < nloc; l += PF_THREADS) key[i0 + l] = sw[l + (l >> 2)];
+    double* __restrict__ key = J.key + i0;
+#pragma unroll
+    for (int q = 0; q < PF_PPT; ++q)
+      if (l0 + q < nloc) key[l0 + q] = cumw(q);
     return;
   }
   const OffspringRule rule = make_rule(J, sc, tstep);
-  int32_t* __restrict__ ocum = J.ocum;
-  int32_t* __restrict__ sOc = reinterpret_cast<int32_t*>(sq64);  // counts, reusing the scan buffer
-  __syncthreads();
-  for (int l = threadIdx.x; l < nloc; l += PF_THREADS) {
-    int32_t c = (int32_t)rule.count(sw[l + (l >> 2)]);
-    if (i0 + l == N - 1) {
+  if (threadIdx.x == 0) s_O0 = (int32_t)rule.count(P0);
+  int32_t c[PF_PPT];
+#pragma unroll
+  for (int q = 0; q < PF_PPT; ++q) {
+    c[q] = 0;
+    if (l0 + q >= nloc) continue;
+    c[q] = (int32_t)rule.count(cumw(q));
+    if (i0 + l0 + q == N - 1) {
       // slots past the last threshold below W_N (rounding) go to the last
       // particle; the reference's walk has no clamp, so they are counted
-      if (c < N) atomicAdd(&sc->clamps, (int32_t)(N - c));
-      c = (int32_t)N;
+      if (c[q] < N) atomicAdd(&sc->clamps, (int32_t)(N - c[q]));
+      c[q] = (int32_t)N;
     }
-    sOc[l] = c;
-    ocum[i0 + l] = c;
   }
-  __shared__ int32_t s_O0;
-  if (threadIdx.x == 0) s_O0 = (int32_t)rule.count(P0);
+  int32_t* __restrict__ ocum = J.ocum + i0 + l0;
+  if (l0 + PF_PPT <= nloc) {
+    *reinterpret_cast<int4*>(ocum) = make_int4(c[0], c[1], c[2], c[3]);
+  } else {
+#pragma unroll
+    for (int q = 0; q < PF_PPT; ++q)
+      if (l0 + q < nloc) ocum[q] = c[q];
+  }
+  // count of the particle before this thread's first one
+  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+  int32_t cprev = __shfl_up_sync(0xffffffffu, c[PF_PPT - 1], 1);
+  if (lane == 31) s_last[wid] = c[PF_PPT - 1];
   __syncthreads();
-  // the particle whose slot run [O_{k-1}, O_k) covers a chunk start c * PF_TILE
-  for (int l = threadIdx.x; l < nloc; l += PF_THREADS) {
-    const int32_t lo = l == 0 ? s_O0 : sOc[l - 1], hi = sOc[l];
-    for (int64_t c0 = ((int64_t)lo + PF_TILE - 1) / PF_TILE * PF_TILE; c0 < hi; c0 += PF_TILE)
-      J.tocum[c0 / PF_TILE] = (int32_t)(i0 + l);
+  if (lane == 0) cprev = wid == 0 ? s_O0 : s_last[wid - 1];
+  // Merge-path partition of the fill: merging particles (consumed when all
+  // their slots are out) with slots j (slot j belongs to the first k with
+  // O_k > j), the state after d items has consumed the largest k with
+  // f(k) = O_{k-1} + k <= d.  f(k+1) - f(k) = offspring_k + 1 >= 1, so the
+  // diagonals d in [f(k), f(k+1)) start at particle k; fill block m starts at
+  // diagonal m * FILL_D.
+#pragma unroll
+  for (int q = 0; q < PF_PPT; ++q) {
+    if (l0 + q >= nloc) break;
+    const int64_t k = i0 + l0 + q;
+    const int64_t flo = (int64_t)(q == 0 ? cprev : c[q - 1]) + k;
+    const int64_t fhi = (int64_t)c[q] + k + 1;
+    for (int64_t d = (flo + FILL_D - 1) / FILL_D * FILL_D; d < fhi; d += FILL_D)
+      J.mpk[d / FILL_D] = (int32_t)k;
   }
 }
 
-// Ancestors (0-based) of the block's PF_TILE slots from the cumulative
-// offspring counts: slot j's ancestor is the first k with ocum[k] > j (the
-// cumulative-offspring form of CUDAExt.jl:90-103).  The particles covering the
-// block's first slot and the next block's first slot bound the search; the
-// range is staged in shared memory when it is short, and every slot then
-// binary-searches it -- balanced however the offspring are distributed.
-constexpr int ANC_STAGE = 4096;
-static __device__ void tile_ancestors(const PfJob& J, int tile, int32_t* s_anc, int32_t* s_oc);
-
-// Fill kernel: per block of PF_TILE slots, ancestors from the cumulative counts
-// (tile_ancestors) written to J.anc, which the next propagate reads coalesced.
+// Fill kernel: ancestors (0-based) of every slot from the cumulative offspring
+// counts (slot j's ancestor is the first k with ocum[k] > j, the cumulative-
+// offspring form of CUDAExt.jl:90-103), written to J.anc, which the next
+// propagate reads coalesced.  Block m merges exactly FILL_D items (particles
+// plus slots) starting at its merge-path point, so the work is balanced
+// however the offspring are distributed: at most FILL_D + 1 counts are staged
+// in shared memory, each thread binary-searches its own start and merges
+// FILL_IPT items, and the block's slots are written out coalesced.
 template <int DUMMY = 0>
-__global__ void __launch_bounds__(PF_THREADS) pf_fill_ancestors_kernel(const PfJob* __restrict__ jobs,
+__global__ void __launch_bounds__(PF_THREADS, 8) pf_fill_ancestors_kernel(const PfJob* __restrict__ jobs,
                                                                       int njobs) {
   const int jb = find_job(jobs, njobs, blockIdx.x, false);
   const PfJob& J = jobs[jb];
   const PfScalars* sc = J.sc;
   if (!sc->resample || sc->status != 0 || sc->t >= J.T || J.resampler == GF_RS_MULTINOMIAL) return;
-  __shared__ int32_t s_anc[PF_TILE];
-  __shared__ int32_t s_oc[ANC_STAGE];
-  const int tile = blockIdx.x - J.tile0;
-  tile_ancestors(J, tile, s_anc, s_oc);
-  const int64_t i0 = (int64_t)tile * PF_TILE;
-  const int nloc = (int)min((int64_t)PF_TILE, J.N - i0);
-  int32_t* __restrict__ anc = J.anc;
-  for (int l = threadIdx.x; l < nloc; l += PF_THREADS) anc[i0 + l] = s_anc[l];
-}
-
-static __device__ void tile_ancestors(const PfJob& J, int tile, int32_t* s_anc, int32_t* s_oc) {
-  __shared__ int64_t s_k[2];
+  __shared__ int32_t s_oc[FILL_D + 1];
+  __shared__ int32_t s_anc[FILL_D];
+  const int m = blockIdx.x - J.tile0;
   const int64_t N = J.N;
-  const int64_t j0 = (int64_t)tile * PF_TILE;
-  const int64_t jl = min(j0 + PF_TILE, N) - 1;
+  const int64_t d0 = (int64_t)m * FILL_D, d1 = min(d0 + FILL_D, 2 * N);
+  const int64_t k0 = J.mpk[m];
+  const int64_t k1 = m + 1 < J.ntiles ? (int64_t)J.mpk[m + 1] : N;
+  const int64_t j0 = d0 - k0, j1 = d1 - k1;
+  const int nk = (int)(min(k1, N - 1) - k0 + 1);  // counts ocum[k0 .. min(k1, N-1)]
   const int32_t* __restrict__ oc = J.ocum;
-  if (threadIdx.x == 0) {
-    s_k[0] = J.tocum[tile];
-    s_k[1] = tile + 1 < J.ntiles ? (int64_t)J.tocum[tile + 1] : N - 1;
-  }
+  for (int q = threadIdx.x; q < nk; q += PF_THREADS) s_oc[q] = oc[k0 + q];
   __syncthreads();
-  const int64_t kf = s_k[0], kl = s_k[1];
-  const int64_t R = kl - kf + 1;
-  if (R <= ANC_STAGE) {
-    for (int q = threadIdx.x; q < (int)R; q += blockDim.x) s_oc[q] = oc[kf + q];
-    __syncthreads();
-    for (int l = threadIdx.x; l < PF_TILE; l += blockDim.x) {
-      const int64_t j = j0 + l;
-      if (j > jl) break;
-      int lo = 0, hi = (int)R - 1;
-      while (lo < hi) {
-        const int mid = (lo + hi) >> 1;
-        if (s_oc[mid] > j) hi = mid;
-        else lo = mid + 1;
-      }
-      s_anc[l] = (int32_t)(kf + lo);
+  const int64_t d = d0 + (int64_t)threadIdx.x * FILL_IPT;
+  if (d < d1) {
+    // largest local k in [0, k1 - k0] with f(k0 + k) <= d (f(k0) <= d0 <= d)
+    int lo = 0, hi = (int)(k1 - k0);
+    while (lo < hi) {
+      const int mid = (lo + hi + 1) >> 1;
+      if ((int64_t)s_oc[mid - 1] + k0 + mid <= d) lo = mid;
+      else hi = mid - 1;
     }
-  } else {
-    for (int l = threadIdx.x; l < PF_TILE; l += blockDim.x) {
-      const int64_t j = j0 + l;
-      if (j > jl) break;
-      int64_t lo = kf, hi = kl;
-      while (lo < hi) {
-        const int64_t mid = (lo + hi) >> 1;
-        if (oc[mid] > j) hi = mid;
-        else lo = mid + 1;
+    int64_t k = k0 + lo, j = d - k;
+    const int64_t de = min(d + FILL_IPT, d1);
+    for (int64_t e = d; e < de; ++e) {
+      if (k < N && j < (int64_t)s_oc[k - k0]) {
+        s_anc[j - j0] = (int32_t)k;
+        ++j;
+      } else {
+        ++k;
       }
-      s_anc[l] = (int32_t)lo;
     }
   }
   __syncthreads();
+  int32_t* __restrict__ anc = J.anc;
+  for (int q = threadIdx.x; q < (int)(j1 - j0); q += PF_THREADS) anc[j0 + q] = s_anc[q];
 }
 
 // ------------------------------------------------------------ lookback scan

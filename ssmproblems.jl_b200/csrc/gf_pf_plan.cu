@@ -25,7 +25,7 @@ struct gf_pf_plan {
   void *params = nullptr, *ystep = nullptr, *X0 = nullptr, *X1 = nullptr, *lw = nullptr;
   double *pp = nullptr, *key = nullptr, *part = nullptr, *mpart = nullptr, *ess1 = nullptr;
   double* tprefix = nullptr;
-  int32_t *ocum = nullptr, *tocum = nullptr, *anc = nullptr;
+  int32_t *ocum = nullptr, *mpk = nullptr, *anc = nullptr;
   unsigned long long* flags = nullptr;
   PfScalars* sc = nullptr;
   int8_t *sched_dev = nullptr, *res1 = nullptr;
@@ -165,7 +165,7 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   ALLOC(lw, p->rsize * (size_t)N);
   ALLOC(key, sizeof(double) * (size_t)N);
   ALLOC(ocum, sizeof(int32_t) * (size_t)N);
-  ALLOC(tocum, sizeof(int32_t) * (size_t)(p->ntiles + 1));
+  ALLOC(mpk, sizeof(int32_t) * (size_t)(p->ntiles + 1));
   ALLOC(anc, sizeof(int32_t) * (size_t)N);
   ALLOC(tprefix, sizeof(double) * (size_t)(p->ntiles + 1));
   ALLOC(part, sizeof(double) * PF_PW * (size_t)p->ntiles);
@@ -202,7 +202,7 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   J.flags = p->flags;
   J.sc = p->sc;
   J.ocum = p->ocum;
-  J.tocum = p->tocum;
+  J.mpk = p->mpk;
   J.anc = p->anc;
   J.tprefix = p->tprefix;
   J.schedule = p->sched_dev;

@@ -454,7 +454,7 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
     return s2;
   };
   void *d_params, *X0, *X1, *lw, *key, *part, *mpart, *flags, *scv, *ess1, *res1, *jobv, *schedv = nullptr;
-  void *ancv, *tprev, *tocv, *fillv;
+  void *ancv, *tprev, *mpkv, *fillv;
   if ((st = get(sizeof(float) * P.size(), &d_params))) return st;
   if ((st = get(sizeof(float) * (size_t)N * width, &X0))) return st;
   if ((st = get(sizeof(float) * (size_t)N * width, &X1))) return st;
@@ -462,7 +462,7 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   if ((st = get(sizeof(double) * (size_t)N, &key))) return st;
   if ((st = get(sizeof(int32_t) * (size_t)N, &ancv))) return st;
   if ((st = get(sizeof(double) * (size_t)(ntiles + 1), &tprev))) return st;
-  if ((st = get(sizeof(int32_t) * (size_t)(ntiles + 1), &tocv))) return st;
+  if ((st = get(sizeof(int32_t) * (size_t)(ntiles + 1), &mpkv))) return st;
   if ((st = get(sizeof(int32_t) * (size_t)N, &fillv))) return st;
   if ((st = get(sizeof(double) * PF_PW * ntiles, &part))) return st;
   if ((st = get(sizeof(double) * ntiles * (dxo + dz), &mpart))) return st;
@@ -553,7 +553,7 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   J.flags = (unsigned long long*)flags;
   J.sc = (PfScalars*)scv;
   J.ocum = (int32_t*)ancv;
-  J.tocum = (int32_t*)tocv;
+  J.mpk = (int32_t*)mpkv;
   J.anc = (int32_t*)fillv;
   J.tprefix = (double*)tprev;
   J.noise = d_noise;

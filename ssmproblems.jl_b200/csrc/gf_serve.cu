@@ -138,7 +138,7 @@ struct Req {
   bool have_dev = false, have_pin = false;
   // device piece offsets (relative to the block)
   size_t d_params = 0, d_pp = 0, d_ys = 0, d_ystep = 0, d_X0 = 0, d_X1 = 0, d_lw = 0, d_key = 0,
-         d_ocum = 0, d_anc = 0, d_tocum = 0, d_tpre = 0, d_part = 0, d_mpart = 0, d_flags = 0,
+         d_ocum = 0, d_anc = 0, d_mpk = 0, d_tpre = 0, d_part = 0, d_mpart = 0, d_flags = 0,
          d_sc = 0, d_ess1 = 0, d_res1 = 0, d_job = 0, d_sched = 0, d_steps = 0, d_means = 0;
   // pinned piece offsets
   size_t p_params = 0, p_pp = 0, p_ys = 0, p_sched = 0, p_job = 0, p_e1 = 0, p_rec = 0, p_mu = 0,
@@ -299,7 +299,7 @@ void pf_layout(Req* r, size_t param_bytes, size_t pp_bytes, size_t rsize, int wi
   r->d_key = d.take(sizeof(double) * (size_t)N);
   r->d_ocum = d.take(sizeof(int32_t) * (size_t)N);
   r->d_anc = d.take(sizeof(int32_t) * (size_t)N);
-  r->d_tocum = d.take(sizeof(int32_t) * (size_t)(ntiles + 1));
+  r->d_mpk = d.take(sizeof(int32_t) * (size_t)(ntiles + 1));
   r->d_tpre = d.take(sizeof(double) * (size_t)(ntiles + 1));
   r->d_part = d.take(sizeof(double) * PF_PW * (size_t)ntiles);
   r->d_mpart = d.take(sizeof(double) * (size_t)ntiles * std::max(1, r->mdim));
@@ -487,7 +487,7 @@ gf_status gf_srv::start_pf(Req* r) {
   J.flags = (unsigned long long*)D(r->d_flags);
   J.sc = (PfScalars*)D(r->d_sc);
   J.ocum = (int32_t*)D(r->d_ocum);
-  J.tocum = (int32_t*)D(r->d_tocum);
+  J.mpk = (int32_t*)D(r->d_mpk);
   J.anc = (int32_t*)D(r->d_anc);
   J.tprefix = (double*)D(r->d_tpre);
   J.schedule = r->sched.empty() ? nullptr : (const int8_t*)D(r->d_sched);
