@@ -148,52 +148,52 @@ def bench_pf(args, world, rank, local):
     dev = f"cuda:{local}"
     torch.cuda.set_device(local)
     ctx = G.Context(local)
-    N, T, dx, dy = 2**20, 1000, 16, 8
+    N, T, dx, dy = 2**20, args.pf_T, 16, 8
     model, ys = W.lgssm_rot(seed=1234, dx=dx, dy=dy, T=T)
     algo = G.BF(N, threshold=0.5)
     ys_dev = torch.tensor(ys, dtype=torch.float64, device=dev)
-    plan = PfPlan(model, algo, T, seed=1000 + rank, ctx=ctx, graph=False)
+    # ---- timed region: graph replay of the plan (its normal form), inputs resident in HBM
+    gplan = PfPlan(model, algo, T, seed=1000 + rank, ctx=ctx, graph=True)
     for _ in range(args.warmup):
-        plan.run(ys_dev)
+        gplan.run(ys_dev)
     ctx.synchronize()
-    # ---- timed region (device-resident inputs)
-    ctx.profile(True)
-    _barrier(world)
-    torch.cuda.synchronize()
-    stream_ptr = ctx.stream
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
     ev0 = torch.cuda.Event(enable_timing=True)
     ev1 = torch.cuda.Event(enable_timing=True)
-    ext = torch.cuda.ExternalStream(stream_ptr, device=dev)
+    _barrier(world)
+    torch.cuda.synchronize()
     with ClockSampler(local) as clk:
         ev0.record(ext)
         for _ in range(args.steps):
-            plan.run(ys_dev)
+            gplan.run(ys_dev)
         ev1.record(ext)
         ev1.synchronize()
     torch.cuda.synchronize()
     _barrier(world)
     ms = ev0.elapsed_time(ev1)
+    ms_max = _max_over_ranks(ms, world, dev)
+    n_res = int(gplan.resampled.sum().item())
+    ll = float(gplan.ll.item())
+    gplan.close()
+    # ---- per-kernel durations: the same K runs launched eagerly on the same
+    # stream with CUDA events around every launch (graph nodes cannot be timed)
+    plan = PfPlan(model, algo, T, seed=1000 + rank, ctx=ctx, graph=False)
+    plan.run(ys_dev)
+    ctx.synchronize()
+    ctx.profile(True)
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    p0.record(ext)
+    for _ in range(args.steps):
+        plan.run(ys_dev)
+    p1.record(ext)
+    p1.synchronize()
+    eager_ms = p0.elapsed_time(p1) / args.steps
     prop_ms, prop_n = ctx.profile_read(0)
     scan_ms, scan_n = ctx.profile_read(1)
     prep_ms, prep_n = ctx.profile_read(4)
     fill_ms, fill_n = ctx.profile_read(5)
     ctx.profile(False)
-    ms_max = _max_over_ranks(ms, world, dev)
-    n_res = int(plan.resampled.sum().item())
-    ll = float(plan.ll.item())
-    # graph replay of the same step (information only)
-    gplan = PfPlan(model, algo, T, seed=1000 + rank, ctx=ctx, graph=True)
-    gplan.run(ys_dev)
-    ctx.synchronize()
-    g0 = torch.cuda.Event(enable_timing=True)
-    g1 = torch.cuda.Event(enable_timing=True)
-    g0.record(ext)
-    for _ in range(args.steps):
-        gplan.run(ys_dev)
-    g1.record(ext)
-    g1.synchronize()
-    graph_ms = g0.elapsed_time(g1) / args.steps
-    gplan.close()
     # ---- e2e through the C ABI with pinned host buffers
     import ctypes as C
     ys_pin = torch.tensor(ys, dtype=torch.float64).pin_memory()
@@ -217,20 +217,18 @@ def bench_pf(args, world, rank, local):
     units = N * T * args.steps * world
     value = units / (ms_max / 1e3)
     peak, peak_kind = _peaks()
-    # algorithmic bytes of the propagate launches (FP32 state):
-    #   every launch: state read + write 8*Dx, log-weight write 4
-    #   non-resampling launches: + log-weight read 4
-    #   resampling launches: + cumulative-weight read 8
+    # algorithmic bytes of one propagate launch (FP32 state): state read + write
+    # 8*Dx, log-weight write 4, and either the log-weight read (no resample) or
+    # the ancestor-index read (resample) 4
     launches = T * args.steps
-    res_launches = n_res * args.steps
-    bytes_total = N * (launches * (8 * dx + 4) + (launches - res_launches) * 4 + res_launches * 8)
+    bytes_total = N * launches * (8 * dx + 8)
     prop_avg_ms = prop_ms / max(prop_n, 1)
     achieved = bytes_total / launches / (prop_avg_ms / 1e3) / 1e9
     traffic = None
     tf = os.path.join(ROOT, "profiles", "pf_propagate_traffic.json")
     if os.path.exists(tf):
         try:
-            traffic = json.load(open(tf)).get("bytes_per_launch")
+            traffic = json.load(open(tf)).get("dram_bytes_per_launch")
         except Exception:
             traffic = None
     line = {
@@ -239,7 +237,7 @@ def bench_pf(args, world, rank, local):
         "ms_per_step": ms_max / args.steps, "higher_is_better": True, "scaling": "weak",
         "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "bootstrap PF, LGSSM Dx=16 Dy=8 (A orthogonal*0.95, Q=0.1I, "
-                               "H~N(0,1/16), R=0.2I), N=2^20, T=1000, systematic at ESS<0.5N",
+                               "H~N(0,1/16), R=0.2I), N=2^20, " f"T={T}, systematic at ESS<0.5N",
                    "N": N, "T": T, "dx": dx, "dy": dy, "precision": "FP32 state, FP64 normaliser",
                    "noise": "in-kernel Philox4x32-10", "parallelism": f"replicas x{world}",
                    "l2": "working set per time step ~140 MB > 126 MB L2 (no flush)",
@@ -247,15 +245,17 @@ def bench_pf(args, world, rank, local):
         "e2e": {"value": units / e2e_s, "unit": "particle-steps/s",
                 "h2d_bytes_per_step": int(ys.nbytes), "d2h_bytes_per_step": int(8 + 8 * T),
                 "call": "gf_pf_run(GF_MEM_HOST) from pinned host buffers"},
-        "gpu_launches": int(prop_n + scan_n + fill_n + prep_n + 3 * args.steps),
+        "gpu_launches": int(prop_n + scan_n + fill_n + prep_n + 2 * args.steps),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic,
-                     "kernel": "pf_lg_propagate<float,16,8>", "peak_source": peak_kind,
+                     "kernel": "pf_lg_propagate_tc<16,8> (tcgen05 3xTF32)", "peak_source": peak_kind,
                      "avg_launch_ms": prop_avg_ms, "launches": prop_n,
                      "bytes_per_launch": bytes_total / launches},
         "kernels_ms": {"propagate": prop_ms, "resample": scan_ms, "ancestor_fill": fill_ms,
                        "prep_init": prep_ms},
-        "graph_ms_per_step": graph_ms,
+        "timing": "value: CUDA events around K graph replays; kernels_ms / roofline: "
+                  "events around every launch in K eager runs on the same stream",
+        "eager_profiled_ms_per_step": eager_ms,
         "clocks": clk.summary(),
     }
     plan.close()
@@ -481,6 +481,8 @@ def main():
     ap.add_argument("--serve-hbm-gb", type=int, default=64)
     ap.add_argument("--kf-filters", type=int, default=65536)
     ap.add_argument("--kf-algo", default="kf", choices=["kf", "srkf"])
+    ap.add_argument("--pf-T", type=int, default=1000,
+                    help="time steps of the PF workload (smaller only for profiler captures)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     args = ap.parse_args()
