@@ -7,7 +7,7 @@ ESS < 0.5 N, FP64 normaliser and cumulative weights, in-kernel Philox noise.
 One step = one full filter run (N * T particle-steps).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload pf|kf|serve]
+                    [--workload pf|pf1d|kf|rbpf|serve]
 
 Under torchrun each rank runs an independent replica (the filters shard by
 filter; no data-path collective).  Rank 0 prints one JSON line.
@@ -442,6 +442,242 @@ def bench_serve(args, world, rank, local):
     return line
 
 
+def _profiled(ctx, fn, reps, classes):
+    """Per-kernel-class (ms per launch, launches) over `reps` calls of fn with
+    CUDA events around every launch on the context stream."""
+    ctx.profile(True)
+    for _ in range(reps):
+        fn()
+    ctx.synchronize()
+    res = {}
+    for cls, name in classes:
+        ms, n = ctx.profile_read(cls)
+        res[name] = (ms, n)
+    ctx.profile(False)
+    return res
+
+
+def bench_rbpf(args, world, rank, local):
+    """Rao-Blackwellised PF: outer 2-D AR(1) state, inner 8-D Kalman bank per
+    particle with stochastic-volatility Q, 4-D observations; N = 65536, T = 500,
+    systematic resampling at ESS < 0.5 N.  One step = one gf_rbpf_run call on
+    device-resident observations (N * T particle-steps)."""
+    import ctypes as C
+
+    import torch
+    import gfb200 as G
+    from gfb200 import _lib as L
+    from gfb200 import workloads as W
+    from gfb200.filtering import _pf_config
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    ctx = G.Context(local)
+    N, T = 65536, 500
+    hm, ys = W.rb_trend(seed=1234, T=T)
+    algo = G.RBPF(G.BF(N, threshold=0.5), G.KalmanFilter())
+    mc = hm._c_struct()
+    cfg, _, _ = _pf_config(algo.pf, T, 7 + rank)
+    lib = L.load()
+    ys_dev = torch.tensor(ys, dtype=torch.float64, device=dev)
+    ll_dev = torch.zeros(1, dtype=torch.float64, device=dev)
+    res_dev = torch.zeros(T, dtype=torch.int8, device=dev)
+    out = L.PFOutC(ll_dev.data_ptr(), None, None, res_dev.data_ptr(), None, None, None, None, None)
+
+    def run():
+        L.check(ctx.h, lib.gf_rbpf_run(ctx.h, C.byref(mc), C.byref(cfg), T, ys_dev.data_ptr(), None,
+                                       None, L.GF_MEM_DEVICE, C.byref(out), None))
+
+    for _ in range(args.warmup):
+        run()
+    ctx.synchronize()
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    _barrier(world)
+    with ClockSampler(local) as clk:
+        e0.record(ext)
+        for _ in range(args.steps):
+            run()
+        e1.record(ext)
+        e1.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1), world, dev)
+    n_res = int(res_dev.sum().item())
+    ll = float(ll_dev.item())
+    prof = _profiled(ctx, run, args.steps, [(3, "rbpf_propagate"), (1, "resample"), (5, "ancestor_fill"),
+                                             (4, "init")])
+    # e2e: host observations in pinned memory, ll back to host
+    ys_pin = torch.tensor(ys, dtype=torch.float64).pin_memory()
+    ll_pin = torch.zeros(1, dtype=torch.float64).pin_memory()
+    hout = L.PFOutC(ll_pin.data_ptr(), None, None, None, None, None, None, None, None)
+    t_e2e = []
+    for i in range(args.warmup + args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        L.check(ctx.h, lib.gf_rbpf_run(ctx.h, C.byref(mc), C.byref(cfg), T, ys_pin.data_ptr(), None,
+                                       None, L.GF_MEM_HOST, C.byref(hout), None))
+        if i >= args.warmup:
+            t_e2e.append(time.perf_counter() - t0)
+    e2e_s = _max_over_ranks(sum(t_e2e), world, dev)
+    units = N * T * args.steps * world
+    value = units / (ms / 1e3)
+    dxo, dz = 2, 8
+    width = dxo + dz + dz * (dz + 1) // 2
+    pms, pn = prof["rbpf_propagate"]
+    avg = pms / max(pn, 1)
+    bytes_launch = N * (8 * width + 8)  # state read + write, log-weight, ancestor / log-weight read
+    peak, peak_kind = _peaks()
+    line = {
+        "metric": "particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "RBPF on a hierarchical LGSSM: outer 2-D z_t = 0.9 z_{t-1} + N(0,0.3^2 I), "
+                               "inner Dx=8 (A orthogonal*0.95, Q = 0.05 exp(z_t[1]) I), H 4x8, R = 0.1 I; "
+                               "N=65536, T=500, systematic at ESS<0.5N",
+                   "N": N, "T": T, "resampled_steps": n_res, "ll": ll,
+                   "precision": "FP32 bank, FP64 innovation Cholesky and normaliser",
+                   "l2": "state 2 x 12 MB per step fits in L2; inputs resident (no flush)"},
+        "e2e": {"value": units / e2e_s, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": int(ys.nbytes), "d2h_bytes_per_step": 8,
+                "call": "gf_rbpf_run(GF_MEM_HOST) from pinned host buffers"},
+        # profiled classes + the unprofiled init, initial scalars and finish launches of each run
+        "gpu_launches": int(sum(v[1] for v in prof.values()) + 3 * args.steps),
+        "roofline": {"bound": "hbm", "achieved": bytes_launch / (avg / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": bytes_launch / (avg / 1e3) / 1e9 / peak, "traffic": None,
+                     "kernel": "rbpf_propagate<2,8,4>", "peak_source": peak_kind,
+                     "avg_launch_ms": avg, "bytes_per_launch": bytes_launch},
+        "kernels_ms": {k: v[0] for k, v in prof.items()},
+        "timing": "value: CUDA events around K gf_rbpf_run calls (allocation included); kernels: "
+                  "events around every launch in K more calls",
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_rbpf(hm, ys, N, seconds=args.cpu_seconds)
+    ctx.close()
+    return line
+
+
+def cpu_baseline_rbpf(hm, ys, N, seconds=12.0, threads=None):
+    """The FP64 oracle's RBPF on this host: same model and N, a bounded number of
+    time steps, all host threads."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    threads = threads or os.cpu_count() or 1
+    op, od = hm.outer_prior, hm.outer_dyn
+    ip, idn, ob = hm.inner_model.prior, hm.inner_model.dyn, hm.inner_model.obs
+    om = O.RBModel(op.mu0, op.Sigma0, od.A, od.b, od.Q, ip.mu0, ip.Sigma0, idn.A, idn.b, idn.C,
+                   idn.Q, ob.H, ob.c, ob.R, q_gamma=idn.q_gamma, q_index=idn.q_index)
+    t0 = time.perf_counter()
+    O.rbpf_run(om, N, ys[:1], threshold=0.5, seed=1, threads=threads)
+    one = time.perf_counter() - t0
+    steps = int(max(1, min(len(ys), seconds / max(one, 1e-3))))
+    t0 = time.perf_counter()
+    O.rbpf_run(om, N, ys[:steps], threshold=0.5, seed=1, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": N * steps / dt, "unit": "particle-steps/s", "cores": threads, "kind": "port",
+            "sample": f"FP64 C oracle RBPF, same model, N={N}, first {steps} of T steps, "
+                      f"{threads} OpenMP threads"}
+
+
+def bench_pf1d(args, world, rank, local):
+    """The README model (x_t = x_{t-1} + N(0, 0.1^2), y_t = x_t + N(0, 0.2^2)),
+    bootstrap PF with N = 1024, T = 100, FP64, systematic at ESS < 0.5 N: a
+    latency case (one filter fits in one block per step); one step = one filter
+    run, the metric its device latency."""
+    import ctypes as C
+
+    import torch
+    import gfb200 as G
+    from gfb200 import _lib as L
+    from gfb200 import workloads as W
+    from gfb200.filtering import _pf_config
+    from gfb200.plans import PfPlan
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    ctx = G.Context(local)
+    N, T = 1024, 100
+    model, ys = W.lgssm_1d(seed=1234, T=T)
+    algo = G.BF(N, threshold=0.5, precision="f64")
+    ys_dev = torch.tensor(ys, dtype=torch.float64, device=dev)
+    plan = PfPlan(model, algo, T, seed=1000 + rank, ctx=ctx, graph=True)
+    for _ in range(args.warmup):
+        plan.run(ys_dev)
+    ctx.synchronize()
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 50  # filter runs per step: one run is ~1 ms
+    _barrier(world)
+    with ClockSampler(local) as clk:
+        e0.record(ext)
+        for _ in range(args.steps * reps):
+            plan.run(ys_dev)
+        e1.record(ext)
+        e1.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1), world, dev) / (args.steps * reps)
+    ll = float(plan.ll.item())
+    plan.close()
+    eplan = PfPlan(model, algo, T, seed=1000 + rank, ctx=ctx, graph=False)
+    eplan.run(ys_dev)
+    prof = _profiled(ctx, lambda: eplan.run(ys_dev), args.steps,
+                     [(0, "propagate"), (1, "resample"), (5, "ancestor_fill"), (4, "prep_init")])
+    eplan.close()
+    # e2e through the C ABI from pinned host memory
+    mc = model._c_struct()
+    cfg, _, _ = _pf_config(algo, T, 7 + rank)
+    ys_pin = torch.tensor(ys, dtype=torch.float64).pin_memory()
+    ll_pin = torch.zeros(1, dtype=torch.float64).pin_memory()
+    out = L.PFOutC(ll_pin.data_ptr(), None, None, None, None, None, None, None, None)
+    lib = L.load()
+    t_e2e = []
+    for i in range(args.warmup + args.steps * 10):
+        t0 = time.perf_counter()
+        L.check(ctx.h, lib.gf_pf_run(ctx.h, C.byref(mc), C.byref(cfg), T, ys_pin.data_ptr(), None,
+                                     None, L.GF_MEM_HOST, C.byref(out)))
+        if i >= args.warmup:
+            t_e2e.append(time.perf_counter() - t0)
+    e2e_ms = statistics.median(t_e2e) * 1e3
+    pms, pn = prof["propagate"]
+    avg = pms / max(pn, 1)
+    bytes_launch = N * (8 * 1 * 2 + 16)  # FP64 state read + write, log-weight write + read / ancestor
+    peak, peak_kind = _peaks()
+    line = {
+        "metric": "filter latency", "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": False, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": {"workload": "README LGSSM (x_t = x_{t-1} + N(0,0.1^2), y_t = x_t + N(0,0.2^2)), "
+                               "bootstrap PF N=1024, T=100, FP64, systematic at ESS<0.5N",
+                   "N": N, "T": T, "ll": ll, "runs_per_step": reps,
+                   "l2": "latency case: the whole filter lives in L2"},
+        "e2e": {"value": e2e_ms, "unit": "ms", "h2d_bytes_per_step": int(ys.nbytes),
+                "d2h_bytes_per_step": 8, "call": "gf_pf_run(GF_MEM_HOST), median"},
+        "gpu_launches": int(sum(v[1] for v in prof.values()) + 2 * args.steps),
+        "roofline": {"bound": "hbm", "achieved": bytes_launch / (avg / 1e3) / 1e9, "peak": peak,
+                     "unit": "GB/s", "frac": bytes_launch / (avg / 1e3) / 1e9 / peak, "traffic": None,
+                     "kernel": "pf_lg_propagate<double,1,1>", "peak_source": peak_kind,
+                     "avg_launch_ms": avg, "bytes_per_launch": bytes_launch,
+                     "note": "launch-latency bound: one 1024-particle block per step"},
+        "kernels_ms": {k: v[0] for k, v in prof.items()},
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        O.build()
+        om = O.LGModel(model.prior.mu0, model.prior.Sigma0, model.dyn.A, model.dyn.b, model.dyn.Q,
+                       model.obs.H, model.obs.c, model.obs.R)
+        tt = []
+        for _ in range(20):
+            t0 = time.perf_counter()
+            O.pf_run(om, N, ys, threshold=0.5, seed=1, threads=1)
+            tt.append(time.perf_counter() - t0)
+        line["cpu_baseline"] = {"value": statistics.median(tt) * 1e3, "unit": "ms", "cores": 1,
+                                "kind": "port",
+                                "sample": "FP64 C oracle, the whole filter (N=1024, T=100), one thread "
+                                          "as the reference, median of 20"}
+    ctx.close()
+    return line
+
+
 def bench_reference(args, world, rank, local):
     """The reference arm: the FP64 oracle port of the reference algorithm on the
     host cores (the reference is Julia and cannot run on this image)."""
@@ -475,7 +711,7 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pf", choices=["pf", "kf", "serve"])
+    ap.add_argument("--workload", default="pf", choices=["pf", "pf1d", "kf", "rbpf", "serve"])
     ap.add_argument("--serve-rate", type=float, default=1000.0)
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-hbm-gb", type=int, default=64)
@@ -501,6 +737,10 @@ def main():
         line = bench_kf(args, world, rank, local)
     elif args.workload == "serve":
         line = bench_serve(args, world, rank, local)
+    elif args.workload == "rbpf":
+        line = bench_rbpf(args, world, rank, local)
+    elif args.workload == "pf1d":
+        line = bench_pf1d(args, world, rank, local)
     else:
         line = bench_pf(args, world, rank, local)
     if rank == 0 and line is not None:
