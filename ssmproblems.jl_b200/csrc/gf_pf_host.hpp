@@ -49,6 +49,12 @@ void launch_prep(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int T, int dx, int
 
 namespace gf {
 
+// Rao-Blackwellised PF propagation: one particle per thread, RB_SPLIT blocks of
+// RB_THREADS threads per 1024-particle tile (its log-sum-exp partials are kept
+// per block, so the job's `part` buffer holds ntiles * RB_SPLIT entries).
+constexpr int RB_THREADS = 128;
+constexpr int RB_SPLIT = 1024 / RB_THREADS;
+
 // Rao-Blackwellised PF kernels of one compiled (dxo, dz, dy).
 struct RbKernels {
   int dxo, dz, dy;

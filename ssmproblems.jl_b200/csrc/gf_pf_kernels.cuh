@@ -256,32 +256,36 @@ struct LseAcc {
 // Baseline: log N after a resample or for the initial TypelessZero weights;
 // otherwise logsumexp of the normalised log-weights, which is 0 up to the
 // rounding of the normalisation (below 1e-15), so it is taken as 0.
+// A tile may be covered by `nparts` blocks (block `part` of tile `tile`); the
+// partials are then kept per part, folded in part order and summed per tile
+// for the tile prefixes.
 static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh, LseAcc a,
-                                    double* red) {
+                                    double* red, int part = 0, int nparts = 1) {
   PfScalars* sc = J.sc;
   __shared__ int s_last;
+  const int nall = J.ntiles * nparts;
   double M = block_max(a.m, red);
   double f = a.m > -INFINITY ? exp(a.m - M) : 0.0;
   double S1 = block_sum(a.s1 * f, red);
   double S2 = block_sum(a.s2 * f * f, red);
   if (threadIdx.x == 0) {
-    double* p = J.part + (size_t)tile * PF_PW;
+    double* p = J.part + ((size_t)tile * nparts + part) * PF_PW;
     p[0] = M;
     p[1] = S1;
     p[2] = S2;
     __threadfence();
     unsigned prev = atomicAdd(&sc->counter, 1u);
-    s_last = (prev == (unsigned)(J.ntiles - 1));
+    s_last = (prev == (unsigned)(nall - 1));
   }
   __syncthreads();
   if (!s_last) return;
   __threadfence();
   // ---- last block: fold all partials in a fixed order (deterministic) ----
   double m = -INFINITY;
-  for (int bb = threadIdx.x; bb < J.ntiles; bb += blockDim.x) m = fmax(m, __ldcg(J.part + (size_t)bb * PF_PW));
+  for (int bb = threadIdx.x; bb < nall; bb += blockDim.x) m = fmax(m, __ldcg(J.part + (size_t)bb * PF_PW));
   double GM = block_max(m, red);
   double s1 = 0.0, s2 = 0.0;
-  for (int bb = threadIdx.x; bb < J.ntiles; bb += blockDim.x) {
+  for (int bb = threadIdx.x; bb < nall; bb += blockDim.x) {
     const double* p = J.part + (size_t)bb * PF_PW;
     double mb = __ldcg(p);
     if (mb > -INFINITY) {
@@ -323,18 +327,21 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
     const int per = (J.ntiles + blockDim.x - 1) / blockDim.x;
     const int b0 = min((int)threadIdx.x * per, J.ntiles), b1 = min(b0 + per, J.ntiles);
     unsigned long long tot = 0ull;
-    for (int bb = b0; bb < b1; ++bb) {
-      const double* p = J.part + (size_t)bb * PF_PW;
-      const double mb = __ldcg(p);
-      if (mb > -INFINITY) tot += __double2ull_rn(__ldcg(p + 1) * exp(mb - lse) * kFix);
-    }
+    auto tile_fix = [&](int bb) {  // fixed-point normalised weight of tile bb
+      unsigned long long w = 0ull;
+      for (int q = 0; q < nparts; ++q) {
+        const double* p = J.part + ((size_t)bb * nparts + q) * PF_PW;
+        const double mb = __ldcg(p);
+        if (mb > -INFINITY) w += __double2ull_rn(__ldcg(p + 1) * exp(mb - lse) * kFix);
+      }
+      return w;
+    };
+    for (int bb = b0; bb < b1; ++bb) tot += tile_fix(bb);
     unsigned long long all = 0ull;
     unsigned long long run = block_excl_scan_u64(tot, s_wsum, &all);
     for (int bb = b0; bb < b1; ++bb) {
       J.tprefix[bb] = (double)run * kInvFix;
-      const double* p = J.part + (size_t)bb * PF_PW;
-      const double mb = __ldcg(p);
-      if (mb > -INFINITY) run += __double2ull_rn(__ldcg(p + 1) * exp(mb - lse) * kFix);
+      run += tile_fix(bb);
     }
     if (threadIdx.x == 0) {
       J.tprefix[J.ntiles] = (double)all * kInvFix;

@@ -35,26 +35,32 @@ __host__ __device__ constexpr int pk(int i, int j, int n) {  // packed upper ind
   return i * n - i * (i - 1) / 2 + (j - i);
 }
 
+static_assert(RB_SPLIT * RB_THREADS == PF_TILE, "RBPF blocks must tile a propagate tile exactly");
+
+// One particle per thread: a particle's Kalman update needs ~250 registers, so
+// a 1024-particle tile is spread over RB_SPLIT blocks of RB_THREADS threads
+// (grid = RB_SPLIT * tiles) to keep every SM busy at moderate N.
 template <int DXO, int DZ, int DY>
-__global__ void __launch_bounds__(PF_THREADS) rbpf_propagate(const PfJob* __restrict__ jobs, int njobs,
+__global__ void __launch_bounds__(RB_THREADS) rbpf_propagate(const PfJob* __restrict__ jobs, int njobs,
                                                             float q_gamma, int q_index, int guided) {
   using L = RbLayout<DXO, DZ, DY>;
   constexpr int NS = L::NS;
   __shared__ float sp[L::total];
   __shared__ double sy[DY];
   __shared__ double red[32];
-  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const int jb = find_job(jobs, njobs, blockIdx.x / RB_SPLIT, false);
   const PfJob& J = jobs[jb];
   PfScalars* sc = J.sc;
   const int t = sc->t + 1;
   if (t > J.T || sc->status != 0) return;
-  const int tile = blockIdx.x - J.tile0;
+  const int tile = blockIdx.x / RB_SPLIT - J.tile0;
+  const int part = blockIdx.x % RB_SPLIT;
   const bool resamp = sc->resample != 0;
   const bool fresh = resamp || sc->uniform != 0;
   const double lse_prev = sc->lse;
   const bool searched = J.resampler == GF_RS_MULTINOMIAL;
   const float* P = reinterpret_cast<const float*>(J.params);
-  for (int k = threadIdx.x; k < L::total; k += PF_THREADS) sp[k] = P[k];
+  for (int k = threadIdx.x; k < L::total; k += RB_THREADS) sp[k] = P[k];
   if (threadIdx.x < DY) sy[threadIdx.x] = J.ys[(size_t)(t - 1) * DY + threadIdx.x];
   __syncthreads();
   const int64_t N = J.N;
@@ -64,8 +70,8 @@ __global__ void __launch_bounds__(PF_THREADS) rbpf_propagate(const PfJob* __rest
   const float* noise = J.noise ? reinterpret_cast<const float*>(J.noise) + (size_t)t * DXO * N : nullptr;
   LseAcc acc;
   int fail = 0;
-  for (int p = 0; p < PF_PPT; ++p) {
-    const int64_t i = (int64_t)tile * PF_TILE + p * PF_THREADS + threadIdx.x;
+  for (int p = 0; p < 1; ++p) {
+    const int64_t i = (int64_t)tile * PF_TILE + part * RB_THREADS + threadIdx.x;
     if (i >= N) break;
     int64_t a = i;
     if (resamp) a = searched ? find_ancestor(J, sc, t, i, 0, N) : (int64_t)J.anc[i];
@@ -309,7 +315,7 @@ __global__ void __launch_bounds__(PF_THREADS) rbpf_propagate(const PfJob* __rest
     acc.add((double)lst);
   }
   if (fail) sc->status = GF_ERR_NOT_PD;
-  block_finish(J, tile, t, fresh, acc, red);
+  block_finish(J, tile, t, fresh, acc, red, part, RB_SPLIT);
 }
 
 template <int DXO, int DZ, int DY>
@@ -464,7 +470,7 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   if ((st = get(sizeof(double) * (size_t)(ntiles + 1), &tprev))) return st;
   if ((st = get(sizeof(int32_t) * (size_t)(ntiles + 1), &mpkv))) return st;
   if ((st = get(sizeof(int32_t) * (size_t)N, &fillv))) return st;
-  if ((st = get(sizeof(double) * PF_PW * ntiles, &part))) return st;
+  if ((st = get(sizeof(double) * PF_PW * ntiles * RB_SPLIT, &part))) return st;
   if ((st = get(sizeof(double) * ntiles * (dxo + dz), &mpart))) return st;
   if ((st = get(sizeof(unsigned long long) * 2 * nstiles, &flags))) return st;
   if ((st = get(sizeof(PfScalars), &scv))) return st;
@@ -579,7 +585,7 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   for (int t = 1; t <= T; ++t) {
     {
       ProfScope ps(ctx, KC_RBPF);
-      K.prop<<<ntiles, PF_THREADS, 0, s>>>(jd, 1, (float)m->q_gamma, m->q_index, guided);
+      K.prop<<<ntiles * RB_SPLIT, RB_THREADS, 0, s>>>(jd, 1, (float)m->q_gamma, m->q_index, guided);
     }
     if (want_means) launch_means(ctx, false, jd, 1, ntiles, (double*)mpart, dxo + dz);
     if (t < T) launch_resample(ctx, false, jd, 1, ntiles);

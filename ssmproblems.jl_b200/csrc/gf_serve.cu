@@ -301,7 +301,7 @@ void pf_layout(Req* r, size_t param_bytes, size_t pp_bytes, size_t rsize, int wi
   r->d_anc = d.take(sizeof(int32_t) * (size_t)N);
   r->d_mpk = d.take(sizeof(int32_t) * (size_t)(ntiles + 1));
   r->d_tpre = d.take(sizeof(double) * (size_t)(ntiles + 1));
-  r->d_part = d.take(sizeof(double) * PF_PW * (size_t)ntiles);
+  r->d_part = d.take(sizeof(double) * PF_PW * (size_t)ntiles * RB_SPLIT);  // RBPF: per-block partials
   r->d_mpart = d.take(sizeof(double) * (size_t)ntiles * std::max(1, r->mdim));
   r->d_flags = d.take(sizeof(unsigned long long) * 2 * (size_t)nstiles);
   r->d_sc = d.take(sizeof(PfScalars));
@@ -766,7 +766,7 @@ bool gf_srv::pf_iterate() {
     }
     cudaMemcpyAsync(g.dev[slot], g.host[slot], sizeof(PfJob) * nj, cudaMemcpyHostToDevice, s);
     for (int k = 0; k < steps; ++k) {
-      if (g.rb) g.rk.prop<<<tiles, PF_THREADS, 0, s>>>(g.dev[slot], nj, g.q_gamma, g.q_index, g.guided);
+      if (g.rb) g.rk.prop<<<tiles * RB_SPLIT, RB_THREADS, 0, s>>>(g.dev[slot], nj, g.q_gamma, g.q_index, g.guided);
       else g.prop<<<tiles, g.threads, g.smem, s>>>(g.dev[slot], nj);
       launch_resample(&pfx, g.dbl, g.dev[slot], nj, tiles);
       launches += 3;
