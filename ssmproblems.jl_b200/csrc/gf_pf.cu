@@ -138,6 +138,7 @@ __global__ void pf_finish_kernel(const PfJob* __restrict__ jobs) {
 void register_lg_f32_small(std::vector<PfLgKernels>& v, bool guided);
 void register_lg_f32_16(std::vector<PfLgKernels>& v, bool guided);
 void register_lg_f32_32(std::vector<PfLgKernels>& v, bool guided);
+void register_lg_f32_64(std::vector<PfLgKernels>& v, bool guided);
 void register_lg_f64(std::vector<PfLgKernels>& v, bool guided);
 
 static std::vector<PfLgKernels> lg_table(bool dbl, bool guided) {
@@ -148,6 +149,7 @@ static std::vector<PfLgKernels> lg_table(bool dbl, bool guided) {
     register_lg_f32_small(v, guided);
     register_lg_f32_16(v, guided);
     register_lg_f32_32(v, guided);
+    register_lg_f32_64(v, guided);
   }
   return v;
 }

@@ -20,6 +20,7 @@ struct PfLgKernels {
   void (*prop_tc)(const PfJob*, int) = nullptr;
   size_t tc_smem = 0;
   int tc_nm = 0;
+  int tc_split = 1;  // blocks per tile of the tensor-core kernel
 };
 
 // FP64 model factors computed once per plan (column-major).
@@ -48,6 +49,9 @@ void launch_prep(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int T, int dx, int
 }  // namespace gf
 
 namespace gf {
+
+// Largest number of blocks per tile of any propagate kernel (sizes `part`).
+constexpr int PF_MAX_SPLIT = 8;
 
 // Rao-Blackwellised PF propagation: one particle per thread, RB_SPLIT blocks of
 // RB_THREADS threads per 1024-particle tile (its log-sum-exp partials are kept
@@ -81,6 +85,7 @@ struct LgJobSetup {
   PfLgKernels k;
   void (*prop)(const PfJob*, int) = nullptr;
   int threads = 0;
+  int split = 1;  // propagate blocks per tile (grid = tiles * split)
   size_t smem = 0;
   std::vector<char> params;
   std::vector<double> pp;

@@ -237,6 +237,13 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_init(const PfJob* __restrict
 // (one lane per particle) and is read back for the weight and the state store.
 constexpr int TC_THREADS = 128;
 constexpr int TC_SUB = PF_TILE / TC_THREADS;
+// Blocks per tile (each TC_SUB / TC_SPLIT sub-tiles, partials kept per block).
+// One: the per-block prologue (operand-B staging, TMEM allocation) and the
+// partial reduction cost more than a shorter last wave saves (2 measured
+// 16 % slower at Dx=16, N=2^20).
+constexpr int TC_SPLIT = 1;
+constexpr int TC_SUB_BLOCK = TC_SUB / TC_SPLIT;
+static_assert(TC_SUB % TC_SPLIT == 0 && TC_SPLIT <= PF_MAX_SPLIT, "tensor-core tile split");
 constexpr uint32_t TC_WAIT = 1u << 22;  // bounded mbarrier polls
 
 template <int DXP, int DYP>
@@ -269,12 +276,13 @@ __global__ void __launch_bounds__(TC_THREADS) pf_lg_propagate_tc(const PfJob* __
   __shared__ uint64_t mbar;
   __shared__ uint32_t tmem_slot;
 
-  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const int jb = find_job(jobs, njobs, blockIdx.x / TC_SPLIT, false);
   const PfJob& J = jobs[jb];
   PfScalars* sc = J.sc;
   const int t = sc->t + 1;
   if (t > J.T || sc->status != 0) return;
-  const int tile = blockIdx.x - J.tile0;
+  const int tile = blockIdx.x / TC_SPLIT - J.tile0;
+  const int part = blockIdx.x % TC_SPLIT;
   const int tid = threadIdx.x;
   const bool resamp = sc->resample != 0;
   const bool fresh = resamp || sc->uniform != 0;
@@ -322,8 +330,8 @@ __global__ void __launch_bounds__(TC_THREADS) pf_lg_propagate_tc(const PfJob* __
   LseAcc acc;
   bool ok = true;
 
-  for (int s = 0; s < TC_SUB; ++s) {
-    const int64_t i = (int64_t)tile * PF_TILE + s * TC_THREADS + tid;
+  for (int s = 0; s < TC_SUB_BLOCK; ++s) {
+    const int64_t i = (int64_t)tile * PF_TILE + (part * TC_SUB_BLOCK + s) * TC_THREADS + tid;
     const bool valid = i < N;
     int64_t a = i;
     if (valid && resamp) a = searched ? find_ancestor(J, sc, t, i, 0, N) : (int64_t)ancv[i];
@@ -402,7 +410,7 @@ __global__ void __launch_bounds__(TC_THREADS) pf_lg_propagate_tc(const PfJob* __
   }
   if (!ok && tid == 0) sc->status = GF_ERR_TIMEOUT;
   if (tid < 32) umma::tmem_dealloc(tbase, TL::NCOLS);
-  block_finish(J, tile, t, fresh, acc, red);
+  block_finish(J, tile, t, fresh, acc, red, part, TC_SPLIT);
 }
 
 template <typename Real, int DXP, int DYP, bool G>
@@ -420,6 +428,7 @@ PfLgKernels make_lg() {
     k.prop_tc = pf_lg_propagate_tc<DXP, DYP>;
     k.tc_smem = TcLayout<DXP, DYP>::smem_bytes;
     k.tc_nm = TcLayout<DXP, DYP>::NM;
+    k.tc_split = TC_SPLIT;
   }
   return k;
 }

@@ -33,6 +33,7 @@ struct gf_pf_plan {
   PfJob job{};
   void (*prop_fn)(const PfJob*, int) = nullptr;  // chosen propagate kernel
   int prop_threads = 0;
+  int prop_split = 1;
   size_t prop_smem = 0;
   cudaGraphExec_t graph = nullptr;
   bool graph_means = false;
@@ -90,10 +91,12 @@ gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cf
     o->prop = o->k.prop_tc;
     o->threads = 128;
     o->smem = o->k.tc_smem;
+    o->split = o->k.tc_split;
   } else {
     o->prop = o->k.prop;
     o->threads = PF_THREADS;
     o->smem = o->k.smem;
+    o->split = 1;
   }
   const int64_t N = cfg->n_particles;
   // step-1 decision with the reference's uniform-weight ESS
@@ -168,7 +171,7 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   ALLOC(mpk, sizeof(int32_t) * (size_t)(p->ntiles + 1));
   ALLOC(anc, sizeof(int32_t) * (size_t)N);
   ALLOC(tprefix, sizeof(double) * (size_t)(p->ntiles + 1));
-  ALLOC(part, sizeof(double) * PF_PW * (size_t)p->ntiles);
+  ALLOC(part, sizeof(double) * PF_PW * (size_t)p->ntiles * PF_MAX_SPLIT);
   ALLOC(mpart, sizeof(double) * (size_t)p->ntiles * m->dx);
   ALLOC(flags, sizeof(unsigned long long) * 2 * (size_t)p->nstiles);
   ALLOC(sc, sizeof(PfScalars));
@@ -187,6 +190,7 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
   p->prop_fn = L.prop;
   p->prop_threads = L.threads;
+  p->prop_split = L.split;
   p->prop_smem = L.smem;
   GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)p->prop_fn,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->prop_smem));
@@ -225,7 +229,7 @@ static void enqueue_run(gf_pf_plan* p, bool means) {
   for (int t = 1; t <= p->T; ++t) {
     {
       ProfScope ps(ctx, KC_PROPAGATE);
-      p->prop_fn<<<p->ntiles, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
+      p->prop_fn<<<p->ntiles * p->prop_split, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
     }
     if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);
     if (t < p->T) launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);

@@ -36,6 +36,7 @@ __host__ __device__ constexpr int pk(int i, int j, int n) {  // packed upper ind
 }
 
 static_assert(RB_SPLIT * RB_THREADS == PF_TILE, "RBPF blocks must tile a propagate tile exactly");
+static_assert(RB_SPLIT <= PF_MAX_SPLIT, "part buffers hold PF_MAX_SPLIT partials per tile");
 
 // One particle per thread: a particle's Kalman update needs ~250 registers, so
 // a 1024-particle tile is spread over RB_SPLIT blocks of RB_THREADS threads
@@ -470,7 +471,7 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   if ((st = get(sizeof(double) * (size_t)(ntiles + 1), &tprev))) return st;
   if ((st = get(sizeof(int32_t) * (size_t)(ntiles + 1), &mpkv))) return st;
   if ((st = get(sizeof(int32_t) * (size_t)N, &fillv))) return st;
-  if ((st = get(sizeof(double) * PF_PW * ntiles * RB_SPLIT, &part))) return st;
+  if ((st = get(sizeof(double) * PF_PW * ntiles * PF_MAX_SPLIT, &part))) return st;
   if ((st = get(sizeof(double) * ntiles * (dxo + dz), &mpart))) return st;
   if ((st = get(sizeof(unsigned long long) * 2 * nstiles, &flags))) return st;
   if ((st = get(sizeof(PfScalars), &scv))) return st;

@@ -156,7 +156,7 @@ struct Req {
 struct Group {
   bool rb = false, dbl = false;
   void (*prop)(const PfJob*, int) = nullptr;
-  int threads = 0;
+  int threads = 0, split = 1;
   size_t smem = 0;
   RbKernels rk{};
   float q_gamma = 0.f;
@@ -301,7 +301,7 @@ void pf_layout(Req* r, size_t param_bytes, size_t pp_bytes, size_t rsize, int wi
   r->d_anc = d.take(sizeof(int32_t) * (size_t)N);
   r->d_mpk = d.take(sizeof(int32_t) * (size_t)(ntiles + 1));
   r->d_tpre = d.take(sizeof(double) * (size_t)(ntiles + 1));
-  r->d_part = d.take(sizeof(double) * PF_PW * (size_t)ntiles * RB_SPLIT);  // RBPF: per-block partials
+  r->d_part = d.take(sizeof(double) * PF_PW * (size_t)ntiles * PF_MAX_SPLIT);  // per-block partials
   r->d_mpart = d.take(sizeof(double) * (size_t)ntiles * std::max(1, r->mdim));
   r->d_flags = d.take(sizeof(unsigned long long) * 2 * (size_t)nstiles);
   r->d_sc = d.take(sizeof(PfScalars));
@@ -452,6 +452,7 @@ Group* gf_srv::group_for(Req* r) {
     g->dbl = r->lg->dbl;
     g->prop = r->lg->prop;
     g->threads = r->lg->threads;
+    g->split = r->lg->split;
     g->smem = r->lg->smem;
     cudaFuncSetAttribute((const void*)g->prop, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)g->smem);
   } else {
@@ -767,7 +768,7 @@ bool gf_srv::pf_iterate() {
     cudaMemcpyAsync(g.dev[slot], g.host[slot], sizeof(PfJob) * nj, cudaMemcpyHostToDevice, s);
     for (int k = 0; k < steps; ++k) {
       if (g.rb) g.rk.prop<<<tiles * RB_SPLIT, RB_THREADS, 0, s>>>(g.dev[slot], nj, g.q_gamma, g.q_index, g.guided);
-      else g.prop<<<tiles, g.threads, g.smem, s>>>(g.dev[slot], nj);
+      else g.prop<<<tiles * g.split, g.threads, g.smem, s>>>(g.dev[slot], nj);
       launch_resample(&pfx, g.dbl, g.dev[slot], nj, tiles);
       launches += 3;
     }

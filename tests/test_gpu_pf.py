@@ -202,7 +202,7 @@ def test_large_pf_converges_to_kf_ll(ctx):
     assert abs(np.median(lls) - llkf) < 2.0 + 3 * sd
 
 
-@pytest.mark.parametrize("dims", [(16, 8), (32, 16), (20, 5)])
+@pytest.mark.parametrize("dims", [(16, 8), (32, 16), (20, 5), (64, 32), (40, 20)])
 def test_tensor_core_path_matches_simt(ctx, dims):
     """The tcgen05 propagation (3xTF32) and the CUDA-core propagation agree to FP32
     accuracy on the same injected noise (no resampling, so particles stay aligned)."""
@@ -229,4 +229,6 @@ def test_tensor_core_path_matches_simt(ctx, dims):
     (s0, w0, l0), (s1, w1, l1) = out[False], out[True]
     np.testing.assert_allclose(s0, s1, rtol=2e-5, atol=2e-5)
     np.testing.assert_allclose(w0, w1, rtol=1e-5, atol=2e-4)
-    np.testing.assert_allclose(l0, l1, rtol=1e-6, atol=1e-5)
+    # per-step ll is a log-sum-exp of the log-weights: its error is bounded by
+    # theirs (FP32 sums of up to 32 squared residuals per particle)
+    np.testing.assert_allclose(l0, l1, rtol=1e-5, atol=1e-5)
