@@ -246,60 +246,53 @@ __global__ void __launch_bounds__(RB_THREADS) rbpf_propagate(const PfJob* __rest
 #pragma unroll
       for (int i2 = 0; i2 < DY; ++i2) K[r][i2] = (float)v[i2];
     }
-    // mu = mp + K z  (K z = PHt L^-T w)
-#pragma unroll
-    for (int r = 0; r < DZ; ++r) {
-      double v = (double)mp[r];
+    // mu = mp + K z
+    {
+      double z[DY];
 #pragma unroll
       for (int i2 = 0; i2 < DY; ++i2) {
         double zi = sy[i2] - (double)sp[L::c + i2];
 #pragma unroll
         for (int k = 0; k < DZ; ++k) zi -= (double)sp[L::H + k * DY + i2] * (double)mp[k];
-        v += (double)K[r][i2] * zi;
+        z[i2] = zi;
       }
-      mu[r] = (float)v;
-    }
-    // Joseph: S = (I-KH) Sp (I-KH)' + K R K'  (upper triangle)
-    {
-      float IKH[DZ][DZ];
-#pragma unroll
-      for (int r = 0; r < DZ; ++r)
-#pragma unroll
-        for (int c = 0; c < DZ; ++c) {
-          float v = r == c ? 1.f : 0.f;
-#pragma unroll
-          for (int k = 0; k < DY; ++k) v = fmaf(-K[r][k], sp[L::H + c * DY + k], v);
-          IKH[r][c] = v;
-        }
 #pragma unroll
       for (int r = 0; r < DZ; ++r) {
-        float Tr[DZ], KRr[DY];
+        double v = (double)mp[r];
 #pragma unroll
-        for (int k = 0; k < DZ; ++k) {
-          float v = 0.f;
+        for (int i2 = 0; i2 < DY; ++i2) v += (double)K[r][i2] * z[i2];
+        mu[r] = (float)v;
+      }
+    }
+    // Joseph form S = (I-KH) Sp (I-KH)' + K R K' (upper triangle), without
+    // forming I - KH: row r of (I-KH) Sp is T_r = Sp_r - K_r (H Sp), where
+    // H Sp = PHt' (Sp symmetric), and then
+    //   S_rc = T_rc + sum_j (K R)_rj K_cj - sum_j (T_r H')_j K_cj.
 #pragma unroll
-          for (int m = 0; m < DZ; ++m) {
-            const float Smk = m <= k ? Sp[pk(m, k, DZ)] : Sp[pk(k, m, DZ)];
-            v = fmaf(IKH[r][m], Smk, v);
-          }
-          Tr[k] = v;
-        }
+    for (int r = 0; r < DZ; ++r) {
+      float Tr[DZ], Cr[DY];
 #pragma unroll
-        for (int k = 0; k < DY; ++k) {
-          float v = 0.f;
+      for (int k = 0; k < DZ; ++k) {
+        float v = r <= k ? Sp[pk(r, k, DZ)] : Sp[pk(k, r, DZ)];
 #pragma unroll
-          for (int m = 0; m < DY; ++m) v = fmaf(K[r][m], sp[L::R + k * DY + m], v);
-          KRr[k] = v;
-        }
+        for (int j = 0; j < DY; ++j) v = fmaf(-K[r][j], PHt[k][j], v);
+        Tr[k] = v;
+      }
 #pragma unroll
-        for (int j = r; j < DZ; ++j) {
-          float v = 0.f;
+      for (int j = 0; j < DY; ++j) {
+        float kr = 0.f, th = 0.f;
 #pragma unroll
-          for (int k = 0; k < DZ; ++k) v = fmaf(Tr[k], IKH[j][k], v);
+        for (int m = 0; m < DY; ++m) kr = fmaf(K[r][m], sp[L::R + j * DY + m], kr);
 #pragma unroll
-          for (int k = 0; k < DY; ++k) v = fmaf(KRr[k], K[j][k], v);
-          S[pk(r, j, DZ)] = v;
-        }
+        for (int k = 0; k < DZ; ++k) th = fmaf(Tr[k], sp[L::H + k * DY + j], th);
+        Cr[j] = kr - th;
+      }
+#pragma unroll
+      for (int c = r; c < DZ; ++c) {
+        float v = Tr[c];
+#pragma unroll
+        for (int j = 0; j < DY; ++j) v = fmaf(Cr[j], K[c][j], v);
+        S[pk(r, c, DZ)] = v;
       }
     }
     const double lin_obs = -0.5 * (qf + 2.0 * ldet + DY * GF_LOG2PI);
