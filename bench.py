@@ -61,6 +61,10 @@ class ClockSampler:
                 stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
             self.t = threading.Thread(target=self._read, daemon=True)
             self.t.start()
+            # let nvidia-smi finish starting up before the timed region begins
+            t0 = time.perf_counter()
+            while not self.rows and time.perf_counter() - t0 < 3.0:
+                time.sleep(0.02)
         except Exception:
             self.proc = None
         return self

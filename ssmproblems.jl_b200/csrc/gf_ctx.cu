@@ -29,15 +29,17 @@ gf_status dev_alloc(gf_ctx* ctx, size_t bytes, void** p) {
   if (ctx->used + bytes > ctx->budget)
     return set_err(ctx, GF_ERR_OOM_BUDGET, "HBM budget exceeded: need %zu more bytes, %zu of %zu used",
                    bytes, ctx->used, ctx->budget);
-  cudaError_t e = cudaMalloc(p, bytes);
-  if (e != cudaSuccess) return cuda_err(ctx, e, "cudaMalloc");
+  cudaError_t e = ctx->pool ? cudaMallocFromPoolAsync(p, bytes, ctx->pool, ctx->stream)
+                            : cudaMalloc(p, bytes);
+  if (e != cudaSuccess) return cuda_err(ctx, e, "device allocation");
   ctx->used += bytes;
   return GF_OK;
 }
 
 void dev_free(gf_ctx* ctx, void* p, size_t bytes) {
   if (!p) return;
-  cudaFree(p);
+  if (ctx->pool) cudaFreeAsync(p, ctx->stream);
+  else cudaFree(p);
   ctx->used = ctx->used >= bytes ? ctx->used - bytes : 0;
 }
 
@@ -136,6 +138,21 @@ gf_status gf_ctx_create(int32_t device, size_t hbm_budget_bytes, gf_ctx** out) {
     return GF_ERR_CUDA;
   }
   ctx->own_stream = true;
+  {
+    cudaMemPoolProps props;
+    std::memset(&props, 0, sizeof props);
+    props.allocType = cudaMemAllocationTypePinned;
+    props.handleTypes = cudaMemHandleTypeNone;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = device;
+    if (cudaMemPoolCreate(&ctx->pool, &props) == cudaSuccess) {
+      uint64_t keep = UINT64_MAX;  // keep freed blocks for reuse until the context goes
+      cudaMemPoolSetAttribute(ctx->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    } else {
+      ctx->pool = nullptr;  // fall back to cudaMalloc / cudaFree
+      cudaGetLastError();
+    }
+  }
   *out = ctx;
   return GF_OK;
 }
@@ -149,6 +166,10 @@ gf_status gf_ctx_destroy(gf_ctx* ctx) {
     cudaEventDestroy(p.b);
   }
   for (auto e : ctx->event_pool) cudaEventDestroy(e);
+  if (ctx->pool) {
+    cudaStreamSynchronize(ctx->stream);
+    cudaMemPoolDestroy(ctx->pool);
+  }
   if (ctx->own_stream) cudaStreamDestroy(ctx->stream);
   delete ctx;
   return GF_OK;

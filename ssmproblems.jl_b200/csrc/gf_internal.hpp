@@ -14,6 +14,9 @@ struct gf_ctx {
   int num_sms = 148;
   cudaStream_t stream = nullptr;
   bool own_stream = false;
+  // private stream-ordered pool for scratch and plan buffers (freed memory stays
+  // cached in the pool, so repeated one-shot calls do not synchronise the device)
+  cudaMemPool_t pool = nullptr;
   size_t budget = 0;
   size_t used = 0;
   std::string err;
