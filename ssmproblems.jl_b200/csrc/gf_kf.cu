@@ -33,14 +33,20 @@ template <int DXP, int DYP>
 struct KfSmem {
   static constexpr int LD = DXP + 1;   // row stride of dx-wide matrices
   static constexpr int LY = DYP + 1;   // row stride of dy-wide matrices
-  float A[DXP * LD], Q[DXP * LD], Sig[DXP * LD], Sp[DXP * LD], T1[DXP * LD], IKH[DXP * LD];
-  float H[DYP * LD], PHt[DXP * LY], K[DXP * LY], KR[DXP * LY], R[DYP * LY];
-  static constexpr int LW = DXP + 2;  // row stride of the solve buffer (dx RHS + z)
-  double S[DYP * LY], Wm[DYP * LW], dinv[DYP];
+  static constexpr int LW = DXP + 1;   // row stride of the FP64 solve buffer (dx RHS + z)
+  // Buffers shared by values whose lifetimes within a step do not overlap:
+  //   Sig : filtered covariance; from step 2 to 8 it holds the prediction Sp
+  //   XZ  : X = A Sig (steps 1-2), then I - KH (steps 7-9); Z = (I - KH) Sp
+  //         (steps 8-9); during the gain solve (steps 4-6) both hold the FP64
+  //         right-hand sides Wm (dy rows of LW doubles fit in 2 * DXP * LD floats)
+  //   PK  : P H' (steps 3-6), then K R (steps 7-9)
+  double S[DYP * LY], dinv[DYP], z[DYP], w[DYP], red[32];
+  alignas(16) float XZ[2 * DXP * LD];
+  float A[DXP * LD], Q[DXP * LD], Sig[DXP * LD];
+  float H[DYP * LD], PK[DXP * LY], K[DXP * LY], R[DYP * LY];
   float mu[DXP], mup[DXP], b[DXP], c[DYP];
-  double z[DYP], w[DYP];
-  double red[32];
   int fid, fail;
+  static_assert(DYP * LW * sizeof(double) <= 2 * DXP * LD * sizeof(float), "Wm must fit in XZ");
 };
 
 __device__ __forceinline__ void group_sync() { __syncthreads(); }
@@ -117,26 +123,26 @@ __device__ bool kf_chol(KfSmem<DXP, DYP>& s, int dy) {
 // columns [0, nf), then back L' X = Y over columns [0, nb).  Lane = row, warps
 // take interleaved column sets; dy <= 32.
 template <int DXP, int DYP>
-__device__ void kf_solves(KfSmem<DXP, DYP>& s, int dy, int nf, int nb) {
+__device__ void kf_solves(KfSmem<DXP, DYP>& s, double* Wm, int dy, int nf, int nb) {
   constexpr int LY = KfSmem<DXP, DYP>::LY, LW = KfSmem<DXP, DYP>::LW;
   const int r = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int i = 0; i < dy; ++i) {
     if (r == i)
-      for (int c = w; c < nf; c += nw) s.Wm[i * LW + c] *= s.dinv[i];
+      for (int c = w; c < nf; c += nw) Wm[i * LW + c] *= s.dinv[i];
     __syncwarp();
     if (r > i && r < dy) {
       const double l = s.S[r * LY + i];
-      for (int c = w; c < nf; c += nw) s.Wm[r * LW + c] -= l * s.Wm[i * LW + c];
+      for (int c = w; c < nf; c += nw) Wm[r * LW + c] -= l * Wm[i * LW + c];
     }
     __syncwarp();
   }
   for (int i = dy - 1; i >= 0; --i) {
     if (r == i)
-      for (int c = w; c < nb; c += nw) s.Wm[i * LW + c] *= s.dinv[i];
+      for (int c = w; c < nb; c += nw) Wm[i * LW + c] *= s.dinv[i];
     __syncwarp();
     if (r < i) {
       const double l = s.S[i * LY + r];
-      for (int c = w; c < nb; c += nw) s.Wm[r * LW + c] -= l * s.Wm[i * LW + c];
+      for (int c = w; c < nb; c += nw) Wm[r * LW + c] -= l * Wm[i * LW + c];
     }
     __syncwarp();
   }
@@ -167,6 +173,13 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
   extern __shared__ __align__(16) unsigned char smraw[];
   SM& s = *reinterpret_cast<SM*>(smraw);
   const int G = blockDim.x;
+  float* const T1 = s.XZ;                      // A Sig
+  float* const IKH = s.XZ;                     // I - K H
+  float* const T2 = s.XZ + DXP * LD;           // (I - K H) Sp
+  float* const Sp = s.Sig;                     // predicted covariance
+  float* const PHt = s.PK;
+  float* const KR = s.PK;
+  double* const Wm = reinterpret_cast<double*>(s.XZ);
   while (true) {
     if (threadIdx.x == 0) {
       unsigned k = atomicAdd(run.counter, 1u);
@@ -195,7 +208,7 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       for (int j = tx; j < dx; j += nx) {
         float acc = 0.f;
         for (int k = 0; k < dx; ++k) acc = fmaf(s.A[i * LD + k], s.Sig[k * LD + j], acc);
-        s.T1[i * LD + j] = acc;
+        T1[i * LD + j] = acc;
       }
       for (int i = threadIdx.x; i < dx; i += G) {
         float acc = s.b[i];
@@ -208,17 +221,17 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       for (int j = tx; j < dx; j += nx) {
         if (j < i) continue;
         float acc = s.Q[i * LD + j];
-        for (int k = 0; k < dx; ++k) acc = fmaf(s.T1[i * LD + k], s.A[j * LD + k], acc);
-        s.Sp[i * LD + j] = acc;
-        s.Sp[j * LD + i] = acc;
+        for (int k = 0; k < dx; ++k) acc = fmaf(T1[i * LD + k], s.A[j * LD + k], acc);
+        Sp[i * LD + j] = acc;
+        Sp[j * LD + i] = acc;
       }
       group_sync();
       // 3. PHt = Sp H' ; z = y - H mup - c
       for (int i = uy; i < dx; i += my)
       for (int j = ux; j < dy; j += mx) {
         float acc = 0.f;
-        for (int k = 0; k < dx; ++k) acc = fmaf(s.Sp[i * LD + k], s.H[j * LD + k], acc);
-        s.PHt[i * LY + j] = acc;
+        for (int k = 0; k < dx; ++k) acc = fmaf(Sp[i * LD + k], s.H[j * LD + k], acc);
+        PHt[i * LY + j] = acc;
       }
       for (int i = threadIdx.x; i < dy; i += G) {
         double acc = y[i] - (double)s.c[i];
@@ -230,7 +243,7 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       for (int i = uy; i < dy; i += my)
       for (int j = ux; j <= i; j += mx) {
         double acc = (double)s.R[i * LY + j];
-        for (int k = 0; k < dx; ++k) acc += (double)s.H[i * LD + k] * (double)s.PHt[k * LY + j];
+        for (int k = 0; k < dx; ++k) acc += (double)s.H[i * LD + k] * (double)PHt[k * LY + j];
         s.S[i * LY + j] = acc;
       }
       group_sync();
@@ -243,12 +256,12 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       //    back solve of the first dx columns gives K' = S^-1 PHt'
       constexpr int LW = SM::LW;
       for (int c = ty; c <= dx; c += ny)
-        for (int i = tx; i < dy; i += nx) s.Wm[i * LW + c] = c < dx ? (double)s.PHt[c * LY + i] : s.z[i];
+        for (int i = tx; i < dy; i += nx) Wm[i * LW + c] = c < dx ? (double)PHt[c * LY + i] : s.z[i];
       __syncthreads();
-      kf_solves<DXP, DYP>(s, dy, dx + 1, dx);
-      for (int i = threadIdx.x; i < dy; i += G) s.w[i] = s.Wm[i * LW + dx];
+      kf_solves<DXP, DYP>(s, Wm, dy, dx + 1, dx);
+      for (int i = threadIdx.x; i < dy; i += G) s.w[i] = Wm[i * LW + dx];
       for (int i = uy; i < dx; i += my)
-        for (int j = ux; j < dy; j += mx) s.K[i * LY + j] = (float)s.Wm[j * LW + i];
+        for (int j = ux; j < dy; j += mx) s.K[i * LY + j] = (float)Wm[j * LW + i];
       group_sync();
       // 7. mu = mup + K z ; IKH = I - K H ; KR = K R
       for (int i = threadIdx.x; i < dx; i += G) {
@@ -260,21 +273,21 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       for (int j = tx; j < dx; j += nx) {
         float acc = (i == j) ? 1.f : 0.f;
         for (int k = 0; k < dy; ++k) acc = fmaf(-s.K[i * LY + k], s.H[k * LD + j], acc);
-        s.IKH[i * LD + j] = acc;
+        IKH[i * LD + j] = acc;
       }
       for (int i = uy; i < dx; i += my)
       for (int j = ux; j < dy; j += mx) {
         float acc = 0.f;
         for (int k = 0; k < dy; ++k) acc = fmaf(s.K[i * LY + k], s.R[k * LY + j], acc);
-        s.KR[i * LY + j] = acc;
+        KR[i * LY + j] = acc;
       }
       group_sync();
       // 8. T1 = IKH Sp
       for (int i = ty; i < dx; i += ny)
       for (int j = tx; j < dx; j += nx) {
         float acc = 0.f;
-        for (int k = 0; k < dx; ++k) acc = fmaf(s.IKH[i * LD + k], s.Sp[k * LD + j], acc);
-        s.T1[i * LD + j] = acc;
+        for (int k = 0; k < dx; ++k) acc = fmaf(IKH[i * LD + k], Sp[k * LD + j], acc);
+        T2[i * LD + j] = acc;
       }
       group_sync();
       // 9. Sig = T1 IKH' + KR K' (+ jitter I), upper triangle mirrored
@@ -283,8 +296,8 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       for (int j = tx; j < dx; j += nx) {
         if (j < i) continue;
         float acc = 0.f;
-        for (int k = 0; k < dx; ++k) acc = fmaf(s.T1[i * LD + k], s.IKH[j * LD + k], acc);
-        for (int k = 0; k < dy; ++k) acc = fmaf(s.KR[i * LY + k], s.K[j * LY + k], acc);
+        for (int k = 0; k < dx; ++k) acc = fmaf(T2[i * LD + k], IKH[j * LD + k], acc);
+        for (int k = 0; k < dy; ++k) acc = fmaf(KR[i * LY + k], s.K[j * LY + k], acc);
         if (run.use_jitter && i == j) acc += (float)run.jitter;
         s.Sig[i * LD + j] = acc;
         s.Sig[j * LD + i] = acc;
