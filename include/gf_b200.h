@@ -152,6 +152,15 @@ gf_status gf_kf_batch(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int3
                       const int32_t* T, const double* ys, double jitter, int32_t use_jitter,
                       int32_t memspace, gf_kf_out* out);
 
+/* smooth(model, KalmanSmoother(), ys) for B models (kalman.jl:206-234): the
+ * forward Kalman filter (no jitter), then the Rauch-Tung-Striebel pass of
+ * backward_smooth (kalman.jl:89-126) from T-1 down to 1.  out->means and
+ * out->covs (required) receive the SMOOTHED p(x_t | y_1:T) of every step,
+ * packed like gf_kf_batch's outputs (the reference returns the one at t_smooth;
+ * every t is given here).  out->ll / ll_steps are the forward log-likelihoods. */
+gf_status gf_kf_smooth(gf_ctx* ctx, const gf_lg_model* models, int32_t B, const int32_t* T,
+                       const double* ys, int32_t memspace, gf_kf_out* out);
+
 /* Batched plan: uploads the models once, buckets filters by dimension,
  * autotunes the per-bucket group shape and captures one CUDA graph of
  * persistent launches.  Run with device-resident ys and outputs. */

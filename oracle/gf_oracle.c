@@ -415,6 +415,90 @@ done:
   return st;
 }
 
+/* smooth(model, KalmanSmoother(), ys) (kalman.jl:206-234) with the RTS step of
+ * backward_smooth (kalman.jl:89-126): the forward filter(model, KalmanFilter(),
+ * ys) without jitter, then for t = T-1 down to 1
+ *   mu_pred = A mu_f + b, Sigma_pred = A Sigma_f A' + Q,
+ *   G = Sigma_f A' Sigma_pred^-1 (Cholesky solve; Sigma_pred as PDMat),
+ *   mu_s = mu_f + G (mu_s' - mu_pred), Sigma_s = Sigma_f + G (Sigma_s' - Sigma_pred) G',
+ *   Sigma_s symmetrised from its upper triangle (PDMat(Symmetric(.))).
+ * Outputs the smoothed mus[T*dx] and Sigmas[T*dx*dx] (column-major) for every t;
+ * the last step is the filtered one.  *ll gets the forward log-likelihood. */
+int or_rts_smooth(const or_lg_model* m, int T, const double* ys, double* ll, double* mus,
+                  double* Sigmas) {
+  const int dx = m->dx;
+  int st = or_kf_filter(m, T, ys, 0.0, 0, ll, NULL, mus, Sigmas);
+  if (st) return st;
+  const size_t n2 = (size_t)dx * dx;
+  double *mp = malloc(8 * dx), *d = malloc(8 * dx), *ms = malloc(8 * dx);
+  double *T1 = malloc(8 * n2), *Sp = malloc(8 * n2), *L = malloc(8 * n2), *X = malloc(8 * n2);
+  double *D = malloc(8 * n2), *T2 = malloc(8 * n2), *Ss = malloc(8 * n2);
+  const double *A = m->A, *b = m->b, *Q = m->Q;
+  for (int t = T - 2; t >= 0 && !st; --t) {
+    const double* mf = mus + (size_t)t * dx;
+    const double* Sf = Sigmas + (size_t)t * n2;
+    const double* mn = mus + (size_t)(t + 1) * dx;   /* smoothed at t+1 */
+    const double* Sn = Sigmas + (size_t)(t + 1) * n2;
+    for (int i = 0; i < dx; ++i) {
+      double v = b[i];
+      for (int k = 0; k < dx; ++k) v += A[i + k * dx] * mf[k];
+      mp[i] = v;
+    }
+    for (int j = 0; j < dx; ++j)
+      for (int i = 0; i < dx; ++i) {
+        double v = 0.0;
+        for (int k = 0; k < dx; ++k) v += A[i + k * dx] * Sf[k + j * dx];
+        T1[i + j * dx] = v; /* A Sigma_f */
+      }
+    /* Sigma_pred = X_A_Xt(Sigma_f, A) + Q through the Cholesky factor of Sigma_f
+     * (kalman_predict, kalman.jl:42-49) */
+    if ((st = or_chol_lower(dx, Sf, L))) break;
+    x_a_xt_chol(dx, dx, A, L, Sp, D);
+    for (size_t e = 0; e < n2; ++e) Sp[e] += Q[e];
+    if ((st = or_chol_lower(dx, Sp, L))) break;
+    /* G' = Sigma_pred^-1 (A Sigma_f): column by column, L L' x = T1(:, j) */
+    for (int j = 0; j < dx; ++j) {
+      double* x = X + (size_t)j * dx;
+      for (int i = 0; i < dx; ++i) x[i] = T1[i + j * dx];
+      for (int i = 0; i < dx; ++i) { /* forward */
+        double v = x[i];
+        for (int k = 0; k < i; ++k) v -= L[i + k * dx] * x[k];
+        x[i] = v / L[i + i * dx];
+      }
+      for (int i = dx - 1; i >= 0; --i) { /* back (L') */
+        double v = x[i];
+        for (int k = i + 1; k < dx; ++k) v -= L[k + i * dx] * x[k];
+        x[i] = v / L[i + i * dx];
+      }
+    }
+    /* X(:, j) = G'(:, j) = G(j, :), i.e. G[i][k] = X[k + i*dx] */
+    for (int i = 0; i < dx; ++i) d[i] = mn[i] - mp[i];
+    for (int i = 0; i < dx; ++i) {
+      double v = mf[i];
+      for (int k = 0; k < dx; ++k) v += X[k + i * dx] * d[k];
+      ms[i] = v;
+    }
+    for (size_t e = 0; e < n2; ++e) D[e] = Sn[e] - Sp[e];
+    for (int j = 0; j < dx; ++j)
+      for (int i = 0; i < dx; ++i) {
+        double v = 0.0;
+        for (int k = 0; k < dx; ++k) v += X[k + i * dx] * D[k + j * dx];
+        T2[i + j * dx] = v; /* G D */
+      }
+    for (int j = 0; j < dx; ++j)
+      for (int i = 0; i <= j; ++i) {
+        double v = Sf[i + j * dx];
+        for (int k = 0; k < dx; ++k) v += T2[i + k * dx] * X[k + j * dx];
+        Ss[i + j * dx] = v;
+        Ss[j + i * dx] = v;
+      }
+    memcpy(mus + (size_t)t * dx, ms, 8 * dx);
+    memcpy(Sigmas + (size_t)t * n2, Ss, 8 * n2);
+  }
+  free(mp); free(d); free(ms); free(T1); free(Sp); free(L); free(X); free(D); free(T2); free(Ss);
+  return st;
+}
+
 /* ------------------------------------------------------------------------ */
 /* Square-root Kalman filter (srkf.jl:93-176).                               */
 /* Householder QR of M (m x n, m >= n), returns R (n x n upper, col-major)

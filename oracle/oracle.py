@@ -132,6 +132,41 @@ def kf_filter(m: LGModel, ys, jitter=None, algo="kf"):
     return ll.value, lls, mus, np.ascontiguousarray(sig.transpose(0, 2, 1))
 
 
+def rts_smooth(m: LGModel, ys):
+    """smooth(model, KalmanSmoother(), ys) for every t -> (ll, mus[T,dx], Sigmas[T,dx,dx])
+    (kalman.jl:89-126,206-234)."""
+    ys = _f64(ys).reshape(-1, m.dy)
+    T = ys.shape[0]
+    ll = C.c_double()
+    mus = np.zeros((T, m.dx))
+    sig = np.zeros((T, m.dx, m.dx))
+    st = lib().or_rts_smooth(C.byref(m._struct()), T, _p(ys), C.byref(ll), _p(mus), _p(sig))
+    if st:
+        raise np.linalg.LinAlgError(f"oracle RTS status {st}")
+    return ll.value, mus, np.ascontiguousarray(sig.transpose(0, 2, 1))
+
+
+def joint_smooth_truth(m: LGModel, ys):
+    """Exact smoothed means/covariances of X_1..X_T given y_1:T by Gaussian
+    conditioning of the joint of compute_joint (the analytic counterpart of the
+    RTS pass)."""
+    ys = np.asarray(ys, np.float64).reshape(-1, m.dy)
+    T = ys.shape[0]
+    mu_Z, S_Z = compute_joint(m, T)
+    Dx, Dy = m.dx, m.dy
+    Iy = slice(Dx * (T + 1), Dx * (T + 1) + T * Dy)
+    Syy = S_Z[Iy, Iy]
+    Syy = (Syy + Syy.T) / 2
+    d = ys.ravel() - mu_Z[Iy]
+    w = np.linalg.solve(Syy, d)
+    mus, Ss = [], []
+    for t in range(1, T + 1):
+        Ix = slice(t * Dx, (t + 1) * Dx)
+        mus.append(mu_Z[Ix] + S_Z[Ix, Iy] @ w)
+        Ss.append(S_Z[Ix, Ix] - S_Z[Ix, Iy] @ np.linalg.solve(Syy, S_Z[Iy, Ix]))
+    return np.array(mus), np.array(Ss)
+
+
 def pf_run(m: LGModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=0.5,
            schedule=None, noise=None, uniforms=None, seed=0, proposal=PROP_BOOTSTRAP,
            k=1.0, want_ancestors=False, want_margins=False, threads=1):

@@ -557,18 +557,191 @@ __global__ void __launch_bounds__(256) srkf_batch_kernel(KfRun run) {
   }
 }
 
+
+// ------------------------------------------------------------ RTS smoother
+// smooth(model, KalmanSmoother(), ys) (kalman.jl:206-234): after the forward
+// bank wrote the filtered means / covariances of every step (run.means,
+// run.covs), one block per filter walks t = T-1 .. 1 and overwrites step t
+// with the smoothed distribution (backward_smooth, kalman.jl:89-126):
+//   mu_pred = A mu_f + b, Sigma_pred = A Sigma_f A' + Q,
+//   G' = Sigma_pred^-1 (A Sigma_f)          (FP64 Cholesky and solves),
+//   mu_s = mu_f + G (mu_s' - mu_pred),
+//   Sigma_s = Sigma_f + G (Sigma_s' - Sigma_pred) G'   (upper triangle mirrored).
+template <int DXP>
+struct RtsSmem {
+  static constexpr int LD = DXP + 1;
+  double Lc[DXP * LD];  // Sigma_pred, then its Cholesky factor (lower)
+  double X[DXP * LD];   // right-hand sides A Sigma_f, then G' (row k, column i = G[i][k])
+  double dinv[DXP];
+  float A[DXP * LD], Q[DXP * LD], Sf[DXP * LD], Sn[DXP * LD], T1[DXP * LD], D[DXP * LD];
+  float b[DXP], mf[DXP], mn[DXP], mp[DXP], dd[DXP];
+  int fid, fail;
+};
+
+template <int DXP>
+__global__ void __launch_bounds__(256) rts_smooth_kernel(KfRun run) {
+  using SM = RtsSmem<DXP>;
+  constexpr int LD = SM::LD;
+  extern __shared__ __align__(16) unsigned char smraw[];
+  SM& s = *reinterpret_cast<SM*>(smraw);
+  const int G = blockDim.x;
+  while (true) {
+    if (threadIdx.x == 0) {
+      unsigned k = atomicAdd(run.counter, 1u);
+      s.fid = k < (unsigned)run.count ? run.order[k] : -1;
+      s.fail = 0;
+    }
+    __syncthreads();
+    const int f = s.fid;
+    if (f < 0) return;
+    const KfDesc D = run.desc[f];
+    const int dx = D.dx, T = D.T;
+    if (run.status[D.index] != GF_OK || T < 2) {
+      __syncthreads();
+      continue;
+    }
+    const float* P = run.params + D.poff;  // A dx*dx | b dx | Q dx*dx | ...
+    for (int e = threadIdx.x; e < dx * dx; e += G) {
+      const int i = e % dx, j = e / dx;  // column-major source
+      s.A[i * LD + j] = P[e];
+      s.Q[i * LD + j] = P[dx * dx + dx + e];
+      s.Sn[i * LD + j] = run.covs[D.coff + (int64_t)(T - 1) * dx * dx + e];
+    }
+    for (int e = threadIdx.x; e < dx; e += G) {
+      s.b[e] = P[dx * dx + e];
+      s.mn[e] = run.means[D.moff + (int64_t)(T - 1) * dx + e];
+    }
+    __syncthreads();
+    for (int t = T - 2; t >= 0; --t) {
+      float* cov = run.covs + D.coff + (int64_t)t * dx * dx;
+      float* mean = run.means + D.moff + (int64_t)t * dx;
+      for (int e = threadIdx.x; e < dx * dx; e += G) s.Sf[(e % dx) * LD + e / dx] = cov[e];
+      for (int e = threadIdx.x; e < dx; e += G) s.mf[e] = mean[e];
+      __syncthreads();
+      // T1 = A Sigma_f ; mu_pred = A mu_f + b
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        const int i = e / dx, j = e - i * dx;
+        float acc = 0.f;
+        for (int k = 0; k < dx; ++k) acc = fmaf(s.A[i * LD + k], s.Sf[k * LD + j], acc);
+        s.T1[i * LD + j] = acc;
+      }
+      for (int i = threadIdx.x; i < dx; i += G) {
+        float acc = s.b[i];
+        for (int k = 0; k < dx; ++k) acc = fmaf(s.A[i * LD + k], s.mf[k], acc);
+        s.mp[i] = acc;
+      }
+      __syncthreads();
+      // Sigma_pred = T1 A' + Q (FP64 copy for the Cholesky), D = Sigma_s' - Sigma_pred,
+      // right-hand sides X = T1 ; dd = mu_s' - mu_pred
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        const int i = e / dx, j = e - i * dx;
+        const int lo = i < j ? i : j, hi = i < j ? j : i;  // upper triangle, mirrored
+        float acc = s.Q[lo * LD + hi];
+        for (int k = 0; k < dx; ++k) acc = fmaf(s.T1[lo * LD + k], s.A[hi * LD + k], acc);
+        s.Lc[i * LD + j] = (double)acc;
+        s.D[i * LD + j] = s.Sn[i * LD + j] - acc;
+        s.X[i * LD + j] = (double)s.T1[i * LD + j];
+      }
+      for (int i = threadIdx.x; i < dx; i += G) s.dd[i] = s.mn[i] - s.mp[i];
+      __syncthreads();
+      // FP64 Cholesky, warp 0, one lane per row (right-looking)
+      if (threadIdx.x < 32) {
+        const int r = threadIdx.x;
+        for (int j = 0; j < dx; ++j) {
+          const double djj = s.Lc[j * LD + j];
+          if (!(djj > 0.0)) {
+            if (r == 0) s.fail = 1;
+            break;
+          }
+          const double dj = sqrt(djj), inv = 1.0 / dj;
+          double lrj = 0.0;
+          if (r > j && r < dx) {
+            lrj = s.Lc[r * LD + j] * inv;
+            s.Lc[r * LD + j] = lrj;
+          }
+          if (r == j) {
+            s.Lc[j * LD + j] = dj;
+            s.dinv[j] = inv;
+          }
+          __syncwarp();
+          if (r > j && r < dx)
+            for (int k = j + 1; k <= r; ++k) s.Lc[r * LD + k] -= lrj * s.Lc[k * LD + j];
+          __syncwarp();
+        }
+      }
+      __syncthreads();
+      if (s.fail) break;
+      // X = Sigma_pred^-1 X: lane = row, warps take interleaved columns
+      {
+        const int r = threadIdx.x & 31, w = threadIdx.x >> 5, nw = G >> 5;
+        for (int i = 0; i < dx; ++i) {
+          if (r == i)
+            for (int c = w; c < dx; c += nw) s.X[i * LD + c] *= s.dinv[i];
+          __syncwarp();
+          if (r > i && r < dx) {
+            const double l = s.Lc[r * LD + i];
+            for (int c = w; c < dx; c += nw) s.X[r * LD + c] -= l * s.X[i * LD + c];
+          }
+          __syncwarp();
+        }
+        for (int i = dx - 1; i >= 0; --i) {
+          if (r == i)
+            for (int c = w; c < dx; c += nw) s.X[i * LD + c] *= s.dinv[i];
+          __syncwarp();
+          if (r < i) {
+            const double l = s.Lc[i * LD + r];
+            for (int c = w; c < dx; c += nw) s.X[r * LD + c] -= l * s.X[i * LD + c];
+          }
+          __syncwarp();
+        }
+      }
+      __syncthreads();
+      // mu_s = mu_f + G dd (G[i][k] = X[k][i]) ; T1 = G D
+      for (int i = threadIdx.x; i < dx; i += G) {
+        double acc = (double)s.mf[i];
+        for (int k = 0; k < dx; ++k) acc += s.X[k * LD + i] * (double)s.dd[k];
+        s.mn[i] = (float)acc;
+      }
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        const int i = e / dx, j = e - i * dx;
+        float acc = 0.f;
+        for (int k = 0; k < dx; ++k) acc = fmaf((float)s.X[k * LD + i], s.D[k * LD + j], acc);
+        s.T1[i * LD + j] = acc;
+      }
+      __syncthreads();
+      // Sigma_s = Sigma_f + T1 G' (upper triangle, mirrored) -> next and output
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        const int i = e / dx, j = e - i * dx;
+        if (j < i) continue;
+        float acc = s.Sf[i * LD + j];
+        for (int k = 0; k < dx; ++k) acc = fmaf(s.T1[i * LD + k], (float)s.X[k * LD + j], acc);
+        s.Sn[i * LD + j] = acc;
+        s.Sn[j * LD + i] = acc;
+      }
+      __syncthreads();
+      for (int e = threadIdx.x; e < dx * dx; e += G) cov[e] = s.Sn[(e % dx) * LD + e / dx];
+      for (int e = threadIdx.x; e < dx; e += G) mean[e] = s.mn[e];
+      __syncthreads();
+    }
+    if (threadIdx.x == 0 && s.fail) run.status[D.index] = GF_ERR_NOT_PD;
+    __syncthreads();
+  }
+}
+
 // ---------------------------------------------------------------- buckets
 struct KfBucketKernels {
   int dxp, dyp;
   void (*kf)(KfRun);
   void (*sr)(KfRun);
   size_t kf_smem, sr_smem;
+  void (*rts)(KfRun);
+  size_t rts_smem;
 };
 
 template <int DXP, int DYP>
 static KfBucketKernels make_bucket() {
   return {DXP, DYP, kf_batch_kernel<DXP, DYP>, srkf_batch_kernel<DXP, DYP>, sizeof(KfSmem<DXP, DYP>),
-          sizeof(SrSmem<DXP, DYP>)};
+          sizeof(SrSmem<DXP, DYP>), rts_smooth_kernel<DXP>, sizeof(RtsSmem<DXP>)};
 }
 
 static const std::vector<KfBucketKernels>& kf_buckets() {
@@ -1039,17 +1212,51 @@ extern "C" gf_status gf_kf_plan_destroy(gf_kf_plan* p) {
   return GF_OK;
 }
 
-extern "C" gf_status gf_kf_batch(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
-                                 const int32_t* T, const double* ys, double jitter,
-                                 int32_t use_jitter, int32_t memspace, gf_kf_out* out) {
+// RTS backward pass of every bucket over the filtered outputs in `out` (device).
+static gf_status kf_smooth_enqueue(gf_kf_plan* p, const gf_kf_out* out) {
+  gf_ctx* ctx = p->ctx;
+  cudaStream_t s = ctx->stream;
+  KfRun r{};
+  r.desc = p->desc;
+  r.params = p->params;
+  r.means = out->means;
+  r.covs = out->covs;
+  r.status = out->status;
+  GF_CHECK_CUDA(ctx, cudaMemsetAsync(p->counters, 0, sizeof(uint32_t) * 64, s));
+  for (size_t b = 0; b < p->buckets.size(); ++b) {
+    const auto& bk = p->buckets[b];
+    const KfBucketKernels& K = kf_buckets()[bk.kidx];
+    GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)K.rts, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)K.rts_smem));
+    KfRun rb = r;
+    rb.order = p->order + bk.start;
+    rb.count = bk.count;
+    rb.counter = p->counters + b;
+    const int group = K.dxp <= 8 ? 32 : 128;
+    int per_sm = 1;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, (const void*)K.rts, group, K.rts_smem);
+    const int grid = std::max(1, std::min(bk.count, std::max(1, per_sm) * ctx->num_sms));
+    ProfScope ps(ctx, KC_KF);
+    K.rts<<<grid, group, K.rts_smem, s>>>(rb);
+  }
+  GF_CHECK_CUDA(ctx, cudaGetLastError());
+  return GF_OK;
+}
+
+static gf_status kf_batch_impl(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
+                               const int32_t* T, const double* ys, double jitter, int32_t use_jitter,
+                               int32_t memspace, gf_kf_out* out, bool smooth) {
   if (!ctx || !out || !ys) return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
+  if (smooth && (!out->means || !out->covs))
+    return set_err(ctx, GF_ERR_ARG, "smoothing needs out->means and out->covs");
   gf_kf_plan* p = nullptr;
   gf_status st = gf_kf_plan_create(ctx, algo, models, B, T, jitter, use_jitter, GF_PLAN_NO_GRAPH, &p);
   if (st) return st;
   std::unique_ptr<gf_kf_plan, gf_status (*)(gf_kf_plan*)> guard(p, gf_kf_plan_destroy);
   if (memspace == GF_MEM_DEVICE) {
     if (!out->status) return set_err(ctx, GF_ERR_ARG, "out->status is required");
-    return gf_kf_plan_run(p, ys, out);
+    if ((st = gf_kf_plan_run(p, ys, out))) return st;
+    return smooth ? kf_smooth_enqueue(p, out) : GF_OK;
   }
   // stage host buffers
   int64_t ny = 0;
@@ -1079,6 +1286,7 @@ extern "C" gf_status gf_kf_batch(gf_ctx* ctx, int32_t algo, const gf_lg_model* m
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(d_ys, ys, sizeof(double) * ny, cudaMemcpyHostToDevice, s));
   gf_kf_out d{(double*)d_ll, (double*)d_steps, (float*)d_means, (float*)d_covs, (int32_t*)d_status};
   if ((st = gf_kf_plan_run(p, (const double*)d_ys, &d))) return st;
+  if (smooth && (st = kf_smooth_enqueue(p, &d))) return st;
   if (out->ll) GF_CHECK_CUDA(ctx, cudaMemcpyAsync(out->ll, d_ll, sizeof(double) * B, cudaMemcpyDeviceToHost, s));
   std::vector<int32_t> hs(B);
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(hs.data(), d_status, sizeof(int32_t) * B, cudaMemcpyDeviceToHost, s));
@@ -1090,4 +1298,15 @@ extern "C" gf_status gf_kf_batch(gf_ctx* ctx, int32_t algo, const gf_lg_model* m
   for (int f = 0; f < B; ++f)
     if (hs[f] != GF_OK) return set_err(ctx, hs[f], "filter %d failed with status %d (S not positive definite)", f, hs[f]);
   return GF_OK;
+}
+
+extern "C" gf_status gf_kf_batch(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
+                                 const int32_t* T, const double* ys, double jitter,
+                                 int32_t use_jitter, int32_t memspace, gf_kf_out* out) {
+  return kf_batch_impl(ctx, algo, models, B, T, ys, jitter, use_jitter, memspace, out, false);
+}
+
+extern "C" gf_status gf_kf_smooth(gf_ctx* ctx, const gf_lg_model* models, int32_t B, const int32_t* T,
+                                  const double* ys, int32_t memspace, gf_kf_out* out) {
+  return kf_batch_impl(ctx, GF_ALGO_KF, models, B, T, ys, 0.0, 0, memspace, out, true);
 }

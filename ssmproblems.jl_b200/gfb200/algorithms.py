@@ -2,6 +2,7 @@
 
 * ``KalmanFilter(jitter=None)`` / ``KF()`` -- algorithms/kalman.jl:16-21
 * ``SRKalmanFilter(jitter=None)`` / ``SRKF()`` -- algorithms/srkf.jl:34-39
+* ``KalmanSmoother()`` / ``KS`` -- algorithms/kalman.jl:83-85
 * ``ParticleFilter(N, proposal; threshold=1.0, resampler=Systematic())`` and
   ``BootstrapFilter(N; ...)`` / ``BF`` -- algorithms/particles.jl:92-108,197-201
 * ``RBPF(pf, af)`` -- algorithms/rbpf.jl:8-14
@@ -95,6 +96,14 @@ class KalmanFilter(AbstractFilter):
 
 def KF():
     return KalmanFilter()
+
+
+class KalmanSmoother(AbstractFilter):
+    """KalmanSmoother() (kalman.jl:83-85): Rauch-Tung-Striebel smoothing after a
+    KalmanFilter() forward pass."""
+
+
+KS = KalmanSmoother()
 
 
 class SRKalmanFilter(AbstractFilter):

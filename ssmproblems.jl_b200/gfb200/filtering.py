@@ -12,7 +12,8 @@ import ctypes as C
 import numpy as np
 
 from . import _lib as L
-from .algorithms import (AlternatingResampler, ESSResampler, KalmanFilter, ParticleFilter, RBPF,
+from .algorithms import (AlternatingResampler, ESSResampler, KalmanFilter, KalmanSmoother,
+                         ParticleFilter, RBPF,
                          SRKalmanFilter)
 from .models import HierarchicalSSM, StateSpaceModel
 
@@ -208,6 +209,50 @@ def filter_batch(models, algo, observations, *, ctx=None, want_steps=True, want_
         mo += t * dx
         co += t * dx * dx
     return res
+
+
+def smooth_batch(models, observations, *, ctx=None):
+    """smooth(model, KalmanSmoother(), ys) for many models in one batched launch
+    set (kalman.jl:206-234).  Returns a list of (means [T, dx], covs [T, dx, dx],
+    ll): the smoothed p(x_t | y_1:T) of every step and the forward log-likelihood."""
+    ctx = _resolve_ctx(ctx)
+    B = len(models)
+    mcs = (L.LGModelC * B)(*[m._c_struct() for m in models])
+    ys_list = [L.f64(y).reshape(-1, m.dy) for y, m in zip(observations, models)]
+    T = np.array([y.shape[0] for y in ys_list], dtype=np.int32)
+    ys = np.concatenate([y.ravel() for y in ys_list]) if B else np.zeros(0)
+    dxs = np.array([m.dx for m in models])
+    out = dict(ll=np.zeros(B), ll_steps=None,
+               means=np.zeros(int((T * dxs).sum()), np.float32),
+               covs=np.zeros(int((T * dxs * dxs).sum()), np.float32),
+               status=np.zeros(B, np.int32))
+    o = L.KFOutC(*[L.ptr(out[k]) for k in ("ll", "ll_steps", "means", "covs", "status")])
+    L.check(ctx.h, L.load().gf_kf_smooth(ctx.h, mcs, B, T.ctypes.data_as(C.POINTER(C.c_int32)),
+                                         L.ptr(ys), L.GF_MEM_HOST, C.byref(o)))
+    res = []
+    mo = co = 0
+    for f, m in enumerate(models):
+        dx, t = m.dx, int(T[f])
+        means = out["means"][mo:mo + t * dx].reshape(t, dx)
+        covs = out["covs"][co:co + t * dx * dx].reshape(t, dx, dx).transpose(0, 2, 1)
+        res.append((means, covs, float(out["ll"][f])))
+        mo += t * dx
+        co += t * dx * dx
+    return res
+
+
+def smooth(model, algo, observations, *, t_smooth=1, ctx=None):
+    """smooth([rng,] model, KalmanSmoother(), observations; t_smooth=1) -> (MvNormal, ll)
+    (kalman.jl:206-234): the smoothed p(x_t | y_1:T) at t = t_smooth (1-based)."""
+    if not isinstance(algo, KalmanSmoother):
+        raise TypeError("smooth supports KalmanSmoother()")
+    means, covs, ll = smooth_batch([model], [observations], ctx=ctx)[0]
+    T = means.shape[0]
+    if not 1 <= t_smooth <= T:
+        raise ValueError(f"t_smooth must be in 1..{T}")
+    st = MvNormal(means[t_smooth - 1], covs[t_smooth - 1])
+    st.means, st.covs = means, covs
+    return st, ll
 
 
 # ------------------------------------------------------------ resampling API

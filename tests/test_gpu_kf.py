@@ -122,3 +122,50 @@ def test_plan_graph_matches_one_shot(ctx):
         assert int(st.abs().sum()) == 0
     finally:
         L.load().gf_kf_plan_destroy(plan)
+
+
+def _check_smooth(res, models, yss, mat_rtol=1e-3):
+    for (means, covs, ll), m, ys in zip(res, models, yss):
+        rll, rmus, rsig = O.rts_smooth(to_oracle(m), ys)
+        assert abs(ll - rll) <= 1e-4 * max(1.0, abs(rll)), (ll, rll)
+        scale_mu = np.abs(rmus).max(axis=1, keepdims=True) + 1e-3
+        assert np.all(np.abs(means - rmus) <= mat_rtol * scale_mu + 1e-5), np.abs(means - rmus).max()
+        scale_s = np.abs(rsig).reshape(len(ys), -1).max(axis=1)[:, None, None]
+        assert np.all(np.abs(covs - rsig) <= mat_rtol * scale_s + 1e-6), np.abs(covs - rsig).max()
+
+
+def test_rts_smoother_bank_matches_oracle(ctx):
+    """smooth(model, KalmanSmoother(), ys) (kalman.jl:89-126,206-234) for a bank of
+    uneven stable models covering every dimension bucket, against the FP64 oracle
+    (same tolerances as the filter)."""
+    models, Ts, _ = W.kf_bank(40, seed=3, dx_range=(2, 32), T_range=(2, 120), make_ys=False)
+    rng = np.random.default_rng(8)
+    yss = [simulate(rng, m, T)[1] for m, T in zip(models, Ts)]
+    res = G.smooth_batch(models, yss, ctx=ctx)
+    _check_smooth(res, models, yss)
+
+
+def test_rts_smoother_matches_joint_gaussian(ctx):
+    """Every smoothed marginal against Gaussian conditioning of the joint."""
+    rng = np.random.default_rng(17)
+    for Dy in (1, 2, 3):
+        m = random_lg(rng, 3, Dy)
+        _, ys = simulate(rng, m, 4)
+        means, covs, ll = G.smooth_batch([m], [ys], ctx=ctx)[0]
+        mt, St = O.joint_smooth_truth(to_oracle(m), ys)
+        np.testing.assert_allclose(means, mt, rtol=1e-4, atol=1e-5)
+        np.testing.assert_allclose(covs, St, rtol=1e-3, atol=1e-5)
+
+
+def test_smooth_api_t_smooth(ctx):
+    """smooth(...; t_smooth) returns that step; at t_smooth = T it is the filtered one."""
+    rng = np.random.default_rng(23)
+    m = random_lg(rng, 4, 2)
+    _, ys = simulate(rng, m, 12)
+    st1, ll = G.smooth(m, G.KalmanSmoother(), ys, ctx=ctx)
+    stT, _ = G.smooth(m, G.KS, ys, t_smooth=12, ctx=ctx)
+    fst, fll = G.filter(m, G.KalmanFilter(), ys, ctx=ctx)
+    assert ll == fll
+    np.testing.assert_array_equal(stT.mu, fst.mu)
+    np.testing.assert_array_equal(stT.Sigma, fst.Sigma)
+    np.testing.assert_array_equal(st1.mu, st1.means[0])

@@ -25,6 +25,21 @@ def test_kf_matches_joint_gaussian(Dy, T):
     np.testing.assert_allclose(S[-1], St, rtol=1e-8, atol=1e-12)
 
 
+@pytest.mark.parametrize("Dy", [1, 2, 3])
+@pytest.mark.parametrize("T", [1, 5])
+def test_rts_smoother_matches_joint_gaussian(Dy, T):
+    """smooth(model, KalmanSmoother(), ys) (kalman.jl:89-126,206-234): every
+    smoothed marginal p(x_t | y_1:T) equals Gaussian conditioning of the joint."""
+    rng = np.random.default_rng(77 + Dy + 10 * T)
+    m = O.create_linear_gaussian_model(rng, 3, Dy)
+    _, ys = O.sample(rng, m, T)
+    ll, mus, S = O.rts_smooth(m, ys)
+    mt, St = O.joint_smooth_truth(m, ys)
+    assert ll == O.kf_filter(m, ys)[0]
+    np.testing.assert_allclose(mus, mt, rtol=1e-9, atol=1e-11)
+    np.testing.assert_allclose(S, St, rtol=1e-8, atol=1e-11)
+
+
 @pytest.mark.parametrize("Dy", [2, 3, 4])
 def test_srkf_equals_kf(Dy):
     """test/algorithms/srkf.jl:3-26."""
