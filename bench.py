@@ -7,7 +7,7 @@ ESS < 0.5 N, FP64 normaliser and cumulative weights, in-kernel Philox noise.
 One step = one full filter run (N * T particle-steps).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload pf|pf1d|kf|rbpf|serve]
+                    [--workload pf|pf1d|kf|smooth|rbpf|serve]
 
 Under torchrun each rank runs an independent replica (the filters shard by
 filter; no data-path collective).  Rank 0 prints one JSON line.
@@ -682,6 +682,71 @@ def bench_pf1d(args, world, rank, local):
     return line
 
 
+def bench_smooth(args, world, rank, local):
+    """RTS smoother (smooth(model, KalmanSmoother(), ys)) over a bank of uneven
+    LGSSMs (Dx 2..32, Dy 1..Dx, T 64..2048): forward Kalman bank plus the
+    backward pass, smoothed means and covariances of every step, on a resident
+    plan.  One step = one smoothing run of the whole bank."""
+    import torch
+    import gfb200 as G
+    from gfb200 import workloads as W
+    from gfb200.plans import KfPlan
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    ctx = G.Context(local)
+    B = args.smooth_filters
+    models, Ts, _ = W.kf_bank(B, seed=7 + rank, make_ys=False)
+    plan = KfPlan(models, G.KalmanFilter(), Ts, ctx=ctx)
+    ys = torch.randn(plan.n_y, dtype=torch.float64, device=dev)
+    means = torch.empty(plan.n_means, dtype=torch.float32, device=dev)
+    covs = torch.empty(plan.n_covs, dtype=torch.float32, device=dev)
+    for _ in range(args.warmup):
+        plan.smooth(ys, means, covs)
+    ctx.synchronize()
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    _barrier(world)
+    with ClockSampler(local) as clk:
+        e0.record(ext)
+        for _ in range(args.steps):
+            plan.smooth(ys, means, covs)
+        e1.record(ext)
+        e1.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1), world, dev)
+    assert int(plan.status.abs().sum().item()) == 0
+    ctx.profile(True)
+    plan.smooth(ys, means, covs)
+    kms, kn = ctx.profile_read(2)
+    ctx.profile(False)
+    n_steps = plan.n_steps
+    value = n_steps * args.steps * world / (ms / 1e3)
+    dxs = np.array([m.dx for m in models], dtype=np.float64)
+    dys = np.array([m.dy for m in models], dtype=np.float64)
+    Tarr = np.array(Ts, dtype=np.float64)
+    # forward outputs, then the backward pass reads them and rewrites them
+    bytes_run = float(np.sum(Tarr * (8 * dys + 8 + 3 * (4 * dxs + 4 * dxs * dxs))))
+    run_s = ms / 1e3 / args.steps
+    peak, peak_kind = _peaks()
+    line = {
+        "metric": "smoothed KF-steps/s", "value": value, "unit": "KF-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": f"RTS smoother over {B} uneven LGSSMs, Dx~U{{2..32}}, Dy~U{{1..Dx}}, "
+                               "T~U{64..2048}: forward Kalman bank + backward pass, smoothed means and "
+                               "covariances of every step", "filters": B, "kf_steps": n_steps,
+                   "l2": "outputs far larger than L2 (no flush)"},
+        "roofline": {"bound": "hbm", "achieved": bytes_run / run_s / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": bytes_run / run_s / 1e9 / peak, "traffic": None, "peak_source": peak_kind},
+        "gpu_launches": int(kn),
+        "kernel_ms_per_run": kms,
+        "clocks": clk.summary(),
+    }
+    plan.close()
+    ctx.close()
+    return line
+
+
 def bench_reference(args, world, rank, local):
     """The reference arm: the FP64 oracle port of the reference algorithm on the
     host cores (the reference is Julia and cannot run on this image)."""
@@ -715,7 +780,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pf", choices=["pf", "pf1d", "kf", "rbpf", "serve"])
+    ap.add_argument("--workload", default="pf", choices=["pf", "pf1d", "kf", "smooth", "rbpf", "serve"])
+    ap.add_argument("--smooth-filters", type=int, default=16384)
     ap.add_argument("--serve-rate", type=float, default=1000.0)
     ap.add_argument("--serve-requests", type=int, default=2000)
     ap.add_argument("--serve-hbm-gb", type=int, default=64)
@@ -741,6 +807,8 @@ def main():
         line = bench_kf(args, world, rank, local)
     elif args.workload == "serve":
         line = bench_serve(args, world, rank, local)
+    elif args.workload == "smooth":
+        line = bench_smooth(args, world, rank, local)
     elif args.workload == "rbpf":
         line = bench_rbpf(args, world, rank, local)
     elif args.workload == "pf1d":

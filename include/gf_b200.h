@@ -169,6 +169,9 @@ gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_model* models
                             const int32_t* T, double jitter, int32_t use_jitter,
                             int32_t flags, gf_kf_plan** out);
 gf_status gf_kf_plan_run(gf_kf_plan* plan, const double* ys_dev, gf_kf_out* out_dev);
+/* Forward run plus the RTS pass (as gf_kf_smooth) on a KalmanFilter() plan
+ * without jitter; out_dev->means and covs receive the smoothed moments. */
+gf_status gf_kf_plan_smooth(gf_kf_plan* plan, const double* ys_dev, gf_kf_out* out_dev);
 gf_status gf_kf_plan_destroy(gf_kf_plan* plan);
 /* plan flags: AUTOTUNE (KF: time each bucket's block shapes and keep the
  * fastest), NO_GRAPH (launch eagerly instead of replaying a CUDA graph), PLAIN

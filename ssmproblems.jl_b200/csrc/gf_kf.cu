@@ -1310,3 +1310,13 @@ extern "C" gf_status gf_kf_smooth(gf_ctx* ctx, const gf_lg_model* models, int32_
                                   const double* ys, int32_t memspace, gf_kf_out* out) {
   return kf_batch_impl(ctx, GF_ALGO_KF, models, B, T, ys, 0.0, 0, memspace, out, true);
 }
+
+extern "C" gf_status gf_kf_plan_smooth(gf_kf_plan* p, const double* ys_dev, gf_kf_out* out) {
+  if (!p || !ys_dev || !out || !out->ll || !out->status || !out->means || !out->covs)
+    return p ? set_err(p->ctx, GF_ERR_ARG, "ys, out->ll, status, means and covs are required") : GF_ERR_ARG;
+  if (p->algo != GF_ALGO_KF || p->use_jitter)
+    return set_err(p->ctx, GF_ERR_ARG, "smoothing runs on a KalmanFilter() plan without jitter");
+  gf_status st = gf_kf_plan_run(p, ys_dev, out);
+  if (st) return st;
+  return kf_smooth_enqueue(p, out);
+}

@@ -28,7 +28,7 @@ GF_REQ_KF, GF_REQ_SRKF, GF_REQ_PF, GF_REQ_RBPF = 0, 1, 2, 3
 EXPORTED = [
     "gf_ctx_create", "gf_ctx_destroy", "gf_last_error", "gf_ctx_set_stream", "gf_ctx_get_stream",
     "gf_ctx_synchronize", "gf_ctx_memory", "gf_ctx_profile", "gf_ctx_profile_read", "gf_version",
-    "gf_kf_batch", "gf_kf_smooth", "gf_kf_plan_create", "gf_kf_plan_run", "gf_kf_plan_destroy",
+    "gf_kf_batch", "gf_kf_smooth", "gf_kf_plan_create", "gf_kf_plan_run", "gf_kf_plan_smooth", "gf_kf_plan_destroy",
     "gf_pf_run", "gf_pf_plan_create", "gf_pf_plan_run", "gf_pf_plan_destroy", "gf_rbpf_run",
     "gf_sample_ancestors", "gf_offspring_to_ancestors", "gf_ancestors_to_offspring",
     "gf_rng_normals", "gf_sample_ancestors_noalloc", "gf_sample_ancestors_noalloc_max_n",
@@ -141,6 +141,7 @@ def load(path: str | None = None):
         "gf_kf_plan_create": (i32, [ctxp, i32, C.POINTER(LGModelC), i32, C.POINTER(i32), dbl,
                                     i32, i32, C.POINTER(_vp)]),
         "gf_kf_plan_run": (i32, [_vp, _vp, C.POINTER(KFOutC)]),
+        "gf_kf_plan_smooth": (i32, [_vp, _vp, C.POINTER(KFOutC)]),
         "gf_kf_plan_destroy": (i32, [_vp]),
         "gf_pf_run": (i32, [ctxp, C.POINTER(LGModelC), C.POINTER(PFConfigC), i32, _vp, _vp,
                             _vp, i32, C.POINTER(PFOutC)]),

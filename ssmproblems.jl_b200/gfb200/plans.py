@@ -84,6 +84,12 @@ class KfPlan:
                      L.ptr(self.status))
         L.check(self.ctx.h, L.load().gf_kf_plan_run(self.h, L.ptr(ys_dev), C.byref(o)))
 
+    def smooth(self, ys_dev, means, covs, ll_steps=None):
+        """Forward run and RTS pass: means / covs receive the smoothed moments."""
+        o = L.KFOutC(L.ptr(self.ll), L.ptr(ll_steps), L.ptr(means), L.ptr(covs),
+                     L.ptr(self.status))
+        L.check(self.ctx.h, L.load().gf_kf_plan_smooth(self.h, L.ptr(ys_dev), C.byref(o)))
+
     def close(self):
         if self.h:
             L.load().gf_kf_plan_destroy(self.h)

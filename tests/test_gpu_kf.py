@@ -169,3 +169,25 @@ def test_smooth_api_t_smooth(ctx):
     np.testing.assert_array_equal(stT.mu, fst.mu)
     np.testing.assert_array_equal(stT.Sigma, fst.Sigma)
     np.testing.assert_array_equal(st1.mu, st1.means[0])
+
+
+def test_plan_smooth_matches_one_shot(ctx):
+    """gf_kf_plan_smooth on a resident plan returns exactly what gf_kf_smooth returns."""
+    import torch
+    from gfb200.plans import KfPlan
+    models, Ts, _ = W.kf_bank(12, seed=5, dx_range=(2, 32), T_range=(3, 40), make_ys=False)
+    rng = np.random.default_rng(2)
+    yss = [simulate(rng, m, T)[1] for m, T in zip(models, Ts)]
+    ref = G.smooth_batch(models, yss, ctx=ctx)
+    plan = KfPlan(models, G.KalmanFilter(), Ts, ctx=ctx)
+    ys = torch.tensor(np.concatenate([y.ravel() for y in yss]), device="cuda:0")
+    means = torch.zeros(plan.n_means, dtype=torch.float32, device="cuda:0")
+    covs = torch.zeros(plan.n_covs, dtype=torch.float32, device="cuda:0")
+    plan.smooth(ys, means, covs)
+    ctx.synchronize()
+    m_all = np.concatenate([r[0].ravel() for r in ref])
+    c_all = np.concatenate([r[1].transpose(0, 2, 1).ravel() for r in ref])
+    np.testing.assert_array_equal(means.cpu().numpy(), m_all)
+    np.testing.assert_array_equal(covs.cpu().numpy(), c_all)
+    np.testing.assert_array_equal(plan.ll.cpu().numpy(), [r[2] for r in ref])
+    plan.close()
