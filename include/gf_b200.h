@@ -112,6 +112,11 @@ typedef struct {
   void* states;        /* [width][N] final particle states (precision of the run) */
   double* log_weights; /* [N] final normalised log-weights */
   int32_t* clamps;     /* [1] slots clamped to N by the ancestor search */
+  /* [T+1][dx][N] ancestral trajectory of every final particle, in the run's
+   * precision: get_ancestry of AncestorCallback / ParticleTree (callbacks.jl:
+   * 90-111, containers.jl:466-631), kept on the device as sparse path storage
+   * with pruning (ext/CUDAExt.jl:146-298).  Linear-Gaussian PF only. */
+  void* paths;
 } gf_pf_out;
 
 /* Outputs of a Kalman batch (per-step arrays are packed filter after filter). */

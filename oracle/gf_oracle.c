@@ -645,6 +645,7 @@ typedef struct { /* nullable outputs */
   double* x_final;    /* N*dx */
   double* logw_final; /* N (normalised) */
   long* clamps;       /* scalar */
+  double* x_all;      /* (T+1)*N*dx: states after initialisation and after every step */
 } or_pf_out;
 
 /* Noise source: injected (noise != NULL, layout [(T+1)][dx][N], step 0 = prior
@@ -762,6 +763,7 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
     mv(dx, dx, L0, e, v);
     for (int d = 0; d < dx; ++d) x[(size_t)i * dx + d] = m->mu0[d] + v[d];
   }
+  if (out && out->x_all) memcpy(out->x_all, x, sizeof(double) * N * dx);
   for (int t = 1; t <= T; ++t) {
     int32_t* anc_t = out && out->ancestors ? out->ancestors + (size_t)(t - 1) * N : NULL;
     double* mar_t = out && out->margins ? out->margins + (size_t)(t - 1) * N : NULL;
@@ -814,6 +816,7 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
       logw[i] = logw[i] + inc + lo;
     }
     uniform = 0;
+    if (out && out->x_all) memcpy(out->x_all + (size_t)t * N * dx, x, sizeof(double) * N * dx);
     /* marginalise! (containers.jl:160-173) */
     double lse = or_logsumexp(logw, N);
     double inc = lse - baseline;

@@ -88,7 +88,8 @@ class _Prop(C.Structure):
 class _PFOut(C.Structure):
     _fields_ = [("ll_steps", _dp), ("ess", _dp), ("resampled", C.POINTER(C.c_int8)),
                 ("ancestors", C.POINTER(C.c_int32)), ("margins", _dp), ("means", _dp),
-                ("x_final", _dp), ("logw_final", _dp), ("clamps", C.POINTER(C.c_long))]
+                ("x_final", _dp), ("logw_final", _dp), ("clamps", C.POINTER(C.c_long)),
+                ("x_all", _dp)]
 
 
 class _RB(C.Structure):
@@ -169,7 +170,7 @@ def joint_smooth_truth(m: LGModel, ys):
 
 def pf_run(m: LGModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=0.5,
            schedule=None, noise=None, uniforms=None, seed=0, proposal=PROP_BOOTSTRAP,
-           k=1.0, want_ancestors=False, want_margins=False, threads=1):
+           k=1.0, want_ancestors=False, want_margins=False, want_states=False, threads=1):
     """filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys).
 
     noise: [(T+1), dx, N] standard normals (step 0 = prior draw) or None for the
@@ -189,6 +190,8 @@ def pf_run(m: LGModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=
                None if anc is None else anc.ctypes.data_as(C.POINTER(C.c_int32)),
                _p(mar), _p(out["means"]), _p(out["x_final"]), _p(out["logw_final"]),
                C.pointer(clamps))
+    xall = np.zeros((T + 1, N, m.dx)) if want_states else None
+    o.x_all = _p(xall)
     sched = None if schedule is None else np.ascontiguousarray(schedule, np.int8)
     rc = _RC(resampler, conv, threshold,
              None if sched is None else sched.ctypes.data_as(C.POINTER(C.c_int8)))
@@ -206,7 +209,22 @@ def pf_run(m: LGModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=
     out["ancestors"] = anc
     out["margins"] = mar
     out["clamps"] = clamps.value
+    out["states"] = xall
     return out
+
+
+def ancestry_paths(ancestors, states):
+    """get_ancestry (containers.jl:587-611): the trajectory of every final particle,
+    rebuilt densely from the 1-based ancestors [T, N] and the states [(T+1), N, dx];
+    returns paths [(T+1), N, dx] with paths[T] = states[T]."""
+    T, N = ancestors.shape
+    paths = np.empty_like(states)
+    idx = np.arange(N)
+    for t in range(T, 0, -1):
+        paths[t] = states[t][idx]
+        idx = ancestors[t - 1][idx] - 1
+    paths[0] = states[0][idx]
+    return paths
 
 
 def pf_step(m: LGModel, x, logw, y, noise_t, u, *, uniform=False, resampler=SYSTEMATIC,

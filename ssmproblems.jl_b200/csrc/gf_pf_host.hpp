@@ -97,3 +97,37 @@ gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cf
                        int32_t flags, LgJobSetup* out);
 
 }  // namespace gf
+
+namespace gf {
+
+// Device path storage of one particle-filter run (AncestorCallback /
+// ParticleTree, callbacks.jl:90-111 and containers.jl:466-631; the GPU
+// ParallelParticleTree of ext/CUDAExt.jl:146-298): a pool of M slots holding
+// particle states with parent links and live-descendant counts.  Each step the
+// lineages that left no offspring are freed (walking up while a parent's count
+// drops to zero) and the new particles take freed slots.
+struct PfTree {
+  int64_t M = 0;              // slots
+  int32_t width = 0;          // state dimensions
+  void* states = nullptr;     // [width][M] (run precision)
+  int32_t* parents = nullptr;    // [M] parent slot, -1 for time-0 states
+  int32_t* offspring = nullptr;  // [M] live children
+  int32_t* stack = nullptr;      // [M] free slots
+  int32_t* top = nullptr;        // [1] number of free slots on the stack
+  int32_t* leaves = nullptr;     // [N] slots of the current particles
+  int32_t* new_leaf = nullptr;   // [N] slots taken by the next generation
+  int32_t* anc = nullptr;        // [N] 0-based ancestors of the step being inserted
+  int32_t* cnt = nullptr;        // [N] offspring counts of the current particles
+};
+
+// Launchers (stream of ctx).  Before step t's propagate: count / prune / assign;
+// after it: insert.  tree_paths writes [T+1][width][N].
+void tree_launch_init(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int64_t N, const PfTree& tr);
+void tree_launch_step_pre(gf_ctx* ctx, const PfJob* job_dev, int64_t N, const PfTree& tr);
+void tree_launch_insert(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int64_t N, const PfTree& tr, int t);
+void tree_launch_paths(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int64_t N, const PfTree& tr, int T,
+                       void* out);
+// Grows the pool from tr.M to M_new slots (new arrays from `alloc`, old ones to `release`).
+void tree_launch_grow_init(gf_ctx* ctx, const PfTree& tr_new, int64_t M_old, int32_t top_old);
+
+}  // namespace gf

@@ -1,0 +1,190 @@
+// gf_pf_tree.cu -- device path storage (ancestry tree) of a particle-filter run.
+//
+// Restates the sparse path storage of AncestorCallback / ParticleTree
+// (callbacks.jl:90-111, containers.jl:466-631) and of the GPU
+// ParallelParticleTree (ext/CUDAExt.jl:146-298), Jacob, Murray & Rubenthaler
+// (2015): per step,
+//   count : a_i = ancestor of new particle i, offspring counts of the current ones
+//   prune : a current particle without offspring frees its slot, and each freed
+//           slot decrements its parent's count; the thread whose atomic decrement
+//           takes a count to zero frees that parent and walks on (so exactly one
+//           thread continues up a dying lineage)
+//   assign: new particle i takes a freed slot, parent = slot of its ancestor
+//   insert: (after the propagate) copy the new states into their slots.
+// The observable result is get_ancestry: the trajectory of every final particle.
+#include "gf_internal.hpp"
+#include "gf_pf_host.hpp"
+#include "gf_pf_kernels.cuh"
+
+namespace gf {
+namespace {
+
+constexpr int TREE_THREADS = 256;
+constexpr int kWalkLimit = 1 << 26;  // bound on a lineage walk (depth <= T + 1)
+
+inline int tree_blocks(int64_t n, int sms) {
+  return (int)std::max<int64_t>(1, std::min<int64_t>((n + TREE_THREADS - 1) / TREE_THREADS, 8 * (int64_t)sms));
+}
+
+template <typename Real>
+__global__ void tree_init_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
+  const PfJob& J = jobs[0];
+  const int64_t N = J.N, M = tr.M;
+  const Real* X = reinterpret_cast<const Real*>(J.X[0]);
+  Real* S = reinterpret_cast<Real*>(tr.states);
+  for (int64_t s = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; s < M; s += (int64_t)gridDim.x * blockDim.x) {
+    tr.offspring[s] = 0;
+    tr.parents[s] = -1;
+    if (s < N) {
+      for (int d = 0; d < tr.width; ++d) S[(size_t)d * M + s] = X[(size_t)d * N + s];
+      tr.leaves[s] = (int32_t)s;
+      tr.cnt[s] = 0;
+    } else {
+      tr.stack[M - 1 - s] = (int32_t)s;  // free slots N..M-1
+    }
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *tr.top = (int32_t)(M - N);
+}
+
+__device__ __forceinline__ bool tree_step_live(const PfJob& J, int* t) {
+  const PfScalars* sc = J.sc;
+  if (sc->status != 0) return false;
+  *t = sc->t + 1;
+  return *t <= J.T;
+}
+
+__global__ void tree_count_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
+  const PfJob& J = jobs[0];
+  int t;
+  if (!tree_step_live(J, &t)) return;
+  PfScalars* sc = J.sc;
+  const bool resamp = sc->resample != 0;
+  const int64_t N = J.N;
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    int64_t a = i;
+    if (resamp) {
+      if (J.resampler == GF_RS_MULTINOMIAL) {
+        a = make_search(J, sc, t, i).first(0, N);  // the propagate's search (clamps counted there)
+        if (a >= N) a = N - 1;
+      } else {
+        a = J.anc[i];
+      }
+    }
+    tr.anc[i] = (int32_t)a;
+    atomicAdd(&tr.cnt[a], 1);
+  }
+}
+
+__global__ void tree_prune_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
+  const PfJob& J = jobs[0];
+  int t;
+  if (!tree_step_live(J, &t)) return;
+  const int64_t N = J.N;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < N; k += (int64_t)gridDim.x * blockDim.x) {
+    int32_t s = tr.leaves[k];
+    const int32_t c = tr.cnt[k];
+    tr.offspring[s] = c;
+    if (c != 0) continue;
+    for (int it = 0; it < kWalkLimit; ++it) {
+      tr.stack[atomicAdd(tr.top, 1)] = s;  // s is free
+      const int32_t p = tr.parents[s];
+      if (p < 0 || atomicSub(&tr.offspring[p], 1) != 1) break;
+      s = p;  // this thread took the parent's count to zero
+    }
+  }
+}
+
+__global__ void tree_assign_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
+  const PfJob& J = jobs[0];
+  int t;
+  if (!tree_step_live(J, &t)) return;
+  const int64_t N = J.N;
+  const int32_t top0 = *tr.top;
+  if (top0 < N) {  // no room: the host sizes the pool before every chunk of steps
+    if (blockIdx.x == 0 && threadIdx.x == 0) J.sc->status = GF_ERR_OOM_BUDGET;
+    return;
+  }
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t nl = tr.stack[top0 - N + i];
+    tr.new_leaf[i] = nl;
+    tr.parents[nl] = tr.leaves[tr.anc[i]];
+    tr.offspring[nl] = 0;
+  }
+}
+
+template <typename Real>
+__global__ void tree_insert_kernel(const PfJob* __restrict__ jobs, PfTree tr, int t) {
+  const PfJob& J = jobs[0];
+  if (J.sc->status != 0) return;
+  const int64_t N = J.N, M = tr.M;
+  const Real* X = reinterpret_cast<const Real*>(J.X[t & 1]);
+  Real* S = reinterpret_cast<Real*>(tr.states);
+  for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t nl = tr.new_leaf[i];
+    for (int d = 0; d < tr.width; ++d) S[(size_t)d * M + nl] = X[(size_t)d * N + i];
+    tr.leaves[i] = nl;
+    tr.cnt[i] = 0;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *tr.top -= (int32_t)N;
+}
+
+template <typename Real>
+__global__ void tree_paths_kernel(const PfJob* __restrict__ jobs, PfTree tr, int T, Real* __restrict__ out) {
+  const PfJob& J = jobs[0];
+  const int64_t N = J.N, M = tr.M;
+  const Real* S = reinterpret_cast<const Real*>(tr.states);
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < N; k += (int64_t)gridDim.x * blockDim.x) {
+    int32_t s = tr.leaves[k];
+    for (int t = T; t >= 0 && s >= 0; --t) {
+      for (int d = 0; d < tr.width; ++d) out[((size_t)t * tr.width + d) * N + k] = S[(size_t)d * M + s];
+      s = tr.parents[s];
+    }
+  }
+}
+
+// New slots M_old..M-1 join the free stack above the surviving entries.
+__global__ void tree_grow_kernel(PfTree tr, int64_t M_old, int32_t top_old) {
+  const int64_t add = tr.M - M_old;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < add; k += (int64_t)gridDim.x * blockDim.x) {
+    const int64_t s = tr.M - 1 - k;
+    tr.parents[s] = -1;
+    tr.offspring[s] = 0;
+    tr.stack[top_old + k] = (int32_t)s;
+  }
+  if (blockIdx.x == 0 && threadIdx.x == 0) *tr.top = (int32_t)(top_old + add);
+}
+
+}  // namespace
+
+void tree_launch_init(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int64_t N, const PfTree& tr) {
+  const int g = tree_blocks(tr.M, ctx->num_sms);
+  if (dbl) tree_init_kernel<double><<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
+  else tree_init_kernel<float><<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
+}
+
+void tree_launch_step_pre(gf_ctx* ctx, const PfJob* job_dev, int64_t N, const PfTree& tr) {
+  const int g = tree_blocks(N, ctx->num_sms);
+  tree_count_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
+  tree_prune_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
+  tree_assign_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
+}
+
+void tree_launch_insert(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int64_t N, const PfTree& tr, int t) {
+  const int g = tree_blocks(N, ctx->num_sms);
+  if (dbl) tree_insert_kernel<double><<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr, t);
+  else tree_insert_kernel<float><<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr, t);
+}
+
+void tree_launch_paths(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int64_t N, const PfTree& tr, int T,
+                       void* out) {
+  const int g = tree_blocks(N, ctx->num_sms);
+  if (dbl) tree_paths_kernel<double><<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr, T, (double*)out);
+  else tree_paths_kernel<float><<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr, T, (float*)out);
+}
+
+void tree_launch_grow_init(gf_ctx* ctx, const PfTree& tr_new, int64_t M_old, int32_t top_old) {
+  const int g = tree_blocks(tr_new.M - M_old, ctx->num_sms);
+  tree_grow_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(tr_new, M_old, top_old);
+}
+
+}  // namespace gf

@@ -63,7 +63,7 @@ class PFConfigC(C.Structure):
 class PFOutC(C.Structure):
     _fields_ = [("ll", _vp), ("ll_steps", _vp), ("ess_steps", _vp), ("resampled", _vp),
                 ("ancestors", _vp), ("means", _vp), ("states", _vp), ("log_weights", _vp),
-                ("clamps", _vp)]
+                ("clamps", _vp), ("paths", _vp)]
 
 
 class KFOutC(C.Structure):

@@ -82,12 +82,14 @@ def _pf_config(algo: ParticleFilter, T: int, seed: int, schedule=None):
 
 
 def filter(model, algo, observations, *, seed: int = 0, noise=None, uniforms=None,
-           ctx=None, want_ancestors=False, want_means=False, schedule=None):
+           ctx=None, want_ancestors=False, want_means=False, schedule=None, want_paths=False):
     """filter([rng,] model, algo, observations) -> (state, ll).
 
     seed     : Philox key of the in-kernel noise and uniforms (the reference's rng)
     noise    : optional injected standard normals [(T+1), dx, N] (step 0 = prior)
     uniforms : optional injected resampling uniforms ([T] systematic, else [T, N])
+    want_paths: keep the ancestry on the device (AncestorCallback / ParticleTree) and
+                return every final particle's trajectory as state.paths [T+1, N, dx]
     """
     ctx = _resolve_ctx(ctx)
     ys = L.f64(observations)
@@ -101,11 +103,12 @@ def filter(model, algo, observations, *, seed: int = 0, noise=None, uniforms=Non
                      schedule)
     if isinstance(algo, ParticleFilter):
         return _pf(model, algo, ys, seed, noise, uniforms, ctx, want_ancestors, want_means,
-                   schedule)
+                   schedule, want_paths)
     raise TypeError(f"unsupported algorithm {type(algo).__name__}")
 
 
-def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, schedule):
+def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, schedule,
+        want_paths=False):
     if not isinstance(model, StateSpaceModel):
         raise TypeError("particle filter needs a linear-Gaussian StateSpaceModel")
     mc = model._c_struct()
@@ -119,9 +122,10 @@ def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sched
                log_weights=np.zeros(N), clamps=np.zeros(1, np.int32))
     out["ancestors"] = np.zeros((T, N), np.int32) if want_anc else None
     out["means"] = np.zeros((T, dx)) if want_means else None
+    out["paths"] = np.zeros((T + 1, dx, N), rdt) if want_paths else None
     o = L.PFOutC(*[L.ptr(out[k]) for k in ("ll", "ll_steps", "ess_steps", "resampled",
                                            "ancestors", "means", "states", "log_weights",
-                                           "clamps")])
+                                           "clamps", "paths")])
     nz = None if noise is None else np.ascontiguousarray(noise, dtype=rdt)
     un = None if uniforms is None else L.f64(uniforms)
     L.check(ctx.h, L.load().gf_pf_run(ctx.h, C.byref(mc), C.byref(cfg), T, L.ptr(ys),
@@ -129,7 +133,8 @@ def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sched
     state = ParticleDistribution(out["states"].T, out["log_weights"], ll_steps=out["ll_steps"],
                                  ess_steps=out["ess_steps"], resampled=out["resampled"],
                                  ancestors=out["ancestors"], means=out["means"],
-                                 clamps=int(out["clamps"][0]))
+                                 clamps=int(out["clamps"][0]),
+                                 paths=None if out["paths"] is None else out["paths"].transpose(0, 2, 1))
     return state, float(out["ll"][0])
 
 

@@ -35,9 +35,12 @@ class PfPlan:
         self.resampled = torch.zeros(self.T, dtype=torch.int8, device=dev) if want_steps else None
 
     def run(self, ys_dev, noise_dev=None, unif_dev=None, states=None, log_weights=None,
-            ancestors=None, means=None):
+            ancestors=None, means=None, paths=None):
+        """paths: optional device buffer [T+1, dx, N] for every final particle's
+        trajectory (device path storage; runs eagerly)."""
         o = L.PFOutC(L.ptr(self.ll), L.ptr(self.ll_steps), L.ptr(self.ess), L.ptr(self.resampled),
-                     L.ptr(ancestors), L.ptr(means), L.ptr(states), L.ptr(log_weights), None)
+                     L.ptr(ancestors), L.ptr(means), L.ptr(states), L.ptr(log_weights), None,
+                     L.ptr(paths))
         L.check(self.ctx.h, L.load().gf_pf_plan_run(self.h, L.ptr(ys_dev), L.ptr(noise_dev),
                                                     L.ptr(unif_dev), C.byref(o)))
 

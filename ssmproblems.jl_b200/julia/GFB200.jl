@@ -65,6 +65,7 @@ struct GfPfOut
     states::Ptr{Cvoid}
     log_weights::Ptr{Float64}
     clamps::Ptr{Int32}
+    paths::Ptr{Cvoid}     # [T+1][dx][N] ancestry (AncestorCallback); C_NULL = off
 end
 
 struct GfKfOut
@@ -176,7 +177,7 @@ function GeneralisedFilters.filter(
         states = zeros(ET, N, dx)              # SoA [dx][N] == Matrix (N, dx)
         logw = zeros(Float64, N)
         out = Ref(GfPfOut(pointer(ll), C_NULL, C_NULL, C_NULL, C_NULL, C_NULL,
-                          Ptr{Cvoid}(pointer(states)), pointer(logw), C_NULL))
+                          Ptr{Cvoid}(pointer(states)), pointer(logw), C_NULL, C_NULL))
         GC.@preserve ll states logw ys begin
             check(ccall((:gf_pf_run, libgfb200), Int32,
                         (Ptr{Cvoid}, Ref{GfLgModel}, Ref{GfPfConfig}, Int32, Ptr{Float64},

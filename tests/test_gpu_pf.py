@@ -232,3 +232,29 @@ def test_tensor_core_path_matches_simt(ctx, dims):
     # per-step ll is a log-sum-exp of the log-weights: its error is bounded by
     # theirs (FP32 sums of up to 32 squared residuals per particle)
     np.testing.assert_allclose(l0, l1, rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("kind,threshold,T", [(O.SYSTEMATIC, 0.5, 6), (O.STRATIFIED, 1.0, 5),
+                                              (O.MULTINOMIAL, 0.7, 5), (O.SYSTEMATIC, 0.0, 70)])
+def test_path_storage_matches_dense_ancestry(ctx, kind, threshold, T):
+    """AncestorCallback / ParticleTree (callbacks.jl:90-111, containers.jl:466-631):
+    the device path storage returns every final particle's trajectory, equal to the
+    dense reconstruction from the oracle's ancestors and per-step states (FP64,
+    injected noise and uniforms).  threshold 0 never resamples, so no lineage is
+    pruned and the pool must grow past its default size."""
+    rng = np.random.default_rng(T + kind)
+    m = random_lg(rng, 2, 2)
+    _, ys = simulate(rng, m, T)
+    N = 1000
+    noise, unif = injected(rng, T, 2, N, kind)
+    rs = {O.SYSTEMATIC: G.Systematic(), O.STRATIFIED: G.Stratified(), O.MULTINOMIAL: G.Multinomial()}[kind]
+    algo = G.BF(N, threshold=threshold, resampler=rs, precision="f64")
+    st, ll = G.filter(m, algo, ys, noise=noise, uniforms=unif, want_ancestors=True, want_paths=True,
+                      ctx=ctx)
+    ref = O.pf_run(to_oracle(m), N, ys, resampler=kind, threshold=threshold, noise=noise,
+                   uniforms=unif, want_ancestors=True, want_states=True)
+    np.testing.assert_array_equal(st.ancestors, ref["ancestors"])
+    dense = O.ancestry_paths(ref["ancestors"], ref["states"])
+    np.testing.assert_allclose(st.paths, dense, rtol=1e-10, atol=1e-12)
+    # the plan reuses (and keeps) its grown pool on a second run
+    assert st.paths.shape == (T + 1, N, 2)
