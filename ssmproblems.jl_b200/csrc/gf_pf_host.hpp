@@ -109,7 +109,7 @@ namespace gf {
 struct PfTree {
   int64_t M = 0;              // slots
   int32_t width = 0;          // state dimensions
-  void* states = nullptr;     // [width][M] (run precision)
+  void* states = nullptr;     // [M][width] (run precision; one particle's state contiguous)
   int32_t* parents = nullptr;    // [M] parent slot, -1 for time-0 states
   int32_t* offspring = nullptr;  // [M] live children
   int32_t* stack = nullptr;      // [M] free slots

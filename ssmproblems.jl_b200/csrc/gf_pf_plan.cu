@@ -318,8 +318,8 @@ static gf_status tree_reserve(gf_pf_plan* p, int64_t need) {
     for (auto& b : bufs) dev_free(ctx, b.p, b.bytes);
     return st;
   }
-  GF_CHECK_CUDA(ctx, cudaMemcpy2DAsync(nt.states, p->rsize * M_new, tr.states, p->rsize * M_old,
-                                       p->rsize * M_old, p->dx, cudaMemcpyDeviceToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.states, tr.states, p->rsize * (size_t)p->dx * M_old,
+                                     cudaMemcpyDeviceToDevice, s));
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.parents, tr.parents, 4 * M_old, cudaMemcpyDeviceToDevice, s));
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.offspring, tr.offspring, 4 * M_old, cudaMemcpyDeviceToDevice, s));
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.stack, tr.stack, 4 * (size_t)top, cudaMemcpyDeviceToDevice, s));

@@ -36,7 +36,7 @@ __global__ void tree_init_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
     tr.offspring[s] = 0;
     tr.parents[s] = -1;
     if (s < N) {
-      for (int d = 0; d < tr.width; ++d) S[(size_t)d * M + s] = X[(size_t)d * N + s];
+      for (int d = 0; d < tr.width; ++d) S[(size_t)s * tr.width + d] = X[(size_t)d * N + s];
       tr.leaves[s] = (int32_t)s;
       tr.cnt[s] = 0;
     } else {
@@ -60,18 +60,20 @@ __global__ void tree_count_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
   PfScalars* sc = J.sc;
   const bool resamp = sc->resample != 0;
   const int64_t N = J.N;
+  const bool multinomial = J.resampler == GF_RS_MULTINOMIAL;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
     int64_t a = i;
-    if (resamp) {
-      if (J.resampler == GF_RS_MULTINOMIAL) {
-        a = make_search(J, sc, t, i).first(0, N);  // the propagate's search (clamps counted there)
-        if (a >= N) a = N - 1;
-      } else {
-        a = J.anc[i];
-      }
+    if (!resamp) {
+      tr.cnt[i] = 1;
+    } else if (multinomial) {
+      a = make_search(J, sc, t, i).first(0, N);  // the propagate's search (clamps counted there)
+      if (a >= N) a = N - 1;
+      atomicAdd(&tr.cnt[a], 1);
+    } else {
+      a = J.anc[i];
+      tr.cnt[i] = J.ocum[i] - (i > 0 ? J.ocum[i - 1] : 0);  // cumulative offspring counts
     }
     tr.anc[i] = (int32_t)a;
-    atomicAdd(&tr.cnt[a], 1);
   }
 }
 
@@ -84,12 +86,21 @@ __global__ void tree_prune_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
     int32_t s = tr.leaves[k];
     const int32_t c = tr.cnt[k];
     tr.offspring[s] = c;
+    // childless particles free their slots: one stack reservation per warp
+    const unsigned act = __activemask();
+    const unsigned dead = __ballot_sync(act, c == 0);
+    const int lane = threadIdx.x & 31;
+    const int leader = __ffs(act) - 1;
+    int base = 0;
+    if (lane == leader && dead) base = atomicAdd(tr.top, __popc(dead));
+    base = __shfl_sync(act, base, leader);
     if (c != 0) continue;
+    tr.stack[base + __popc(dead & ((1u << lane) - 1u))] = s;
     for (int it = 0; it < kWalkLimit; ++it) {
-      tr.stack[atomicAdd(tr.top, 1)] = s;  // s is free
       const int32_t p = tr.parents[s];
       if (p < 0 || atomicSub(&tr.offspring[p], 1) != 1) break;
-      s = p;  // this thread took the parent's count to zero
+      s = p;  // this thread took the parent's count to zero: the parent is free too
+      tr.stack[atomicAdd(tr.top, 1)] = s;
     }
   }
 }
@@ -121,7 +132,7 @@ __global__ void tree_insert_kernel(const PfJob* __restrict__ jobs, PfTree tr, in
   Real* S = reinterpret_cast<Real*>(tr.states);
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
     const int32_t nl = tr.new_leaf[i];
-    for (int d = 0; d < tr.width; ++d) S[(size_t)d * M + nl] = X[(size_t)d * N + i];
+    for (int d = 0; d < tr.width; ++d) S[(size_t)nl * tr.width + d] = X[(size_t)d * N + i];
     tr.leaves[i] = nl;
     tr.cnt[i] = 0;
   }
@@ -136,7 +147,7 @@ __global__ void tree_paths_kernel(const PfJob* __restrict__ jobs, PfTree tr, int
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < N; k += (int64_t)gridDim.x * blockDim.x) {
     int32_t s = tr.leaves[k];
     for (int t = T; t >= 0 && s >= 0; --t) {
-      for (int d = 0; d < tr.width; ++d) out[((size_t)t * tr.width + d) * N + k] = S[(size_t)d * M + s];
+      for (int d = 0; d < tr.width; ++d) out[((size_t)t * tr.width + d) * N + k] = S[(size_t)s * tr.width + d];
       s = tr.parents[s];
     }
   }
