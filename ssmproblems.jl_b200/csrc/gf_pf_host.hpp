@@ -123,7 +123,9 @@ struct PfTree {
 // Launchers (stream of ctx).  Before step t's propagate: count / prune / assign;
 // after it: insert.  tree_paths writes [T+1][width][N].
 void tree_launch_init(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int64_t N, const PfTree& tr);
-void tree_launch_step_pre(gf_ctx* ctx, const PfJob* job_dev, int64_t N, const PfTree& tr);
+// sorted_ancestors: the rule keeps ancestors nondecreasing (systematic, stratified)
+void tree_launch_step_pre(gf_ctx* ctx, const PfJob* job_dev, int64_t N, const PfTree& tr,
+                          bool sorted_ancestors);
 void tree_launch_insert(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int64_t N, const PfTree& tr, int t);
 void tree_launch_paths(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int64_t N, const PfTree& tr, int T,
                        void* out);

@@ -354,7 +354,7 @@ static gf_status enqueue_run_paths(gf_pf_plan* p, bool means, void* paths) {
       const int64_t steps = std::min<int64_t>(kTreeChunk, p->T - t + 1);
       if ((st = tree_reserve(p, steps * p->N))) return st;
     }
-    tree_launch_step_pre(ctx, p->job_dev, p->N, p->tree);
+    tree_launch_step_pre(ctx, p->job_dev, p->N, p->tree, p->cfg.resampler != GF_RS_MULTINOMIAL);
     p->prop_fn<<<p->ntiles * p->prop_split, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
     tree_launch_insert(ctx, p->dbl, p->job_dev, p->N, p->tree, t);
     if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);

@@ -12,6 +12,8 @@
 //   assign: new particle i takes a freed slot, parent = slot of its ancestor
 //   insert: (after the propagate) copy the new states into their slots.
 // The observable result is get_ancestry: the trajectory of every final particle.
+#include <type_traits>
+
 #include "gf_internal.hpp"
 #include "gf_pf_host.hpp"
 #include "gf_pf_kernels.cuh"
@@ -105,6 +107,51 @@ __global__ void tree_prune_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
   }
 }
 
+// Sorted-ancestor rules (systematic, stratified, or no resampling): the children
+// of one parent are consecutive particles, so each warp sums its dead children
+// per parent (segmented scan over equal keys) and issues one atomic per parent;
+// a weight collapse otherwise serialises thousands of decrements on one count.
+__global__ void tree_prune_sorted_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
+  const PfJob& J = jobs[0];
+  int t;
+  if (!tree_step_live(J, &t)) return;
+  const int64_t N = J.N;
+  const int lane = threadIdx.x & 31;
+  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < N; k += (int64_t)gridDim.x * blockDim.x) {
+    const int32_t s = tr.leaves[k];
+    const int32_t c = tr.cnt[k];
+    tr.offspring[s] = c;
+    const unsigned act = __activemask();
+    const unsigned dead = __ballot_sync(act, c == 0);
+    const int leader = __ffs(act) - 1;
+    int base = 0;
+    if (lane == leader && dead) base = atomicAdd(tr.top, __popc(dead));
+    base = __shfl_sync(act, base, leader);
+    if (c == 0) tr.stack[base + __popc(dead & ((1u << lane) - 1u))] = s;
+    // dead children per parent: segmented inclusive sum over runs of equal parents
+    const int32_t key = tr.parents[s];
+    int sum = c == 0 ? 1 : 0;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(act, sum, o);
+      const int32_t kk = __shfl_up_sync(act, key, o);
+      if (lane >= o && ((act >> (lane - o)) & 1u) && kk == key) sum += v;
+    }
+    const int32_t next = __shfl_down_sync(act, key, 1);
+    const bool tail = lane == 31 || !((act >> (lane + 1)) & 1u) || next != key;
+    if (!tail || sum == 0 || key < 0) continue;
+    if (atomicSub(&tr.offspring[key], sum) != sum) continue;
+    // this warp took the parent's count to zero: free it and walk on
+    int32_t q = key;
+    for (int it = 0; it < kWalkLimit; ++it) {
+      tr.stack[atomicAdd(tr.top, 1)] = q;
+      const int32_t p = tr.parents[q];
+      if (p < 0 || atomicSub(&tr.offspring[p], 1) != 1) break;
+      q = p;
+    }
+  }
+}
+
 __global__ void tree_assign_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
   const PfJob& J = jobs[0];
   int t;
@@ -130,9 +177,22 @@ __global__ void tree_insert_kernel(const PfJob* __restrict__ jobs, PfTree tr, in
   const int64_t N = J.N, M = tr.M;
   const Real* X = reinterpret_cast<const Real*>(J.X[t & 1]);
   Real* S = reinterpret_cast<Real*>(tr.states);
+  constexpr int V = 16 / sizeof(Real);  // elements per 16-byte store
+  using Vec = typename std::conditional<sizeof(Real) == 4, float4, double2>::type;
+  const bool vec = tr.width % V == 0;
   for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
     const int32_t nl = tr.new_leaf[i];
-    for (int d = 0; d < tr.width; ++d) S[(size_t)nl * tr.width + d] = X[(size_t)d * N + i];
+    Real* dst = S + (size_t)nl * tr.width;
+    if (vec) {
+      for (int d0 = 0; d0 < tr.width; d0 += V) {
+        Real v[V];
+#pragma unroll
+        for (int q = 0; q < V; ++q) v[q] = X[(size_t)(d0 + q) * N + i];
+        *reinterpret_cast<Vec*>(dst + d0) = *reinterpret_cast<const Vec*>(v);
+      }
+    } else {
+      for (int d = 0; d < tr.width; ++d) dst[d] = X[(size_t)d * N + i];
+    }
     tr.leaves[i] = nl;
     tr.cnt[i] = 0;
   }
@@ -173,10 +233,12 @@ void tree_launch_init(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int64_t N, co
   else tree_init_kernel<float><<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
 }
 
-void tree_launch_step_pre(gf_ctx* ctx, const PfJob* job_dev, int64_t N, const PfTree& tr) {
+void tree_launch_step_pre(gf_ctx* ctx, const PfJob* job_dev, int64_t N, const PfTree& tr,
+                          bool sorted_ancestors) {
   const int g = tree_blocks(N, ctx->num_sms);
   tree_count_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
-  tree_prune_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
+  if (sorted_ancestors) tree_prune_sorted_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
+  else tree_prune_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
   tree_assign_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
 }
 
