@@ -255,6 +255,50 @@ int64_t gf_sample_ancestors_noalloc_max_n(void);
 gf_status gf_rng_normals(gf_ctx* ctx, uint64_t seed, int32_t t, int32_t dx, int64_t n,
                          int32_t precision, void* out_dev);
 
+/* ------------------------------------------------- conditional SMC (PMCMC) */
+/* Trajectory refreshment of ConditionalSMC (csmc.jl:10-40). */
+enum { GF_CSMC_NONE = 0, GF_CSMC_ANCESTOR = 1, GF_CSMC_BACKWARD = 2 };
+
+typedef struct {
+  int32_t N;          /* particles per sweep, 1..gf_csmc_max_particles() */
+  double threshold;   /* BF(N; threshold): resample iff threshold*N >= ESS.  Ancestor
+                         sampling resamples at every step, as csmc.jl:261 does */
+  int32_t resampler;  /* GF_RS_*, GF_CONV_CPU rule (resamplers.jl:214-238) */
+  int32_t refresh;    /* GF_CSMC_* */
+  uint64_t seed;      /* Philox key for in-kernel noise and uniforms */
+} gf_csmc_config;
+
+typedef struct {
+  /* [chains][iters-burnin][T+1][dx] the trajectory each kept sweep returned */
+  double* trajectories;
+  double* ll;       /* [chains][iters-burnin] log-likelihood estimate of each kept sweep */
+  /* [chains][T+1][dx], in and out: the reference trajectory the first sweep is
+   * conditioned on (when ref_given) and, on return, the last sampled one.
+   * Required. */
+  double* ref;
+  int32_t* status;  /* [chains] per-chain gf_status (nullable) */
+} gf_csmc_out;
+
+/* `iters` sweeps of ConditionalSMC(BF(N; threshold, resampler), refresh) per
+ * chain (_csmc_sample, csmc.jl:231-434, driven by AbstractMCMC.step :438-450)
+ * on a linear-Gaussian model, for `chains` independent chains at once.  Each
+ * sweep conditions on the previous sweep's trajectory (the first on `ref` when
+ * ref_given, else none) and samples a new one: by the final weights from the
+ * ancestry (NONE, ANCESTOR: get_ancestry of the path store) or by backward
+ * simulation over the dense history (BACKWARD).  Single draws from weights
+ * take the first k with cumsum(w)_k >= u*sum(w) (StatsBase.sample).
+ * ys: [T][dy] FP64.  noise (nullable): [chains][iters][T+1][N][dx] N(0,1),
+ * row 0 the prior draw; uniforms (nullable): [chains][iters][T+1][N+1]: in row
+ * t >= 1, slots 0..N-1 are the resampling uniforms of step t and slot N the
+ * ancestor-sampling draw of step t (ANCESTOR) or the backward draw of time
+ * t-1 (BACKWARD); row 0 slot N is the final draw.  Bootstrap proposal, FP64.
+ * Limits: dx, dy <= 16, T < 2^20. */
+gf_status gf_csmc_run(gf_ctx* ctx, const gf_lg_model* model, const gf_csmc_config* cfg, int32_t T,
+                      const double* ys, int32_t chains, int32_t iters, int32_t burnin,
+                      int32_t ref_given, const double* noise, const double* uniforms,
+                      int32_t memspace, gf_csmc_out* out);
+int32_t gf_csmc_max_particles(void);
+
 /* ------------------------------------------------------------------ serving */
 /* No reference counterpart: the reference runs one synchronous filter() call
  * at a time (GeneralisedFilters.jl:58-84).  A server owns one GPU through a

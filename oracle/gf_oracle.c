@@ -1024,3 +1024,229 @@ done:
   free(Lo0); free(LQo); free(Lqo); free(LZ0); free(LR);
   return st;
 }
+
+/* ------------------------------------------------------------------------ */
+/* Conditional SMC sweeps (csmc.jl:231-434) on a linear-Gaussian model with the
+ * bootstrap proposal, FP64, one chain after another (chains in parallel with
+ * or_set_threads).  Restates, per sweep:
+ *   initialise (particles.jl:36-50): particle 1 <- ref[0] when conditioned;
+ *   per step t: [ancestor sampling, csmc.jl:250-258: a* drawn from
+ *   logw_i + log p(ref_t | x_i)]; resample by the ESS rule (resamplers.jl:
+ *   179-183) or always under ancestor sampling (csmc.jl:261 calls resample);
+ *   _set_ref_index! (resamplers.jl:51) or a*; x_1 <- ref_t, the others
+ *   A x_a + b + LQ e; logw = (0 if resampled else logw) + log p(y_t | x);
+ *   ll += LSE(logw) - (log N if resampled else LSE of the previous weights);
+ *   next reference: get_ancestry of a particle drawn by its final weight
+ *   (csmc.jl:103-108, containers.jl:421-440) or backward simulation
+ *   (csmc.jl:378-434, weights logw_t + log p(x*_{t+1} | x_t), logw_0 = 0).
+ * Draws from weights take the first k with cumsum(w)_k >= u * sum(w)
+ * (StatsBase.sample); resampling uses the resamplers.jl:214-238 rules.
+ * Sums run in index order; the CUDA kernel's block reductions agree to
+ * rounding.  Randomness: injected (noise [chains][iters][T+1][N][dx], uniforms
+ * [chains][iters][T+1][N+1], the CUDA library's layout) or, when NULL, the
+ * CUDA library's Philox counters (sweep, chain, t<<12 | slot, tag). */
+#define TAG_CS_NORMAL 0x43534E4Du
+#define TAG_CS_UNIF 0x43535546u
+typedef struct {
+  const double *noise, *unif;
+  uint64_t seed;
+  int iters, T, N, dx;
+} cs_rng;
+static double cs_uniform(const cs_rng* r, int chain, int it, int t, int slot) {
+  if (r->unif) return r->unif[(((size_t)chain * r->iters + it) * (r->T + 1) + t) * (r->N + 1) + slot];
+  uint32_t ctr[4] = {(uint32_t)it, (uint32_t)chain, ((uint32_t)t << 12) | (uint32_t)slot, TAG_CS_UNIF}, w[4];
+  philox4x32_10(ctr, (uint32_t)r->seed, (uint32_t)(r->seed >> 32), w);
+  uint64_t bits = ((uint64_t)(w[0] >> 5) << 26) | (uint64_t)(w[1] >> 6);
+  return (double)bits * (1.0 / 9007199254740992.0);
+}
+static void cs_normals(const cs_rng* r, int chain, int it, int t, int i, double* e) {
+  if (r->noise) {
+    memcpy(e, r->noise + ((((size_t)chain * r->iters + it) * (r->T + 1) + t) * r->N + i) * r->dx,
+           sizeof(double) * r->dx);
+    return;
+  }
+  for (int q = 0; 4 * q < r->dx; ++q) {
+    uint32_t ctr[4] = {(uint32_t)it, (uint32_t)chain, ((uint32_t)t << 12) | (uint32_t)(4 * i + q),
+                       TAG_CS_NORMAL}, w[4];
+    philox4x32_10(ctr, (uint32_t)r->seed, (uint32_t)(r->seed >> 32), w);
+    for (int p = 0; p < 2; ++p) {
+      double u1 = ((double)w[2 * p] + 1.0) * (1.0 / 4294967296.0);
+      double u2 = (double)w[2 * p + 1] * (1.0 / 4294967296.0);
+      double rr = sqrt(-2.0 * log(u1));
+      double th = 6.283185307179586 * u2;
+      if (4 * q + 2 * p < r->dx) e[4 * q + 2 * p] = rr * cos(th);
+      if (4 * q + 2 * p + 1 < r->dx) e[4 * q + 2 * p + 1] = rr * sin(th);
+    }
+  }
+}
+/* exp(v - max(v)) in place followed by the running sum; returns nothing. */
+static void cs_exp_cumsum(double* W, int N) {
+  double m = -INFINITY;
+  for (int i = 0; i < N; ++i) m = W[i] > m ? W[i] : m;
+  double acc = 0.0;
+  for (int i = 0; i < N; ++i) { acc += exp(W[i] - m); W[i] = acc; }
+}
+static int cs_draw(const double* W, int N, double u) {
+  double target = u * W[N - 1];
+  int k = 0;
+  while (k < N && W[k] < target) ++k;
+  return k < N ? k : N - 1;
+}
+static double cs_trans_logpdf(int dx, const double* A, const double* b, const double* LQ,
+                              double trans_const, const double* xn, const double* x, double* r) {
+  for (int i = 0; i < dx; ++i) {
+    double s = xn[i] - b[i];
+    for (int k = 0; k < dx; ++k) s -= A[i + k * dx] * x[k];
+    r[i] = s;
+  }
+  trsv_lower(dx, LQ, r);
+  double q = 0.0;
+  for (int i = 0; i < dx; ++i) q += r[i] * r[i];
+  return trans_const - 0.5 * q;
+}
+
+int or_csmc_run(const or_lg_model* m, int N, double threshold, int resampler, int refresh,
+                int T, const double* ys, int chains, int iters, int burnin, int ref_given,
+                const double* noise, const double* uniforms, uint64_t seed, double* ref,
+                double* traj_out, double* ll_out) {
+  const int dx = m->dx, dy = m->dy;
+  double *LQ = calloc((size_t)dx * dx, 8), *LR = calloc((size_t)dy * dy, 8), *L0 = calloc((size_t)dx * dx, 8);
+  int st = OR_OK;
+  if ((st = or_chol_lower(dx, m->Q, LQ)) || (st = or_chol_lower(dy, m->R, LR)) ||
+      (st = or_chol_lower(dx, m->Sigma0, L0))) {
+    free(LQ); free(LR); free(L0);
+    return st;
+  }
+  double ldq = 0.0, ldr = 0.0;
+  for (int i = 0; i < dx; ++i) ldq += log(LQ[i + i * dx]);
+  for (int i = 0; i < dy; ++i) ldr += log(LR[i + i * dy]);
+  const double trans_const = -ldq - 0.5 * dx * LOG2PI, obs_const = -ldr - 0.5 * dy * LOG2PI;
+  const cs_rng rng = {noise, uniforms, seed, iters, T, N, dx};
+  int fail = 0;
+#pragma omp parallel for num_threads(g_threads) schedule(dynamic) reduction(| : fail)
+  for (int c = 0; c < chains; ++c) {
+    double* X = malloc(sizeof(double) * (size_t)(T + 1) * N * dx);
+    double* LW = malloc(sizeof(double) * (size_t)(T + 1) * N);
+    int* ANC = malloc(sizeof(int) * (size_t)T * N);
+    double *W = malloc(sizeof(double) * N), *LWP = malloc(sizeof(double) * N);
+    int* AN = malloc(sizeof(int) * N);
+    double e[16], xa[16], x[16], r[16], z[16];
+    double* REF = ref + (size_t)c * (T + 1) * dx;
+    for (int it = 0; it < iters && !fail; ++it) {
+      const int has_ref = it > 0 || ref_given;
+      for (int i = 0; i < N; ++i) {
+        double* xo = X + (size_t)i * dx;
+        if (has_ref && i == 0) { memcpy(xo, REF, sizeof(double) * dx); }
+        else {
+          cs_normals(&rng, c, it, 0, i, e);
+          for (int rr = 0; rr < dx; ++rr) {
+            double s = m->mu0[rr];
+            for (int k = 0; k <= rr; ++k) s += L0[rr + k * dx] * e[k];
+            xo[rr] = s;
+          }
+        }
+        LW[i] = 0.0;
+      }
+      double ll = 0.0;
+      for (int t = 1; t <= T; ++t) {
+        const double* Xp = X + (size_t)(t - 1) * N * dx;
+        const double* LWp = LW + (size_t)(t - 1) * N;
+        double mx = -INFINITY, s1 = 0.0, s2 = 0.0;
+        for (int i = 0; i < N; ++i) mx = LWp[i] > mx ? LWp[i] : mx;
+        for (int i = 0; i < N; ++i) { double w = exp(LWp[i] - mx); s1 += w; s2 += w * w; }
+        const double lse = mx + log(s1), ess = s1 * s1 / s2;
+        const int resamp = refresh == 1 || threshold * (double)N >= ess;
+        int as_idx = 0;
+        if (refresh == 1 && has_ref) {
+          for (int i = 0; i < N; ++i)
+            W[i] = LWp[i] + cs_trans_logpdf(dx, m->A, m->b, LQ, trans_const, REF + (size_t)t * dx,
+                                            Xp + (size_t)i * dx, r);
+          cs_exp_cumsum(W, N);
+          as_idx = cs_draw(W, N, cs_uniform(&rng, c, it, t, N));
+        }
+        if (resamp) {
+          double acc = 0.0;
+          for (int i = 0; i < N; ++i) { acc += exp(LWp[i] - lse); W[i] = acc; }
+          const double nd = (double)N, wn = W[N - 1];
+          for (int i = 0; i < N; ++i) {
+            double uu;
+            if (resampler == OR_SYSTEMATIC) uu = cs_uniform(&rng, c, it, t, 0) + (double)i;
+            else if (resampler == OR_STRATIFIED) uu = (double)i + cs_uniform(&rng, c, it, t, i);
+            else uu = cs_uniform(&rng, c, it, t, i) * wn;
+            int k = 0;
+            if (resampler == OR_MULTINOMIAL) while (k < N && !(W[k] >= uu)) ++k;
+            else while (k < N && !(W[k] * nd > uu)) ++k;
+            AN[i] = k < N ? k : N - 1;
+            LWP[i] = 0.0;
+          }
+        } else {
+          for (int i = 0; i < N; ++i) { AN[i] = i; LWP[i] = LWp[i]; }
+        }
+        const double base = resamp ? log((double)N) : lse;
+        if (has_ref) AN[0] = as_idx;
+        const double* y = ys + (size_t)(t - 1) * dy;
+        double* Xt = X + (size_t)t * N * dx;
+        double* LWt = LW + (size_t)t * N;
+        for (int i = 0; i < N; ++i) {
+          if (has_ref && i == 0) memcpy(x, REF + (size_t)t * dx, sizeof(double) * dx);
+          else {
+            memcpy(xa, Xp + (size_t)AN[i] * dx, sizeof(double) * dx);
+            cs_normals(&rng, c, it, t, i, e);
+            for (int rr = 0; rr < dx; ++rr) {
+              double s = m->b[rr];
+              for (int k = 0; k < dx; ++k) s += m->A[rr + k * dx] * xa[k];
+              for (int k = 0; k <= rr; ++k) s += LQ[rr + k * dx] * e[k];
+              x[rr] = s;
+            }
+          }
+          for (int j = 0; j < dy; ++j) {
+            double s = y[j] - m->c[j];
+            for (int k = 0; k < dx; ++k) s -= m->H[j + k * dy] * x[k];
+            z[j] = s;
+          }
+          trsv_lower(dy, LR, z);
+          double q = 0.0;
+          for (int j = 0; j < dy; ++j) q += z[j] * z[j];
+          memcpy(Xt + (size_t)i * dx, x, sizeof(double) * dx);
+          LWt[i] = LWP[i] + obs_const - 0.5 * q;
+          ANC[(size_t)(t - 1) * N + i] = AN[i];
+        }
+        double M = -INFINITY, s = 0.0;
+        for (int i = 0; i < N; ++i) M = LWt[i] > M ? LWt[i] : M;
+        for (int i = 0; i < N; ++i) s += exp(LWt[i] - M);
+        const double lse_new = M + log(s);
+        if (!(lse_new > -INFINITY) || isnan(lse_new)) { fail = 1; break; }
+        ll += lse_new - base;
+      }
+      if (fail) break;
+      for (int i = 0; i < N; ++i) W[i] = LW[(size_t)T * N + i];
+      cs_exp_cumsum(W, N);
+      int k = cs_draw(W, N, cs_uniform(&rng, c, it, 0, N));
+      if (refresh != 2) {
+        for (int t = T; t >= 0; --t) {
+          memcpy(REF + (size_t)t * dx, X + ((size_t)t * N + k) * dx, sizeof(double) * dx);
+          if (t > 0) k = ANC[(size_t)(t - 1) * N + k];
+        }
+      } else {
+        memcpy(REF + (size_t)T * dx, X + ((size_t)T * N + k) * dx, sizeof(double) * dx);
+        for (int t = T - 1; t >= 0; --t) {
+          for (int i = 0; i < N; ++i)
+            W[i] = LW[(size_t)t * N + i] + cs_trans_logpdf(dx, m->A, m->b, LQ, trans_const,
+                                                           REF + (size_t)(t + 1) * dx,
+                                                           X + ((size_t)t * N + i) * dx, r);
+          cs_exp_cumsum(W, N);
+          k = cs_draw(W, N, cs_uniform(&rng, c, it, t + 1, N));
+          memcpy(REF + (size_t)t * dx, X + ((size_t)t * N + k) * dx, sizeof(double) * dx);
+        }
+      }
+      if (it >= burnin) {
+        size_t kk = (size_t)c * (iters - burnin) + (it - burnin);
+        if (traj_out) memcpy(traj_out + kk * (T + 1) * dx, REF, sizeof(double) * (T + 1) * dx);
+        if (ll_out) ll_out[kk] = ll;
+      }
+    }
+    free(X); free(LW); free(ANC); free(W); free(LWP); free(AN);
+  }
+  free(LQ); free(LR); free(L0);
+  return fail ? OR_ARG : OR_OK;
+}

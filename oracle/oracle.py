@@ -360,6 +360,39 @@ def rbpf_run(m: RBModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshol
 # --------------------------------------------------------------------------- #
 # numpy restatements of the reference's test fixtures                          #
 # --------------------------------------------------------------------------- #
+CSMC_NONE, CSMC_ANCESTOR, CSMC_BACKWARD = 0, 1, 2
+
+
+def csmc_run(m: LGModel, N, ys, *, threshold=0.6, resampler=SYSTEMATIC, refresh=CSMC_NONE,
+             chains=1, iters=1, burnin=0, ref=None, noise=None, uniforms=None, seed=0, threads=1):
+    """`iters` ConditionalSMC sweeps per chain (csmc.jl:231-450) with the
+    randomness injected (layouts of gf_csmc_run) or drawn from the CUDA
+    library's Philox counters.  Returns (trajectories [chains, iters-burnin,
+    T+1, dx], lls [chains, iters-burnin], last [chains, T+1, dx])."""
+    ys = _f64(ys).reshape(-1, m.dy)
+    T, dx = ys.shape[0], m.dx
+    keep = iters - burnin
+    trajs = np.zeros((chains, keep, T + 1, dx))
+    lls = np.zeros((chains, keep))
+    refs = np.zeros((chains, T + 1, dx))
+    if ref is not None:
+        refs[:] = _f64(ref).reshape(-1, T + 1, dx)
+    nz = None if noise is None else _f64(noise)
+    un = None if uniforms is None else _f64(uniforms)
+    lib().or_set_threads(int(threads))
+    f = lib().or_csmc_run
+    f.argtypes = [C.c_void_p, C.c_int, C.c_double, C.c_int, C.c_int, C.c_int, _dp, C.c_int, C.c_int,
+                  C.c_int, C.c_int, _dp, _dp, C.c_uint64, _dp, _dp, _dp]
+    st = f(C.byref(m._struct()), int(N), float(threshold), int(resampler), int(refresh), T, _p(ys),
+           int(chains), int(iters), int(burnin), int(ref is not None),
+           None if nz is None else _p(nz), None if un is None else _p(un),
+           C.c_uint64(int(seed) & (2**64 - 1)), _p(refs), _p(trajs), _p(lls))
+    lib().or_set_threads(1)
+    if st:
+        raise FloatingPointError(f"oracle CSMC status {st}")
+    return trajs, lls, refs
+
+
 def rand_cov(rng, d, scale=1.0, var_range=(0.8, 1.2)):
     """GFTest/utils.jl:15-36: random correlation matrix rescaled by variances."""
     A = rng.random((d, d))

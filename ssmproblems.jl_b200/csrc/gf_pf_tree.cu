@@ -79,77 +79,72 @@ __global__ void tree_count_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
   }
 }
 
+// Freed slots are collected per block in shared memory and pushed with one
+// reservation on the global free stack per block; a single stack counter would
+// otherwise serialise one atomic per warp and per freed lineage node.
+constexpr int PRUNE_BUF = 4096;
+
+struct FreeList {
+  int32_t* buf;
+  int* n;
+  __device__ __forceinline__ void push(const PfTree& tr, int32_t slot) const {
+    const int pos = atomicAdd(n, 1);
+    if (pos < PRUNE_BUF) buf[pos] = slot;
+    else tr.stack[atomicAdd(tr.top, 1)] = slot;  // buffer full: push directly
+  }
+};
+
+// SORTED: the rule keeps ancestors nondecreasing (systematic, stratified, or no
+// resampling), so the children of one parent are consecutive particles; each
+// warp sums its dead children per parent (segmented scan over equal parents)
+// and issues one atomic per parent, where a weight collapse would otherwise
+// serialise thousands of decrements on one count.
+template <bool SORTED>
 __global__ void tree_prune_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
   const PfJob& J = jobs[0];
   int t;
   if (!tree_step_live(J, &t)) return;
-  const int64_t N = J.N;
-  for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < N; k += (int64_t)gridDim.x * blockDim.x) {
-    int32_t s = tr.leaves[k];
-    const int32_t c = tr.cnt[k];
-    tr.offspring[s] = c;
-    // childless particles free their slots: one stack reservation per warp
-    const unsigned act = __activemask();
-    const unsigned dead = __ballot_sync(act, c == 0);
-    const int lane = threadIdx.x & 31;
-    const int leader = __ffs(act) - 1;
-    int base = 0;
-    if (lane == leader && dead) base = atomicAdd(tr.top, __popc(dead));
-    base = __shfl_sync(act, base, leader);
-    if (c != 0) continue;
-    tr.stack[base + __popc(dead & ((1u << lane) - 1u))] = s;
-    for (int it = 0; it < kWalkLimit; ++it) {
-      const int32_t p = tr.parents[s];
-      if (p < 0 || atomicSub(&tr.offspring[p], 1) != 1) break;
-      s = p;  // this thread took the parent's count to zero: the parent is free too
-      tr.stack[atomicAdd(tr.top, 1)] = s;
-    }
-  }
-}
-
-// Sorted-ancestor rules (systematic, stratified, or no resampling): the children
-// of one parent are consecutive particles, so each warp sums its dead children
-// per parent (segmented scan over equal keys) and issues one atomic per parent;
-// a weight collapse otherwise serialises thousands of decrements on one count.
-__global__ void tree_prune_sorted_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
-  const PfJob& J = jobs[0];
-  int t;
-  if (!tree_step_live(J, &t)) return;
+  __shared__ int32_t s_buf[PRUNE_BUF];
+  __shared__ int s_n, s_base;
+  if (threadIdx.x == 0) s_n = 0;
+  __syncthreads();
+  const FreeList fl{s_buf, &s_n};
   const int64_t N = J.N;
   const int lane = threadIdx.x & 31;
   for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < N; k += (int64_t)gridDim.x * blockDim.x) {
     const int32_t s = tr.leaves[k];
     const int32_t c = tr.cnt[k];
     tr.offspring[s] = c;
-    const unsigned act = __activemask();
-    const unsigned dead = __ballot_sync(act, c == 0);
-    const int leader = __ffs(act) - 1;
-    int base = 0;
-    if (lane == leader && dead) base = atomicAdd(tr.top, __popc(dead));
-    base = __shfl_sync(act, base, leader);
-    if (c == 0) tr.stack[base + __popc(dead & ((1u << lane) - 1u))] = s;
-    // dead children per parent: segmented inclusive sum over runs of equal parents
-    const int32_t key = tr.parents[s];
-    int sum = c == 0 ? 1 : 0;
+    if (c == 0) fl.push(tr, s);
+    int32_t walk = -1;  // a parent whose count this thread took to zero
+    if constexpr (SORTED) {
+      const unsigned act = __activemask();
+      const int32_t key = tr.parents[s];
+      int sum = c == 0 ? 1 : 0;
 #pragma unroll
-    for (int o = 1; o < 32; o <<= 1) {
-      const int v = __shfl_up_sync(act, sum, o);
-      const int32_t kk = __shfl_up_sync(act, key, o);
-      if (lane >= o && ((act >> (lane - o)) & 1u) && kk == key) sum += v;
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(act, sum, o);
+        const int32_t kk = __shfl_up_sync(act, key, o);
+        if (lane >= o && ((act >> (lane - o)) & 1u) && kk == key) sum += v;
+      }
+      const int32_t next = __shfl_down_sync(act, key, 1);
+      const bool tail = lane == 31 || !((act >> (lane + 1)) & 1u) || next != key;
+      if (tail && sum > 0 && key >= 0 && atomicSub(&tr.offspring[key], sum) == sum) walk = key;
+    } else if (c == 0) {
+      const int32_t p = tr.parents[s];
+      if (p >= 0 && atomicSub(&tr.offspring[p], 1) == 1) walk = p;
     }
-    const int32_t next = __shfl_down_sync(act, key, 1);
-    const bool tail = lane == 31 || !((act >> (lane + 1)) & 1u) || next != key;
-    if (!tail || sum == 0 || key < 0) continue;
-    if (atomicSub(&tr.offspring[key], sum) != sum) continue;
-    // this warp took the parent's count to zero: free it and walk on
-    int32_t q = key;
-    for (int it = 0; it < kWalkLimit; ++it) {
-      tr.stack[atomicAdd(tr.top, 1)] = q;
-      const int32_t p = tr.parents[q];
-      if (p < 0 || atomicSub(&tr.offspring[p], 1) != 1) break;
-      q = p;
+    for (int it = 0; walk >= 0 && it < kWalkLimit; ++it) {
+      fl.push(tr, walk);
+      const int32_t p = tr.parents[walk];
+      walk = (p >= 0 && atomicSub(&tr.offspring[p], 1) == 1) ? p : -1;
     }
   }
+  __syncthreads();
+  const int n = min(s_n, PRUNE_BUF);
+  if (threadIdx.x == 0 && n > 0) s_base = atomicAdd(tr.top, n);
+  __syncthreads();
+  for (int q = threadIdx.x; q < n; q += blockDim.x) tr.stack[s_base + q] = s_buf[q];
 }
 
 __global__ void tree_assign_kernel(const PfJob* __restrict__ jobs, PfTree tr) {
@@ -237,8 +232,8 @@ void tree_launch_step_pre(gf_ctx* ctx, const PfJob* job_dev, int64_t N, const Pf
                           bool sorted_ancestors) {
   const int g = tree_blocks(N, ctx->num_sms);
   tree_count_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
-  if (sorted_ancestors) tree_prune_sorted_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
-  else tree_prune_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
+  if (sorted_ancestors) tree_prune_kernel<true><<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
+  else tree_prune_kernel<false><<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
   tree_assign_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(job_dev, tr);
 }
 

@@ -20,3 +20,5 @@ from .models import (HierarchicalSSM, HomogeneousGaussianPrior,  # noqa: F401
                      LatentDynamics, ObservationProcess, StatePrior, StateSpaceModel,
                      create_homogeneous_linear_gaussian_model)
 from .serving import Server  # noqa: F401,E402
+from .csmc import (AncestorSampling, BackwardSimulation, ConditionalSMC, CSMCModel,  # noqa: F401,E402
+                   CSMCState, NoRefreshment)

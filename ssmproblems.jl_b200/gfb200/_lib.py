@@ -24,6 +24,7 @@ GF_PROP_BOOTSTRAP, GF_PROP_OPTIMAL, GF_PROP_OVERDISPERSED = 0, 1, 2
 GF_ALGO_KF, GF_ALGO_SRKF = 0, 1
 GF_PLAN_AUTOTUNE, GF_PLAN_NO_GRAPH, GF_PLAN_PLAIN, GF_PLAN_SIMT = 1, 2, 4, 8
 GF_REQ_KF, GF_REQ_SRKF, GF_REQ_PF, GF_REQ_RBPF = 0, 1, 2, 3
+GF_CSMC_NONE, GF_CSMC_ANCESTOR, GF_CSMC_BACKWARD = 0, 1, 2
 
 EXPORTED = [
     "gf_ctx_create", "gf_ctx_destroy", "gf_last_error", "gf_ctx_set_stream", "gf_ctx_get_stream",
@@ -34,6 +35,7 @@ EXPORTED = [
     "gf_rng_normals", "gf_sample_ancestors_noalloc", "gf_sample_ancestors_noalloc_max_n",
     "gf_srv_create", "gf_srv_submit", "gf_srv_poll", "gf_srv_drain", "gf_srv_stats",
     "gf_srv_reset_stats", "gf_srv_last_error", "gf_srv_destroy",
+    "gf_csmc_run", "gf_csmc_max_particles",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -64,6 +66,15 @@ class PFOutC(C.Structure):
     _fields_ = [("ll", _vp), ("ll_steps", _vp), ("ess_steps", _vp), ("resampled", _vp),
                 ("ancestors", _vp), ("means", _vp), ("states", _vp), ("log_weights", _vp),
                 ("clamps", _vp), ("paths", _vp)]
+
+
+class CsmcConfigC(C.Structure):
+    _fields_ = [("N", C.c_int32), ("threshold", C.c_double), ("resampler", C.c_int32),
+                ("refresh", C.c_int32), ("seed", C.c_uint64)]
+
+
+class CsmcOutC(C.Structure):
+    _fields_ = [("trajectories", _vp), ("ll", _vp), ("ref", _vp), ("status", _vp)]
 
 
 class KFOutC(C.Structure):
@@ -165,6 +176,9 @@ def load(path: str | None = None):
         "gf_srv_reset_stats": (i32, [_vp]),
         "gf_srv_last_error": (C.c_char_p, [_vp]),
         "gf_srv_destroy": (i32, [_vp]),
+        "gf_csmc_run": (i32, [ctxp, C.POINTER(LGModelC), C.POINTER(CsmcConfigC), i32, _vp, i32,
+                              i32, i32, i32, _vp, _vp, i32, C.POINTER(CsmcOutC)]),
+        "gf_csmc_max_particles": (i32, []),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

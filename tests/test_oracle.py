@@ -40,6 +40,41 @@ def test_rts_smoother_matches_joint_gaussian(Dy, T):
     np.testing.assert_allclose(S, St, rtol=1e-8, atol=1e-11)
 
 
+@pytest.mark.parametrize("refresh", [O.CSMC_NONE, O.CSMC_ANCESTOR, O.CSMC_BACKWARD])
+def test_csmc_oracle_targets_the_smoothing_distribution(refresh):
+    """test/algorithms/csmc.jl:5-98 on the oracle restatement (smaller run):
+    the sampled trajectories' mean at t_smooth = 2 matches the RTS smoother and
+    1/Z-hat is unbiased for 1/Z (multinomial resampling)."""
+    rng = np.random.default_rng(1234)
+    m = O.create_linear_gaussian_model(rng, 1, 1)
+    _, ys = O.sample(rng, m, 10)
+    _, mus, _ = O.rts_smooth(m, ys)
+    kf_ll = O.kf_filter(m, ys)[0]
+    tr, lls, _ = O.csmc_run(m, 10, ys, threshold=0.6, resampler=O.MULTINOMIAL, refresh=refresh,
+                            chains=64, iters=1600, burnin=100, seed=31 + refresh, threads=4)
+    np.testing.assert_allclose(tr[:, :, 2, 0].mean(), mus[1, 0], rtol=6e-3)
+    l = -lls.ravel()
+    np.testing.assert_allclose(l.max() + np.log(np.mean(np.exp(l - l.max()))), -kf_ll, rtol=1e-3)
+
+
+def test_csmc_oracle_pins_reference_particle():
+    """With NoRefreshment and threshold 0 (no resampling) every particle keeps
+    its own lineage, so the sampled trajectory is one particle's path and, when
+    the final draw lands on particle 1, the reference itself."""
+    rng = np.random.default_rng(3)
+    m = O.create_linear_gaussian_model(rng, 2, 1)
+    T, N = 5, 6
+    _, ys = O.sample(rng, m, T)
+    ref = rng.standard_normal((1, T + 1, 2))
+    unif = rng.random((1, 1, T + 1, N + 1))
+    unif[0, 0, 0, N] = 0.0  # final draw: the first particle with nonzero weight, particle 1
+    noise = rng.standard_normal((1, 1, T + 1, N, 2))
+    tr, _, last = O.csmc_run(m, N, ys, threshold=0.0, refresh=O.CSMC_NONE, ref=ref,
+                             noise=noise, uniforms=unif)
+    np.testing.assert_array_equal(tr[0, 0], ref[0])
+    np.testing.assert_array_equal(last[0], ref[0])
+
+
 @pytest.mark.parametrize("Dy", [2, 3, 4])
 def test_srkf_equals_kf(Dy):
     """test/algorithms/srkf.jl:3-26."""
