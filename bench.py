@@ -7,7 +7,7 @@ ESS < 0.5 N, FP64 normaliser and cumulative weights, in-kernel Philox noise.
 One step = one full filter run (N * T particle-steps).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload pf|pf1d|kf|smooth|rbpf|serve]
+                    [--workload pf|pf1d|kf|smooth|rbpf|serve|csmc]
 
 Under torchrun each rank runs an independent replica (the filters shard by
 filter; no data-path collective).  Rank 0 prints one JSON line.
@@ -747,6 +747,120 @@ def bench_smooth(args, world, rank, local):
     return line
 
 
+def cpu_baseline_csmc(model, ys, N, seconds=12.0, threads=None):
+    """The FP64 oracle's CSMC-AS on this host: same model and N, chains spread
+    over all host threads, a bounded number of sweeps."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    threads = threads or os.cpu_count() or 1
+    p, d, o = model.prior, model.dyn, model.obs
+    om = O.LGModel(p.mu0, p.Sigma0, d.A, d.b, d.Q, o.H, o.c, o.R)
+    T = len(ys)
+    t0 = time.perf_counter()
+    O.csmc_run(om, N, ys, threshold=0.6, refresh=O.CSMC_ANCESTOR, chains=threads, iters=1, seed=1,
+               threads=threads)
+    one = time.perf_counter() - t0
+    iters = int(max(1, seconds / max(one, 1e-4)))
+    t0 = time.perf_counter()
+    O.csmc_run(om, N, ys, threshold=0.6, refresh=O.CSMC_ANCESTOR, chains=threads, iters=iters,
+               seed=1, threads=threads)
+    dt = time.perf_counter() - t0
+    return {"value": threads * iters * T * N / dt, "unit": "particle-steps/s", "cores": threads,
+            "kind": "port",
+            "sample": f"FP64 C oracle CSMC-AS, same model and N={N}, T={T}, {threads} chains x "
+                      f"{iters} sweeps, {threads} OpenMP threads (one chain per thread)"}
+
+
+def bench_csmc(args, world, rank, local):
+    """Particle Gibbs: ConditionalSMC(BF(256; threshold=0.6), AncestorSampling())
+    on an LGSSM Dx=4, Dy=2, K=100.  One step = `--csmc-sweeps` conditional SMC
+    sweeps of each of `--csmc-chains` chains (one CTA per chain, a whole chain
+    per launch), each chain continuing from its previous step's reference."""
+    import ctypes as C
+
+    import torch
+    import gfb200 as G
+    from gfb200 import _lib as L
+    from gfb200 import csmc as CS
+    from gfb200 import workloads as W
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    ctx = G.Context(local)
+    lib = L.load()
+    K, N, dx = 100, 256, 4
+    chains, sweeps = args.csmc_chains, args.csmc_sweeps
+    model, ys = W.lgssm_rot(seed=1234 + rank, dx=dx, dy=2, T=K)
+    yd = torch.tensor(ys, dtype=torch.float64, device=dev)
+    traj = torch.empty((chains, sweeps, K + 1, dx), dtype=torch.float64, device=dev)
+    lls = torch.empty((chains, sweeps), dtype=torch.float64, device=dev)
+    ref = torch.zeros((chains, K + 1, dx), dtype=torch.float64, device=dev)
+    status = torch.zeros(chains, dtype=torch.int32, device=dev)
+    cfg = L.CsmcConfigC(N, 0.6, L.GF_RS_SYSTEMATIC, L.GF_CSMC_ANCESTOR, 0)
+    out = L.CsmcOutC(L.ptr(traj), L.ptr(lls), L.ptr(ref), L.ptr(status))
+    mc = model._c_struct()
+
+    def run(i):
+        cfg.seed = 1000 + i
+        L.check(ctx.h, lib.gf_csmc_run(ctx.h, C.byref(mc), C.byref(cfg), K, L.ptr(yd), chains, sweeps, 0,
+                                       int(i > 0), None, None, L.GF_MEM_DEVICE, C.byref(out)))
+
+    for i in range(args.warmup):
+        run(i)
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    _barrier(world)
+    with ClockSampler(local) as clk:
+        e0.record(ext)
+        for i in range(args.steps):
+            run(args.warmup + i)
+        e1.record(ext)
+        e1.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1), world, dev)
+    assert int(status.abs().sum().item()) == 0
+    psteps = chains * sweeps * K * N
+    value = psteps * args.steps * world / (ms / 1e3)
+    # end to end: the public API with host buffers (ys in, every kept trajectory
+    # and log-likelihood out), continuing the chains from the device references
+    last = ref.cpu().numpy()
+    cm = G.CSMCModel(model, ys)
+    csmc = G.ConditionalSMC(G.BF(N, threshold=0.6), G.AncestorSampling())
+    CS.sample(cm, csmc, sweeps, chains=chains, seed=7, initial=last, ctx=ctx)
+    t0 = time.perf_counter()
+    for i in range(args.steps):
+        _, _, last = CS.sample(cm, csmc, sweeps, chains=chains, seed=8 + i, initial=last, ctx=ctx)
+    e2e_s = time.perf_counter() - t0
+    h2d = ys.nbytes + last.nbytes
+    d2h = chains * sweeps * (K + 1) * dx * 8 + chains * sweeps * 8 + last.nbytes
+    # algorithmic bytes per particle-step: state write + gathered read (16 dx),
+    # log-weight write + read (16), ancestor write (4)
+    b_ps = 16 * dx + 20
+    run_s = ms / 1e3 / args.steps
+    peak, peak_kind = _peaks()
+    line = {
+        "metric": "CSMC particle-steps/s", "value": value, "unit": "particle-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"particle Gibbs: ConditionalSMC(BF({N}; threshold=0.6), AncestorSampling()) "
+                               f"on LGSSM Dx={dx} Dy=2 K={K}; {chains} chains x {sweeps} sweeps per step, "
+                               "one CTA per chain", "chains": chains, "sweeps_per_step": sweeps,
+                   "sweeps_per_s": chains * sweeps * args.steps * world / (ms / 1e3),
+                   "l2": "per-chain histories (1 MB each) stay in L2 between steps; no flush"},
+        "roofline": {"bound": "hbm", "achieved": psteps * b_ps / run_s / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": psteps * b_ps / run_s / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+                     "limiter": "per-step CTA barriers of each chain (latency); 4 chains per SM"},
+        "e2e": {"value": psteps * args.steps / e2e_s, "unit": "particle-steps/s",
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_csmc(model, ys, N, seconds=args.cpu_seconds)
+    ctx.close()
+    return line
+
+
 def bench_reference(args, world, rank, local):
     """The reference arm: the FP64 oracle port of the reference algorithm on the
     host cores (the reference is Julia and cannot run on this image)."""
@@ -780,7 +894,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pf", choices=["pf", "pf1d", "kf", "smooth", "rbpf", "serve"])
+    ap.add_argument("--workload", default="pf", choices=["pf", "pf1d", "kf", "smooth", "rbpf", "serve", "csmc"])
+    ap.add_argument("--csmc-chains", type=int, default=592)
+    ap.add_argument("--csmc-sweeps", type=int, default=20)
     ap.add_argument("--smooth-filters", type=int, default=16384)
     ap.add_argument("--serve-rate", type=float, default=1000.0)
     ap.add_argument("--serve-requests", type=int, default=2000)
@@ -813,6 +929,8 @@ def main():
         line = bench_rbpf(args, world, rank, local)
     elif args.workload == "pf1d":
         line = bench_pf1d(args, world, rank, local)
+    elif args.workload == "csmc":
+        line = bench_csmc(args, world, rank, local)
     else:
         line = bench_pf(args, world, rank, local)
     if rank == 0 and line is not None:

@@ -176,8 +176,9 @@ __device__ __forceinline__ double cs_trans_logpdf(const CsmcArgs& a, const doubl
   return a.trans_const - 0.5 * q;
 }
 
+// Up to dx = 4 four 256-thread chains fit on an SM (<= 64 registers).
 template <int DXP>
-__global__ void __launch_bounds__(256) csmc_kernel(CsmcArgs a) {
+__global__ void __launch_bounds__(256, DXP <= 4 ? 4 : 1) csmc_kernel(CsmcArgs a) {
   extern __shared__ __align__(16) unsigned char smraw[];
   const int N = a.N, T = a.T, dx = a.dx, dy = a.dy;
   double* W = reinterpret_cast<double*>(smraw);  // [N] weights, then cumulative weights
