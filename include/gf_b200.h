@@ -54,6 +54,10 @@ enum { GF_PREC_F32 = 0, GF_PREC_F64 = 1 };
  * (GFTest/proposals.jl:11-31); GFTest OverdispersedProposal (:33-50). */
 enum { GF_PROP_BOOTSTRAP = 0, GF_PROP_OPTIMAL = 1, GF_PROP_OVERDISPERSED = 2 };
 enum { GF_ALGO_KF = 0, GF_ALGO_SRKF = 1 };
+/* AuxiliaryParticleFilter(pf, RepresentativeStateLookAhead(pp)) (particles.jl:
+ * 247-357): GF_LOOKAHEAD_MEAN scores each particle by log p(y_t | A x + b), the
+ * mean and mode of its transition (MeanPredictive, ModePredictive). */
+enum { GF_LOOKAHEAD_NONE = 0, GF_LOOKAHEAD_MEAN = 1 };
 
 typedef struct gf_ctx gf_ctx;
 
@@ -99,6 +103,7 @@ typedef struct {
   uint64_t seed;          /* Philox key for in-kernel noise / uniforms */
   const int8_t* schedule; /* nullable, host [T]: -1 ESS rule, 0 keep, 1 resample
                              (GFTest AlternatingResampler-style forcing) */
+  int32_t lookahead;      /* GF_LOOKAHEAD_*: AuxiliaryParticleFilter(pf, ...) first stage */
 } gf_pf_config;
 
 /* Outputs of one particle-filter run; every pointer but `ll` is nullable. */

@@ -633,6 +633,7 @@ typedef struct {
 typedef struct {
   int kind;           /* OR_PROP_* */
   double k;           /* overdispersion factor */
+  int lookahead;      /* 1: AuxiliaryParticleFilter(pf, MeanPredictive()) first stage */
 } or_proposal;
 
 typedef struct { /* nullable outputs */
@@ -718,6 +719,8 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
   double* logw = calloc(N, 8);
   double* wbuf = malloc(sizeof(double) * N);
   double* ubuf = malloc(sizeof(double) * N);
+  double* eta = malloc(sizeof(double) * N);
+  double* aux = malloc(sizeof(double) * N);
   double *L0 = calloc((size_t)dx * dx, 8), *LQ = calloc((size_t)dx * dx, 8);
   double *LR = calloc((size_t)dy * dy, 8), *Lq = calloc((size_t)dx * dx, 8);
   double *Kq = calloc((size_t)dx * dy, 8), *Sq = calloc((size_t)dx * dx, 8);
@@ -767,14 +770,61 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
   for (int t = 1; t <= T; ++t) {
     int32_t* anc_t = out && out->ancestors ? out->ancestors + (size_t)(t - 1) * N : NULL;
     double* mar_t = out && out->margins ? out->margins + (size_t)(t - 1) * N : NULL;
-    double ess = 0.0;
-    int was_uniform = uniform;
-    int res = maybe_resample(rc, t, N, dx, x, xtmp, logw, &uniform, wbuf, ubuf, uniforms, seed,
-                             anc_t, mar_t, &ess, &clamps);
+    double ess = 0.0, baseline;
+    int res;
+    if (prop->lookahead) {
+      /* AuxiliaryParticleFilter step (particles.jl:311-345): log eta_i =
+       * logpdf(obs, A x_i + b, y_t) (MeanPredictive, :359-365; predictive_loglik
+       * :386-394), then maybe_resample with AuxiliaryResampler (resamplers.jl:
+       * 109-116): weights softmax(logw + log eta), ESS decision on them. */
+      const double* yl = ys + (size_t)(t - 1) * dy;
+      for (long i = 0; i < N; ++i) {
+        double mx[64], hx[64], dif[64], tmpd[64];
+        mv(dx, dx, m->A, x + (size_t)i * dx, mx);
+        for (int d = 0; d < dx; ++d) mx[d] += m->b[d];
+        mv(dy, dx, m->H, mx, hx);
+        for (int k = 0; k < dy; ++k) dif[k] = yl[k] - hx[k] - m->c[k];
+        eta[i] = logpdf_chol(dy, LR, dif, tmpd);
+        aux[i] = (uniform ? 0.0 : logw[i]) + eta[i];
+      }
+      softmax(aux, N, wbuf);
+      ess = ess_of(wbuf, N);
+      int sched = rc->schedule ? rc->schedule[t - 1] : -1;
+      res = sched >= 0 ? sched : (rc->threshold * (double)N >= ess);
+      if (res) {
+        /* construct_new_state with auxiliary weights (resamplers.jl:118-143):
+         * log_w = -log eta[a]; ll_baseline = -((LSE_1 - LSE_2) + (LSE_3 - LSE_4)) */
+        draw_uniforms(uniforms, seed, rc->kind, N, t, ubuf);
+        int32_t* a = anc_t ? anc_t : (int32_t*)malloc(sizeof(int32_t) * N);
+        clamps += or_sample_ancestors(rc->kind, rc->conv, N, wbuf, ubuf, a, mar_t);
+        memcpy(xtmp, x, sizeof(double) * N * dx);
+        for (long i = 0; i < N; ++i)
+          memcpy(x + (size_t)i * dx, xtmp + (size_t)(a[i] - 1) * dx, sizeof(double) * dx);
+        const double lse1 = or_logsumexp(aux, N);
+        const double lse2 = uniform ? log((double)N) : or_logsumexp(logw, N);
+        for (long i = 0; i < N; ++i) logw[i] = -eta[a[i] - 1];
+        const double lse3 = or_logsumexp(logw, N), lse4 = log((double)N);
+        const double llb = -((lse1 - lse2) + (lse3 - lse4));
+        /* predict (particles.jl:70-73): logsumexp(log_weights) + ll_baseline */
+        baseline = lse3 + llb;
+        uniform = 0;
+        if (!anc_t) free(a);
+      } else {
+        if (anc_t)
+          for (long i = 0; i < N; ++i) anc_t[i] = (int32_t)(i + 1);
+        if (mar_t)
+          for (long i = 0; i < N; ++i) mar_t[i] = 0.0;
+        baseline = uniform ? log((double)N) : or_logsumexp(logw, N);
+      }
+    } else {
+      int was_uniform = uniform;
+      res = maybe_resample(rc, t, N, dx, x, xtmp, logw, &uniform, wbuf, ubuf, uniforms, seed,
+                           anc_t, mar_t, &ess, &clamps);
+      /* predict (particles.jl:52-74): baseline = logsumexp(log_weights) */
+      baseline = (was_uniform && !res) ? log((double)N) : or_logsumexp(logw, N);
+    }
     if (out && out->ess) out->ess[t - 1] = ess;
     if (out && out->resampled) out->resampled[t - 1] = (int8_t)res;
-    /* predict (particles.jl:52-74): baseline = logsumexp(log_weights) */
-    double baseline = (was_uniform && !res) ? log((double)N) : or_logsumexp(logw, N);
     const double* y = ys + (size_t)(t - 1) * dy;
 #pragma omp parallel for num_threads(g_threads) schedule(static)
     for (long i = 0; i < N; ++i) {
@@ -837,7 +887,7 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
 done:
   if (out && out->clamps) *out->clamps = clamps;
   *ll = tot;
-  free(x); free(xtmp); free(logw); free(wbuf); free(ubuf);
+  free(x); free(xtmp); free(logw); free(wbuf); free(ubuf); free(eta); free(aux);
   free(L0); free(LQ); free(LR); free(Lq); free(Kq); free(Sq);
   return st;
 }

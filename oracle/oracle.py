@@ -82,7 +82,7 @@ class _RC(C.Structure):
 
 
 class _Prop(C.Structure):
-    _fields_ = [("kind", C.c_int), ("k", C.c_double)]
+    _fields_ = [("kind", C.c_int), ("k", C.c_double), ("lookahead", C.c_int)]
 
 
 class _PFOut(C.Structure):
@@ -170,8 +170,10 @@ def joint_smooth_truth(m: LGModel, ys):
 
 def pf_run(m: LGModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=0.5,
            schedule=None, noise=None, uniforms=None, seed=0, proposal=PROP_BOOTSTRAP,
-           k=1.0, want_ancestors=False, want_margins=False, want_states=False, threads=1):
-    """filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys).
+           k=1.0, want_ancestors=False, want_margins=False, want_states=False, threads=1,
+           lookahead=0):
+    """filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys), or with
+    lookahead=1 filter(rng, model, AuxiliaryParticleFilter(pf, MeanPredictive()), ys).
 
     noise: [(T+1), dx, N] standard normals (step 0 = prior draw) or None for the
     shared Philox stream with ``seed``; uniforms: systematic [T], else [T, N].
@@ -199,7 +201,7 @@ def pf_run(m: LGModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=
     un = None if uniforms is None else _f64(uniforms)
     ll = C.c_double()
     lib().or_set_threads(int(threads))
-    st = lib().or_pf_run(C.byref(m._struct()), C.byref(_Prop(proposal, k)), C.byref(rc),
+    st = lib().or_pf_run(C.byref(m._struct()), C.byref(_Prop(proposal, k, int(lookahead))), C.byref(rc),
                          C.c_long(N), T, _p(ys), _p(nz), _p(un), C.c_uint64(seed),
                          C.byref(ll), C.byref(o))
     lib().or_set_threads(1)

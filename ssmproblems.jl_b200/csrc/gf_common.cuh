@@ -124,6 +124,8 @@ struct PfScalars {
   double u0;          // systematic uniform of the pending resample
   double wn;          // total normalised weight (fixed-point sum / 2^62)
   double wtotal;      // sum of raw weights (standalone sample_ancestors)
+  double lse_aux;     // auxiliary filter: LSE(logw + log eta) of the pending resample
+  double base_adj;    // auxiliary filter: shift of the post-resample baseline log N
   int32_t t;          // last completed step (0 after initialisation)
   int32_t resample;   // 1 if step t+1 starts with a resample
   int32_t uniform;    // 1 while the weights are the initial TypelessZero ones

@@ -67,6 +67,8 @@ __global__ void pf_init_scalars(PfJob* jobs, int njobs, const double* ess1, cons
   sc->scan_tile = 0;
   sc->clamps = 0;
   sc->mcounter = 0;
+  sc->lse_aux = 0.0;
+  sc->base_adj = 0.0;
   if (J.ess_steps) J.ess_steps[0] = ess1[j];
   if (J.res_steps) J.res_steps[0] = res1[j];
 }

@@ -14,6 +14,7 @@ struct PfLgKernels {
   int dxp = 0, dyp = 0;
   void (*prop)(const PfJob*, int) = nullptr;
   void (*init)(const PfJob*, int, int, int) = nullptr;
+  void (*lookahead)(const PfJob*, int) = nullptr;  // auxiliary filter first stage
   size_t smem = 0;
   int params_len = 0, off_mu0 = 0, off_L0 = 0;
   // tensor-core bootstrap propagation (FP32, state dim >= 16), null if none

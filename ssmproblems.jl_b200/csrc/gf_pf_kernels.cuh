@@ -63,6 +63,7 @@ struct PfJob {
   int32_t* ocum;             // [N] cumulative offspring counts of the pending resample
   int32_t* mpk;              // [ntiles + 1] merge-path start particle of each fill block
   int32_t* anc;              // [N] 0-based ancestors of the pending resample
+  void* eta;                 // auxiliary filter: [N] lookahead log eta of the current particles (else null)
 };
 
 __device__ __forceinline__ int find_job(const PfJob* jobs, int njobs, int block, bool scan) {
@@ -250,17 +251,10 @@ struct LseAcc {
   }
 };
 
-// Folds the block's accumulators into part[tile] and lets the last block of
-// the job finalise the step (containers.jl:160-173 marginalise!,
-// particles.jl:70-73 baseline, resamplers.jl:179-183 ESS decision).
-// Baseline: log N after a resample or for the initial TypelessZero weights;
-// otherwise logsumexp of the normalised log-weights, which is 0 up to the
-// rounding of the normalisation (below 1e-15), so it is taken as 0.
-// A tile may be covered by `nparts` blocks (block `part` of tile `tile`); the
-// partials are then kept per part, folded in part order and summed per tile
-// for the tile prefixes.
-static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh, LseAcc a,
-                                    double* red, int part = 0, int nparts = 1) {
+// Folds the block's accumulators into part[tile * nparts + part]; true in the
+// job's last block to arrive (which then folds every partial).
+static __device__ bool fold_partials(const PfJob& J, int tile, LseAcc a, double* red, int part,
+                                     int nparts) {
   PfScalars* sc = J.sc;
   __shared__ int s_last;
   const int nall = J.ntiles * nparts;
@@ -278,9 +272,15 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
     s_last = (prev == (unsigned)(nall - 1));
   }
   __syncthreads();
-  if (!s_last) return;
+  if (!s_last) return false;
   __threadfence();
-  // ---- last block: fold all partials in a fixed order (deterministic) ----
+  return true;
+}
+
+// Last block: (max, sum e, sum e^2) over every partial, in a fixed order.
+static __device__ void global_stats(const PfJob& J, int nparts, double* red, double* GM_out,
+                                    double* GS1_out, double* GS2_out) {
+  const int nall = J.ntiles * nparts;
   double m = -INFINITY;
   for (int bb = threadIdx.x; bb < nall; bb += blockDim.x) m = fmax(m, __ldcg(J.part + (size_t)bb * PF_PW));
   double GM = block_max(m, red);
@@ -294,9 +294,62 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
       s2 += __ldcg(p + 2) * ff * ff;
     }
   }
-  double GS1 = block_sum(s1, red);
-  double GS2 = block_sum(s2, red);
-  const double base = fresh ? J.log_n : 0.0;
+  *GM_out = GM;
+  *GS1_out = block_sum(s1, red);
+  *GS2_out = block_sum(s2, red);
+}
+
+// Last block: cumulative normalised weight at every tile start,
+// P_b = sum_{b'<b} S1_b' e^{M_b' - lse}, summed in 64-bit fixed point (2^-62
+// units): integer sums are exact, so the parallel scan gives the same monotone
+// prefixes in any order.
+static __device__ void write_tile_prefixes(const PfJob& J, int nparts, double lse) {
+  PfScalars* sc = J.sc;
+  __shared__ unsigned long long s_wsum[32];
+  const int per = (J.ntiles + blockDim.x - 1) / blockDim.x;
+  const int b0 = min((int)threadIdx.x * per, J.ntiles), b1 = min(b0 + per, J.ntiles);
+  unsigned long long tot = 0ull;
+  auto tile_fix = [&](int bb) {  // fixed-point normalised weight of tile bb
+    unsigned long long w = 0ull;
+    for (int q = 0; q < nparts; ++q) {
+      const double* p = J.part + ((size_t)bb * nparts + q) * PF_PW;
+      const double mb = __ldcg(p);
+      if (mb > -INFINITY) w += __double2ull_rn(__ldcg(p + 1) * exp(mb - lse) * kFix);
+    }
+    return w;
+  };
+  for (int bb = b0; bb < b1; ++bb) tot += tile_fix(bb);
+  unsigned long long all = 0ull;
+  unsigned long long run = block_excl_scan_u64(tot, s_wsum, &all);
+  for (int bb = b0; bb < b1; ++bb) {
+    J.tprefix[bb] = (double)run * kInvFix;
+    run += tile_fix(bb);
+  }
+  if (threadIdx.x == 0) {
+    J.tprefix[J.ntiles] = (double)all * kInvFix;
+    sc->wn = (double)all * kInvFix;
+  }
+}
+
+// Folds the block's accumulators into part[tile] and lets the last block of
+// the job finalise the step (containers.jl:160-173 marginalise!,
+// particles.jl:70-73 baseline, resamplers.jl:179-183 ESS decision).
+// Baseline: log N after a resample or for the initial TypelessZero weights
+// (plus the auxiliary filter's first-stage shift sc->base_adj after one of its
+// resamples, resamplers.jl:118-138); otherwise logsumexp of the normalised
+// log-weights, which is 0 up to the rounding of the normalisation (below
+// 1e-15), so it is taken as 0.
+// A tile may be covered by `nparts` blocks (block `part` of tile `tile`); the
+// partials are then kept per part, folded in part order and summed per tile
+// for the tile prefixes.
+static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh, LseAcc a,
+                                    double* red, int part = 0, int nparts = 1) {
+  PfScalars* sc = J.sc;
+  if (!fold_partials(J, tile, a, red, part, nparts)) return;
+  // ---- last block: fold all partials in a fixed order (deterministic) ----
+  double GM, GS1, GS2;
+  global_stats(J, nparts, red, &GM, &GS1, &GS2);
+  const double base = fresh ? J.log_n + sc->base_adj : 0.0;
   __shared__ int s_res;
   const double lse = GM + log(GS1);
   if (threadIdx.x == 0) {
@@ -316,38 +369,12 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
     sc->lse = lse;
     sc->ess = ess;
     sc->resample = res;
+    sc->base_adj = 0.0;
     s_res = res;
   }
   __syncthreads();
-  if (s_res) {
-    // Cumulative normalised weight at every tile start, P_b = sum_{b'<b} S1_b' e^{M_b' - LSE},
-    // summed in 64-bit fixed point (2^-62 units): integer sums are exact, so the
-    // parallel scan gives the same monotone prefixes in any order.
-    __shared__ unsigned long long s_wsum[32];
-    const int per = (J.ntiles + blockDim.x - 1) / blockDim.x;
-    const int b0 = min((int)threadIdx.x * per, J.ntiles), b1 = min(b0 + per, J.ntiles);
-    unsigned long long tot = 0ull;
-    auto tile_fix = [&](int bb) {  // fixed-point normalised weight of tile bb
-      unsigned long long w = 0ull;
-      for (int q = 0; q < nparts; ++q) {
-        const double* p = J.part + ((size_t)bb * nparts + q) * PF_PW;
-        const double mb = __ldcg(p);
-        if (mb > -INFINITY) w += __double2ull_rn(__ldcg(p + 1) * exp(mb - lse) * kFix);
-      }
-      return w;
-    };
-    for (int bb = b0; bb < b1; ++bb) tot += tile_fix(bb);
-    unsigned long long all = 0ull;
-    unsigned long long run = block_excl_scan_u64(tot, s_wsum, &all);
-    for (int bb = b0; bb < b1; ++bb) {
-      J.tprefix[bb] = (double)run * kInvFix;
-      run += tile_fix(bb);
-    }
-    if (threadIdx.x == 0) {
-      J.tprefix[J.ntiles] = (double)all * kInvFix;
-      sc->wn = (double)all * kInvFix;
-    }
-  }
+  // the auxiliary filter decides in its lookahead kernel instead
+  if (s_res && !J.eta) write_tile_prefixes(J, nparts, lse);
   __syncthreads();
   if (threadIdx.x == 0) {
     sc->uniform = 0;
@@ -355,6 +382,40 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
     sc->counter = 0u;
     __threadfence();
     sc->t = t;
+  }
+}
+
+// Auxiliary particle filter, last block of the lookahead launch of step t:
+// the ESS decision on softmax(logw + log eta) (AuxiliaryResampler,
+// resamplers.jl:109-116, 179-183), and after a resample the tile prefixes of
+// those weights and the baseline shift LSE(logw) - LSE(logw + log eta) that
+// construct_new_state folds into ll_baseline (resamplers.jl:118-138; with the
+// particles' new log-weights -log eta[a], LSE_3 cancels in predict).
+static __device__ void apf_finish(const PfJob& J, int tile, int t, LseAcc a, double* red) {
+  PfScalars* sc = J.sc;
+  if (!fold_partials(J, tile, a, red, 0, 1)) return;
+  double GM, GS1, GS2;
+  global_stats(J, 1, red, &GM, &GS1, &GS2);
+  const double lse1 = GM + log(GS1);
+  __shared__ int s_res;
+  if (threadIdx.x == 0) {
+    const double ess = GS1 * GS1 / GS2;
+    const int s = J.schedule ? (int)J.schedule[t - 1] : -1;
+    const int res = s >= 0 ? (s != 0) : (J.threshold * (double)J.N >= ess);
+    if (!(lse1 > -INFINITY) || isnan(lse1)) sc->status = GF_ERR_ARG;
+    if (J.ess_steps) J.ess_steps[t - 1] = ess;
+    if (J.res_steps) J.res_steps[t - 1] = (int8_t)res;
+    sc->resample = res;
+    sc->lse_aux = lse1;
+    sc->base_adj = res ? sc->lse - lse1 : 0.0;
+    s_res = res;
+  }
+  __syncthreads();
+  if (s_res) write_tile_prefixes(J, 1, lse1);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    sc->counter = 0u;
+    __threadfence();
   }
 }
 
@@ -380,7 +441,9 @@ __global__ void __launch_bounds__(PF_THREADS, 6) pf_resample_kernel(const PfJob*
   const int tile = blockIdx.x - J.tile0;
   const int64_t N = J.N, i0 = (int64_t)tile * PF_TILE;
   const int nloc = (int)min((int64_t)PF_TILE, N - i0);
-  const double lse = sc->lse;
+  // auxiliary filter: weights softmax(logw + log eta) (resamplers.jl:109-116)
+  const bool aux = J.eta != nullptr;
+  const double lse = aux ? sc->lse_aux : sc->lse;
   const double P0 = J.tprefix[tile], P1 = J.tprefix[tile + 1];
   // this thread's PF_PPT consecutive particles (vector loads; tiles start 16-byte aligned)
   const int l0 = PF_PPT * threadIdx.x;
@@ -398,11 +461,20 @@ __global__ void __launch_bounds__(PF_THREADS, 6) pf_resample_kernel(const PfJob*
 #pragma unroll
     for (int q = 0; q < PF_PPT; ++q) x[q] = l0 + q < nloc ? lw[q] : (Real)0;
   }
+  double xv[PF_PPT];
+#pragma unroll
+  for (int q = 0; q < PF_PPT; ++q) xv[q] = (double)x[q];
+  if (aux) {
+    const Real* eta = reinterpret_cast<const Real*>(J.eta) + i0 + l0;
+#pragma unroll
+    for (int q = 0; q < PF_PPT; ++q)
+      if (l0 + q < nloc) xv[q] += (double)eta[q];
+  }
   // W_k = P0 + (fixed-point running sum inside the tile), clamped to the tile's end
   unsigned long long loc[PF_PPT], acc = 0ull;
 #pragma unroll
   for (int q = 0; q < PF_PPT; ++q) {
-    if (l0 + q < nloc) acc += __double2ull_rn(exp((double)x[q] - lse) * kFix);
+    if (l0 + q < nloc) acc += __double2ull_rn(exp(xv[q] - lse) * kFix);
     loc[q] = acc;
   }
   unsigned long long all;

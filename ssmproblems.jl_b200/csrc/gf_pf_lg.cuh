@@ -93,6 +93,8 @@ __global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __
   const uint64_t seed = J.seed;
   const bool diag = J.diag_l != 0;
   const double obs_const = J.obs_const, prop_const = J.prop_const;
+  const Real* eta = reinterpret_cast<const Real*>(J.eta);
+  const bool apf = resamp && eta != nullptr;
   LseAcc acc;
 
   for (int p = 0; p < PF_PPT; ++p) {
@@ -103,7 +105,8 @@ __global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __
     Real x[DXP];
 #pragma unroll
     for (int d = 0; d < DXP; ++d) x[d] = d < dx ? Xs[(size_t)d * N + a] : Real(0);
-    const double lin = fresh ? 0.0 : (double)lw[i] - lse_prev;
+    // after an auxiliary resample the particle starts from -log eta of its ancestor
+    const double lin = fresh ? (apf ? -(double)eta[a] : 0.0) : (double)lw[i] - lse_prev;
     // mean part: x' = A x + b (bootstrap, simulate(dyn) = rand(MvNormal(A x + b, Q)))
     // or M x + v_t (guided), with ma = A x + b kept for log p(x'|x)
     Real xn[DXP];
@@ -325,6 +328,8 @@ __global__ void __launch_bounds__(TC_THREADS) pf_lg_propagate_tc(const PfJob* __
   int32_t* __restrict__ anc_out = J.anc_out;
   const uint64_t seed = J.seed;
   const double obs_const = J.obs_const;
+  const float* eta = reinterpret_cast<const float*>(J.eta);
+  const bool apf = resamp && eta != nullptr;
   const uint32_t idesc = umma::idesc_tf32(128, NM);
   const uint32_t kstride = 128, mstride = (uint32_t)(K / 4) * 128;
   LseAcc acc;
@@ -353,7 +358,7 @@ __global__ void __launch_bounds__(TC_THREADS) pf_lg_propagate_tc(const PfJob* __
 #pragma unroll
       for (int cc = 0; cc < 4; ++cc) xe[DXP + 4 * q + cc] = e4[cc];
     }
-    const double lin = (fresh || !valid) ? 0.0 : (double)lw[i] - lse_prev;
+    const double lin = !valid ? 0.0 : fresh ? (apf ? -(double)eta[a] : 0.0) : (double)lw[i] - lse_prev;
     // this particle's row of the A operand, split hi / lo, 16-byte chunks
 #pragma unroll
     for (int k4 = 0; k4 < K / 4; ++k4) {
@@ -413,6 +418,62 @@ __global__ void __launch_bounds__(TC_THREADS) pf_lg_propagate_tc(const PfJob* __
   block_finish(J, tile, t, fresh, acc, red, part, TC_SPLIT);
 }
 
+// Auxiliary particle filter, first stage of step t (particles.jl:273-357):
+// log eta_i = log p(y_t | x*_i) with x*_i = A x_i + b, the mean and the mode of
+// the transition MvNormal(A x + b, Q) (MeanPredictive, ModePredictive), then
+// the resampling decision on softmax(logw + log eta) in apf_finish.
+template <typename Real, int DXP, int DYP>
+__global__ void __launch_bounds__(PF_THREADS) pf_apf_lookahead(const PfJob* __restrict__ jobs, int njobs) {
+  using Lay = LgLayout<DXP, DYP>;
+  __shared__ Real sA[DXP * DXP], sb[DXP], sH[DYP * DXP], sy[DYP];
+  __shared__ double red[32];
+  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const PfJob& J = jobs[jb];
+  PfScalars* sc = J.sc;
+  const int t = sc->t + 1;
+  if (t > J.T || sc->status != 0) return;
+  const int tile = blockIdx.x - J.tile0;
+  const Real* P = reinterpret_cast<const Real*>(J.params);
+  for (int k = threadIdx.x; k < DXP * DXP; k += PF_THREADS) sA[k] = P[Lay::A + k];
+  for (int k = threadIdx.x; k < DYP * DXP; k += PF_THREADS) sH[k] = P[Lay::H + k];
+  for (int k = threadIdx.x; k < DXP; k += PF_THREADS) sb[k] = P[Lay::b + k];
+  const Real* Y = reinterpret_cast<const Real*>(J.ystep) + (size_t)(t - 1) * J.ystride;
+  for (int k = threadIdx.x; k < DYP; k += PF_THREADS) sy[k] = Y[k];
+  __syncthreads();
+  const int64_t N = J.N;
+  const int dx = J.dx;
+  const Real* Xs = reinterpret_cast<const Real*>(J.X[(t - 1) & 1]);
+  const Real* lw = reinterpret_cast<const Real*>(J.lw);
+  Real* eta = reinterpret_cast<Real*>(J.eta);
+  const double obs_const = J.obs_const;
+  LseAcc acc;
+  for (int p = 0; p < PF_PPT; ++p) {
+    const int64_t i = (int64_t)tile * PF_TILE + p * PF_THREADS + threadIdx.x;
+    if (i >= N) break;
+    Real m[DXP];
+#pragma unroll
+    for (int r = 0; r < DXP; ++r) m[r] = sb[r];
+#pragma unroll
+    for (int c = 0; c < DXP; ++c) {
+      const Real xc = c < dx ? Xs[(size_t)c * N + i] : Real(0);
+#pragma unroll
+      for (int r = 0; r < DXP; ++r) m[r] = fma(sA[c * DXP + r], xc, m[r]);
+    }
+    Real q = 0;
+#pragma unroll
+    for (int k = 0; k < DYP; ++k) {
+      Real r = sy[k];
+#pragma unroll
+      for (int c = 0; c < DXP; ++c) r = fma(-sH[c * DYP + k], m[c], r);
+      q = fma(r, r, q);
+    }
+    const Real le = (Real)(obs_const - 0.5 * (double)q);
+    eta[i] = le;
+    acc.add((double)lw[i] + (double)le);
+  }
+  apf_finish(J, tile, t, acc, red);
+}
+
 template <typename Real, int DXP, int DYP, bool G>
 PfLgKernels make_lg() {
   PfLgKernels k;
@@ -420,6 +481,7 @@ PfLgKernels make_lg() {
   k.dyp = DYP;
   k.prop = pf_lg_propagate<Real, DXP, DYP, G>;
   k.init = pf_lg_init<Real, DXP>;
+  k.lookahead = pf_apf_lookahead<Real, DXP, DYP>;
   k.smem = sizeof(Real) * (G ? LgLayout<DXP, DYP>::smem_guided : LgLayout<DXP, DYP>::smem_boot);
   k.params_len = LgLayout<DXP, DYP>::total;
   k.off_mu0 = LgLayout<DXP, DYP>::mu0;

@@ -26,6 +26,7 @@ struct gf_pf_plan {
   double *pp = nullptr, *key = nullptr, *part = nullptr, *mpart = nullptr, *ess1 = nullptr;
   double* tprefix = nullptr;
   int32_t *ocum = nullptr, *mpk = nullptr, *anc = nullptr;
+  void* eta = nullptr;  // auxiliary filter: lookahead log eta [N]
   unsigned long long* flags = nullptr;
   PfScalars* sc = nullptr;
   int8_t *sched_dev = nullptr, *res1 = nullptr;
@@ -68,7 +69,8 @@ static gf_status validate_cfg(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_con
   if (cfg->convention < 0 || cfg->convention > 1) return set_err(ctx, GF_ERR_ARG, "unknown convention");
   if (cfg->precision != GF_PREC_F32 && cfg->precision != GF_PREC_F64)
     return set_err(ctx, GF_ERR_ARG, "unknown precision");
-  if (cfg->convention == GF_CONV_CUDAEXT && cfg->resampler == GF_RS_MULTINOMIAL) return GF_OK;
+  if (cfg->lookahead != GF_LOOKAHEAD_NONE && cfg->lookahead != GF_LOOKAHEAD_MEAN)
+    return set_err(ctx, GF_ERR_ARG, "unknown lookahead");
   return GF_OK;
 }
 
@@ -175,6 +177,7 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   ALLOC(ocum, sizeof(int32_t) * (size_t)N);
   ALLOC(mpk, sizeof(int32_t) * (size_t)(p->ntiles + 1));
   ALLOC(anc, sizeof(int32_t) * (size_t)N);
+  if (cfg->lookahead != GF_LOOKAHEAD_NONE) { ALLOC(eta, p->rsize * (size_t)N); }
   ALLOC(tprefix, sizeof(double) * (size_t)(p->ntiles + 1));
   ALLOC(part, sizeof(double) * PF_PW * (size_t)p->ntiles * PF_MAX_SPLIT);
   ALLOC(mpart, sizeof(double) * (size_t)p->ntiles * m->dx);
@@ -214,12 +217,21 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   J.mpk = p->mpk;
   J.anc = p->anc;
   J.tprefix = p->tprefix;
+  J.eta = p->eta;
   J.schedule = p->sched_dev;
   *out = p.release();
   return GF_OK;
 }
 
 // Enqueues one full filter run (prep, init, T steps, outputs) on the stream.
+// Auxiliary filter: the first-stage scores and the resampling decision of the
+// coming step, between a propagate and the resample.
+static void launch_lookahead(gf_pf_plan* p) {
+  if (!p->eta) return;
+  ProfScope ps(p->ctx, KC_SCAN);
+  p->k.lookahead<<<p->ntiles, PF_THREADS, 0, p->ctx->stream>>>(p->job_dev, 1);
+}
+
 static void enqueue_run(gf_pf_plan* p, bool means) {
   gf_ctx* ctx = p->ctx;
   cudaStream_t s = ctx->stream;
@@ -230,6 +242,7 @@ static void enqueue_run(gf_pf_plan* p, bool means) {
     ProfScope ps(ctx, KC_PREP);
     p->k.init<<<p->ntiles, PF_THREADS, 0, s>>>(p->job_dev, 1, p->k.off_mu0, p->k.off_L0);
   }
+  launch_lookahead(p);
   launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
   for (int t = 1; t <= p->T; ++t) {
     {
@@ -237,7 +250,10 @@ static void enqueue_run(gf_pf_plan* p, bool means) {
       p->prop_fn<<<p->ntiles * p->prop_split, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
     }
     if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);
-    if (t < p->T) launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
+    if (t < p->T) {
+      launch_lookahead(p);
+      launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
+    }
   }
   launch_finish(ctx, p->dbl, p->job_dev, p->N);
 }
@@ -348,6 +364,7 @@ static gf_status enqueue_run_paths(gf_pf_plan* p, bool means, void* paths) {
   GF_CHECK_CUDA(ctx, cudaMemsetAsync(p->flags, 0, sizeof(unsigned long long) * 2 * p->nstiles, s));
   p->k.init<<<p->ntiles, PF_THREADS, 0, s>>>(p->job_dev, 1, p->k.off_mu0, p->k.off_L0);
   tree_launch_init(ctx, p->dbl, p->job_dev, p->N, p->tree);
+  launch_lookahead(p);
   launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
   for (int t = 1; t <= p->T; ++t) {
     if ((t - 1) % kTreeChunk == 0) {
@@ -358,7 +375,10 @@ static gf_status enqueue_run_paths(gf_pf_plan* p, bool means, void* paths) {
     p->prop_fn<<<p->ntiles * p->prop_split, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
     tree_launch_insert(ctx, p->dbl, p->job_dev, p->N, p->tree, t);
     if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);
-    if (t < p->T) launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
+    if (t < p->T) {
+      launch_lookahead(p);
+      launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
+    }
   }
   launch_finish(ctx, p->dbl, p->job_dev, p->N);
   tree_launch_paths(ctx, p->dbl, p->job_dev, p->N, p->tree, p->T, paths);

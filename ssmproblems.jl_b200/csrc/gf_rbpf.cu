@@ -424,6 +424,8 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
     return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
   if (cfg->precision != GF_PREC_F32) return set_err(ctx, GF_ERR_UNSUPPORTED, "RBPF runs in FP32 only");
   if (out->paths) return set_err(ctx, GF_ERR_UNSUPPORTED, "path storage is for the linear-Gaussian PF");
+  if (cfg->lookahead != GF_LOOKAHEAD_NONE)
+    return set_err(ctx, GF_ERR_UNSUPPORTED, "the auxiliary filter is built for the linear-Gaussian PF");
   if (cfg->proposal == GF_PROP_OPTIMAL)
     return set_err(ctx, GF_ERR_UNSUPPORTED, "RBPF supports bootstrap and overdispersed outer proposals");
   if (cfg->n_particles < 1 || T < 1) return set_err(ctx, GF_ERR_ARG, "bad N or T");

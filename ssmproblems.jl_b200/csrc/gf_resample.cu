@@ -42,6 +42,8 @@ __global__ void sa_setup(const double* __restrict__ part, int nparts, PfScalars*
     sc->status = s > 0.0 ? 0 : GF_ERR_ARG;
     sc->counter = 0;
     sc->scan_tile = 0;
+    sc->lse_aux = 0.0;
+    sc->base_adj = 0.0;
     sc->clamps = 0;
     sc->mcounter = 0;
   }

@@ -364,6 +364,8 @@ static gf_status prepare(gf_ctx* ectx, const gf_srv_request* q, Req* r) {
   }
   if (!q->pf) return set_err(ectx, GF_ERR_ARG, "particle-filter request needs pf");
   const gf_pf_config& cfg = *q->pf;
+  if (cfg.lookahead != GF_LOOKAHEAD_NONE)
+    return set_err(ectx, GF_ERR_UNSUPPORTED, "the serving loop runs bootstrap and guided filters, not the auxiliary filter");
   if (cfg.n_particles < 1 || cfg.n_particles > (int64_t(1) << 31) - 1)
     return set_err(ectx, GF_ERR_ARG, "n_particles must be in [1, 2^31)");
   r->N = cfg.n_particles;

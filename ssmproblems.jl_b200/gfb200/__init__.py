@@ -7,10 +7,11 @@ B200 library libgfb200.so (C ABI in include/gf_b200.h).
     state, ll = filter(model, BF(2**20, threshold=0.5), ys, seed=1)
 """
 from ._lib import (Context, GFError, PosDefException, default_context, load)  # noqa: F401
-from .algorithms import (BF, KF, KS, PF, RBPF, SRKF, AlternatingResampler, BootstrapFilter,  # noqa: F401
-                         ESSResampler, KalmanFilter, KalmanSmoother, LatentProposal, Multinomial,
-                         OptimalProposal, OverdispersedProposal, ParticleFilter, SRKalmanFilter,
-                         Stratified, Systematic)
+from .algorithms import (APF, BF, KF, KS, PF, RBPF, SRKF, AlternatingResampler,  # noqa: F401
+                         AuxiliaryParticleFilter, BootstrapFilter, DrawPredictive, ESSResampler,
+                         KalmanFilter, KalmanSmoother, LatentProposal, MeanPredictive, ModePredictive,
+                         Multinomial, OptimalProposal, OverdispersedProposal, ParticleFilter,
+                         RepresentativeStateLookAhead, SRKalmanFilter, Stratified, Systematic)
 from .filtering import (MvNormal, ParticleDistribution, ancestors_to_offspring, filter,  # noqa: F401
                         filter_batch, offspring_to_ancestors, rng_normals, sample_ancestors,
                         smooth, smooth_batch)

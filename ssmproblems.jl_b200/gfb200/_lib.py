@@ -25,6 +25,7 @@ GF_ALGO_KF, GF_ALGO_SRKF = 0, 1
 GF_PLAN_AUTOTUNE, GF_PLAN_NO_GRAPH, GF_PLAN_PLAIN, GF_PLAN_SIMT = 1, 2, 4, 8
 GF_REQ_KF, GF_REQ_SRKF, GF_REQ_PF, GF_REQ_RBPF = 0, 1, 2, 3
 GF_CSMC_NONE, GF_CSMC_ANCESTOR, GF_CSMC_BACKWARD = 0, 1, 2
+GF_LOOKAHEAD_NONE, GF_LOOKAHEAD_MEAN = 0, 1
 
 EXPORTED = [
     "gf_ctx_create", "gf_ctx_destroy", "gf_last_error", "gf_ctx_set_stream", "gf_ctx_get_stream",
@@ -59,7 +60,7 @@ class PFConfigC(C.Structure):
     _fields_ = [("n_particles", C.c_int64), ("resampler", C.c_int32), ("convention", C.c_int32),
                 ("threshold", C.c_double), ("precision", C.c_int32), ("proposal", C.c_int32),
                 ("proposal_k", C.c_double), ("seed", C.c_uint64),
-                ("schedule", C.POINTER(C.c_int8))]
+                ("schedule", C.POINTER(C.c_int8)), ("lookahead", C.c_int32)]
 
 
 class PFOutC(C.Structure):

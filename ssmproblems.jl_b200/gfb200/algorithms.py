@@ -147,6 +147,52 @@ def BootstrapFilter(N, **kw):
 BF = BootstrapFilter
 
 
+class PredictiveStatistic:
+    """How AuxiliaryParticleFilter picks a particle's representative next state
+    (particles.jl:359-384)."""
+    lookahead = -1
+
+
+class MeanPredictive(PredictiveStatistic):
+    """mean(transition) = A x + b."""
+    lookahead = 1
+
+
+class ModePredictive(PredictiveStatistic):
+    """mode(transition) = A x + b for the Gaussian transition (same scores as MeanPredictive)."""
+    lookahead = 1
+
+
+class DrawPredictive(PredictiveStatistic):
+    """A draw from the transition: not built (needs a second noise stream per step)."""
+    lookahead = -1
+
+
+class RepresentativeStateLookAhead:
+    def __init__(self, pp: PredictiveStatistic):
+        self.pp = pp
+
+
+class AuxiliaryParticleFilter(AbstractFilter):
+    """AuxiliaryParticleFilter(pf, pp) (particles.jl:270-357): first-stage weights
+    log p(y_t | x*) with x* the predictive statistic `pp` of each particle's
+    transition, resampling on softmax(logw + log eta) (AuxiliaryResampler,
+    resamplers.jl:85-143), second-stage weights corrected by -log eta[a]."""
+
+    def __init__(self, pf: "ParticleFilter", pp):
+        if isinstance(pp, RepresentativeStateLookAhead):
+            pp = pp.pp
+        if not isinstance(pp, PredictiveStatistic):
+            raise TypeError("AuxiliaryParticleFilter(pf, MeanPredictive() | ModePredictive())")
+        if pp.lookahead < 0:
+            raise NotImplementedError(f"{type(pp).__name__} lookahead is not built")
+        self.pf = pf
+        self.weight_strategy = RepresentativeStateLookAhead(pp)
+
+
+APF = AuxiliaryParticleFilter
+
+
 class RBPF(AbstractFilter):
     """RBPF(pf, af) (rbpf.jl:8-14); af must be a KalmanFilter."""
 

@@ -12,9 +12,8 @@ import ctypes as C
 import numpy as np
 
 from . import _lib as L
-from .algorithms import (AlternatingResampler, ESSResampler, KalmanFilter, KalmanSmoother,
-                         ParticleFilter, RBPF,
-                         SRKalmanFilter)
+from .algorithms import (AlternatingResampler, AuxiliaryParticleFilter, ESSResampler, KalmanFilter,
+                         KalmanSmoother, ParticleFilter, RBPF, SRKalmanFilter)
 from .models import HierarchicalSSM, StateSpaceModel
 
 
@@ -69,7 +68,7 @@ def _rs_params(algo: ParticleFilter, T: int):
     return threshold, base.kind, sched
 
 
-def _pf_config(algo: ParticleFilter, T: int, seed: int, schedule=None):
+def _pf_config(algo: ParticleFilter, T: int, seed: int, schedule=None, lookahead=0):
     threshold, kind, sched = _rs_params(algo, T)
     if schedule is not None:
         sched = np.asarray(schedule, dtype=np.int8)
@@ -77,7 +76,8 @@ def _pf_config(algo: ParticleFilter, T: int, seed: int, schedule=None):
     conv = L.GF_CONV_CUDAEXT if algo.convention == "cudaext" else L.GF_CONV_CPU
     cfg = L.PFConfigC(algo.N, kind, conv, threshold, prec, algo.proposal.kind,
                       float(getattr(algo.proposal, "k", 1.0)), int(seed) & (2**64 - 1),
-                      None if sched is None else sched.ctypes.data_as(C.POINTER(C.c_int8)))
+                      None if sched is None else sched.ctypes.data_as(C.POINTER(C.c_int8)),
+                      int(lookahead))
     return cfg, sched, prec
 
 
@@ -104,17 +104,20 @@ def filter(model, algo, observations, *, seed: int = 0, noise=None, uniforms=Non
     if isinstance(algo, ParticleFilter):
         return _pf(model, algo, ys, seed, noise, uniforms, ctx, want_ancestors, want_means,
                    schedule, want_paths)
+    if isinstance(algo, AuxiliaryParticleFilter):
+        return _pf(model, algo.pf, ys, seed, noise, uniforms, ctx, want_ancestors, want_means,
+                   schedule, want_paths, lookahead=algo.weight_strategy.pp.lookahead)
     raise TypeError(f"unsupported algorithm {type(algo).__name__}")
 
 
 def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, schedule,
-        want_paths=False):
+        want_paths=False, lookahead=0):
     if not isinstance(model, StateSpaceModel):
         raise TypeError("particle filter needs a linear-Gaussian StateSpaceModel")
     mc = model._c_struct()
     ys = ys.reshape(-1, model.dy)
     T = ys.shape[0]
-    cfg, sched, prec = _pf_config(algo, T, seed, schedule)
+    cfg, sched, prec = _pf_config(algo, T, seed, schedule, lookahead)
     N, dx = algo.N, model.dx
     rdt = np.float64 if prec == L.GF_PREC_F64 else np.float32
     out = dict(ll=np.zeros(1), ll_steps=np.zeros(T), ess_steps=np.zeros(T),

@@ -53,6 +53,7 @@ struct GfPfConfig
     proposal_k::Float64
     seed::UInt64
     schedule::Ptr{Int8}
+    lookahead::Int32   # GF_LOOKAHEAD_*
 end
 
 struct GfPfOut
@@ -169,7 +170,7 @@ function GeneralisedFilters.filter(
     cfg = Ref(GfPfConfig(N, resampler_code(algo.resampler.resampler), 0,
                          algo.resampler.threshold,
                          precision === :f64 ? GF_PREC_F64 : GF_PREC_F32, GF_PROP_BOOTSTRAP, 1.0,
-                         rand(rng, UInt64), C_NULL))
+                         rand(rng, UInt64), C_NULL, Int32(0)))
     return with_lg_model(model) do m
         dx = Int(m.dx)
         ET = precision === :f64 ? Float64 : Float32

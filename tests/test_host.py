@@ -62,3 +62,14 @@ def test_workloads_shapes():
     reqs = W.serving_mix(200, rate=1000.0, seed=0)
     kinds = [k for _, k, _ in reqs]
     assert kinds.count("kf") > kinds.count("bf") > kinds.count("rbpf")
+
+
+def test_apf_config_and_unbuilt_lookahead():
+    """AuxiliaryParticleFilter(pf, MeanPredictive()/ModePredictive()) maps to
+    GF_LOOKAHEAD_MEAN; DrawPredictive is not built."""
+    apf = G.APF(G.BF(100, threshold=0.7), G.MeanPredictive())
+    cfg, _, _ = _pf_config(apf.pf, 5, 1, lookahead=apf.weight_strategy.pp.lookahead)
+    assert cfg.lookahead == L.GF_LOOKAHEAD_MEAN and cfg.threshold == 0.7
+    assert G.APF(G.BF(10), G.ModePredictive()).weight_strategy.pp.lookahead == L.GF_LOOKAHEAD_MEAN
+    with pytest.raises(NotImplementedError):
+        G.APF(G.BF(10), G.DrawPredictive())

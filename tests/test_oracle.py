@@ -188,3 +188,26 @@ def test_philox_known_answer():
     assert abs(vals.mean() - 0.5) < 0.01 and abs(vals.var() - 1 / 12) < 0.005
     z = O.philox_normals(7, 4000, 4, 1)
     assert abs(z.mean()) < 0.03 and abs(z.var() - 1) < 0.05
+
+
+def test_apf_oracle_without_resampling_is_the_bootstrap_filter():
+    """preserve_sample keeps the weights, so the auxiliary scores only act through
+    a resample: with threshold 0 the APF run equals the BF run exactly."""
+    rng = np.random.default_rng(12)
+    m = O.create_linear_gaussian_model(rng, 2, 2)
+    _, ys = O.sample(rng, m, 5)
+    a = O.pf_run(m, 500, ys, threshold=0.0, seed=4, lookahead=1)
+    b = O.pf_run(m, 500, ys, threshold=0.0, seed=4, lookahead=0)
+    assert a["ll"] == b["ll"]
+
+
+def test_apf_oracle_converges_to_kf():
+    """test/algorithms/particles.jl:57-82 with every step resampling (threshold 1.0):
+    the APF log-evidence estimate is unbiased for the Kalman filter's."""
+    rng = np.random.default_rng(1234)
+    m = O.create_linear_gaussian_model(rng, 1, 1)
+    _, ys = O.sample(rng, m, 4)
+    kll = O.kf_filter(m, ys)[0]
+    r = O.pf_run(m, 200_000, ys, threshold=1.0, seed=2, lookahead=1, threads=4)
+    assert r["resampled"].all()
+    assert abs(r["ll"] - kll) < 3e-3
