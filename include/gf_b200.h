@@ -122,6 +122,14 @@ typedef struct {
    * 90-111, containers.jl:466-631), kept on the device as sparse path storage
    * with pruning (ext/CUDAExt.jl:146-298).  Linear-Gaussian PF only. */
   void* paths;
+  /* Dense particle history of DenseAncestorCallback / DenseParticleContainer
+   * (callbacks.jl:47-81, containers.jl:296-419): [T+1][dx][N] the states after
+   * initialisation and after every step, in the run's precision, and [T][N]
+   * the normalised log-weights after every update (the PostUpdate weights).
+   * With `ancestors` they are the container; gf_pf_dense_ancestry walks it.
+   * Linear-Gaussian PF only. */
+  void* history;
+  double* log_weight_history;
 } gf_pf_out;
 
 /* Outputs of a Kalman batch (per-step arrays are packed filter after filter). */
@@ -209,6 +217,16 @@ gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* model, const gf_pf_c
 gf_status gf_pf_plan_run(gf_pf_plan* plan, const double* ys_dev, const void* noise_dev,
                          const double* uniforms_dev, gf_pf_out* out_dev);
 gf_status gf_pf_plan_destroy(gf_pf_plan* plan);
+
+/* get_ancestry(container, i) for a DenseParticleContainer (containers.jl:
+ * 421-440): for each requested final particle, the trajectory read from the
+ * dense history by walking the 1-based ancestors back from time T.
+ * history [T+1][dx][N] and paths [T+1][dx][M] in `precision`
+ * (GF_PREC_F32 / GF_PREC_F64); ancestors [T][N] int32, 1-based; indices
+ * (nullable = all N particles, M = N) [M] 1-based final-particle indices. */
+gf_status gf_pf_dense_ancestry(gf_ctx* ctx, int32_t T, int64_t N, int32_t dx, int32_t precision,
+                               const void* history, const int32_t* ancestors, int64_t M,
+                               const int32_t* indices, int32_t memspace, void* paths);
 
 /* filter(rng, hier_model, RBPF(PF(N, ...), KalmanFilter()), ys) (rbpf.jl:8-84).
  * Supports GF_PROP_BOOTSTRAP and GF_PROP_OVERDISPERSED outer proposals.

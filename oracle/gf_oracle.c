@@ -647,6 +647,7 @@ typedef struct { /* nullable outputs */
   double* logw_final; /* N (normalised) */
   long* clamps;       /* scalar */
   double* x_all;      /* (T+1)*N*dx: states after initialisation and after every step */
+  double* logw_all;   /* T*N: normalised log-weights after every update (PostUpdate) */
 } or_pf_out;
 
 /* Noise source: injected (noise != NULL, layout [(T+1)][dx][N], step 0 = prior
@@ -873,6 +874,7 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
     for (long i = 0; i < N; ++i) logw[i] -= lse;
     tot += inc;
     if (out && out->ll_steps) out->ll_steps[t - 1] = inc;
+    if (out && out->logw_all) memcpy(out->logw_all + (size_t)(t - 1) * N, logw, sizeof(double) * N);
     if (out && out->means) {
       double* mo = out->means + (size_t)(t - 1) * dx;
       for (int d = 0; d < dx; ++d) mo[d] = 0.0;

@@ -89,7 +89,7 @@ class _PFOut(C.Structure):
     _fields_ = [("ll_steps", _dp), ("ess", _dp), ("resampled", C.POINTER(C.c_int8)),
                 ("ancestors", C.POINTER(C.c_int32)), ("margins", _dp), ("means", _dp),
                 ("x_final", _dp), ("logw_final", _dp), ("clamps", C.POINTER(C.c_long)),
-                ("x_all", _dp)]
+                ("x_all", _dp), ("logw_all", _dp)]
 
 
 class _RB(C.Structure):
@@ -194,6 +194,8 @@ def pf_run(m: LGModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=
                C.pointer(clamps))
     xall = np.zeros((T + 1, N, m.dx)) if want_states else None
     o.x_all = _p(xall)
+    lwall = np.zeros((T, N)) if want_states else None
+    o.logw_all = _p(lwall)
     sched = None if schedule is None else np.ascontiguousarray(schedule, np.int8)
     rc = _RC(resampler, conv, threshold,
              None if sched is None else sched.ctypes.data_as(C.POINTER(C.c_int8)))
@@ -212,6 +214,7 @@ def pf_run(m: LGModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=
     out["margins"] = mar
     out["clamps"] = clamps.value
     out["states"] = xall
+    out["log_weights_all"] = lwall
     return out
 
 

@@ -135,6 +135,53 @@ __global__ void pf_finish_kernel(const PfJob* __restrict__ jobs) {
   }
 }
 
+// DenseAncestorCallback (callbacks.jl:47-81): after initialisation (t = 0)
+// and after every update, the states of step t and, for t >= 1, the
+// normalised log-weights the PostUpdate callback sees (marginalise! has
+// subtracted the LSE, containers.jl:160-173).
+template <typename Real>
+__global__ void pf_record_kernel(const PfJob* __restrict__ jobs) {
+  const PfJob& J = jobs[0];
+  const PfScalars* sc = J.sc;
+  if (sc->status != 0) return;
+  const int t = sc->t;
+  const int64_t N = J.N;
+  const Real* X = reinterpret_cast<const Real*>(J.X[t & 1]);
+  const Real* lw = reinterpret_cast<const Real*>(J.lw);
+  Real* H = J.hist ? reinterpret_cast<Real*>(J.hist) + (size_t)t * J.width * N : nullptr;
+  const double lse = sc->lse;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < N; i += (int64_t)gridDim.x * blockDim.x) {
+    if (H)
+      for (int d = 0; d < J.width; ++d) H[(size_t)d * N + i] = X[(size_t)d * N + i];
+    if (J.lwh && t >= 1) J.lwh[(size_t)(t - 1) * N + i] = (double)lw[i] - lse;
+  }
+}
+
+// get_ancestry(container, i) (containers.jl:421-440) for M final particles.
+template <typename Real>
+__global__ void pf_dense_ancestry_kernel(int T, int64_t N, int dx, const Real* __restrict__ hist,
+                                         const int32_t* __restrict__ anc, int64_t M,
+                                         const int32_t* __restrict__ idx, Real* __restrict__ out,
+                                         int32_t* __restrict__ bad) {
+  for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < M; k += (int64_t)gridDim.x * blockDim.x) {
+    int64_t a = idx ? (int64_t)idx[k] - 1 : k;
+    for (int t = T; t >= 0; --t) {
+      if (a < 0 || a >= N) {  // an index outside 1..N: report it, write nothing more
+        atomicExch(bad, 1);
+        break;
+      }
+      for (int d = 0; d < dx; ++d) out[((size_t)t * dx + d) * M + k] = hist[((size_t)t * dx + d) * N + a];
+      if (t > 0) a = (int64_t)anc[(size_t)(t - 1) * N + a] - 1;
+    }
+  }
+}
+
+void launch_record(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int64_t N) {
+  int blocks = (int)std::min<int64_t>((N + 255) / 256, 8 * (int64_t)ctx->num_sms);
+  if (dbl) pf_record_kernel<double><<<blocks, 256, 0, ctx->stream>>>(jobs_dev);
+  else pf_record_kernel<float><<<blocks, 256, 0, ctx->stream>>>(jobs_dev);
+}
+
 // -------------------------------------------------------- kernel registry
 // Instantiations live in gf_pf_inst_*.cu so they compile in parallel.
 void register_lg_f32_small(std::vector<PfLgKernels>& v, bool guided);
@@ -405,3 +452,74 @@ void pack_params(const LgFactors& f, bool dbl, int dxp, int dyp, std::vector<cha
 }
 
 }  // namespace gf
+
+extern "C" gf_status gf_pf_dense_ancestry(gf_ctx* ctx, int32_t T, int64_t N, int32_t dx, int32_t precision,
+                                          const void* history, const int32_t* ancestors, int64_t M,
+                                          const int32_t* indices, int32_t memspace, void* paths) {
+  using namespace gf;
+  if (!ctx) return GF_ERR_ARG;
+  if (!history || !paths || (T > 0 && !ancestors)) return set_err(ctx, GF_ERR_ARG, "null argument");
+  if (T < 0 || N < 1 || dx < 1) return set_err(ctx, GF_ERR_ARG, "need T >= 0, N >= 1, dx >= 1");
+  if (precision != GF_PREC_F32 && precision != GF_PREC_F64) return set_err(ctx, GF_ERR_ARG, "unknown precision");
+  if (memspace != GF_MEM_HOST && memspace != GF_MEM_DEVICE) return set_err(ctx, GF_ERR_ARG, "bad memspace");
+  if (!indices) M = N;
+  if (M < 1) return set_err(ctx, GF_ERR_ARG, "need M >= 1");
+  cudaSetDevice(ctx->device);
+  cudaStream_t s = ctx->stream;
+  const size_t rs = precision == GF_PREC_F64 ? 8 : 4;
+  const size_t hb = rs * (size_t)(T + 1) * dx * N, ab = sizeof(int32_t) * (size_t)T * N;
+  const size_t ob = rs * (size_t)(T + 1) * dx * M, ib = indices ? sizeof(int32_t) * (size_t)M : 0;
+  std::vector<DevBuf> bufs;
+  struct Cleanup {
+    gf_ctx* c;
+    std::vector<DevBuf>* v;
+    ~Cleanup() {
+      cudaStreamSynchronize(c->stream);
+      for (auto& b : *v) dev_free(c, b.p, b.bytes);
+    }
+  } cleanup{ctx, &bufs};
+  auto get = [&](size_t bytes, void** p) -> gf_status {
+    gf_status st = dev_alloc(ctx, bytes, p);
+    if (!st) bufs.push_back({*p, bytes});
+    return st;
+  };
+  gf_status st;
+  const void* h = history;
+  const int32_t* a = ancestors;
+  const int32_t* ix = indices;
+  void* o = paths;
+  void* pbad;
+  if ((st = get(sizeof(int32_t), &pbad))) return st;
+  GF_CHECK_CUDA(ctx, cudaMemsetAsync(pbad, 0, sizeof(int32_t), s));
+  if (memspace == GF_MEM_HOST) {
+    void* p;
+    if ((st = get(hb, &p))) return st;
+    GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p, history, hb, cudaMemcpyHostToDevice, s));
+    h = p;
+    if (T > 0) {
+      if ((st = get(ab, &p))) return st;
+      GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p, ancestors, ab, cudaMemcpyHostToDevice, s));
+      a = (const int32_t*)p;
+    }
+    if (indices) {
+      if ((st = get(ib, &p))) return st;
+      GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p, indices, ib, cudaMemcpyHostToDevice, s));
+      ix = (const int32_t*)p;
+    }
+    if ((st = get(ob, &o))) return st;
+  }
+  const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>((M + 255) / 256, 8 * (int64_t)ctx->num_sms));
+  if (precision == GF_PREC_F64)
+    pf_dense_ancestry_kernel<double><<<blocks, 256, 0, s>>>(T, N, dx, (const double*)h, a, M, ix, (double*)o,
+                                                            (int32_t*)pbad);
+  else
+    pf_dense_ancestry_kernel<float><<<blocks, 256, 0, s>>>(T, N, dx, (const float*)h, a, M, ix, (float*)o,
+                                                           (int32_t*)pbad);
+  GF_CHECK_CUDA(ctx, cudaGetLastError());
+  if (memspace == GF_MEM_HOST) GF_CHECK_CUDA(ctx, cudaMemcpyAsync(paths, o, ob, cudaMemcpyDeviceToHost, s));
+  int32_t bad = 0;
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(&bad, pbad, sizeof bad, cudaMemcpyDeviceToHost, s));
+  GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+  if (bad) return set_err(ctx, GF_ERR_ARG, "an index or ancestor lies outside 1..N");
+  return GF_OK;
+}

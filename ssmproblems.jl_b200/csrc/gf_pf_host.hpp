@@ -44,6 +44,7 @@ void launch_init_scalars(gf_ctx* ctx, PfJob* jobs_dev, int njobs, const double* 
 void launch_means(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int njobs, int total_tiles,
                   double* mpart, int mdim);
 void launch_finish(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int64_t N);
+void launch_record(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int64_t N);
 void launch_prep(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int T, int dx, int dy, int dxp,
                  int dyp, const double* pp, void* out);
 

@@ -64,6 +64,8 @@ struct PfJob {
   int32_t* mpk;              // [ntiles + 1] merge-path start particle of each fill block
   int32_t* anc;              // [N] 0-based ancestors of the pending resample
   void* eta;                 // auxiliary filter: [N] lookahead log eta of the current particles (else null)
+  void* hist;                // nullable [T+1][dx][N] dense state history
+  double* lwh;               // nullable [T][N] normalised log-weight history
 };
 
 __device__ __forceinline__ int find_job(const PfJob* jobs, int njobs, int block, bool scan) {

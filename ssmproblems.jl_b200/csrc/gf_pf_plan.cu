@@ -38,6 +38,7 @@ struct gf_pf_plan {
   size_t prop_smem = 0;
   cudaGraphExec_t graph = nullptr;
   bool graph_means = false;
+  bool graph_record = false;
   bool use_graph = true;
   // path storage (allocated on the first run that asks for paths)
   PfTree tree;
@@ -232,7 +233,7 @@ static void launch_lookahead(gf_pf_plan* p) {
   p->k.lookahead<<<p->ntiles, PF_THREADS, 0, p->ctx->stream>>>(p->job_dev, 1);
 }
 
-static void enqueue_run(gf_pf_plan* p, bool means) {
+static void enqueue_run(gf_pf_plan* p, bool means, bool record) {
   gf_ctx* ctx = p->ctx;
   cudaStream_t s = ctx->stream;
   launch_prep(ctx, p->dbl, p->job_dev, p->T, p->dx, p->dy, p->k.dxp, p->k.dyp, p->pp, p->ystep);
@@ -242,6 +243,7 @@ static void enqueue_run(gf_pf_plan* p, bool means) {
     ProfScope ps(ctx, KC_PREP);
     p->k.init<<<p->ntiles, PF_THREADS, 0, s>>>(p->job_dev, 1, p->k.off_mu0, p->k.off_L0);
   }
+  if (record) launch_record(ctx, p->dbl, p->job_dev, p->N);
   launch_lookahead(p);
   launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
   for (int t = 1; t <= p->T; ++t) {
@@ -250,6 +252,7 @@ static void enqueue_run(gf_pf_plan* p, bool means) {
       p->prop_fn<<<p->ntiles * p->prop_split, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
     }
     if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);
+    if (record) launch_record(ctx, p->dbl, p->job_dev, p->N);
     if (t < p->T) {
       launch_lookahead(p);
       launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
@@ -354,7 +357,7 @@ static gf_status tree_reserve(gf_pf_plan* p, int64_t need) {
 }
 
 // One run with path storage (eager launches: the pool is sized between chunks).
-static gf_status enqueue_run_paths(gf_pf_plan* p, bool means, void* paths) {
+static gf_status enqueue_run_paths(gf_pf_plan* p, bool means, bool record, void* paths) {
   gf_ctx* ctx = p->ctx;
   cudaStream_t s = ctx->stream;
   gf_status st = tree_prepare(p);
@@ -364,6 +367,7 @@ static gf_status enqueue_run_paths(gf_pf_plan* p, bool means, void* paths) {
   GF_CHECK_CUDA(ctx, cudaMemsetAsync(p->flags, 0, sizeof(unsigned long long) * 2 * p->nstiles, s));
   p->k.init<<<p->ntiles, PF_THREADS, 0, s>>>(p->job_dev, 1, p->k.off_mu0, p->k.off_L0);
   tree_launch_init(ctx, p->dbl, p->job_dev, p->N, p->tree);
+  if (record) launch_record(ctx, p->dbl, p->job_dev, p->N);
   launch_lookahead(p);
   launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
   for (int t = 1; t <= p->T; ++t) {
@@ -375,6 +379,7 @@ static gf_status enqueue_run_paths(gf_pf_plan* p, bool means, void* paths) {
     p->prop_fn<<<p->ntiles * p->prop_split, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
     tree_launch_insert(ctx, p->dbl, p->job_dev, p->N, p->tree, t);
     if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);
+    if (record) launch_record(ctx, p->dbl, p->job_dev, p->N);
     if (t < p->T) {
       launch_lookahead(p);
       launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
@@ -404,28 +409,32 @@ extern "C" gf_status gf_pf_plan_run(gf_pf_plan* p, const double* ys_dev, const v
   J.states_out = out->states;
   J.clamps_out = out->clamps;
   J.means_out = out->means;
+  J.hist = out->history;
+  J.lwh = out->log_weight_history;
   cudaStream_t s = ctx->stream;
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->job_dev, &J, sizeof(PfJob), cudaMemcpyHostToDevice, s));
   const bool means = out->means != nullptr;
-  if (out->paths) return enqueue_run_paths(p, means, out->paths);
+  const bool record = out->history || out->log_weight_history;
+  if (out->paths) return enqueue_run_paths(p, means, record, out->paths);
   if (p->use_graph && !ctx->profiling) {
-    if (!p->graph || p->graph_means != means) {
+    if (!p->graph || p->graph_means != means || p->graph_record != record) {
       if (p->graph) {
         cudaGraphExecDestroy(p->graph);
         p->graph = nullptr;
       }
       cudaGraph_t g;
       GF_CHECK_CUDA(ctx, cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal));
-      enqueue_run(p, means);
+      enqueue_run(p, means, record);
       GF_CHECK_CUDA(ctx, cudaStreamEndCapture(s, &g));
       cudaError_t e = cudaGraphInstantiate(&p->graph, g, 0);
       cudaGraphDestroy(g);
       if (e != cudaSuccess) return cuda_err(ctx, e, "cudaGraphInstantiate");
       p->graph_means = means;
+      p->graph_record = record;
     }
     GF_CHECK_CUDA(ctx, cudaGraphLaunch(p->graph, s));
   } else {
-    enqueue_run(p, means);
+    enqueue_run(p, means, record);
     GF_CHECK_CUDA(ctx, cudaGetLastError());
   }
   return GF_OK;
@@ -523,6 +532,9 @@ extern "C" gf_status gf_pf_run(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_co
   if ((st = mk(out->log_weights, (void**)&d.log_weights, sizeof(double) * (size_t)N))) return st;
   if ((st = mk(out->clamps, (void**)&d.clamps, sizeof(int32_t)))) return st;
   if ((st = mk(out->paths, (void**)&d.paths, rs * (size_t)(T + 1) * m->dx * N))) return st;
+  if ((st = mk(out->history, (void**)&d.history, rs * (size_t)(T + 1) * m->dx * N))) return st;
+  if ((st = mk(out->log_weight_history, (void**)&d.log_weight_history, sizeof(double) * (size_t)T * N)))
+    return st;
   if ((st = gf_pf_plan_run(p, (const double*)d_ys, d_noise, (const double*)d_unif, &d))) return st;
   for (auto& mp : maps)
     GF_CHECK_CUDA(ctx, cudaMemcpyAsync(mp.host, *mp.dev, mp.bytes, cudaMemcpyDeviceToHost, s));

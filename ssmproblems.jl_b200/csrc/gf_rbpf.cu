@@ -423,7 +423,8 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   if (!ctx || !m || !cfg || !out || !ys || !out->ll)
     return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
   if (cfg->precision != GF_PREC_F32) return set_err(ctx, GF_ERR_UNSUPPORTED, "RBPF runs in FP32 only");
-  if (out->paths) return set_err(ctx, GF_ERR_UNSUPPORTED, "path storage is for the linear-Gaussian PF");
+  if (out->paths || out->history || out->log_weight_history)
+    return set_err(ctx, GF_ERR_UNSUPPORTED, "path storage and dense history are for the linear-Gaussian PF");
   if (cfg->lookahead != GF_LOOKAHEAD_NONE)
     return set_err(ctx, GF_ERR_UNSUPPORTED, "the auxiliary filter is built for the linear-Gaussian PF");
   if (cfg->proposal == GF_PROP_OPTIMAL)

@@ -36,7 +36,7 @@ EXPORTED = [
     "gf_rng_normals", "gf_sample_ancestors_noalloc", "gf_sample_ancestors_noalloc_max_n",
     "gf_srv_create", "gf_srv_submit", "gf_srv_poll", "gf_srv_drain", "gf_srv_stats",
     "gf_srv_reset_stats", "gf_srv_last_error", "gf_srv_destroy",
-    "gf_csmc_run", "gf_csmc_max_particles",
+    "gf_csmc_run", "gf_csmc_max_particles", "gf_pf_dense_ancestry",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -66,7 +66,7 @@ class PFConfigC(C.Structure):
 class PFOutC(C.Structure):
     _fields_ = [("ll", _vp), ("ll_steps", _vp), ("ess_steps", _vp), ("resampled", _vp),
                 ("ancestors", _vp), ("means", _vp), ("states", _vp), ("log_weights", _vp),
-                ("clamps", _vp), ("paths", _vp)]
+                ("clamps", _vp), ("paths", _vp), ("history", _vp), ("log_weight_history", _vp)]
 
 
 class CsmcConfigC(C.Structure):
@@ -180,6 +180,7 @@ def load(path: str | None = None):
         "gf_csmc_run": (i32, [ctxp, C.POINTER(LGModelC), C.POINTER(CsmcConfigC), i32, _vp, i32,
                               i32, i32, i32, _vp, _vp, i32, C.POINTER(CsmcOutC)]),
         "gf_csmc_max_particles": (i32, []),
+        "gf_pf_dense_ancestry": (i32, [ctxp, i32, i64, i32, i32, _vp, _vp, i64, _vp, i32, _vp]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

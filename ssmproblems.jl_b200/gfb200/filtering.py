@@ -81,8 +81,79 @@ def _pf_config(algo: ParticleFilter, T: int, seed: int, schedule=None, lookahead
     return cfg, sched, prec
 
 
+class AncestorCallback:
+    """AncestorCallback (callbacks.jl:83-111): pass as filter(..., callback=cb); the
+    device path storage fills cb.tree, whose get_ancestry gives every final
+    particle's trajectory."""
+
+    def __init__(self, tree=None):
+        self.tree = tree
+
+
+class DenseAncestorCallback:
+    """DenseAncestorCallback (callbacks.jl:47-81): pass as filter(..., callback=cb);
+    cb.container is the DenseParticleContainer of the run."""
+
+    def __init__(self, container=None):
+        self.container = container
+
+
+class ParticleTree:
+    """The trajectories kept by the device path storage: paths [T+1, N, dx]."""
+
+    def __init__(self, paths):
+        self.paths = paths
+
+    def __len__(self):
+        return self.paths.shape[1]
+
+
+class DenseParticleContainer:
+    """DenseParticleContainer (containers.jl:296-419): initial_states [N, dx],
+    states [T, N, dx] (times 1..T), weights [T, N] (normalised log-weights after
+    each update), ancestors [T, N] (1-based)."""
+
+    def __init__(self, history, log_weights, ancestors, ctx=None):
+        self._hist = history  # [T+1, dx, N], the library's layout
+        self.weights = log_weights
+        self.ancestors = ancestors
+        self._ctx = ctx
+
+    @property
+    def initial_states(self):
+        return self._hist[0].T
+
+    @property
+    def states(self):
+        return self._hist[1:].transpose(0, 2, 1)
+
+
+def get_ancestry(container, i=None, *, ctx=None):
+    """get_ancestry(container, i) (containers.jl:421-440, 587-631): the trajectory
+    [T+1, dx] of final particle i (1-based), or of every final particle
+    ([N, T+1, dx]) when i is None.  A ParticleTree already holds them all."""
+    if isinstance(container, ParticleTree):
+        paths = container.paths.transpose(1, 0, 2)
+        return paths if i is None else paths[i - 1]
+    if not isinstance(container, DenseParticleContainer):
+        raise TypeError("get_ancestry takes a DenseParticleContainer or a ParticleTree")
+    ctx = _resolve_ctx(ctx if ctx is not None else container._ctx)
+    hist = container._hist
+    T1, dx, N = hist.shape
+    prec = L.GF_PREC_F64 if hist.dtype == np.float64 else L.GF_PREC_F32
+    idx = None if i is None else np.atleast_1d(np.asarray(i, dtype=np.int32))
+    M = N if idx is None else idx.size
+    out = np.empty((T1, dx, M), hist.dtype)
+    anc = np.ascontiguousarray(container.ancestors, dtype=np.int32)
+    L.check(ctx.h, L.load().gf_pf_dense_ancestry(ctx.h, T1 - 1, N, dx, prec, L.ptr(np.ascontiguousarray(hist)),
+                                                 L.ptr(anc), M, L.ptr(idx), L.GF_MEM_HOST, L.ptr(out)))
+    paths = out.transpose(2, 0, 1)  # [M, T+1, dx]
+    return paths if i is None or np.ndim(i) > 0 else paths[0]
+
+
 def filter(model, algo, observations, *, seed: int = 0, noise=None, uniforms=None,
-           ctx=None, want_ancestors=False, want_means=False, schedule=None, want_paths=False):
+           ctx=None, want_ancestors=False, want_means=False, schedule=None, want_paths=False,
+           callback=None):
     """filter([rng,] model, algo, observations) -> (state, ll).
 
     seed     : Philox key of the in-kernel noise and uniforms (the reference's rng)
@@ -90,9 +161,28 @@ def filter(model, algo, observations, *, seed: int = 0, noise=None, uniforms=Non
     uniforms : optional injected resampling uniforms ([T] systematic, else [T, N])
     want_paths: keep the ancestry on the device (AncestorCallback / ParticleTree) and
                 return every final particle's trajectory as state.paths [T+1, N, dx]
+    callback : AncestorCallback() (fills cb.tree) or DenseAncestorCallback() (fills
+               cb.container); particle filters only
     """
     ctx = _resolve_ctx(ctx)
     ys = L.f64(observations)
+    if callback is not None:
+        if not isinstance(algo, (ParticleFilter, AuxiliaryParticleFilter)):
+            raise TypeError("ancestry callbacks are built for the linear-Gaussian particle filters")
+        if isinstance(callback, AncestorCallback):
+            st, ll = filter(model, algo, observations, seed=seed, noise=noise, uniforms=uniforms, ctx=ctx,
+                            want_ancestors=want_ancestors, want_means=want_means, schedule=schedule,
+                            want_paths=True)
+            callback.tree = ParticleTree(st.paths)
+            return st, ll
+        if isinstance(callback, DenseAncestorCallback):
+            pf = algo.pf if isinstance(algo, AuxiliaryParticleFilter) else algo
+            la = algo.weight_strategy.pp.lookahead if isinstance(algo, AuxiliaryParticleFilter) else 0
+            st, ll = _pf(model, pf, ys, seed, noise, uniforms, ctx, True, want_means, schedule,
+                         want_paths, lookahead=la, want_history=True)
+            callback.container = DenseParticleContainer(st._history, st._lw_history, st.ancestors, ctx)
+            return st, ll
+        raise TypeError(f"unsupported callback {type(callback).__name__}")
     if isinstance(algo, (KalmanFilter, SRKalmanFilter)):
         if not isinstance(model, StateSpaceModel):
             raise TypeError("Kalman filters need a linear-Gaussian StateSpaceModel")
@@ -111,7 +201,7 @@ def filter(model, algo, observations, *, seed: int = 0, noise=None, uniforms=Non
 
 
 def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, schedule,
-        want_paths=False, lookahead=0):
+        want_paths=False, lookahead=0, want_history=False):
     if not isinstance(model, StateSpaceModel):
         raise TypeError("particle filter needs a linear-Gaussian StateSpaceModel")
     mc = model._c_struct()
@@ -126,9 +216,11 @@ def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sched
     out["ancestors"] = np.zeros((T, N), np.int32) if want_anc else None
     out["means"] = np.zeros((T, dx)) if want_means else None
     out["paths"] = np.zeros((T + 1, dx, N), rdt) if want_paths else None
+    out["history"] = np.zeros((T + 1, dx, N), rdt) if want_history else None
+    out["log_weight_history"] = np.zeros((T, N)) if want_history else None
     o = L.PFOutC(*[L.ptr(out[k]) for k in ("ll", "ll_steps", "ess_steps", "resampled",
                                            "ancestors", "means", "states", "log_weights",
-                                           "clamps", "paths")])
+                                           "clamps", "paths", "history", "log_weight_history")])
     nz = None if noise is None else np.ascontiguousarray(noise, dtype=rdt)
     un = None if uniforms is None else L.f64(uniforms)
     L.check(ctx.h, L.load().gf_pf_run(ctx.h, C.byref(mc), C.byref(cfg), T, L.ptr(ys),
@@ -138,6 +230,7 @@ def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sched
                                  ancestors=out["ancestors"], means=out["means"],
                                  clamps=int(out["clamps"][0]),
                                  paths=None if out["paths"] is None else out["paths"].transpose(0, 2, 1))
+    state._history, state._lw_history = out["history"], out["log_weight_history"]
     return state, float(out["ll"][0])
 
 

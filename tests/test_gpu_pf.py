@@ -258,3 +258,54 @@ def test_path_storage_matches_dense_ancestry(ctx, kind, threshold, T):
     np.testing.assert_allclose(st.paths, dense, rtol=1e-10, atol=1e-12)
     # the plan reuses (and keeps) its grown pool on a second run
     assert st.paths.shape == (T + 1, N, 2)
+
+
+@pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.MULTINOMIAL])
+@pytest.mark.parametrize("apf", [False, True])
+def test_dense_ancestry_container_matches_oracle(ctx, kind, apf):
+    """DenseAncestorCallback / DenseParticleContainer (callbacks.jl:47-81,
+    containers.jl:296-440): the per-step states and normalised PostUpdate
+    log-weights equal the oracle's (FP64, injected noise), and get_ancestry over
+    the container equals the oracle's dense reconstruction and the device path
+    storage."""
+    rng = np.random.default_rng(60 + kind)
+    m = random_lg(rng, 3, 2)
+    T, N = 7, 900
+    _, ys = simulate(rng, m, T)
+    noise, unif = injected(rng, T, 3, N, kind)
+    bf = G.BF(N, threshold=0.8, resampler=RS[kind], precision="f64")
+    algo = G.APF(bf, G.MeanPredictive()) if apf else bf
+    cb = G.DenseAncestorCallback()
+    st, ll = G.filter(m, algo, ys, noise=noise, uniforms=unif, callback=cb, ctx=ctx)
+    ref = O.pf_run(to_oracle(m), N, ys, resampler=kind, threshold=0.8, noise=noise, uniforms=unif,
+                   want_ancestors=True, want_states=True, lookahead=int(apf))
+    c = cb.container
+    np.testing.assert_array_equal(c.ancestors, ref["ancestors"])
+    np.testing.assert_allclose(c.initial_states, ref["states"][0], rtol=1e-12, atol=1e-14)
+    np.testing.assert_allclose(c.states, ref["states"][1:], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(c.weights, ref["log_weights_all"], atol=1e-9)
+    dense = O.ancestry_paths(ref["ancestors"], ref["states"])  # [T+1, N, dx]
+    paths = G.get_ancestry(c, ctx=ctx)                          # [N, T+1, dx]
+    np.testing.assert_allclose(paths, dense.transpose(1, 0, 2), rtol=1e-10, atol=1e-12)
+    one = G.get_ancestry(c, 5, ctx=ctx)
+    np.testing.assert_array_equal(one, paths[4])
+    tcb = G.AncestorCallback()
+    G.filter(m, algo, ys, noise=noise, uniforms=unif, callback=tcb, ctx=ctx)
+    np.testing.assert_array_equal(G.get_ancestry(tcb.tree), paths)
+
+
+def test_dense_ancestry_walk_with_shifting_ancestors(ctx):
+    """test/algorithms/rbpf.jl:236-277 pattern: with ancestors a_i = mod1(i - 1, N)
+    at every step, the trajectory of final particle N is x0 = initial_states[N - K]
+    and x_t = states[t][N - K + t] (the walk through the container alone)."""
+    K, N, dx = 5, 10, 2
+    rng = np.random.default_rng(0)
+    hist = rng.standard_normal((K + 1, dx, N))
+    anc = np.tile(np.array([((a - 2) % N) + 1 for a in range(1, N + 1)], np.int32), (K, 1))
+    c = G.DenseParticleContainer(hist, np.zeros((K, N)), anc, ctx)
+    traj = G.get_ancestry(c, N, ctx=ctx)
+    np.testing.assert_array_equal(traj[0], c.initial_states[N - K - 1])
+    for t in range(1, K + 1):
+        np.testing.assert_array_equal(traj[t], c.states[t - 1][N - K + t - 1])
+    with pytest.raises(G.GFError):
+        G.get_ancestry(c, N + 1, ctx=ctx)
