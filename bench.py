@@ -7,7 +7,7 @@ ESS < 0.5 N, FP64 normaliser and cumulative weights, in-kernel Philox noise.
 One step = one full filter run (N * T particle-steps).
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
-                    [--workload pf|pf1d|kf|smooth|rbpf|serve|csmc]
+                    [--workload pf|pf1d|kf|smooth|rbpf|serve|csmc|kfgrad]
 
 Under torchrun each rank runs an independent replica (the filters shard by
 filter; no data-path collective).  Rank 0 prints one JSON line.
@@ -747,6 +747,106 @@ def bench_smooth(args, world, rank, local):
     return line
 
 
+def bench_kfgrad(args, world, rank, local):
+    """Gradients of kf_loglikelihood (the ChainRules pullback) for a bank of
+    uneven LGSSMs (Dx 2..16, Dy 1..Dx, T 64..512), FP64: one step = forward
+    filter with checkpoints plus the backward gradient recursion of every
+    model (gf_kf_loglikelihood_grad on device buffers)."""
+    import ctypes as C
+
+    import torch
+    import gfb200 as G
+    from gfb200 import _lib as L
+    from gfb200 import workloads as W
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    ctx = G.Context(local)
+    lib = L.load()
+    B = args.kfgrad_models
+    models, Ts, yss = W.kf_bank(B, seed=11 + rank, dx_range=(2, 16), T_range=(64, 512))
+    mcs = (L.LGModelC * B)(*[m._c_struct() for m in models])
+    Ta = np.array(Ts, np.int32)
+    ys_h = np.concatenate([np.asarray(y, np.float64).ravel() for y in yss])
+    yd = torch.tensor(ys_h, device=dev)
+    dxs = np.array([m.dx for m in models])
+    dys = np.array([m.dy for m in models])
+    sizes = [B, dxs.sum(), (dxs * dxs).sum(), (dxs * dxs).sum(), dxs.sum(), (dxs * dxs).sum(),
+             (dys * dxs).sum(), dys.sum(), (dys * dys).sum()]
+    outs = [torch.empty(int(n), dtype=torch.float64, device=dev) for n in sizes]
+    status = torch.zeros(B, dtype=torch.int32, device=dev)
+    o = L.KFGradOutC(*[L.ptr(t) for t in outs], L.ptr(status))
+
+    def run():
+        L.check(ctx.h, lib.gf_kf_loglikelihood_grad(ctx.h, mcs, B, Ta.ctypes.data_as(C.POINTER(C.c_int32)),
+                                                    L.ptr(yd), 0.0, 0, L.GF_MEM_DEVICE, C.byref(o)))
+
+    for _ in range(args.warmup):
+        run()
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    _barrier(world)
+    with ClockSampler(local) as clk:
+        e0.record(ext)
+        for _ in range(args.steps):
+            run()
+        e1.record(ext)
+        e1.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1), world, dev)
+    assert int(status.abs().sum().item()) == 0
+    n_steps = int(np.sum(Ts))
+    value = n_steps * args.steps * world / (ms / 1e3)
+    # end to end through the public API with host buffers
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        G.kf_loglikelihood_grad_batch(models, yss, ctx=ctx)
+    e2e_s = time.perf_counter() - t0
+    Tarr = np.array(Ts, dtype=np.float64)
+    # checkpoint write + read (8 (dx + dx^2) each) and y read (8 dy) per step
+    bytes_run = float(np.sum(Tarr * (16 * (dxs + dxs * dxs) + 8 * dys)))
+    run_s = ms / 1e3 / args.steps
+    peak, peak_kind = _peaks()
+    line = {
+        "metric": "KF gradient steps/s", "value": value, "unit": "KF-steps/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic",
+        "config": {"workload": f"kf_loglikelihood pullback over {B} uneven LGSSMs, Dx~U{{2..16}}, "
+                               "Dy~U{1..Dx}, T~U{64..512}: FP64 forward with checkpoints + backward "
+                               "gradient recursion, gradients of mu0, Sigma0, A, b, Q, H, c, R",
+                   "models": B, "kf_steps": n_steps, "l2": "no flush (latency-bound)"},
+        "roofline": {"bound": "hbm", "achieved": bytes_run / run_s / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": bytes_run / run_s / 1e9 / peak, "traffic": None, "peak_source": peak_kind,
+                     "limiter": "serial FP64 per-step chain of each model (one CTA per model)"},
+        "e2e": {"value": n_steps * args.steps / e2e_s, "unit": "KF-steps/s",
+                "h2d_bytes_per_step": int(ys_h.nbytes), "d2h_bytes_per_step": int(sum(n * 8 for n in sizes))},
+        "gpu_launches": args.steps,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline_kfgrad(models, yss, seconds=args.cpu_seconds)
+    ctx.close()
+    return line
+
+
+def cpu_baseline_kfgrad(models, yss, seconds=12.0):
+    """The FP64 oracle's pullback (numpy, one core) over the bank's models in
+    order until `seconds` have passed."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    steps, done = 0, 0
+    t0 = time.perf_counter()
+    for m, ys in zip(models, yss):
+        p, d, o = m.prior, m.dyn, m.obs
+        O.kf_loglikelihood_grad(O.LGModel(p.mu0, p.Sigma0, d.A, d.b, d.Q, o.H, o.c, o.R), ys)
+        steps += len(ys)
+        done += 1
+        if time.perf_counter() - t0 > seconds:
+            break
+    dt = time.perf_counter() - t0
+    return {"value": steps / dt, "unit": "KF-steps/s", "cores": 1, "kind": "port",
+            "sample": f"FP64 numpy oracle pullback, the first {done} models of the bank ({steps} KF steps)"}
+
+
 def cpu_baseline_csmc(model, ys, N, seconds=12.0, threads=None):
     """The FP64 oracle's CSMC-AS on this host: same model and N, chains spread
     over all host threads, a bounded number of sweeps."""
@@ -894,7 +994,8 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="pf", choices=["pf", "pf1d", "kf", "smooth", "rbpf", "serve", "csmc"])
+    ap.add_argument("--workload", default="pf", choices=["pf", "pf1d", "kf", "smooth", "rbpf", "serve", "csmc", "kfgrad"])
+    ap.add_argument("--kfgrad-models", type=int, default=8192)
     ap.add_argument("--csmc-chains", type=int, default=592)
     ap.add_argument("--csmc-sweeps", type=int, default=20)
     ap.add_argument("--smooth-filters", type=int, default=16384)
@@ -931,6 +1032,8 @@ def main():
         line = bench_pf1d(args, world, rank, local)
     elif args.workload == "csmc":
         line = bench_csmc(args, world, rank, local)
+    elif args.workload == "kfgrad":
+        line = bench_kfgrad(args, world, rank, local)
     else:
         line = bench_pf(args, world, rank, local)
     if rank == 0 and line is not None:

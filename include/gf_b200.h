@@ -170,6 +170,28 @@ gf_status gf_kf_batch(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int3
                       const int32_t* T, const double* ys, double jitter, int32_t use_jitter,
                       int32_t memspace, gf_kf_out* out);
 
+/* Gradients of kf_loglikelihood (integrations/logdensity.jl:136-161) for B
+ * homogeneous models: the ChainRules pullback (integrations/kalman_rrule.jl:
+ * 22-107, step rules kalman_gradient.jl:89-263) with Delta ll = 1, summed over
+ * time for A, b, Q, H, c, R.  Matrices column-major, packed model after model.
+ * Every pointer but ll is nullable. */
+typedef struct {
+  double* ll;       /* [B] */
+  double* d_mu0;    /* [sum dx] */
+  double* d_Sigma0; /* [sum dx*dx] */
+  double* d_A;      /* [sum dx*dx] */
+  double* d_b;      /* [sum dx] */
+  double* d_Q;      /* [sum dx*dx] */
+  double* d_H;      /* [sum dy*dx] */
+  double* d_c;      /* [sum dy] */
+  double* d_R;      /* [sum dy*dy] */
+  int32_t* status;  /* [B] per-model gf_status */
+} gf_kf_grad_out;
+/* FP64, one CTA per model, dx, dy <= 16; jitter as in gf_kf_batch. */
+gf_status gf_kf_loglikelihood_grad(gf_ctx* ctx, const gf_lg_model* models, int32_t B, const int32_t* T,
+                                   const double* ys, double jitter, int32_t use_jitter, int32_t memspace,
+                                   gf_kf_grad_out* out);
+
 /* smooth(model, KalmanSmoother(), ys) for B models (kalman.jl:206-234): the
  * forward Kalman filter (no jitter), then the Rauch-Tung-Striebel pass of
  * backward_smooth (kalman.jl:89-126) from T-1 down to 1.  out->means and

@@ -484,3 +484,64 @@ def random_orthogonal(rng, d):
     Z = rng.standard_normal((d, d))
     Qm, Rm = np.linalg.qr(Z)
     return Qm * np.sign(np.diag(Rm))
+
+
+def kf_loglikelihood_grad(m: LGModel, ys, jitter=None):
+    """kf_loglikelihood and its pullback for a homogeneous model (kalman_rrule.jl:
+    22-107 with the step rules of kalman_gradient.jl:12-263), FP64 numpy.
+
+    Forward: kalman_predict (kalman.jl:42-49) and _kalman_update_cached (Joseph
+    form).  Backward, per step t = T..1, in the NLL convention of the reference:
+    gradient_c/H/R (:172-263), backward_gradient_update (:97-120, eqs 8-9),
+    gradient_b/A/Q (:150-205), backward_gradient_predict (:138-143, eqs 10-11).
+    Returns (ll, grads) with grads the gradients of ll (the pullback with
+    Delta ll = 1: minus the NLL gradients), summed over t for A, b, Q, H, c, R."""
+    ys = _f64(ys).reshape(-1, m.dy)
+    T = ys.shape[0]
+    A, b, Q, H, c, R = (np.asarray(v, np.float64) for v in (m.A, m.b, m.Q, m.H, m.c, m.R))
+    mu, S0 = np.asarray(m.mu0, np.float64).copy(), np.asarray(m.Sigma0, np.float64).copy()
+    dx, dy = A.shape[0], H.shape[0]
+    prev, caches, ll = [], [], 0.0
+    Sig = S0
+    for t in range(T):
+        prev.append((mu, Sig))
+        mp = A @ mu + b
+        Sp = A @ Sig @ A.T + Q
+        z = ys[t] - H @ mp - c
+        S = H @ Sp @ H.T + R
+        S = (S + S.T) / 2
+        K = Sp @ H.T @ np.linalg.inv(S)
+        IKH = np.eye(dx) - K @ H
+        Sf = IKH @ Sp @ IKH.T + K @ R @ K.T
+        if jitter is not None:
+            Sf = Sf + jitter * np.eye(dx)
+        mf = mp + K @ z
+        sign, logdet = np.linalg.slogdet(S)
+        ll += -0.5 * (dy * np.log(2 * np.pi) + logdet + z @ np.linalg.solve(S, z))
+        caches.append(dict(mp=mp, Sp=Sp, mf=mf, S=S, K=K, z=z, IKH=IKH))
+        mu, Sig = mf, Sf
+    dmu, dS = np.zeros(dx), np.zeros((dx, dx))
+    g = {k: np.zeros_like(v) for k, v in (("A", A), ("b", b), ("Q", Q), ("H", H), ("c", c), ("R", R))}
+    Rinv = np.linalg.inv(R)
+    for t in range(T - 1, -1, -1):
+        C_ = caches[t]
+        mp, Sp, mf, S, K, z, IKH = (C_[k] for k in ("mp", "Sp", "mf", "S", "K", "z", "IKH"))
+        Si = np.linalg.inv(S)
+        Siz = np.linalg.solve(S, z)
+        g["c"] += -Siz - K.T @ dmu
+        Pf = IKH @ Sp
+        g["H"] += (Si @ H @ Sp - np.outer(Siz, mp) - np.outer(Siz, Siz) @ H @ Sp
+                   + np.outer(Siz, dmu) @ Pf - K.T @ np.outer(dmu, mf) - 2 * K.T @ dS @ Pf)
+        g["R"] += K.T @ dS @ K - 0.5 * (K.T @ np.outer(dmu, Siz) + np.outer(Siz, dmu) @ K) \
+            + 0.5 * (Si - np.outer(Siz, Siz))
+        dmp = IKH.T @ dmu - H.T @ Siz
+        Riz = Rinv @ z
+        cross = 0.5 * (np.outer(dmu, Riz @ H) + np.outer(H.T @ Riz, dmu))
+        dSp = IKH.T @ (dS + cross) @ IKH + 0.5 * (H.T @ Si @ H - H.T @ np.outer(Siz, Siz) @ H)
+        mu_prev, S_prev = prev[t]
+        g["b"] += dmp
+        g["A"] += np.outer(dmp, mu_prev) + 2 * dSp @ A @ S_prev
+        g["Q"] += dSp
+        dmu, dS = A.T @ dmp, A.T @ dSp @ A
+    g["mu0"], g["Sigma0"] = dmu, dS
+    return ll, {k: -v for k, v in g.items()}

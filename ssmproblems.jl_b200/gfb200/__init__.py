@@ -13,7 +13,7 @@ from .algorithms import (APF, BF, KF, KS, PF, RBPF, SRKF, AlternatingResampler, 
                          Multinomial, OptimalProposal, OverdispersedProposal, ParticleFilter,
                          RepresentativeStateLookAhead, SRKalmanFilter, Stratified, Systematic)
 from .filtering import (AncestorCallback, DenseAncestorCallback, DenseParticleContainer,  # noqa: F401
-                        ParticleTree, get_ancestry)
+                        ParticleTree, get_ancestry, kf_loglikelihood_grad, kf_loglikelihood_grad_batch)
 from .filtering import (MvNormal, ParticleDistribution, ancestors_to_offspring, filter,  # noqa: F401
                         filter_batch, offspring_to_ancestors, rng_normals, sample_ancestors,
                         smooth, smooth_batch)

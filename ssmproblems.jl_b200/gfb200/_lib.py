@@ -36,7 +36,7 @@ EXPORTED = [
     "gf_rng_normals", "gf_sample_ancestors_noalloc", "gf_sample_ancestors_noalloc_max_n",
     "gf_srv_create", "gf_srv_submit", "gf_srv_poll", "gf_srv_drain", "gf_srv_stats",
     "gf_srv_reset_stats", "gf_srv_last_error", "gf_srv_destroy",
-    "gf_csmc_run", "gf_csmc_max_particles", "gf_pf_dense_ancestry",
+    "gf_csmc_run", "gf_csmc_max_particles", "gf_pf_dense_ancestry", "gf_kf_loglikelihood_grad",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -76,6 +76,11 @@ class CsmcConfigC(C.Structure):
 
 class CsmcOutC(C.Structure):
     _fields_ = [("trajectories", _vp), ("ll", _vp), ("ref", _vp), ("status", _vp)]
+
+
+class KFGradOutC(C.Structure):
+    _fields_ = [(n, _vp) for n in ("ll", "d_mu0", "d_Sigma0", "d_A", "d_b", "d_Q", "d_H", "d_c", "d_R",
+                                   "status")]
 
 
 class KFOutC(C.Structure):
@@ -181,6 +186,8 @@ def load(path: str | None = None):
                               i32, i32, i32, _vp, _vp, i32, C.POINTER(CsmcOutC)]),
         "gf_csmc_max_particles": (i32, []),
         "gf_pf_dense_ancestry": (i32, [ctxp, i32, i64, i32, i32, _vp, _vp, i64, _vp, i32, _vp]),
+        "gf_kf_loglikelihood_grad": (i32, [ctxp, C.POINTER(LGModelC), i32, C.POINTER(i32), _vp, dbl, i32,
+                                           i32, C.POINTER(KFGradOutC)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

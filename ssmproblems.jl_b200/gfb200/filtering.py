@@ -402,3 +402,49 @@ def rng_normals(seed, t, dx, n, precision="f32", *, ctx=None):
     L.check(ctx.h, L.load().gf_rng_normals(ctx.h, int(seed), int(t), int(dx), int(n), prec,
                                            L.ptr(out)))
     return out
+
+
+# --------------------------------------------------- log-likelihood gradients
+GRAD_KEYS = ("mu0", "Sigma0", "A", "b", "Q", "H", "c", "R")
+
+
+def kf_loglikelihood_grad_batch(models, observations, *, jitter=None, ctx=None):
+    """kf_loglikelihood and its pullback (integrations/logdensity.jl:136-161,
+    integrations/kalman_rrule.jl:22-107) for many homogeneous models at once.
+    Returns a list of (ll, grads): grads maps mu0, Sigma0, A, b, Q, H, c, R to
+    the gradient of ll (summed over time for the dynamics and observation
+    parameters)."""
+    ctx = _resolve_ctx(ctx)
+    B = len(models)
+    if B != len(observations):
+        raise ValueError("one observation sequence per model")
+    mcs = (L.LGModelC * B)(*[m._c_struct() for m in models])
+    Ts = np.array([np.asarray(y).reshape(-1, m.dy).shape[0] for m, y in zip(models, observations)], np.int32)
+    ys = L.f64(np.concatenate([np.asarray(y, np.float64).ravel() for y in observations]))
+    dxs = np.array([m.dx for m in models])
+    dys = np.array([m.dy for m in models])
+    sizes = dict(mu0=dxs, Sigma0=dxs * dxs, A=dxs * dxs, b=dxs, Q=dxs * dxs, H=dys * dxs, c=dys, R=dys * dys)
+    bufs = {k: np.zeros(int(v.sum())) for k, v in sizes.items()}
+    ll = np.zeros(B)
+    status = np.zeros(B, np.int32)
+    out = L.KFGradOutC(L.ptr(ll), *[L.ptr(bufs[k]) for k in GRAD_KEYS], L.ptr(status))
+    L.check(ctx.h, L.load().gf_kf_loglikelihood_grad(
+        ctx.h, mcs, B, Ts.ctypes.data_as(C.POINTER(C.c_int32)), L.ptr(ys),
+        float(jitter or 0.0), int(jitter is not None), L.GF_MEM_HOST, C.byref(out)))
+    res = []
+    off = {k: 0 for k in GRAD_KEYS}
+    for f, m in enumerate(models):
+        g = {}
+        shapes = dict(mu0=(m.dx,), Sigma0=(m.dx, m.dx), A=(m.dx, m.dx), b=(m.dx,), Q=(m.dx, m.dx),
+                      H=(m.dy, m.dx), c=(m.dy,), R=(m.dy, m.dy))
+        for k in GRAD_KEYS:
+            n = int(np.prod(shapes[k]))
+            g[k] = bufs[k][off[k]:off[k] + n].reshape(shapes[k][::-1]).T  # column-major
+            off[k] += n
+        res.append((float(ll[f]), g))
+    return res
+
+
+def kf_loglikelihood_grad(model, observations, *, jitter=None, ctx=None):
+    """(ll, grads) of kf_loglikelihood for one homogeneous model."""
+    return kf_loglikelihood_grad_batch([model], [observations], jitter=jitter, ctx=ctx)[0]

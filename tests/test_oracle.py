@@ -211,3 +211,46 @@ def test_apf_oracle_converges_to_kf():
     r = O.pf_run(m, 200_000, ys, threshold=1.0, seed=2, lookahead=1, threads=4)
     assert r["resampled"].all()
     assert abs(r["ll"] - kll) < 3e-3
+
+
+@pytest.mark.parametrize("seed,D,T", [(1234, 2, 3), (7, 3, 6)])
+def test_kf_gradient_oracle_matches_finite_differences(seed, D, T):
+    """test/components/kalman_gradient.jl: the pullback of kf_loglikelihood equals
+    central differences of the Kalman log-likelihood (5-point stencil; Q, R and
+    Sigma0 perturbed symmetrically, as make_nll_func's make_pd does)."""
+    rng = np.random.default_rng(seed)
+    m = O.create_linear_gaussian_model(rng, D, D)
+    _, ys = O.sample(rng, m, T)
+    ll, g = O.kf_loglikelihood_grad(m, ys)
+    assert abs(ll - O.kf_filter(m, ys)[0]) <= 1e-12 * abs(ll)
+
+    def kfll(p):
+        A, b, Q, H, c, R, mu, S = (np.asarray(p[k], float) for k in ("A", "b", "Q", "H", "c", "R", "mu0", "Sigma0"))
+        tot = 0.0
+        for y in ys:
+            mp, Sp = A @ mu + b, A @ S @ A.T + Q
+            z, Sy = y - H @ mp - c, H @ Sp @ H.T + R
+            K = Sp @ H.T @ np.linalg.inv(Sy)
+            IKH = np.eye(len(mu)) - K @ H
+            S, mu = IKH @ Sp @ IKH.T + K @ R @ K.T, mp + K @ z
+            tot += -0.5 * (len(y) * np.log(2 * np.pi) + np.linalg.slogdet(Sy)[1] + z @ np.linalg.solve(Sy, z))
+        return tot
+
+    P = {n: np.array(getattr(m, n), float) for n in ("mu0", "Sigma0", "A", "b", "Q", "H", "c", "R")}
+    h = 1e-5
+    for name, base in P.items():
+        fd = np.zeros(base.size)
+        for k in range(base.size):
+            vals = []
+            for s in (-2, -1, 1, 2):
+                q = dict(P)
+                p = base.copy().ravel()
+                p[k] += s * h
+                p = p.reshape(base.shape)
+                if name in ("Sigma0", "Q", "R"):
+                    p = (p + p.T) / 2
+                q[name] = p
+                vals.append(kfll(q))
+            fd[k] = (vals[0] - 8 * vals[1] + 8 * vals[2] - vals[3]) / (12 * h)
+        fd = fd.reshape(base.shape)
+        np.testing.assert_allclose(g[name], fd, rtol=0, atol=1e-6 * (np.abs(fd).max() + 1e-12), err_msg=name)
