@@ -25,7 +25,7 @@ namespace {
 
 constexpr int KG_MAXD = 16;
 constexpr int LD = KG_MAXD;  // column stride of every shared matrix
-constexpr int KG_THREADS = 128;
+constexpr int KG_THREADS = 256;
 constexpr int KG_MATS = 26;  // shared matrices of LD x LD doubles
 
 struct KgDesc {
@@ -88,31 +88,35 @@ __device__ void symmetrize(double* M, int n) {
 }
 
 // Cholesky of S (n x n) into L, S^{-1} into Si and log det S; false if S is
-// not positive definite.
+// not positive definite.  Column by column: one thread takes the pivot, the
+// block fills the column below it.
 __device__ bool chol_inv(const double* S, double* L, double* Si, int n, double* logdet, int* s_ok) {
   if (threadIdx.x == 0) {
-    int ok = 1;
-    double ld = 0.0;
-    for (int j = 0; j < n && ok; ++j) {
-      double d = S[j + j * LD];
-      for (int p = 0; p < j; ++p) d -= L[j + p * LD] * L[j + p * LD];
-      if (!(d > 0.0)) {
-        ok = 0;
-        break;
-      }
-      const double ljj = sqrt(d);
-      L[j + j * LD] = ljj;
-      ld += 2.0 * log(ljj);
-      for (int i = j + 1; i < n; ++i) {
-        double s = S[i + j * LD];
-        for (int p = 0; p < j; ++p) s -= L[i + p * LD] * L[j + p * LD];
-        L[i + j * LD] = s / ljj;
-      }
-    }
-    *s_ok = ok;
-    *logdet = ld;
+    *s_ok = 1;
+    *logdet = 0.0;
   }
   __syncthreads();
+  for (int j = 0; j < n; ++j) {
+    if (threadIdx.x == 0) {
+      double d = S[j + j * LD];
+      for (int p = 0; p < j; ++p) d -= L[j + p * LD] * L[j + p * LD];
+      if (d > 0.0) {
+        L[j + j * LD] = sqrt(d);
+        *logdet += log(d);
+      } else {
+        *s_ok = 0;
+        L[j + j * LD] = 1.0;  // keeps the column fill finite; the result is discarded
+      }
+    }
+    __syncthreads();
+    const double ljj = L[j + j * LD];
+    for (int i = j + 1 + threadIdx.x; i < n; i += blockDim.x) {
+      double s = S[i + j * LD];
+      for (int p = 0; p < j; ++p) s -= L[i + p * LD] * L[j + p * LD];
+      L[i + j * LD] = s / ljj;
+    }
+    __syncthreads();
+  }
   if (!*s_ok) return false;
   for (int j = threadIdx.x; j < n; j += blockDim.x) {  // column j of S^{-1}
     double w[KG_MAXD];
