@@ -192,6 +192,28 @@ gf_status gf_kf_loglikelihood_grad(gf_ctx* ctx, const gf_lg_model* models, int32
                                    const double* ys, double jitter, int32_t use_jitter, int32_t memspace,
                                    gf_kf_grad_out* out);
 
+/* BackwardInformationPredictor(; initial_jitter, jitter) (kalman.jl:236-334) for
+ * B homogeneous models: every backward predictive likelihood in information
+ * form exp(lam'x - x'Om x / 2), packed model after model, row t = time t+1:
+ * *_upd = p(y_{t:T} | x_t) (backward_initialise at T, then backward_update),
+ * *_pred = p(y_{t+1:T} | x_t) (backward_predict; zero at T).  mu_smooth /
+ * Sigma_smooth: two_filter_smooth (kalman.jl:336-370) of the forward filter
+ * with *_pred at every t, i.e. p(x_t | y_1:T).  Every pointer is nullable;
+ * FP64, one CTA per model, dx, dy <= 16. */
+typedef struct {
+  double* lam_pred;     /* [sum T*dx] */
+  double* Om_pred;      /* [sum T*dx*dx] column-major */
+  double* lam_upd;      /* [sum T*dx] */
+  double* Om_upd;       /* [sum T*dx*dx] */
+  double* mu_smooth;    /* [sum T*dx] */
+  double* Sigma_smooth; /* [sum T*dx*dx] */
+  int32_t* status;      /* [B] */
+} gf_kf_backward_out;
+gf_status gf_kf_backward_information(gf_ctx* ctx, const gf_lg_model* models, int32_t B, const int32_t* T,
+                                     const double* ys, double initial_jitter, int32_t use_initial_jitter,
+                                     double jitter, int32_t use_jitter, int32_t memspace,
+                                     gf_kf_backward_out* out);
+
 /* smooth(model, KalmanSmoother(), ys) for B models (kalman.jl:206-234): the
  * forward Kalman filter (no jitter), then the Rauch-Tung-Striebel pass of
  * backward_smooth (kalman.jl:89-126) from T-1 down to 1.  out->means and

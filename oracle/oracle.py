@@ -545,3 +545,62 @@ def kf_loglikelihood_grad(m: LGModel, ys, jitter=None):
         dmu, dS = A.T @ dmp, A.T @ dSp @ A
     g["mu0"], g["Sigma0"] = dmu, dS
     return ll, {k: -v for k, v in g.items()}
+
+
+def backward_information(m: LGModel, ys, initial_jitter=None, jitter=None):
+    """BackwardInformationPredictor (kalman.jl:236-334), FP64 numpy: the backward
+    predictive likelihoods in information form, exp(lam'x - x'Om x / 2).
+    Returns (lam_pred [T, dx], Om_pred [T, dx, dx], lam_upd, Om_upd): row t
+    (0-based, time t+1) of *_pred is p(y_{t+2:T} | x_{t+1}) after backward_predict
+    (zero at the last time), of *_upd is p(y_{t+1:T} | x_{t+1}) after
+    backward_initialise / backward_update."""
+    ys = _f64(ys).reshape(-1, m.dy)
+    T = ys.shape[0]
+    A, b, Q, H, c, R = (np.asarray(v, np.float64) for v in (m.A, m.b, m.Q, m.H, m.c, m.R))
+    dx = A.shape[0]
+    Ri = np.linalg.inv(R)
+    F = np.linalg.cholesky(Q)
+    lp, Op = np.zeros((T, dx)), np.zeros((T, dx, dx))
+    lu, Ou = np.zeros((T, dx)), np.zeros((T, dx, dx))
+
+    def sym(M):  # PDMat(Symmetric(M)): the upper triangle mirrored
+        return np.triu(M) + np.triu(M, 1).T
+
+    lam = H.T @ Ri @ (ys[T - 1] - c)
+    Om = H.T @ Ri @ H
+    if initial_jitter is not None:
+        Om = Om + initial_jitter * np.eye(dx)
+    Om = sym(Om)
+    lu[T - 1], Ou[T - 1] = lam, Om
+    for t in range(T - 2, -1, -1):
+        mvec = lam - Om @ b
+        Lam = F.T @ Om @ F + np.eye(dx)
+        FLF = F @ np.linalg.solve(Lam, F.T)
+        Im = np.eye(dx) - Om @ FLF
+        Om_h = A.T @ Im @ Om @ A
+        lam_h = A.T @ Im @ mvec
+        if jitter is not None:
+            Om_h = Om_h + jitter * np.eye(dx)
+        Om_h = sym(Om_h)
+        lp[t], Op[t] = lam_h, Om_h
+        lam = lam_h + H.T @ Ri @ (ys[t] - c)
+        Om = sym(Om_h + H.T @ Ri @ H)
+        lu[t], Ou[t] = lam, Om
+    return lp, Op, lu, Ou
+
+
+def two_filter_smooth(m: LGModel, ys, initial_jitter=None, jitter=None):
+    """two_filter_smooth (kalman.jl:336-370) at every time: the forward filtered
+    N(mu_t, Sigma_t) (the KF of kf_filter) combined with p(y_{t+1:T} | x_t) from
+    backward_information.  Returns (mus [T, dx], Sigmas [T, dx, dx])."""
+    _, _, mus_f, Sf = kf_filter(m, ys)
+    lp, Op, _, _ = backward_information(m, ys, initial_jitter, jitter)
+    T, dx = mus_f.shape
+    mus, Ss = np.zeros((T, dx)), np.zeros((T, dx, dx))
+    for t in range(T):
+        Si = np.linalg.inv(Sf[t])
+        Om_s = Si + Op[t]
+        S_s = np.linalg.inv(Om_s)
+        mus[t] = S_s @ (Si @ mus_f[t] + lp[t])
+        Ss[t] = S_s
+    return mus, Ss

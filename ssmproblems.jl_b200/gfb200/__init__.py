@@ -13,7 +13,8 @@ from .algorithms import (APF, BF, KF, KS, PF, RBPF, SRKF, AlternatingResampler, 
                          Multinomial, OptimalProposal, OverdispersedProposal, ParticleFilter,
                          RepresentativeStateLookAhead, SRKalmanFilter, Stratified, Systematic)
 from .filtering import (AncestorCallback, DenseAncestorCallback, DenseParticleContainer,  # noqa: F401
-                        ParticleTree, get_ancestry, kf_loglikelihood_grad, kf_loglikelihood_grad_batch)
+                        ParticleTree, get_ancestry, kf_loglikelihood_grad, kf_loglikelihood_grad_batch,
+                        InformationLikelihood, backward_information_batch, two_filter_smooth_all)
 from .filtering import (MvNormal, ParticleDistribution, ancestors_to_offspring, filter,  # noqa: F401
                         filter_batch, offspring_to_ancestors, rng_normals, sample_ancestors,
                         smooth, smooth_batch)

@@ -37,6 +37,7 @@ EXPORTED = [
     "gf_srv_create", "gf_srv_submit", "gf_srv_poll", "gf_srv_drain", "gf_srv_stats",
     "gf_srv_reset_stats", "gf_srv_last_error", "gf_srv_destroy",
     "gf_csmc_run", "gf_csmc_max_particles", "gf_pf_dense_ancestry", "gf_kf_loglikelihood_grad",
+    "gf_kf_backward_information",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -80,6 +81,11 @@ class CsmcOutC(C.Structure):
 
 class KFGradOutC(C.Structure):
     _fields_ = [(n, _vp) for n in ("ll", "d_mu0", "d_Sigma0", "d_A", "d_b", "d_Q", "d_H", "d_c", "d_R",
+                                   "status")]
+
+
+class KFBackOutC(C.Structure):
+    _fields_ = [(n, _vp) for n in ("lam_pred", "Om_pred", "lam_upd", "Om_upd", "mu_smooth", "Sigma_smooth",
                                    "status")]
 
 
@@ -188,6 +194,8 @@ def load(path: str | None = None):
         "gf_pf_dense_ancestry": (i32, [ctxp, i32, i64, i32, i32, _vp, _vp, i64, _vp, i32, _vp]),
         "gf_kf_loglikelihood_grad": (i32, [ctxp, C.POINTER(LGModelC), i32, C.POINTER(i32), _vp, dbl, i32,
                                            i32, C.POINTER(KFGradOutC)]),
+        "gf_kf_backward_information": (i32, [ctxp, C.POINTER(LGModelC), i32, C.POINTER(i32), _vp, dbl, i32,
+                                             dbl, i32, i32, C.POINTER(KFBackOutC)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

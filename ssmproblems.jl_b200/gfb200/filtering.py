@@ -448,3 +448,62 @@ def kf_loglikelihood_grad_batch(models, observations, *, jitter=None, ctx=None):
 def kf_loglikelihood_grad(model, observations, *, jitter=None, ctx=None):
     """(ll, grads) of kf_loglikelihood for one homogeneous model."""
     return kf_loglikelihood_grad_batch([model], [observations], jitter=jitter, ctx=ctx)[0]
+
+
+# ------------------------------------------------- backward information filter
+class InformationLikelihood:
+    """InformationLikelihood (containers.jl): exp(lam'x - x'Om x / 2) up to a constant."""
+
+    def __init__(self, lam, Om):
+        self.lam, self.Om = lam, Om
+
+    def natural_params(self):
+        return self.lam, self.Om
+
+
+def backward_information_batch(models, observations, *, initial_jitter=None, jitter=None, smooth=True,
+                               ctx=None):
+    """BackwardInformationPredictor(; initial_jitter, jitter) (kalman.jl:236-334) run
+    backward over every model, and with smooth=True two_filter_smooth (kalman.jl:
+    336-370) at every time.  Returns one dict per model: lam_pred [T, dx], Om_pred
+    [T, dx, dx] (p(y_{t+1:T} | x_t)), lam_upd, Om_upd (p(y_{t:T} | x_t)), and
+    mu_smooth [T, dx], Sigma_smooth [T, dx, dx] (p(x_t | y_1:T))."""
+    ctx = _resolve_ctx(ctx)
+    B = len(models)
+    mcs = (L.LGModelC * B)(*[m._c_struct() for m in models])
+    Ts = np.array([np.asarray(y).reshape(-1, m.dy).shape[0] for m, y in zip(models, observations)], np.int32)
+    ys = L.f64(np.concatenate([np.asarray(y, np.float64).ravel() for y in observations]))
+    dxs = np.array([m.dx for m in models])
+    nv, nm = int(np.sum(Ts * dxs)), int(np.sum(Ts * dxs * dxs))
+    names = ("lam_pred", "Om_pred", "lam_upd", "Om_upd", "mu_smooth", "Sigma_smooth")
+    bufs = {k: np.zeros(nm if k.startswith(("Om", "Sigma")) else nv) for k in names}
+    if not smooth:
+        bufs["mu_smooth"] = bufs["Sigma_smooth"] = None
+    status = np.zeros(B, np.int32)
+    out = L.KFBackOutC(*[L.ptr(bufs[k]) for k in names], L.ptr(status))
+    L.check(ctx.h, L.load().gf_kf_backward_information(
+        ctx.h, mcs, B, Ts.ctypes.data_as(C.POINTER(C.c_int32)), L.ptr(ys),
+        float(initial_jitter or 0.0), int(initial_jitter is not None), float(jitter or 0.0),
+        int(jitter is not None), L.GF_MEM_HOST, C.byref(out)))
+    res, ov, om = [], 0, 0
+    for f, m in enumerate(models):
+        T, d = int(Ts[f]), m.dx
+        r = {}
+        for k in names:
+            if bufs[k] is None:
+                continue
+            if k.startswith(("Om", "Sigma")):
+                r[k] = bufs[k][om:om + T * d * d].reshape(T, d, d).transpose(0, 2, 1)  # column-major
+            else:
+                r[k] = bufs[k][ov:ov + T * d].reshape(T, d)
+        ov += T * d
+        om += T * d * d
+        res.append(r)
+    return res
+
+
+def two_filter_smooth_all(model, observations, *, initial_jitter=None, jitter=None, ctx=None):
+    """p(x_t | y_1:T) at every t by the two-filter smoother: (means [T, dx], covs [T, dx, dx])."""
+    r = backward_information_batch([model], [observations], initial_jitter=initial_jitter, jitter=jitter,
+                                   ctx=ctx)[0]
+    return r["mu_smooth"], r["Sigma_smooth"]

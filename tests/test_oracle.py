@@ -254,3 +254,41 @@ def test_kf_gradient_oracle_matches_finite_differences(seed, D, T):
             fd[k] = (vals[0] - 8 * vals[1] + 8 * vals[2] - vals[3]) / (12 * h)
         fd = fd.reshape(base.shape)
         np.testing.assert_allclose(g[name], fd, rtol=0, atol=1e-6 * (np.abs(fd).max() + 1e-12), err_msg=name)
+
+
+@pytest.mark.parametrize("Dy", [2, 3, 4])
+def test_backward_information_matches_joint_gaussian(Dy):
+    """test/algorithms/kalman.jl:83-137: after backward_initialise at T and two
+    backward predict/update steps, the natural parameters of p(y_{T-2:T} | x_{T-2})
+    equal F' S^-1 (y - g) and F' S^-1 F of the joint of (y_{T-2}, y_{T-1}, y_T)
+    given x_{T-2} (F = [H; HA; HA^2])."""
+    rng = np.random.default_rng(1234 + Dy)
+    m = O.create_linear_gaussian_model(rng, 3, Dy)
+    T = 4
+    _, ys = O.sample(rng, m, T)
+    _, _, lu, Ou = O.backward_information(m, ys, initial_jitter=1e-8)
+    A, b, Q, H, c, R = (np.asarray(v) for v in (m.A, m.b, m.Q, m.H, m.c, m.R))
+    Z = np.zeros((Dy, Dy))
+    F = np.vstack([H, H @ A, H @ A @ A])
+    g = np.concatenate([c, H @ b + c, H @ (A @ b + b) + c])
+    S = np.block([[R, Z, Z],
+                  [Z, H @ Q @ H.T + R, H @ Q @ A.T @ H.T],
+                  [Z, H @ A @ Q @ H.T, H @ (A @ Q @ A.T + Q) @ H.T + R]])
+    y = np.concatenate([ys[T - 3], ys[T - 2], ys[T - 1]])
+    lam_t = F.T @ np.linalg.solve(S, y - g)
+    Om_t = F.T @ np.linalg.solve(S, F)
+    np.testing.assert_allclose(lu[T - 3], lam_t, rtol=1e-7)
+    np.testing.assert_allclose(Ou[T - 3], Om_t, atol=1e-6)
+
+
+@pytest.mark.parametrize("Dy", [1, 2, 3])
+def test_two_filter_smoother_equals_rts(Dy):
+    """test/algorithms/kalman.jl:363-412: the two-filter smoother (forward filter x
+    backward predictive likelihood) equals the RTS smoother at every time."""
+    rng = np.random.default_rng(50 + Dy)
+    m = O.create_linear_gaussian_model(rng, 3, Dy)
+    _, ys = O.sample(rng, m, 6)
+    mus, Ss = O.two_filter_smooth(m, ys, initial_jitter=1e-10)
+    _, mr, Sr = O.rts_smooth(m, ys)
+    np.testing.assert_allclose(mus, mr, rtol=1e-7, atol=1e-9)
+    np.testing.assert_allclose(Ss, Sr, rtol=1e-7, atol=1e-9)
