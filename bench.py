@@ -586,7 +586,7 @@ def cpu_baseline_rbpf(hm, ys, N, seconds=12.0, threads=None):
 def bench_pf1d(args, world, rank, local):
     """The README model (x_t = x_{t-1} + N(0, 0.1^2), y_t = x_t + N(0, 0.2^2)),
     bootstrap PF with N = 1024, T = 100, FP64, systematic at ESS < 0.5 N: a
-    latency case (one filter fits in one block per step); one step = one filter
+    latency case (the whole filter runs in one block); one step = one filter
     run, the metric its device latency."""
     import ctypes as C
 
@@ -642,7 +642,9 @@ def bench_pf1d(args, world, rank, local):
     e2e_ms = statistics.median(t_e2e) * 1e3
     pms, pn = prof["propagate"]
     avg = pms / max(pn, 1)
-    bytes_launch = N * (8 * 1 * 2 + 16)  # FP64 state read + write, log-weight write + read / ancestor
+    # one launch runs the whole filter in one block: per particle-step FP64 state
+    # read + write, log-weight write + read / ancestor
+    bytes_launch = T * N * (8 * 1 * 2 + 16)
     peak, peak_kind = _peaks()
     line = {
         "metric": "filter latency", "value": ms, "unit": "ms", "n_gpus": world, "steps": args.steps,
@@ -657,9 +659,10 @@ def bench_pf1d(args, world, rank, local):
         "gpu_launches": int(sum(v[1] for v in prof.values()) + 2 * args.steps),
         "roofline": {"bound": "hbm", "achieved": bytes_launch / (avg / 1e3) / 1e9, "peak": peak,
                      "unit": "GB/s", "frac": bytes_launch / (avg / 1e3) / 1e9 / peak, "traffic": None,
-                     "kernel": "pf_lg_propagate<double,1,1>", "peak_source": peak_kind,
-                     "avg_launch_ms": avg, "bytes_per_launch": bytes_launch,
-                     "note": "launch-latency bound: one 1024-particle block per step"},
+                     "kernel": "pf_lg_small_filter<double,1,1> (all T steps in one block)",
+                     "peak_source": peak_kind, "avg_launch_ms": avg, "bytes_per_launch": bytes_launch,
+                     "note": "latency-bound: one block walks the filter's steps, each a chain of "
+                             "block-wide phases"},
         "kernels_ms": {k: v[0] for k, v in prof.items()},
         "clocks": clk.summary(),
     }

@@ -238,8 +238,10 @@ gf_status gf_kf_plan_destroy(gf_kf_plan* plan);
 /* plan flags: AUTOTUNE (KF: time each bucket's block shapes and keep the
  * fastest), NO_GRAPH (launch eagerly instead of replaying a CUDA graph), PLAIN
  * (KF: one launch per filter, the unbatched baseline form), SIMT (PF: keep the
- * CUDA-core propagation even where the tensor-core path applies). */
-enum { GF_PLAN_AUTOTUNE = 1, GF_PLAN_NO_GRAPH = 2, GF_PLAN_PLAIN = 4, GF_PLAN_SIMT = 8 };
+ * CUDA-core propagation even where the tensor-core path applies), NO_FUSE (PF:
+ * run filters of N <= 1024 as separate kernels per step instead of one block
+ * for the whole filter). */
+enum { GF_PLAN_AUTOTUNE = 1, GF_PLAN_NO_GRAPH = 2, GF_PLAN_PLAIN = 4, GF_PLAN_SIMT = 8, GF_PLAN_NO_FUSE = 16 };
 
 /* -------------------------------------------------------- particle filters */
 /* filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys)

@@ -421,6 +421,26 @@ static __device__ void apf_finish(const PfJob& J, int tile, int t, LseAcc a, dou
   }
 }
 
+// Final outputs of a filter run by one block: normalised log-weights
+// (lw - LSE), states, ll and clamps.
+template <typename Real>
+__device__ __forceinline__ void pf_finish_block(const PfJob& J) {
+  const Real* lw = reinterpret_cast<const Real*>(J.lw);
+  const double lse = J.sc->lse;
+  const int tcur = J.sc->t;
+  const Real* X = reinterpret_cast<const Real*>(J.X[tcur & 1]);
+  Real* so = reinterpret_cast<Real*>(J.states_out);
+  for (int64_t i = threadIdx.x; i < J.N; i += blockDim.x) {
+    if (J.logw_out) J.logw_out[i] = (double)lw[i] - lse;
+    if (so)
+      for (int d = 0; d < J.width; ++d) so[(size_t)d * J.N + i] = X[(size_t)d * J.N + i];
+  }
+  if (threadIdx.x == 0) {
+    if (J.ll_out) *J.ll_out = J.sc->ll;
+    if (J.clamps_out) *J.clamps_out = J.sc->clamps;
+  }
+}
+
 // ---------------------------------------------------------- resample kernel
 // Runs after a propagate whose finalise decided to resample: per propagate
 // tile, the cumulative normalised weights W_k = P_b + (running sum inside the
@@ -430,17 +450,13 @@ static __device__ void apf_finish(const PfJob& J, int tile, int t, LseAcc a, dou
 // Multinomial ancestors (unsorted uniforms) instead take W_k to the per-slot
 // search of the next propagate.
 template <typename Real>
-__global__ void __launch_bounds__(PF_THREADS, 6) pf_resample_kernel(const PfJob* __restrict__ jobs,
-                                                                   int njobs) {
-  const int jb = find_job(jobs, njobs, blockIdx.x, false);
-  const PfJob& J = jobs[jb];
+__device__ __forceinline__ void resample_tile(const PfJob& J, int tile) {
   PfScalars* sc = J.sc;
   if (!sc->resample || sc->status != 0 || sc->t >= J.T) return;
   __shared__ unsigned long long s_wsum[32];
   __shared__ int32_t s_last[PF_THREADS / 32];
   __shared__ int32_t s_O0;
   const int tstep = sc->t + 1;
-  const int tile = blockIdx.x - J.tile0;
   const int64_t N = J.N, i0 = (int64_t)tile * PF_TILE;
   const int nloc = (int)min((int64_t)PF_TILE, N - i0);
   // auxiliary filter: weights softmax(logw + log eta) (resamplers.jl:109-116)
@@ -538,6 +554,14 @@ __global__ void __launch_bounds__(PF_THREADS, 6) pf_resample_kernel(const PfJob*
   }
 }
 
+template <typename Real>
+__global__ void __launch_bounds__(PF_THREADS, 6) pf_resample_kernel(const PfJob* __restrict__ jobs,
+                                                                   int njobs) {
+  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const PfJob& J = jobs[jb];
+  resample_tile<Real>(J, blockIdx.x - J.tile0);
+}
+
 // Fill kernel: ancestors (0-based) of every slot from the cumulative offspring
 // counts (slot j's ancestor is the first k with ocum[k] > j, the cumulative-
 // offspring form of CUDAExt.jl:90-103), written to J.anc, which the next
@@ -546,16 +570,14 @@ __global__ void __launch_bounds__(PF_THREADS, 6) pf_resample_kernel(const PfJob*
 // however the offspring are distributed: at most FILL_D + 1 counts are staged
 // in shared memory, each thread binary-searches its own start and merges
 // FILL_IPT items, and the block's slots are written out coalesced.
-template <int DUMMY = 0>
-__global__ void __launch_bounds__(PF_THREADS, 8) pf_fill_ancestors_kernel(const PfJob* __restrict__ jobs,
-                                                                      int njobs) {
-  const int jb = find_job(jobs, njobs, blockIdx.x, false);
-  const PfJob& J = jobs[jb];
+// COHERENT: read the counts through L2, for a caller that wrote them earlier
+// in the same kernel.
+template <bool COHERENT>
+__device__ __forceinline__ void fill_block(const PfJob& J, int m) {
   const PfScalars* sc = J.sc;
   if (!sc->resample || sc->status != 0 || sc->t >= J.T || J.resampler == GF_RS_MULTINOMIAL) return;
   __shared__ int32_t s_oc[FILL_D + 1];
   __shared__ int32_t s_anc[FILL_D];
-  const int m = blockIdx.x - J.tile0;
   const int64_t N = J.N;
   const int64_t d0 = (int64_t)m * FILL_D, d1 = min(d0 + FILL_D, 2 * N);
   const int64_t k0 = J.mpk[m];
@@ -563,7 +585,7 @@ __global__ void __launch_bounds__(PF_THREADS, 8) pf_fill_ancestors_kernel(const 
   const int64_t j0 = d0 - k0, j1 = d1 - k1;
   const int nk = (int)(min(k1, N - 1) - k0 + 1);  // counts ocum[k0 .. min(k1, N-1)]
   const int32_t* __restrict__ oc = J.ocum;
-  for (int q = threadIdx.x; q < nk; q += PF_THREADS) s_oc[q] = oc[k0 + q];
+  for (int q = threadIdx.x; q < nk; q += PF_THREADS) s_oc[q] = COHERENT ? __ldcg(oc + k0 + q) : oc[k0 + q];
   __syncthreads();
   const int64_t d = d0 + (int64_t)threadIdx.x * FILL_IPT;
   if (d < d1) {
@@ -588,6 +610,14 @@ __global__ void __launch_bounds__(PF_THREADS, 8) pf_fill_ancestors_kernel(const 
   __syncthreads();
   int32_t* __restrict__ anc = J.anc;
   for (int q = threadIdx.x; q < (int)(j1 - j0); q += PF_THREADS) anc[j0 + q] = s_anc[q];
+}
+
+template <int DUMMY = 0>
+__global__ void __launch_bounds__(PF_THREADS, 8) pf_fill_ancestors_kernel(const PfJob* __restrict__ jobs,
+                                                                      int njobs) {
+  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const PfJob& J = jobs[jb];
+  fill_block<false>(J, blockIdx.x - J.tile0);
 }
 
 // ------------------------------------------------------------ lookback scan

@@ -47,9 +47,11 @@ __device__ __forceinline__ void draw_noise(const PfJob& J, const Real* noise, in
   }
 }
 
-template <typename Real, int DXP, int DYP, bool GUIDED>
-__global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __restrict__ jobs,
-                                                             int njobs) {
+// One 1024-particle tile of the propagate (a whole filter when N <= 1024).
+// COHERENT: read the ancestors through L2, for a caller that wrote them earlier
+// in the same kernel.
+template <typename Real, int DXP, int DYP, bool GUIDED, bool COHERENT>
+__device__ __forceinline__ void lg_propagate_tile(const PfJob& J, int tile) {
   using Lay = LgLayout<DXP, DYP>;
   extern __shared__ __align__(16) unsigned char smraw[];
   Real* sA = reinterpret_cast<Real*>(smraw);
@@ -62,12 +64,9 @@ __global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __
   Real* sQi = sM + DXP * DXP;
   __shared__ double red[32];
 
-  const int jb = find_job(jobs, njobs, blockIdx.x, false);
-  const PfJob& J = jobs[jb];
   PfScalars* sc = J.sc;
   const int t = sc->t + 1;
   if (t > J.T || sc->status != 0) return;
-  const int tile = blockIdx.x - J.tile0;
   const bool resamp = sc->resample != 0;
   const bool fresh = resamp || sc->uniform != 0;
   const double lse_prev = sc->lse;
@@ -101,7 +100,7 @@ __global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __
     const int64_t i = (int64_t)tile * PF_TILE + p * PF_THREADS + threadIdx.x;
     if (i >= N) break;
     int64_t a = i;
-    if (resamp) a = searched ? find_ancestor(J, sc, t, i, 0, N) : (int64_t)ancv[i];
+    if (resamp) a = searched ? find_ancestor(J, sc, t, i, 0, N) : (int64_t)(COHERENT ? __ldcg(ancv + i) : ancv[i]);
     Real x[DXP];
 #pragma unroll
     for (int d = 0; d < DXP; ++d) x[d] = d < dx ? Xs[(size_t)d * N + a] : Real(0);
@@ -195,13 +194,17 @@ __global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __
   block_finish(J, tile, t, fresh, acc, red);
 }
 
-// x_0 ~ MvNormal(mu0, Sigma0) (particles.jl:36-50, models/linear_gaussian.jl:23-29)
-template <typename Real, int DXP>
-__global__ void __launch_bounds__(PF_THREADS) pf_lg_init(const PfJob* __restrict__ jobs, int njobs,
-                                                        int mu_off, int l0_off) {
+template <typename Real, int DXP, int DYP, bool GUIDED>
+__global__ void __launch_bounds__(PF_THREADS, 3) pf_lg_propagate(const PfJob* __restrict__ jobs,
+                                                             int njobs) {
   const int jb = find_job(jobs, njobs, blockIdx.x, false);
   const PfJob& J = jobs[jb];
-  const int tile = blockIdx.x - J.tile0;
+  lg_propagate_tile<Real, DXP, DYP, GUIDED, false>(J, blockIdx.x - J.tile0);
+}
+
+// x_0 ~ MvNormal(mu0, Sigma0) (particles.jl:36-50, models/linear_gaussian.jl:23-29)
+template <typename Real, int DXP>
+__device__ __forceinline__ void lg_init_tile(const PfJob& J, int tile, int mu_off, int l0_off) {
   const int64_t N = J.N;
   const int dx = J.dx;
   const Real* P = reinterpret_cast<const Real*>(J.params);
@@ -228,6 +231,44 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_init(const PfJob* __restrict
     J.tprefix[tile] = (double)((int64_t)tile * PF_TILE) / (double)N;
     if (tile == J.ntiles - 1) J.tprefix[J.ntiles] = 1.0;
   }
+}
+
+template <typename Real, int DXP>
+__global__ void __launch_bounds__(PF_THREADS) pf_lg_init(const PfJob* __restrict__ jobs, int njobs,
+                                                        int mu_off, int l0_off) {
+  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const PfJob& J = jobs[jb];
+  lg_init_tile<Real, DXP>(J, blockIdx.x - J.tile0, mu_off, l0_off);
+}
+
+// A whole filter of N <= 1024 particles (one tile) in one block: the
+// initialisation, then per step the propagate with its finalise, the resample
+// and the ancestor fill of the multi-kernel run, separated by block barriers
+// instead of kernel boundaries, and the final outputs.  Same arithmetic in the
+// same order as the multi-kernel run, so the same ancestors and log-likelihood.
+// Systematic and stratified rules (the multinomial search reads its keys
+// through the read-only cache, which a kernel must not write).
+template <typename Real, int DXP, int DYP, bool GUIDED>
+__global__ void __launch_bounds__(PF_THREADS) pf_lg_small_filter(const PfJob* __restrict__ jobs, int mu_off,
+                                                                int l0_off) {
+  const PfJob& J = jobs[0];
+  lg_init_tile<Real, DXP>(J, 0, mu_off, l0_off);
+  __syncthreads();
+  resample_tile<Real>(J, 0);
+  __syncthreads();
+  fill_block<true>(J, 0);
+  __syncthreads();
+  for (int t = 1; t <= J.T; ++t) {
+    lg_propagate_tile<Real, DXP, DYP, GUIDED, true>(J, 0);
+    __syncthreads();
+    if (t < J.T) {
+      resample_tile<Real>(J, 0);
+      __syncthreads();
+      fill_block<true>(J, 0);
+      __syncthreads();
+    }
+  }
+  pf_finish_block<Real>(J);
 }
 
 
@@ -481,6 +522,7 @@ PfLgKernels make_lg() {
   k.dyp = DYP;
   k.prop = pf_lg_propagate<Real, DXP, DYP, G>;
   k.init = pf_lg_init<Real, DXP>;
+  k.small = pf_lg_small_filter<Real, DXP, DYP, G>;
   k.lookahead = pf_apf_lookahead<Real, DXP, DYP>;
   k.smem = sizeof(Real) * (G ? LgLayout<DXP, DYP>::smem_guided : LgLayout<DXP, DYP>::smem_boot);
   k.params_len = LgLayout<DXP, DYP>::total;

@@ -38,6 +38,7 @@ struct gf_pf_plan {
   size_t prop_smem = 0;
   cudaGraphExec_t graph = nullptr;
   bool graph_means = false;
+  bool small = false;  // N <= 1024 filters run in one block (pf_lg_small_filter)
   bool graph_record = false;
   bool use_graph = true;
   // path storage (allocated on the first run that asks for paths)
@@ -197,6 +198,10 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->ess1, &L.ess1, sizeof(double), cudaMemcpyHostToDevice, s));
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->res1, &L.res1, 1, cudaMemcpyHostToDevice, s));
   GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+  p->small = p->N <= PF_TILE && cfg->resampler != GF_RS_MULTINOMIAL && p->k.small && !(flags & GF_PLAN_NO_FUSE);
+  if (p->small)
+    GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)p->k.small, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            (int)p->k.smem));
   p->prop_fn = L.prop;
   p->prop_threads = L.threads;
   p->prop_split = L.split;
@@ -238,6 +243,12 @@ static void enqueue_run(gf_pf_plan* p, bool means, bool record) {
   cudaStream_t s = ctx->stream;
   launch_prep(ctx, p->dbl, p->job_dev, p->T, p->dx, p->dy, p->k.dxp, p->k.dyp, p->pp, p->ystep);
   launch_init_scalars(ctx, p->job_dev, 1, p->ess1, p->res1);
+  if (p->small && !means && !record && !p->eta) {
+    // the whole filter in one block (N <= 1024): no per-step launches
+    ProfScope ps(ctx, KC_PROPAGATE);
+    p->k.small<<<1, PF_THREADS, p->k.smem, s>>>(p->job_dev, p->k.off_mu0, p->k.off_L0);
+    return;
+  }
   cudaMemsetAsync(p->flags, 0, sizeof(unsigned long long) * 2 * p->nstiles, s);
   {
     ProfScope ps(ctx, KC_PREP);

@@ -309,3 +309,36 @@ def test_dense_ancestry_walk_with_shifting_ancestors(ctx):
         np.testing.assert_array_equal(traj[t], c.states[t - 1][N - K + t - 1])
     with pytest.raises(G.GFError):
         G.get_ancestry(c, N + 1, ctx=ctx)
+
+
+@pytest.mark.parametrize("prec", ["f64", "f32"])
+@pytest.mark.parametrize("kind,conv", [(O.SYSTEMATIC, "cpu"), (O.STRATIFIED, "cpu"), (O.SYSTEMATIC, "cudaext"),
+                                       (O.STRATIFIED, "cudaext")])
+@pytest.mark.parametrize("N,guided", [(1024, False), (777, False), (1000, True), (5, False)])
+def test_small_filter_in_one_block_equals_step_kernels(ctx, prec, kind, conv, N, guided):
+    """Filters of N <= 1024 run as one block for the whole filter; the result equals
+    the per-step kernels' run bit for bit (ll, per-step outputs, ancestors, final
+    states and log-weights), in-kernel Philox noise and uniforms."""
+    import torch
+    from gfb200.plans import PfPlan
+    rng = np.random.default_rng(N + kind)
+    m = random_lg(rng, 3, 2)
+    T = 40
+    _, ys = simulate(rng, m, T)
+    yd = torch.tensor(ys, device="cuda:0")
+    prop = G.OptimalProposal() if guided else G.LatentProposal()
+    algo = G.PF(N, prop, threshold=0.7, resampler=RS[kind], precision=prec, convention=conv)
+    dt = torch.float64 if prec == "f64" else torch.float32
+    res = []
+    for fuse in (True, False):
+        plan = PfPlan(m, algo, T, seed=31, ctx=ctx, fuse=fuse)
+        st = torch.zeros((3, N), dtype=dt, device="cuda:0")
+        lw = torch.zeros(N, dtype=torch.float64, device="cuda:0")
+        anc = torch.zeros((T, N), dtype=torch.int32, device="cuda:0")
+        plan.run(yd, states=st, log_weights=lw, ancestors=anc)
+        ctx.synchronize()
+        res.append([x.cpu().numpy() for x in (plan.ll, plan.ll_steps, plan.ess, plan.resampled, st, lw, anc)])
+        plan.close()
+    assert res[0][3].sum() >= 1
+    for a, b in zip(*res):
+        np.testing.assert_array_equal(a, b)
