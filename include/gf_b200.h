@@ -120,14 +120,15 @@ typedef struct {
   /* [T+1][dx][N] ancestral trajectory of every final particle, in the run's
    * precision: get_ancestry of AncestorCallback / ParticleTree (callbacks.jl:
    * 90-111, containers.jl:466-631), kept on the device as sparse path storage
-   * with pruning (ext/CUDAExt.jl:146-298).  Linear-Gaussian PF only. */
+   * with pruning (ext/CUDAExt.jl:146-298).  RBPF runs give the packed device
+   * state [dxo + dz + dz*(dz+1)/2] per particle (x, mu, Sigma upper by rows). */
   void* paths;
   /* Dense particle history of DenseAncestorCallback / DenseParticleContainer
    * (callbacks.jl:47-81, containers.jl:296-419): [T+1][dx][N] the states after
    * initialisation and after every step, in the run's precision, and [T][N]
    * the normalised log-weights after every update (the PostUpdate weights).
    * With `ancestors` they are the container; gf_pf_dense_ancestry walks it.
-   * Linear-Gaussian PF only. */
+   * RBPF runs use the packed device state, as for `paths`. */
   void* history;
   double* log_weight_history;
 } gf_pf_out;

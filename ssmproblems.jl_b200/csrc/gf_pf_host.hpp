@@ -123,6 +123,22 @@ struct PfTree {
   int32_t* cnt = nullptr;        // [N] offspring counts of the current particles
 };
 
+// Host side of a run's path storage: the tree and the device buffers it holds.
+// Set ctx, N, width and rsize (bytes per state element) before the first
+// tree_host_prepare; the pool grows between chunks of steps.
+struct TreeHost {
+  gf_ctx* ctx = nullptr;
+  int64_t N = 0;
+  int width = 0;
+  size_t rsize = 4;
+  PfTree tree;
+  std::vector<DevBuf> bufs;
+};
+constexpr int kTreeChunk = 32;  // steps between host checks of the free-slot count
+gf_status tree_host_prepare(TreeHost& h);
+gf_status tree_host_reserve(TreeHost& h, int64_t need);
+void tree_host_release(TreeHost& h);
+
 // Launchers (stream of ctx).  Before step t's propagate: count / prune / assign;
 // after it: insert.  tree_paths writes [T+1][width][N].
 void tree_launch_init(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int64_t N, const PfTree& tr);

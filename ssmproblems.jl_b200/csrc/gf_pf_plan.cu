@@ -42,8 +42,7 @@ struct gf_pf_plan {
   bool graph_record = false;
   bool use_graph = true;
   // path storage (allocated on the first run that asks for paths)
-  PfTree tree;
-  std::vector<DevBuf> tree_bufs;
+  TreeHost tree;
 };
 
 static gf_status plan_alloc(gf_pf_plan* p, size_t bytes, void** out) {
@@ -57,8 +56,7 @@ static void plan_release(gf_pf_plan* p) {
   if (p->graph) cudaGraphExecDestroy(p->graph);
   for (auto& b : p->bufs) dev_free(p->ctx, b.p, b.bytes);
   p->bufs.clear();
-  for (auto& b : p->tree_bufs) dev_free(p->ctx, b.p, b.bytes);
-  p->tree_bufs.clear();
+  tree_host_release(p->tree);
 }
 
 static gf_status validate_cfg(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg, int T) {
@@ -273,122 +271,32 @@ static void enqueue_run(gf_pf_plan* p, bool means, bool record) {
 }
 
 // ---------------------------------------------------------- path storage
-constexpr int kTreeChunk = 32;  // steps between host checks of the free-slot count
-
-// Pool arrays of M slots (states, parents, offspring, stack) into `bufs`.
-static gf_status tree_pool_alloc(gf_pf_plan* p, int64_t M, PfTree* tr, std::vector<DevBuf>* bufs) {
-  gf_ctx* ctx = p->ctx;
-  auto get = [&](size_t bytes, void** v) -> gf_status {
-    gf_status st = dev_alloc(ctx, bytes, v);
-    if (!st) bufs->push_back({*v, bytes});
-    return st;
-  };
-  void* v;
-  gf_status st;
-  tr->M = M;
-  if ((st = get(p->rsize * (size_t)p->dx * M, &v))) return st;
-  tr->states = v;
-  if ((st = get(sizeof(int32_t) * (size_t)M, &v))) return st;
-  tr->parents = (int32_t*)v;
-  if ((st = get(sizeof(int32_t) * (size_t)M, &v))) return st;
-  tr->offspring = (int32_t*)v;
-  if ((st = get(sizeof(int32_t) * (size_t)M, &v))) return st;
-  tr->stack = (int32_t*)v;
-  return GF_OK;
-}
-
-// Sets up the tree for a run: per-particle arrays once, the pool at its default
-// size N (2 + ceil(log2 N)) (grown during the run as needed).
-static gf_status tree_prepare(gf_pf_plan* p) {
-  const int64_t N = p->N;
-  PfTree& tr = p->tree;
-  tr.width = p->dx;
-  if (!tr.leaves) {
-    std::vector<DevBuf> bufs;
-    void* v;
-    gf_status st;
-    for (int32_t** f : {&tr.leaves, &tr.new_leaf, &tr.anc, &tr.cnt}) {
-      if ((st = dev_alloc(p->ctx, sizeof(int32_t) * (size_t)N, &v))) return st;
-      bufs.push_back({v, sizeof(int32_t) * (size_t)N});
-      *f = (int32_t*)v;
-    }
-    if ((st = dev_alloc(p->ctx, 256, &v))) return st;
-    bufs.push_back({v, 256});
-    tr.top = (int32_t*)v;
-    p->tree_bufs.insert(p->tree_bufs.end(), bufs.begin(), bufs.end());
-  }
-  if (!tr.states) {
-    int64_t lg = 1;
-    while ((int64_t(1) << lg) < N) ++lg;
-    const int64_t M = std::min<int64_t>(N * (2 + lg), INT32_MAX);
-    std::vector<DevBuf> bufs;
-    gf_status st = tree_pool_alloc(p, M, &tr, &bufs);
-    p->tree_bufs.insert(p->tree_bufs.end(), bufs.begin(), bufs.end());
-    if (st) return st;
-  }
-  return GF_OK;
-}
-
-// Makes room for `need` slots: doubles the pool (at least) when fewer are free.
-static gf_status tree_reserve(gf_pf_plan* p, int64_t need) {
-  gf_ctx* ctx = p->ctx;
-  cudaStream_t s = ctx->stream;
-  PfTree& tr = p->tree;
-  int32_t top = 0;
-  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(&top, tr.top, sizeof top, cudaMemcpyDeviceToHost, s));
-  GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
-  if (top >= need) return GF_OK;
-  const int64_t M_old = tr.M;
-  const int64_t M_new = std::max<int64_t>(2 * M_old, M_old + need - top);
-  if (M_new > INT32_MAX) return set_err(ctx, GF_ERR_OOM_BUDGET, "ancestry tree exceeds 2^31 slots");
-  PfTree nt = tr;
-  std::vector<DevBuf> bufs;
-  gf_status st = tree_pool_alloc(p, M_new, &nt, &bufs);
-  if (st) {
-    for (auto& b : bufs) dev_free(ctx, b.p, b.bytes);
-    return st;
-  }
-  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.states, tr.states, p->rsize * (size_t)p->dx * M_old,
-                                     cudaMemcpyDeviceToDevice, s));
-  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.parents, tr.parents, 4 * M_old, cudaMemcpyDeviceToDevice, s));
-  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.offspring, tr.offspring, 4 * M_old, cudaMemcpyDeviceToDevice, s));
-  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.stack, tr.stack, 4 * (size_t)top, cudaMemcpyDeviceToDevice, s));
-  tree_launch_grow_init(ctx, nt, M_old, top);
-  // release the old pool arrays (the first four pool buffers after the per-particle ones)
-  for (void* old : {tr.states, (void*)tr.parents, (void*)tr.offspring, (void*)tr.stack})
-    for (size_t i = 0; i < p->tree_bufs.size(); ++i)
-      if (p->tree_bufs[i].p == old) {
-        dev_free(ctx, old, p->tree_bufs[i].bytes);
-        p->tree_bufs.erase(p->tree_bufs.begin() + i);
-        break;
-      }
-  p->tree_bufs.insert(p->tree_bufs.end(), bufs.begin(), bufs.end());
-  tr = nt;
-  return GF_OK;
-}
-
 // One run with path storage (eager launches: the pool is sized between chunks).
 static gf_status enqueue_run_paths(gf_pf_plan* p, bool means, bool record, void* paths) {
   gf_ctx* ctx = p->ctx;
   cudaStream_t s = ctx->stream;
-  gf_status st = tree_prepare(p);
+  p->tree.ctx = ctx;
+  p->tree.N = p->N;
+  p->tree.width = p->dx;
+  p->tree.rsize = p->rsize;
+  gf_status st = tree_host_prepare(p->tree);
   if (st) return st;
   launch_prep(ctx, p->dbl, p->job_dev, p->T, p->dx, p->dy, p->k.dxp, p->k.dyp, p->pp, p->ystep);
   launch_init_scalars(ctx, p->job_dev, 1, p->ess1, p->res1);
   GF_CHECK_CUDA(ctx, cudaMemsetAsync(p->flags, 0, sizeof(unsigned long long) * 2 * p->nstiles, s));
   p->k.init<<<p->ntiles, PF_THREADS, 0, s>>>(p->job_dev, 1, p->k.off_mu0, p->k.off_L0);
-  tree_launch_init(ctx, p->dbl, p->job_dev, p->N, p->tree);
+  tree_launch_init(ctx, p->dbl, p->job_dev, p->N, p->tree.tree);
   if (record) launch_record(ctx, p->dbl, p->job_dev, p->N);
   launch_lookahead(p);
   launch_resample(ctx, p->dbl, p->job_dev, 1, p->ntiles);
   for (int t = 1; t <= p->T; ++t) {
     if ((t - 1) % kTreeChunk == 0) {
       const int64_t steps = std::min<int64_t>(kTreeChunk, p->T - t + 1);
-      if ((st = tree_reserve(p, steps * p->N))) return st;
+      if ((st = tree_host_reserve(p->tree, steps * p->N))) return st;
     }
-    tree_launch_step_pre(ctx, p->job_dev, p->N, p->tree, p->cfg.resampler != GF_RS_MULTINOMIAL);
+    tree_launch_step_pre(ctx, p->job_dev, p->N, p->tree.tree, p->cfg.resampler != GF_RS_MULTINOMIAL);
     p->prop_fn<<<p->ntiles * p->prop_split, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
-    tree_launch_insert(ctx, p->dbl, p->job_dev, p->N, p->tree, t);
+    tree_launch_insert(ctx, p->dbl, p->job_dev, p->N, p->tree.tree, t);
     if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);
     if (record) launch_record(ctx, p->dbl, p->job_dev, p->N);
     if (t < p->T) {
@@ -397,7 +305,7 @@ static gf_status enqueue_run_paths(gf_pf_plan* p, bool means, bool record, void*
     }
   }
   launch_finish(ctx, p->dbl, p->job_dev, p->N);
-  tree_launch_paths(ctx, p->dbl, p->job_dev, p->N, p->tree, p->T, paths);
+  tree_launch_paths(ctx, p->dbl, p->job_dev, p->N, p->tree.tree, p->T, paths);
   GF_CHECK_CUDA(ctx, cudaGetLastError());
   return GF_OK;
 }

@@ -255,4 +255,104 @@ void tree_launch_grow_init(gf_ctx* ctx, const PfTree& tr_new, int64_t M_old, int
   tree_grow_kernel<<<g, TREE_THREADS, 0, ctx->stream>>>(tr_new, M_old, top_old);
 }
 
+
+// ------------------------------------------------------------ host side
+// Pool arrays of M slots (states, parents, offspring, stack) into `bufs`.
+static gf_status tree_pool_alloc(TreeHost& h, int64_t M, PfTree* tr, std::vector<DevBuf>* bufs) {
+  gf_ctx* ctx = h.ctx;
+  auto get = [&](size_t bytes, void** v) -> gf_status {
+    gf_status st = dev_alloc(ctx, bytes, v);
+    if (!st) bufs->push_back({*v, bytes});
+    return st;
+  };
+  void* v;
+  gf_status st;
+  tr->M = M;
+  if ((st = get(h.rsize * (size_t)h.width * M, &v))) return st;
+  tr->states = v;
+  if ((st = get(sizeof(int32_t) * (size_t)M, &v))) return st;
+  tr->parents = (int32_t*)v;
+  if ((st = get(sizeof(int32_t) * (size_t)M, &v))) return st;
+  tr->offspring = (int32_t*)v;
+  if ((st = get(sizeof(int32_t) * (size_t)M, &v))) return st;
+  tr->stack = (int32_t*)v;
+  return GF_OK;
+}
+
+// Per-particle arrays once, the pool at its default size N (2 + ceil(log2 N))
+// (grown during the run as needed).
+gf_status tree_host_prepare(TreeHost& h) {
+  const int64_t N = h.N;
+  PfTree& tr = h.tree;
+  tr.width = h.width;
+  if (!tr.leaves) {
+    std::vector<DevBuf> bufs;
+    void* v;
+    gf_status st;
+    for (int32_t** f : {&tr.leaves, &tr.new_leaf, &tr.anc, &tr.cnt}) {
+      if ((st = dev_alloc(h.ctx, sizeof(int32_t) * (size_t)N, &v))) return st;
+      bufs.push_back({v, sizeof(int32_t) * (size_t)N});
+      *f = (int32_t*)v;
+    }
+    if ((st = dev_alloc(h.ctx, 256, &v))) return st;
+    bufs.push_back({v, 256});
+    tr.top = (int32_t*)v;
+    h.bufs.insert(h.bufs.end(), bufs.begin(), bufs.end());
+  }
+  if (!tr.states) {
+    int64_t lg = 1;
+    while ((int64_t(1) << lg) < N) ++lg;
+    const int64_t M = std::min<int64_t>(N * (2 + lg), INT32_MAX);
+    std::vector<DevBuf> bufs;
+    gf_status st = tree_pool_alloc(h, M, &tr, &bufs);
+    h.bufs.insert(h.bufs.end(), bufs.begin(), bufs.end());
+    if (st) return st;
+  }
+  return GF_OK;
+}
+
+// Makes room for `need` slots: doubles the pool (at least) when fewer are free.
+gf_status tree_host_reserve(TreeHost& h, int64_t need) {
+  gf_ctx* ctx = h.ctx;
+  cudaStream_t s = ctx->stream;
+  PfTree& tr = h.tree;
+  int32_t top = 0;
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(&top, tr.top, sizeof top, cudaMemcpyDeviceToHost, s));
+  GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
+  if (top >= need) return GF_OK;
+  const int64_t M_old = tr.M;
+  const int64_t M_new = std::max<int64_t>(2 * M_old, M_old + need - top);
+  if (M_new > INT32_MAX) return set_err(ctx, GF_ERR_OOM_BUDGET, "ancestry tree exceeds 2^31 slots");
+  PfTree nt = tr;
+  std::vector<DevBuf> bufs;
+  gf_status st = tree_pool_alloc(h, M_new, &nt, &bufs);
+  if (st) {
+    for (auto& b : bufs) dev_free(ctx, b.p, b.bytes);
+    return st;
+  }
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.states, tr.states, h.rsize * (size_t)h.width * M_old,
+                                     cudaMemcpyDeviceToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.parents, tr.parents, 4 * M_old, cudaMemcpyDeviceToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.offspring, tr.offspring, 4 * M_old, cudaMemcpyDeviceToDevice, s));
+  GF_CHECK_CUDA(ctx, cudaMemcpyAsync(nt.stack, tr.stack, 4 * (size_t)top, cudaMemcpyDeviceToDevice, s));
+  tree_launch_grow_init(ctx, nt, M_old, top);
+  // release the old pool arrays
+  for (void* old : {tr.states, (void*)tr.parents, (void*)tr.offspring, (void*)tr.stack})
+    for (size_t i = 0; i < h.bufs.size(); ++i)
+      if (h.bufs[i].p == old) {
+        dev_free(ctx, old, h.bufs[i].bytes);
+        h.bufs.erase(h.bufs.begin() + i);
+        break;
+      }
+  h.bufs.insert(h.bufs.end(), bufs.begin(), bufs.end());
+  tr = nt;
+  return GF_OK;
+}
+
+void tree_host_release(TreeHost& h) {
+  for (auto& b : h.bufs) dev_free(h.ctx, b.p, b.bytes);
+  h.bufs.clear();
+  h.tree = PfTree();
+}
+
 }  // namespace gf

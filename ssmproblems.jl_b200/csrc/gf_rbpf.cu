@@ -423,8 +423,6 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   if (!ctx || !m || !cfg || !out || !ys || !out->ll)
     return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
   if (cfg->precision != GF_PREC_F32) return set_err(ctx, GF_ERR_UNSUPPORTED, "RBPF runs in FP32 only");
-  if (out->paths || out->history || out->log_weight_history)
-    return set_err(ctx, GF_ERR_UNSUPPORTED, "path storage and dense history are for the linear-Gaussian PF");
   if (cfg->lookahead != GF_LOOKAHEAD_NONE)
     return set_err(ctx, GF_ERR_UNSUPPORTED, "the auxiliary filter is built for the linear-Gaussian PF");
   if (cfg->proposal == GF_PROP_OPTIMAL)
@@ -523,6 +521,10 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
     if ((st = mk(out->states, (void**)&d.states, sizeof(float) * (size_t)N * width))) return st;
     if ((st = mk(out->log_weights, (void**)&d.log_weights, sizeof(double) * (size_t)N))) return st;
     if ((st = mk(out->clamps, (void**)&d.clamps, sizeof(int32_t)))) return st;
+    if ((st = mk(out->paths, (void**)&d.paths, sizeof(float) * (size_t)(T + 1) * width * N))) return st;
+    if ((st = mk(out->history, (void**)&d.history, sizeof(float) * (size_t)(T + 1) * width * N))) return st;
+    if ((st = mk(out->log_weight_history, (void**)&d.log_weight_history, sizeof(double) * (size_t)T * N)))
+      return st;
   }
   const bool want_means = out->means || zmeans;
   if (want_means && !host)
@@ -573,22 +575,56 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   J.states_out = d.states;
   J.clamps_out = d.clamps;
   J.means_out = d_means;
+  J.hist = d.history;
+  J.lwh = d.log_weight_history;
   PfJob* jd = (PfJob*)jobv;
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(jd, &J, sizeof J, cudaMemcpyHostToDevice, s));
   launch_init_scalars(ctx, jd, 1, (const double*)ess1, (const int8_t*)res1);
   GF_CHECK_CUDA(ctx, cudaMemsetAsync(flags, 0, sizeof(unsigned long long) * 2 * nstiles, s));
   K.init<<<ntiles, PF_THREADS, 0, s>>>(jd, 1);
+  // ancestry: the device path storage (AncestorCallback) and the dense history
+  // (DenseAncestorCallback) over the packed device state [x | mu | Sigma upper]
+  const bool paths = d.paths != nullptr, record = d.history || d.log_weight_history;
+  TreeHost th;
+  struct TreeGuard {
+    TreeHost* h;
+    ~TreeGuard() {
+      if (h->ctx) {
+        cudaStreamSynchronize(h->ctx->stream);
+        tree_host_release(*h);
+      }
+    }
+  } tree_guard{&th};
+  if (paths) {
+    th.ctx = ctx;
+    th.N = N;
+    th.width = width;
+    th.rsize = sizeof(float);
+    if ((st = tree_host_prepare(th))) return st;
+    tree_launch_init(ctx, false, jd, N, th.tree);
+  }
+  if (record) launch_record(ctx, false, jd, N);
   launch_resample(ctx, false, jd, 1, ntiles);
   const int guided = cfg->proposal == GF_PROP_OVERDISPERSED;
   for (int t = 1; t <= T; ++t) {
+    if (paths) {
+      if ((t - 1) % kTreeChunk == 0) {
+        const int64_t steps = std::min<int64_t>(kTreeChunk, T - t + 1);
+        if ((st = tree_host_reserve(th, steps * N))) return st;
+      }
+      tree_launch_step_pre(ctx, jd, N, th.tree, cfg->resampler != GF_RS_MULTINOMIAL);
+    }
     {
       ProfScope ps(ctx, KC_RBPF);
       K.prop<<<ntiles * RB_SPLIT, RB_THREADS, 0, s>>>(jd, 1, (float)m->q_gamma, m->q_index, guided);
     }
+    if (paths) tree_launch_insert(ctx, false, jd, N, th.tree, t);
     if (want_means) launch_means(ctx, false, jd, 1, ntiles, (double*)mpart, dxo + dz);
+    if (record) launch_record(ctx, false, jd, N);
     if (t < T) launch_resample(ctx, false, jd, 1, ntiles);
   }
   launch_finish(ctx, false, jd, N);
+  if (paths) tree_launch_paths(ctx, false, jd, N, th.tree, T, d.paths);
   GF_CHECK_CUDA(ctx, cudaGetLastError());
   // ---- outputs
   std::vector<double> hm;
@@ -608,6 +644,9 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
     back(out->ancestors, d.ancestors, sizeof(int32_t) * (size_t)T * N);
     back(out->log_weights, d.log_weights, sizeof(double) * (size_t)N);
     back(out->clamps, d.clamps, sizeof(int32_t));
+    back(out->paths, d.paths, sizeof(float) * (size_t)(T + 1) * width * N);
+    back(out->history, d.history, sizeof(float) * (size_t)(T + 1) * width * N);
+    back(out->log_weight_history, d.log_weight_history, sizeof(double) * (size_t)T * N);
     if (out->states) {
       // unpack: [x | mu | Sigma packed] -> [x | mu | Sigma column-major]
       std::vector<float> hs((size_t)N * width);

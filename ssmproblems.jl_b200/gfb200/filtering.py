@@ -166,9 +166,20 @@ def filter(model, algo, observations, *, seed: int = 0, noise=None, uniforms=Non
     """
     ctx = _resolve_ctx(ctx)
     ys = L.f64(observations)
+    if callback is not None and isinstance(algo, RBPF):
+        if not isinstance(callback, (AncestorCallback, DenseAncestorCallback)):
+            raise TypeError(f"unsupported callback {type(callback).__name__}")
+        dense = isinstance(callback, DenseAncestorCallback)
+        st, ll = _rbpf(model, algo, ys, seed, noise, uniforms, ctx, True, want_means, schedule,
+                       want_paths=not dense, want_history=dense)
+        if dense:
+            callback.container = DenseParticleContainer(st._history, st._lw_history, st.ancestors, ctx)
+        else:
+            callback.tree = ParticleTree(st.paths)
+        return st, ll
     if callback is not None:
         if not isinstance(algo, (ParticleFilter, AuxiliaryParticleFilter)):
-            raise TypeError("ancestry callbacks are built for the linear-Gaussian particle filters")
+            raise TypeError("ancestry callbacks are built for the particle filters")
         if isinstance(callback, AncestorCallback):
             st, ll = filter(model, algo, observations, seed=seed, noise=noise, uniforms=uniforms, ctx=ctx,
                             want_ancestors=want_ancestors, want_means=want_means, schedule=schedule,
@@ -234,7 +245,10 @@ def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sched
     return state, float(out["ll"][0])
 
 
-def _rbpf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, schedule):
+def _rbpf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, schedule,
+          want_paths=False, want_history=False):
+    """RBPF run; paths and history hold the packed device state per particle
+    [x (dxo) | mu (dz) | Sigma upper triangle by rows (dz (dz + 1) / 2)]."""
     if not isinstance(model, HierarchicalSSM):
         raise TypeError("RBPF needs a HierarchicalSSM")
     mc = model._c_struct()
@@ -250,9 +264,13 @@ def _rbpf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sch
     out["ancestors"] = np.zeros((T, N), np.int32) if want_anc else None
     out["means"] = np.zeros((T, dxo)) if want_means else None
     zmeans = np.zeros((T, dz)) if want_means else None
+    pw = dxo + dz + dz * (dz + 1) // 2
+    out["paths"] = np.zeros((T + 1, pw, N), np.float32) if want_paths else None
+    out["history"] = np.zeros((T + 1, pw, N), np.float32) if want_history else None
+    out["log_weight_history"] = np.zeros((T, N)) if want_history else None
     o = L.PFOutC(*[L.ptr(out[k]) for k in ("ll", "ll_steps", "ess_steps", "resampled",
                                            "ancestors", "means", "states", "log_weights",
-                                           "clamps")])
+                                           "clamps", "paths", "history", "log_weight_history")])
     nz = None if noise is None else np.ascontiguousarray(noise, dtype=np.float32)
     un = None if uniforms is None else L.f64(uniforms)
     L.check(ctx.h, L.load().gf_rbpf_run(ctx.h, C.byref(mc), C.byref(cfg), T, L.ptr(ys),
@@ -266,7 +284,9 @@ def _rbpf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sch
                                  ll_steps=out["ll_steps"], ess_steps=out["ess_steps"],
                                  resampled=out["resampled"], ancestors=out["ancestors"],
                                  means=out["means"], zmeans=zmeans,
-                                 clamps=int(out["clamps"][0]))
+                                 clamps=int(out["clamps"][0]),
+                                 paths=None if out["paths"] is None else out["paths"].transpose(0, 2, 1))
+    state._history, state._lw_history = out["history"], out["log_weight_history"]
     return state, float(out["ll"][0])
 
 

@@ -74,3 +74,29 @@ def test_trend_model_full_size(ctx):
     assert np.all(st.ess_steps > 0) and np.all(st.ess_steps <= 65536 * (1 + 1e-9))
     S = st.particles["Sigma"]
     assert np.all(np.linalg.eigvalsh(S[:1000].astype(np.float64)) > 0)
+
+
+@pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.MULTINOMIAL])
+def test_rbpf_ancestry_callbacks(ctx, kind):
+    """test/algorithms/rbpf.jl:211-234 (AncestorCallback on an RBPF gives one path per
+    particle) and the dense container of the same run: the device path storage's
+    trajectories equal the walk through the recorded per-step states (packed
+    [x | mu | Sigma upper] states), and the last recorded states are the final ones."""
+    rng = np.random.default_rng(21 + kind)
+    full, hier = dummy_rb_model(rng, 1, 2, 1)
+    T, N = 6, 3000
+    _, ys = simulate(rng, full, T)
+    rs = {O.SYSTEMATIC: G.Systematic(), O.MULTINOMIAL: G.Multinomial()}[kind]
+    algo = G.RBPF(G.BF(N, threshold=0.8, resampler=rs), G.KalmanFilter())
+    cb = G.AncestorCallback()
+    st, ll = G.filter(hier, algo, ys, seed=3, callback=cb, ctx=ctx)
+    paths = G.get_ancestry(cb.tree)
+    assert len(paths) == N and paths.shape[1] == T + 1
+    dcb = G.DenseAncestorCallback()
+    st2, ll2 = G.filter(hier, algo, ys, seed=3, callback=dcb, ctx=ctx)
+    assert ll2 == ll
+    dense = G.get_ancestry(dcb.container, ctx=ctx)
+    np.testing.assert_array_equal(paths, dense)
+    last = dcb.container.states[-1]  # [N, width]: x (1), mu (2), Sigma packed (3)
+    np.testing.assert_array_equal(last[:, :1], np.asarray(st2.particles["x"]).reshape(N, 1))
+    np.testing.assert_array_equal(last[:, 1:3], np.asarray(st2.particles["mu"]).reshape(N, 2))
