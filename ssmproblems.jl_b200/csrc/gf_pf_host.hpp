@@ -14,7 +14,8 @@ struct PfLgKernels {
   int dxp = 0, dyp = 0;
   void (*prop)(const PfJob*, int) = nullptr;
   void (*init)(const PfJob*, int, int, int) = nullptr;
-  void (*small)(const PfJob*, int, int) = nullptr;  // whole filter in one block, N <= 1024
+  void (*small)(const PfJob*, int, int, double*) = nullptr;  // whole filter in one block, N <= 1024
+  void (*small_means)(const PfJob*, int, int, double*) = nullptr;  // the same with weighted means
   void (*lookahead)(const PfJob*, int) = nullptr;  // auxiliary filter first stage
   size_t smem = 0;
   int params_len = 0, off_mu0 = 0, off_L0 = 0;

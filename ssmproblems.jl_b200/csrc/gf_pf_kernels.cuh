@@ -421,6 +421,47 @@ static __device__ void apf_finish(const PfJob& J, int tile, int t, LseAcc a, dou
   }
 }
 
+// Weighted filtered means sum_i exp(lw_i - LSE) x_i after step t (optional output).
+template <typename Real>
+__device__ __forceinline__ void pf_means_kernel(const PfJob* __restrict__ jobs, int njobs, double* __restrict__ mpart,
+                                double* __restrict__ means, int mdim) {
+  const int jb = find_job(jobs, njobs, blockIdx.x, false);
+  const PfJob& J = jobs[jb];
+  PfScalars* sc = J.sc;
+  const int t = sc->t;
+  if (t < 1 || sc->status != 0) return;
+  const int tile = blockIdx.x - J.tile0;
+  const int64_t N = J.N;
+  const Real* X = reinterpret_cast<const Real*>(J.X[t & 1]);
+  const Real* lw = reinterpret_cast<const Real*>(J.lw);
+  const double lse = sc->lse;
+  __shared__ double red[32];
+  __shared__ int s_last;
+  for (int d = 0; d < mdim; ++d) {
+    double s = 0.0;
+    for (int p = 0; p < PF_PPT; ++p) {
+      const int64_t i = (int64_t)tile * PF_TILE + p * PF_THREADS + threadIdx.x;
+      if (i < N) s += exp((double)lw[i] - lse) * (double)X[(size_t)d * N + i];
+    }
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) mpart[(size_t)tile * mdim + d] = s;
+  }
+  if (threadIdx.x == 0) {
+    __threadfence();
+    s_last = atomicAdd(&sc->mcounter, 1u) == (unsigned)(J.ntiles - 1);
+  }
+  __syncthreads();
+  if (!s_last) return;
+  __threadfence();
+  for (int d = 0; d < mdim; ++d) {
+    double s = 0.0;
+    for (int b = threadIdx.x; b < J.ntiles; b += blockDim.x) s += __ldcg(mpart + (size_t)b * mdim + d);
+    s = block_sum(s, red);
+    if (threadIdx.x == 0) means[(size_t)(t - 1) * mdim + d] = s;
+  }
+  if (threadIdx.x == 0) sc->mcounter = 0;
+}
+
 // Final outputs of a filter run by one block: normalised log-weights
 // (lw - LSE), states, ll and clamps.
 template <typename Real>

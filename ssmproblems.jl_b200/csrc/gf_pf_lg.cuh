@@ -247,21 +247,29 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_init(const PfJob* __restrict
 // instead of kernel boundaries, and the final outputs.  Same arithmetic in the
 // same order as the multi-kernel run, so the same ancestors and log-likelihood.
 // Systematic and stratified rules (the multinomial search reads its keys
-// through the read-only cache, which a kernel must not write).
-template <typename Real, int DXP, int DYP, bool GUIDED>
+// through the read-only cache, which a kernel must not write); weighted means
+// as the per-step means kernel computes them.
+template <typename Real, int DXP, int DYP, bool GUIDED, bool MEANS>
 __global__ void __launch_bounds__(PF_THREADS) pf_lg_small_filter(const PfJob* __restrict__ jobs, int mu_off,
-                                                                int l0_off) {
+                                                                int l0_off, double* __restrict__ mpart) {
   const PfJob& J = jobs[0];
+  // loop-invariant job fields in registers (the job lives in global memory)
+  const int T = J.T, dx = J.dx;
+  double* const means_out = J.means_out;
   lg_init_tile<Real, DXP>(J, 0, mu_off, l0_off);
   __syncthreads();
   resample_tile<Real>(J, 0);
   __syncthreads();
   fill_block<true>(J, 0);
   __syncthreads();
-  for (int t = 1; t <= J.T; ++t) {
+  for (int t = 1; t <= T; ++t) {
     lg_propagate_tile<Real, DXP, DYP, GUIDED, true>(J, 0);
     __syncthreads();
-    if (t < J.T) {
+    if (MEANS) {
+      pf_means_kernel<Real>(jobs, 1, mpart, means_out, dx);
+      __syncthreads();
+    }
+    if (t < T) {
       resample_tile<Real>(J, 0);
       __syncthreads();
       fill_block<true>(J, 0);
@@ -522,7 +530,8 @@ PfLgKernels make_lg() {
   k.dyp = DYP;
   k.prop = pf_lg_propagate<Real, DXP, DYP, G>;
   k.init = pf_lg_init<Real, DXP>;
-  k.small = pf_lg_small_filter<Real, DXP, DYP, G>;
+  k.small = pf_lg_small_filter<Real, DXP, DYP, G, false>;
+  k.small_means = pf_lg_small_filter<Real, DXP, DYP, G, true>;
   k.lookahead = pf_apf_lookahead<Real, DXP, DYP>;
   k.smem = sizeof(Real) * (G ? LgLayout<DXP, DYP>::smem_guided : LgLayout<DXP, DYP>::smem_boot);
   k.params_len = LgLayout<DXP, DYP>::total;

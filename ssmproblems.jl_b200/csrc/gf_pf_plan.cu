@@ -198,8 +198,9 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
   p->small = p->N <= PF_TILE && cfg->resampler != GF_RS_MULTINOMIAL && p->k.small && !(flags & GF_PLAN_NO_FUSE);
   if (p->small)
-    GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)p->k.small, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                            (int)p->k.smem));
+    for (auto f : {p->k.small, p->k.small_means})
+      GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)f, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                              (int)p->k.smem));
   p->prop_fn = L.prop;
   p->prop_threads = L.threads;
   p->prop_split = L.split;
@@ -241,10 +242,11 @@ static void enqueue_run(gf_pf_plan* p, bool means, bool record) {
   cudaStream_t s = ctx->stream;
   launch_prep(ctx, p->dbl, p->job_dev, p->T, p->dx, p->dy, p->k.dxp, p->k.dyp, p->pp, p->ystep);
   launch_init_scalars(ctx, p->job_dev, 1, p->ess1, p->res1);
-  if (p->small && !means && !record && !p->eta) {
+  if (p->small && !record && !p->eta) {
     // the whole filter in one block (N <= 1024): no per-step launches
     ProfScope ps(ctx, KC_PROPAGATE);
-    p->k.small<<<1, PF_THREADS, p->k.smem, s>>>(p->job_dev, p->k.off_mu0, p->k.off_L0);
+    (means ? p->k.small_means : p->k.small)<<<1, PF_THREADS, p->k.smem, s>>>(p->job_dev, p->k.off_mu0,
+                                                                          p->k.off_L0, p->mpart);
     return;
   }
   cudaMemsetAsync(p->flags, 0, sizeof(unsigned long long) * 2 * p->nstiles, s);

@@ -317,8 +317,8 @@ def test_dense_ancestry_walk_with_shifting_ancestors(ctx):
 @pytest.mark.parametrize("N,guided", [(1024, False), (777, False), (1000, True), (5, False)])
 def test_small_filter_in_one_block_equals_step_kernels(ctx, prec, kind, conv, N, guided):
     """Filters of N <= 1024 run as one block for the whole filter; the result equals
-    the per-step kernels' run bit for bit (ll, per-step outputs, ancestors, final
-    states and log-weights), in-kernel Philox noise and uniforms."""
+    the per-step kernels' run bit for bit (ll, per-step outputs, ancestors, weighted
+    means, final states and log-weights), in-kernel Philox noise and uniforms."""
     import torch
     from gfb200.plans import PfPlan
     rng = np.random.default_rng(N + kind)
@@ -335,9 +335,11 @@ def test_small_filter_in_one_block_equals_step_kernels(ctx, prec, kind, conv, N,
         st = torch.zeros((3, N), dtype=dt, device="cuda:0")
         lw = torch.zeros(N, dtype=torch.float64, device="cuda:0")
         anc = torch.zeros((T, N), dtype=torch.int32, device="cuda:0")
-        plan.run(yd, states=st, log_weights=lw, ancestors=anc)
+        means = torch.zeros((T, 3), dtype=torch.float64, device="cuda:0")
+        plan.run(yd, states=st, log_weights=lw, ancestors=anc, means=means)
         ctx.synchronize()
-        res.append([x.cpu().numpy() for x in (plan.ll, plan.ll_steps, plan.ess, plan.resampled, st, lw, anc)])
+        res.append([x.cpu().numpy() for x in (plan.ll, plan.ll_steps, plan.ess, plan.resampled, st, lw, anc,
+                                              means)])
         plan.close()
     assert res[0][3].sum() >= 1
     for a, b in zip(*res):
