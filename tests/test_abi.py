@@ -4,6 +4,8 @@ import ctypes as C
 import os
 import re
 
+import pytest
+
 ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
 
 
@@ -33,3 +35,47 @@ def test_python_binding_covers_the_header():
 def test_version_callable_without_gpu():
     from gfb200 import _lib as L
     assert L.load().gf_version() >= 100
+
+
+STRUCTS = {  # C type in include/gf_b200.h -> ctypes mirror in gfb200._lib
+    "gf_lg_model": "LGModelC", "gf_rb_model": "RBModelC", "gf_pf_config": "PFConfigC",
+    "gf_pf_out": "PFOutC", "gf_kf_out": "KFOutC", "gf_kf_grad_out": "KFGradOutC",
+    "gf_kf_backward_out": "KFBackOutC", "gf_csmc_config": "CsmcConfigC", "gf_csmc_out": "CsmcOutC",
+    "gf_srv_config": "SrvConfigC", "gf_srv_request": "SrvRequestC", "gf_srv_result": "SrvResultC",
+    "gf_srv_metrics": "SrvMetricsC",
+}
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """Every ABI struct's size and field offsets, as gcc lays them out from the
+    header, equal the ctypes mirror's (a stale mirror would make the library read
+    past the caller's struct)."""
+    import ctypes
+    import json
+    import shutil
+    import subprocess
+
+    from gfb200 import _lib as L
+    if shutil.which("gcc") is None:
+        pytest.skip("no gcc")
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gf_b200.h"', "int main(void) {",
+             '  printf("{");']
+    first = True
+    for cname, pyname in STRUCTS.items():
+        fields = [f[0] for f in getattr(L, pyname)._fields_]
+        sep = "" if first else ","
+        first = False
+        lines.append(f'  printf("{sep}\\"{cname}\\": [%zu", sizeof({cname}));')
+        for f in fields:
+            lines.append(f'  printf(",%zu", offsetof({cname}, {f}));')
+        lines.append('  printf("]");')
+    lines += ['  printf("}\\n");', "  return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.check_call(["gcc", "-I", os.path.join(ROOT, "include"), str(src), "-o", str(exe)])
+    got = json.loads(subprocess.check_output([str(exe)]).decode())
+    for cname, pyname in STRUCTS.items():
+        st = getattr(L, pyname)
+        want = [ctypes.sizeof(st)] + [getattr(st, f[0]).offset for f in st._fields_]
+        assert got[cname] == want, (cname, got[cname], want)
