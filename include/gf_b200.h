@@ -55,9 +55,12 @@ enum { GF_PREC_F32 = 0, GF_PREC_F64 = 1 };
 enum { GF_PROP_BOOTSTRAP = 0, GF_PROP_OPTIMAL = 1, GF_PROP_OVERDISPERSED = 2 };
 enum { GF_ALGO_KF = 0, GF_ALGO_SRKF = 1 };
 /* AuxiliaryParticleFilter(pf, RepresentativeStateLookAhead(pp)) (particles.jl:
- * 247-357): GF_LOOKAHEAD_MEAN scores each particle by log p(y_t | A x + b), the
- * mean and mode of its transition (MeanPredictive, ModePredictive). */
-enum { GF_LOOKAHEAD_NONE = 0, GF_LOOKAHEAD_MEAN = 1 };
+ * 247-384): GF_LOOKAHEAD_MEAN scores each particle by log p(y_t | A x + b), the
+ * mean and mode of its transition (MeanPredictive, ModePredictive);
+ * GF_LOOKAHEAD_DRAW by log p(y_t | x*) with x* one draw from the transition
+ * (DrawPredictive; bootstrap proposal; the draws come from their own Philox
+ * stream even when the propagation noise is injected). */
+enum { GF_LOOKAHEAD_NONE = 0, GF_LOOKAHEAD_MEAN = 1, GF_LOOKAHEAD_DRAW = 2 };
 
 typedef struct gf_ctx gf_ctx;
 

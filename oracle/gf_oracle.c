@@ -64,9 +64,16 @@ void or_philox4x32_10(const uint32_t ctr[4], uint32_t k0, uint32_t k1, uint32_t 
 
 /* 4 standard normals for (particle i, step t, block q) -- Box-Muller on
  * 24-bit uniforms u1 in (0,1], u2 in [0,1), angle 2*pi*u2 - pi. */
+#define TAG_LOOKAHEAD 0x4C4B4844u /* DrawPredictive draws of the auxiliary filter */
+static void philox_normals4_tag(uint64_t seed, uint32_t i, uint32_t t, uint32_t q, uint32_t tag,
+                                double out[4]);
 void or_philox_normals4(uint64_t seed, uint32_t i, uint32_t t, uint32_t q,
                         double out[4]) {
-  uint32_t ctr[4] = {i, t, q, TAG_NORMAL}, w[4];
+  philox_normals4_tag(seed, i, t, q, TAG_NORMAL, out);
+}
+static void philox_normals4_tag(uint64_t seed, uint32_t i, uint32_t t, uint32_t q, uint32_t tag,
+                                double out[4]) {
+  uint32_t ctr[4] = {i, t, q, tag}, w[4];
   philox4x32_10(ctr, (uint32_t)seed, (uint32_t)(seed >> 32), w);
   for (int p = 0; p < 2; ++p) {
     double u1 = ((double)(w[2 * p] >> 8) + 1.0) * (1.0 / 16777216.0);
@@ -633,7 +640,7 @@ typedef struct {
 typedef struct {
   int kind;           /* OR_PROP_* */
   double k;           /* overdispersion factor */
-  int lookahead;      /* 1: AuxiliaryParticleFilter(pf, MeanPredictive()) first stage */
+  int lookahead;      /* AuxiliaryParticleFilter first stage: 1 MeanPredictive, 2 DrawPredictive */
 } or_proposal;
 
 typedef struct { /* nullable outputs */
@@ -783,6 +790,17 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
         double mx[64], hx[64], dif[64], tmpd[64];
         mv(dx, dx, m->A, x + (size_t)i * dx, mx);
         for (int d = 0; d < dx; ++d) mx[d] += m->b[d];
+        if (prop->lookahead == 2) {
+          /* DrawPredictive (particles.jl:377-384): x* ~ MvNormal(A x + b, Q), the draw
+           * from the Philox stream tagged TAG_LOOKAHEAD with counters (i, t, q) */
+          double e[64], v[64], buf[4];
+          for (int q = 0; 4 * q < dx; ++q) {
+            philox_normals4_tag(seed, (uint32_t)i, (uint32_t)t, (uint32_t)q, TAG_LOOKAHEAD, buf);
+            for (int r = 0; r < 4 && 4 * q + r < dx; ++r) e[4 * q + r] = buf[r];
+          }
+          mv(dx, dx, LQ, e, v);
+          for (int d = 0; d < dx; ++d) mx[d] += v[d];
+        }
         mv(dy, dx, m->H, mx, hx);
         for (int k = 0; k < dy; ++k) dif[k] = yl[k] - hx[k] - m->c[k];
         eta[i] = logpdf_chol(dy, LR, dif, tmpd);

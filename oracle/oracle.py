@@ -173,7 +173,9 @@ def pf_run(m: LGModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=
            k=1.0, want_ancestors=False, want_margins=False, want_states=False, threads=1,
            lookahead=0):
     """filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys), or with
-    lookahead=1 filter(rng, model, AuxiliaryParticleFilter(pf, MeanPredictive()), ys).
+    lookahead=1 filter(rng, model, AuxiliaryParticleFilter(pf, MeanPredictive()), ys) and
+    lookahead=2 the same with DrawPredictive() (its draw from the Philox stream tagged
+    0x4C4B4844, counters (i, t, q), key seed).
 
     noise: [(T+1), dx, N] standard normals (step 0 = prior draw) or None for the
     shared Philox stream with ``seed``; uniforms: systematic [T], else [T, N].

@@ -18,6 +18,7 @@ namespace gf {
 //   uniforms: ctr = (slot j, step t, 0, 'UNIF'), one FP64 uniform per call
 constexpr uint32_t kTagNormal = 0x4E4F524Du;
 constexpr uint32_t kTagUnif = 0x554E4946u;
+constexpr uint32_t kTagLookahead = 0x4C4B4844u;  // DrawPredictive draws of the auxiliary filter
 
 __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2,
                                                        uint32_t c3, uint32_t k0, uint32_t k1,
@@ -50,9 +51,9 @@ __host__ __device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1,
 // angle 2*pi*u2 - pi (keeps the fast sin/cos argument inside [-pi, pi]).
 template <typename Real>
 __device__ __forceinline__ void philox_normals4(uint64_t seed, uint32_t i, uint32_t t, uint32_t q,
-                                                Real out[4]) {
+                                                Real out[4], uint32_t tag = kTagNormal) {
   uint32_t w[4];
-  philox4x32_10(i, t, q, kTagNormal, (uint32_t)seed, (uint32_t)(seed >> 32), w);
+  philox4x32_10(i, t, q, tag, (uint32_t)seed, (uint32_t)(seed >> 32), w);
 #pragma unroll
   for (int p = 0; p < 2; ++p) {
     if constexpr (sizeof(Real) == 4) {

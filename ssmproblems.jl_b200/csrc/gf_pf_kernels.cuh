@@ -38,7 +38,8 @@ struct PfJob {
   uint64_t seed;
   const void* params;        // model parameters in the run's precision
   const void* ystep;         // per-step vectors [T][ystride]
-  int32_t ystride, pad1;
+  int32_t ystride;
+  int32_t lookahead_draw;    // auxiliary filter: DrawPredictive (x* drawn from the transition)
   void* X[2];                // SoA state ping-pong [width][N]
   void* lw;                  // stored log-weights [N]
   double* key;               // cumulative normalised weights [N]

@@ -469,12 +469,14 @@ __global__ void __launch_bounds__(TC_THREADS) pf_lg_propagate_tc(const PfJob* __
 
 // Auxiliary particle filter, first stage of step t (particles.jl:273-357):
 // log eta_i = log p(y_t | x*_i) with x*_i = A x_i + b, the mean and the mode of
-// the transition MvNormal(A x + b, Q) (MeanPredictive, ModePredictive), then
-// the resampling decision on softmax(logw + log eta) in apf_finish.
+// the transition MvNormal(A x + b, Q) (MeanPredictive, ModePredictive), or a
+// draw A x_i + b + chol(Q) e' from it (DrawPredictive, :377-384; e' from the
+// Philox stream tagged kTagLookahead, counters (i, t, q) as the propagation's),
+// then the resampling decision on softmax(logw + log eta) in apf_finish.
 template <typename Real, int DXP, int DYP>
 __global__ void __launch_bounds__(PF_THREADS) pf_apf_lookahead(const PfJob* __restrict__ jobs, int njobs) {
   using Lay = LgLayout<DXP, DYP>;
-  __shared__ Real sA[DXP * DXP], sb[DXP], sH[DYP * DXP], sy[DYP];
+  __shared__ Real sA[DXP * DXP], sb[DXP], sH[DYP * DXP], sy[DYP], sL[DXP * DXP];
   __shared__ double red[32];
   const int jb = find_job(jobs, njobs, blockIdx.x, false);
   const PfJob& J = jobs[jb];
@@ -483,7 +485,10 @@ __global__ void __launch_bounds__(PF_THREADS) pf_apf_lookahead(const PfJob* __re
   if (t > J.T || sc->status != 0) return;
   const int tile = blockIdx.x - J.tile0;
   const Real* P = reinterpret_cast<const Real*>(J.params);
-  for (int k = threadIdx.x; k < DXP * DXP; k += PF_THREADS) sA[k] = P[Lay::A + k];
+  for (int k = threadIdx.x; k < DXP * DXP; k += PF_THREADS) {
+    sA[k] = P[Lay::A + k];
+    sL[k] = P[Lay::L + k];
+  }
   for (int k = threadIdx.x; k < DYP * DXP; k += PF_THREADS) sH[k] = P[Lay::H + k];
   for (int k = threadIdx.x; k < DXP; k += PF_THREADS) sb[k] = P[Lay::b + k];
   const Real* Y = reinterpret_cast<const Real*>(J.ystep) + (size_t)(t - 1) * J.ystride;
@@ -495,6 +500,7 @@ __global__ void __launch_bounds__(PF_THREADS) pf_apf_lookahead(const PfJob* __re
   const Real* lw = reinterpret_cast<const Real*>(J.lw);
   Real* eta = reinterpret_cast<Real*>(J.eta);
   const double obs_const = J.obs_const;
+  const bool draw = J.lookahead_draw != 0;
   LseAcc acc;
   for (int p = 0; p < PF_PPT; ++p) {
     const int64_t i = (int64_t)tile * PF_TILE + p * PF_THREADS + threadIdx.x;
@@ -507,6 +513,20 @@ __global__ void __launch_bounds__(PF_THREADS) pf_apf_lookahead(const PfJob* __re
       const Real xc = c < dx ? Xs[(size_t)c * N + i] : Real(0);
 #pragma unroll
       for (int r = 0; r < DXP; ++r) m[r] = fma(sA[c * DXP + r], xc, m[r]);
+    }
+    if (draw) {
+#pragma unroll
+      for (int qq = 0; qq < (DXP + 3) / 4; ++qq) {
+        Real e4[4];
+        philox_normals4<Real>(J.seed, (uint32_t)i, (uint32_t)t, (uint32_t)qq, e4, kTagLookahead);
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+          const int c = 4 * qq + cc;
+          if (c < DXP && c < dx)
+#pragma unroll
+            for (int r = c; r < DXP; ++r) m[r] = fma(sL[c * DXP + r], e4[cc], m[r]);
+        }
+      }
     }
     Real q = 0;
 #pragma unroll

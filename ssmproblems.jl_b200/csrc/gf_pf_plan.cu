@@ -69,8 +69,10 @@ static gf_status validate_cfg(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_con
   if (cfg->convention < 0 || cfg->convention > 1) return set_err(ctx, GF_ERR_ARG, "unknown convention");
   if (cfg->precision != GF_PREC_F32 && cfg->precision != GF_PREC_F64)
     return set_err(ctx, GF_ERR_ARG, "unknown precision");
-  if (cfg->lookahead != GF_LOOKAHEAD_NONE && cfg->lookahead != GF_LOOKAHEAD_MEAN)
+  if (cfg->lookahead < GF_LOOKAHEAD_NONE || cfg->lookahead > GF_LOOKAHEAD_DRAW)
     return set_err(ctx, GF_ERR_ARG, "unknown lookahead");
+  if (cfg->lookahead == GF_LOOKAHEAD_DRAW && cfg->proposal != GF_PROP_BOOTSTRAP)
+    return set_err(ctx, GF_ERR_UNSUPPORTED, "DrawPredictive lookahead is built for the bootstrap proposal");
   return GF_OK;
 }
 
@@ -133,6 +135,7 @@ gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cf
   J.prop_const = f.prop_const;
   J.seed = cfg->seed;
   J.ystride = o->k.dyp + o->k.dxp;
+  J.lookahead_draw = cfg->lookahead == GF_LOOKAHEAD_DRAW ? 1 : 0;
   return GF_OK;
 }
 

@@ -25,7 +25,7 @@ GF_ALGO_KF, GF_ALGO_SRKF = 0, 1
 GF_PLAN_AUTOTUNE, GF_PLAN_NO_GRAPH, GF_PLAN_PLAIN, GF_PLAN_SIMT, GF_PLAN_NO_FUSE = 1, 2, 4, 8, 16
 GF_REQ_KF, GF_REQ_SRKF, GF_REQ_PF, GF_REQ_RBPF = 0, 1, 2, 3
 GF_CSMC_NONE, GF_CSMC_ANCESTOR, GF_CSMC_BACKWARD = 0, 1, 2
-GF_LOOKAHEAD_NONE, GF_LOOKAHEAD_MEAN = 0, 1
+GF_LOOKAHEAD_NONE, GF_LOOKAHEAD_MEAN, GF_LOOKAHEAD_DRAW = 0, 1, 2
 
 EXPORTED = [
     "gf_ctx_create", "gf_ctx_destroy", "gf_last_error", "gf_ctx_set_stream", "gf_ctx_get_stream",

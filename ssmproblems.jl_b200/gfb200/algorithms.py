@@ -164,8 +164,9 @@ class ModePredictive(PredictiveStatistic):
 
 
 class DrawPredictive(PredictiveStatistic):
-    """A draw from the transition: not built (needs a second noise stream per step)."""
-    lookahead = -1
+    """A draw from the transition, A x + b + chol(Q) e' (bootstrap proposal; e' from its
+    own in-kernel Philox stream)."""
+    lookahead = 2
 
 
 class RepresentativeStateLookAhead:

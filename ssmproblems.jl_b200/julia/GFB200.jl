@@ -16,7 +16,8 @@ using GeneralisedFilters
 using GeneralisedFilters: KalmanFilter, SRKalmanFilter, ParticleFilter, ESSResampler,
     Systematic, Stratified, Multinomial, LatentProposal, RBPF, HierarchicalSSM,
     ParticleDistribution, Particle, TypelessZero, AuxiliaryParticleFilter, MeanPredictive,
-    ModePredictive, ConditionalSMC, NoRefreshment, AncestorSampling, BackwardSimulation
+    ModePredictive, DrawPredictive, ConditionalSMC, NoRefreshment, AncestorSampling,
+    BackwardSimulation
 using SSMProblems
 using Distributions: MvNormal
 using LinearAlgebra
@@ -186,8 +187,9 @@ function GeneralisedFilters.filter(
 end
 
 # --- filter(rng, model, BF(N; threshold, resampler), ys) --------------------------
-# AuxiliaryParticleFilter(BF(...), MeanPredictive() | ModePredictive()) takes the same
-# call with the lookahead stage on (particles.jl:270-357).
+# AuxiliaryParticleFilter(BF(...), MeanPredictive() | ModePredictive() | DrawPredictive())
+# takes the same call with the lookahead stage on (particles.jl:270-384); the draw comes
+# from the library's own Philox stream, seeded from rng.
 function GeneralisedFilters.filter(
     rng::AbstractRNG,
     model::GeneralisedFilters.LinearGaussianStateSpaceModel,
@@ -196,9 +198,10 @@ function GeneralisedFilters.filter(
     kwargs...,
 )
     pp = algo.weight_strategy.pp
-    pp isa Union{MeanPredictive,ModePredictive} ||
-        throw(ArgumentError("GFB200 builds the mean / mode lookahead only"))
-    return _bf(rng, model, algo.pf, observations, Int32(1); kwargs...)
+    pp isa Union{MeanPredictive,ModePredictive,DrawPredictive} ||
+        throw(ArgumentError("GFB200 builds the mean / mode / draw lookahead only"))
+    return _bf(rng, model, algo.pf, observations, pp isa DrawPredictive ? Int32(2) : Int32(1);
+               kwargs...)
 end
 
 function GeneralisedFilters.filter(

@@ -119,3 +119,41 @@ def test_apf_with_path_storage(ctx):
     np.testing.assert_allclose(st.paths, O.ancestry_paths(ref["ancestors"], ref["states"]),
                                rtol=1e-10, atol=1e-12)
 
+
+
+@pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.STRATIFIED])
+def test_apf_draw_predictive_matches_oracle(ctx, kind):
+    """DrawPredictive (particles.jl:377-384): the lookahead point is one draw from the
+    transition, from its own Philox stream (regenerated by the oracle); in-kernel
+    Philox propagation noise and uniforms, FP64."""
+    rng = np.random.default_rng(90 + kind)
+    m = random_lg(rng, 3, 2)
+    T, N = 8, 2048
+    _, ys = simulate(rng, m, T)
+    algo = G.APF(G.BF(N, threshold=1.0, resampler=RS[kind], precision="f64"), G.DrawPredictive())
+    st, ll = G.filter(m, algo, ys, seed=77, want_ancestors=True, ctx=ctx)
+    ref = O.pf_run(to_oracle(m), N, ys, resampler=kind, threshold=1.0, seed=77, want_ancestors=True,
+                   want_margins=True, lookahead=2)
+    np.testing.assert_array_equal(st.resampled, ref["resampled"])
+    bad, boundary = ancestors_match(st.ancestors, ref["ancestors"], ref["margins"], 1e-9)
+    assert bad == 0
+    np.testing.assert_allclose(st.ll_steps, ref["ll_steps"], atol=1e-9, rtol=0)
+
+
+def test_apf_draw_predictive_converges_to_kf(ctx):
+    rng = np.random.default_rng(1234)
+    m = random_lg(rng, 1, 1)
+    _, ys = simulate(rng, m, 4)
+    st, ll = G.filter(m, G.APF(G.BF(10**6, threshold=1.0), G.DrawPredictive()), ys, seed=5, ctx=ctx)
+    kll = O.kf_filter(to_oracle(m), ys)[0]
+    assert abs(ll - kll) <= 1e-3
+
+
+def test_apf_draw_predictive_needs_bootstrap_proposal(ctx):
+    """The lookahead draw uses the transition covariance; other proposals are refused."""
+    rng = np.random.default_rng(3)
+    m = random_lg(rng, 2, 1)
+    _, ys = simulate(rng, m, 3)
+    pf = G.ParticleFilter(256, G.OverdispersedProposal(k=2.0), precision="f64")
+    with pytest.raises(G.GFError):
+        G.filter(m, G.APF(pf, G.DrawPredictive()), ys, seed=1, ctx=ctx)

@@ -66,10 +66,9 @@ def test_workloads_shapes():
 
 def test_apf_config_and_unbuilt_lookahead():
     """AuxiliaryParticleFilter(pf, MeanPredictive()/ModePredictive()) maps to
-    GF_LOOKAHEAD_MEAN; DrawPredictive is not built."""
+    GF_LOOKAHEAD_MEAN, DrawPredictive() to GF_LOOKAHEAD_DRAW."""
     apf = G.APF(G.BF(100, threshold=0.7), G.MeanPredictive())
     cfg, _, _ = _pf_config(apf.pf, 5, 1, lookahead=apf.weight_strategy.pp.lookahead)
     assert cfg.lookahead == L.GF_LOOKAHEAD_MEAN and cfg.threshold == 0.7
     assert G.APF(G.BF(10), G.ModePredictive()).weight_strategy.pp.lookahead == L.GF_LOOKAHEAD_MEAN
-    with pytest.raises(NotImplementedError):
-        G.APF(G.BF(10), G.DrawPredictive())
+    assert G.APF(G.BF(10), G.DrawPredictive()).weight_strategy.pp.lookahead == L.GF_LOOKAHEAD_DRAW
