@@ -291,8 +291,8 @@ constexpr int TC_THREADS = 128;
 constexpr int TC_SUB = PF_TILE / TC_THREADS;
 // Blocks per tile (each TC_SUB / TC_SPLIT sub-tiles, partials kept per block).
 // One: the per-block prologue (operand-B staging, TMEM allocation) and the
-// partial reduction cost more than a shorter last wave saves (2 measured
-// 16 % slower at Dx=16, N=2^20).
+// partial reduction cost more than shorter waves save (at Dx=16, N=2^20 the
+// propagate took 1.16x, 1.5x and 2.5x as long with 2, 4 and 8 blocks per tile).
 constexpr int TC_SPLIT = 1;
 constexpr int TC_SUB_BLOCK = TC_SUB / TC_SPLIT;
 static_assert(TC_SUB % TC_SPLIT == 0 && TC_SPLIT <= PF_MAX_SPLIT, "tensor-core tile split");
@@ -308,10 +308,16 @@ struct TcLayout {
   static constexpr int Hb_off = B_off + NM * K;
   static constexpr int total = Hb_off + DYP;
   static constexpr size_t smem_bytes = sizeof(float) * (2 * 128 * K + 2 * NM * K + DXP + 2 * DYP);
+  // Resident blocks per SM that shared memory allows (228 KB per SM, 1 KB
+  // reserved per block, ~1 KB of static shared arrays), at most 5: the launch
+  // bound caps registers to match (Dx=16: 91 instead of 156 registers, 5 blocks
+  // per SM instead of 3, propagate 1.2x faster at N=2^20).
+  static constexpr int by_smem = (int)((228u * 1024u) / (smem_bytes + 2048u));
+  static constexpr int min_blocks = by_smem < 1 ? 1 : (by_smem > 5 ? 5 : by_smem);
 };
 
 template <int DXP, int DYP>
-__global__ void __launch_bounds__(TC_THREADS) pf_lg_propagate_tc(const PfJob* __restrict__ jobs,
+__global__ void __launch_bounds__(TC_THREADS, (TcLayout<DXP, DYP>::min_blocks)) pf_lg_propagate_tc(const PfJob* __restrict__ jobs,
                                                                int njobs) {
   using Lay = LgLayout<DXP, DYP>;
   using TL = TcLayout<DXP, DYP>;

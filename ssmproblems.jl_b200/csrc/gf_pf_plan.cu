@@ -210,6 +210,11 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   p->prop_smem = L.smem;
   GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)p->prop_fn,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->prop_smem));
+  // all of the SM's shared memory, so the tensor-core propagate reaches its
+  // register-bound residency (5 blocks per SM at Dx=16)
+  GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)p->prop_fn,
+                                          cudaFuncAttributePreferredSharedMemoryCarveout,
+                                          (int)cudaSharedmemCarveoutMaxShared));
   PfJob& J = p->job;
   J = L.J;
   J.params = p->params;
