@@ -597,7 +597,9 @@ __device__ __forceinline__ void resample_tile(const PfJob& J, int tile) {
 }
 
 template <typename Real>
-__global__ void __launch_bounds__(PF_THREADS, 6) pf_resample_kernel(const PfJob* __restrict__ jobs,
+// 4 blocks per SM: 64 registers, no spills (a bound of 6 spilled at 40 registers
+// and still needed two waves for 1,024 tiles)
+__global__ void __launch_bounds__(PF_THREADS, 4) pf_resample_kernel(const PfJob* __restrict__ jobs,
                                                                    int njobs) {
   const int jb = find_job(jobs, njobs, blockIdx.x, false);
   const PfJob& J = jobs[jb];
