@@ -316,9 +316,12 @@ gf_status gf_ancestors_to_offspring(gf_ctx* ctx, int64_t n, const int64_t* ances
  * GF_ERR_DIM.  All scratch lives in one fixed device array (about 2.1 MB) that
  * every device loading the library holds until the process exits.  The first
  * call on a device resolves that array's address (cudaGetSymbolAddress), so
- * make the first call before any stream capture.  Calls share the array:
- * calls that overlap on the GPU (other streams, other host threads on the
- * same device) race and must be serialised by the caller. */
+ * make the first call before any stream capture.  The address is cached for
+ * the life of the process: no call may follow a cudaDeviceReset of that
+ * device.  Every call reads its status back and waits for `stream`
+ * (cudaStreamSynchronize) before it returns.  Calls share the array: calls
+ * that overlap on the GPU (other streams, other host threads on the same
+ * device) race and must be serialised by the caller. */
 gf_status gf_sample_ancestors_noalloc(int32_t resampler, int32_t convention, int64_t n,
                                       const double* weights_dev, const double* uniforms_dev,
                                       int64_t* ancestors_dev, void* stream);

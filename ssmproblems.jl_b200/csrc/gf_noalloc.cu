@@ -44,7 +44,13 @@ __global__ void sa_setup(const double* __restrict__ part, int nparts, PfScalars*
                          const double* __restrict__ unif, int kind);
 __global__ void sa_search(const PfJob* __restrict__ jobs, int64_t* __restrict__ anc);
 
-// Device address of the scratch array, resolved once per device.
+// Writes the call's job descriptor into the scratch array: the descriptor
+// travels as a kernel argument, so no host-to-device copy from pageable
+// memory is needed.
+__global__ void na_write_job(PfJob job, PfJob* dst) { *dst = job; }
+
+// Device address of the scratch array, resolved once per device and cached
+// for the life of the process (a cudaDeviceReset would leave it stale).
 static std::mutex g_noalloc_mu;
 static void* g_noalloc_ptr[64] = {nullptr};
 
@@ -93,7 +99,7 @@ extern "C" gf_status gf_sample_ancestors_noalloc(int32_t resampler, int32_t conv
   J.unif = uniforms_dev;
   J.wraw = weights_dev;
   J.lw = (void*)weights_dev;  // not read when wraw is set
-  if (cudaMemcpyAsync(&S->job, &J, sizeof J, cudaMemcpyHostToDevice, s) != cudaSuccess) return GF_ERR_CUDA;
+  na_write_job<<<1, 1, 0, s>>>(J, &S->job);
   if (cudaMemsetAsync(S->flags, 0, sizeof(unsigned long long) * 2 * nst, s) != cudaSuccess) return GF_ERR_CUDA;
   sa_partial_sum<<<kNoAllocParts, 256, 0, s>>>(weights_dev, n, S->part);
   sa_setup<<<1, 256, 0, s>>>(S->part, kNoAllocParts, &S->sc, uniforms_dev, resampler);

@@ -665,6 +665,57 @@ __global__ void __launch_bounds__(PF_THREADS, 8) pf_fill_ancestors_kernel(const 
 }
 
 // ------------------------------------------------------------ lookback scan
+// Decoupled lookback of tile b, run by one full warp: publishes the tile's
+// aggregate `tot` (fagg[b]), walks back over the predecessors' inclusive
+// prefixes (finc) or aggregates 32 tiles at a time, publishes the inclusive
+// prefix finc[b] and returns the exclusive prefix.  Every flag carries kReady
+// once written.  A predecessor whose flag stays unset is polled at most
+// `spin_limit` times; then *fail is set (all lanes), finc[b] stays
+// unpublished and the return value is meaningless.
+__device__ __forceinline__ unsigned long long lookback_exclusive(unsigned long long* fagg,
+                                                                 unsigned long long* finc, int b,
+                                                                 unsigned long long tot,
+                                                                 long long spin_limit, bool* fail) {
+  const int lane = threadIdx.x & 31;
+  unsigned long long excl = 0ull;
+  *fail = false;
+  if (b == 0) {
+    if (lane == 0) atomicExch(finc, kReady | tot);
+    return 0ull;
+  }
+  if (lane == 0) atomicExch(fagg + b, kReady | tot);
+  int j = b - 1;
+  long long spins = 0;
+  while (true) {
+    const int k = j - lane;
+    unsigned long long vi = 0ull, va = 0ull;
+    if (k >= 0) {
+      vi = *(volatile unsigned long long*)(finc + k);
+      if (!(vi & kReady)) va = *(volatile unsigned long long*)(fagg + k);
+    }
+    const int st = k < 0 ? 3 : ((vi & kReady) ? 2 : ((va & kReady) ? 1 : 0));
+    const unsigned prefix_mask = __ballot_sync(0xffffffffu, st >= 2);
+    const int stop = prefix_mask ? __ffs(prefix_mask) - 1 : 32;  // first lane holding a prefix
+    const unsigned notready = __ballot_sync(0xffffffffu, st == 0);
+    const unsigned need = stop >= 32 ? 0xffffffffu : ((2u << stop) - 1u);
+    if (notready & need) {
+      if (++spins > spin_limit) {
+        *fail = true;
+        return 0ull;
+      }
+      continue;
+    }
+    unsigned long long val = 0ull;
+    if (lane <= stop && st < 3) val = (st == 2 ? vi : va) & ~kReady;
+    for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
+    excl += val;
+    if (stop < 32) break;
+    j -= 32;
+  }
+  if (lane == 0) atomicExch(finc + b, kReady | (excl + tot));
+  return excl;
+}
+
 // Cumulative normalised weights W_k = sum_{i<=k} exp(lw_i - LSE) for the
 // pending resample.  Each weight is rounded once to 64-bit fixed point (2^-62
 // units); integer sums are associative, so the decoupled lookback's result is
@@ -731,47 +782,16 @@ __global__ void __launch_bounds__(SCAN_THREADS) pf_scan_kernel(const PfJob* __re
   unsigned long long texcl = wpre + x - acc;
   // decoupled lookback (warp 0)
   if (wid == 0) {
-    unsigned long long* fagg = J.flags;
-    unsigned long long* finc = J.flags + J.nstiles;
-    unsigned long long excl = 0ull;
-    if (b == 0) {
-      if (lane == 0) atomicExch(finc, kReady | tot);
-    } else {
-      if (lane == 0) atomicExch(fagg + b, kReady | tot);
-      int j = b - 1;
-      long long spins = 0;
-      while (true) {
-        int k = j - lane;
-        unsigned long long vi = 0ull, va = 0ull;
-        if (k >= 0) {
-          vi = *(volatile unsigned long long*)(finc + k);
-          if (!(vi & kReady)) va = *(volatile unsigned long long*)(fagg + k);
-        }
-        int st = k < 0 ? 3 : ((vi & kReady) ? 2 : ((va & kReady) ? 1 : 0));
-        unsigned prefix_mask = __ballot_sync(0xffffffffu, st >= 2);
-        int stop = prefix_mask ? __ffs(prefix_mask) - 1 : 32;  // first lane holding a prefix
-        unsigned notready = __ballot_sync(0xffffffffu, st == 0);
-        unsigned need = stop >= 32 ? 0xffffffffu : ((2u << stop) - 1u);
-        if (notready & need) {
-          if (++spins > kSpinLimit) {
-            if (lane == 0) {
-              sc->status = GF_ERR_TIMEOUT;
-              s_fail = 1;
-            }
-            break;
-          }
-          continue;
-        }
-        unsigned long long val = 0ull;
-        if (lane <= stop && st < 3) val = (st == 2 ? vi : va) & ~kReady;
-        for (int o = 16; o > 0; o >>= 1) val += __shfl_xor_sync(0xffffffffu, val, o);
-        excl += val;
-        if (stop < 32) break;
-        j -= 32;
+    bool fail = false;
+    const unsigned long long excl = lookback_exclusive(J.flags, J.flags + J.nstiles, b, tot,
+                                                       kSpinLimit, &fail);
+    if (lane == 0) {
+      if (fail) {
+        sc->status = GF_ERR_TIMEOUT;
+        s_fail = 1;
       }
-      if (lane == 0 && !s_fail) atomicExch(finc + b, kReady | (excl + tot));
+      s_excl = excl;
     }
-    if (lane == 0) s_excl = excl;
   }
   __syncthreads();
   if (s_fail) return;

@@ -12,8 +12,7 @@ namespace gf {
 
 __global__ void __launch_bounds__(128) umma_selftest_kernel(const float* __restrict__ A,
                                                           const float* __restrict__ B, float* D,
-                                                          int N, int K, int split3, int swap,
-                                                          int* status) {
+                                                          int N, int K, int split3, int* status) {
   extern __shared__ __align__(128) unsigned char smem[];
   float* sAh = reinterpret_cast<float*>(smem);
   float* sAl = sAh + 128 * K;
@@ -51,14 +50,13 @@ __global__ void __launch_bounds__(128) umma_selftest_kernel(const float* __restr
   const uint32_t tbase = tmem_base;
   if (r == 0) {
     const uint32_t kstride = 128, mstride = (uint32_t)(K / 4) * 128;
-    const uint32_t lbo = swap ? mstride : kstride, sbo = swap ? kstride : mstride;
     const uint32_t idesc = umma::idesc_tf32(128, N);
     for (int s = 0; s < K / 8; ++s) {
       const uint32_t koff = (uint32_t)s * 2 * kstride;
-      const uint64_t ah = umma::desc(umma::smem_u32(sAh) + koff, lbo, sbo);
-      const uint64_t al = umma::desc(umma::smem_u32(sAl) + koff, lbo, sbo);
-      const uint64_t bh = umma::desc(umma::smem_u32(sBh) + koff, lbo, sbo);
-      const uint64_t bl = umma::desc(umma::smem_u32(sBl) + koff, lbo, sbo);
+      const uint64_t ah = umma::desc(umma::smem_u32(sAh) + koff, kstride, mstride);
+      const uint64_t al = umma::desc(umma::smem_u32(sAl) + koff, kstride, mstride);
+      const uint64_t bh = umma::desc(umma::smem_u32(sBh) + koff, kstride, mstride);
+      const uint64_t bl = umma::desc(umma::smem_u32(sBl) + koff, kstride, mstride);
       umma::mma_tf32(tbase, ah, bh, idesc, s > 0 ? 1u : 0u);
       if (split3) {
         umma::mma_tf32(tbase, ah, bl, idesc, 1u);
@@ -89,7 +87,7 @@ __global__ void __launch_bounds__(128) umma_selftest_kernel(const float* __restr
 // Host wrapper: A [128 x K], B [N x K] row-major FP32 host arrays, D [128 x N].
 // K a multiple of 8, N a multiple of 16 in [16, 256].  Returns 0 on success.
 extern "C" int gfx_umma_selftest(const float* A, const float* B, float* D, int N, int K,
-                                 int split3, int swap) {
+                                 int split3) {
   if (K % 8 || N % 16 || N < 16 || N > 256 || K > 256) return 6;
   float *dA, *dB, *dD;
   int* dst;
@@ -103,7 +101,7 @@ extern "C" int gfx_umma_selftest(const float* A, const float* B, float* D, int N
   cudaMemset(dD, 0, sizeof(float) * 128 * N);
   cudaMemset(dst, 0, sizeof(int));
   cudaFuncSetAttribute(gf::umma_selftest_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  gf::umma_selftest_kernel<<<1, 128, smem>>>(dA, dB, dD, N, K, split3, swap, dst);
+  gf::umma_selftest_kernel<<<1, 128, smem>>>(dA, dB, dD, N, K, split3, dst);
   cudaError_t e = cudaDeviceSynchronize();
   int st = 0;
   cudaMemcpy(&st, dst, sizeof(int), cudaMemcpyDeviceToHost);

@@ -27,6 +27,16 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_library_exports_every_diagnostic_symbol():
+    src = open(os.path.join(ROOT, "include", "gf_b200_diag.h")).read()
+    src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
+    names = sorted(set(re.findall(r"\b(gfx_[a-z0-9_]+)\s*\(", src)))
+    assert names == ["gfx_umma_selftest", "gfx_wait_selftest"]
+    from gfb200 import _lib as L
+    lib = C.CDLL(L.LIB_PATH)
+    assert all(hasattr(lib, n) for n in names)
+
+
 def test_python_binding_covers_the_header():
     from gfb200 import _lib as L
     assert sorted(L.EXPORTED) == _declared()

@@ -14,12 +14,12 @@ def test_umma_tf32_tile(ctx, N, K):
     from gfb200 import _lib as L
     lib = C.CDLL(L.LIB_PATH)
     f = lib.gfx_umma_selftest
-    f.argtypes = [C.c_void_p] * 3 + [C.c_int] * 4
+    f.argtypes = [C.c_void_p] * 3 + [C.c_int] * 3
     rng = np.random.default_rng(N + K)
     A = rng.standard_normal((128, K)).astype(np.float32)
     B = rng.standard_normal((N, K)).astype(np.float32)
     ref = A.astype(np.float64) @ B.astype(np.float64).T
     for split, tol in ((1, 2e-6), (0, 2e-3)):
         D = np.zeros((128, N), np.float32)
-        assert f(A.ctypes.data, B.ctypes.data, D.ctypes.data, N, K, split, 0) == 0
+        assert f(A.ctypes.data, B.ctypes.data, D.ctypes.data, N, K, split) == 0
         assert np.abs(D - ref).max() / np.abs(ref).max() < tol
