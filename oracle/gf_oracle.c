@@ -974,6 +974,43 @@ typedef struct {
   const double *H, *c, *R;                               /* obs on inner */
 } or_rb_model;
 
+/* One particle's RBPF move (rbpf.jl:24-84): outer propogate with noise e
+ * (particles.jl:175-245), inner KF predict with (prev_outer, new_outer)
+ * (rbpf.jl:45-55), inner KF update with y; p = [x | mu | Sigma | L] is updated
+ * in place and *inc receives the log-weight increment (proposal ratio plus the
+ * inner predictive log-likelihood).  Returns nonzero if a Cholesky failed. */
+static int rb_particle_step(const or_rb_model* m, const or_proposal* prop, const double* LQo,
+                            const double* Lqo, const double* LR, const double* y, const double* e,
+                            double* p, double* Qt, kf_ws* ws, double* inc_out) {
+  int dxo = m->dxo, dz = m->dz, dy = m->dy;
+  double mx[64], v[64], xn[64], dif[64], tmpd[64], bt[64];
+  double *xo = p, *mu = p + dxo, *Sig = p + dxo + dz, *L = p + dxo + dz + dz * dz;
+  mv(dxo, dxo, m->A_o, xo, mx);
+  for (int d = 0; d < dxo; ++d) mx[d] += m->b_o[d];
+  double inc = 0.0;
+  if (prop->kind == OR_PROP_BOOTSTRAP) {
+    mv(dxo, dxo, LQo, e, v);
+    for (int d = 0; d < dxo; ++d) xn[d] = mx[d] + v[d];
+  } else {
+    mv(dxo, dxo, Lqo, e, v);
+    for (int d = 0; d < dxo; ++d) xn[d] = mx[d] + v[d];
+    for (int d = 0; d < dxo; ++d) dif[d] = xn[d] - mx[d];
+    double lp = logpdf_chol(dxo, LQo, dif, tmpd);
+    double lq = logpdf_chol(dxo, Lqo, dif, tmpd);
+    inc = lp - lq;
+  }
+  mv(dz, dxo, m->C_z, xo, bt);
+  for (int d = 0; d < dz; ++d) bt[d] += m->b_z[d];
+  double qs = exp(m->q_gamma * xn[m->q_index]);
+  for (int k = 0; k < dz * dz; ++k) Qt[k] = m->Q_z[k] * qs;
+  int s1 = kf_predict(dz, m->A_z, bt, Qt, mu, Sig, L, ws);
+  double lin = 0.0;
+  int s2 = s1 ? s1 : kf_update(dz, dy, m->H, m->c, m->R, LR, y, 0.0, 0, mu, Sig, L, &lin, ws);
+  memcpy(xo, xn, 8 * dxo);
+  *inc_out = inc + lin;
+  return s2;
+}
+
 int or_rbpf_run(const or_rb_model* m, const or_proposal* prop, const or_resample_cfg* rc, long N,
                 int T, const double* ys, const double* noise, const double* uniforms,
                 uint64_t seed, double* ll, or_pf_out* out, double* zmeans /* T*dz */) {
@@ -1028,36 +1065,12 @@ int or_rbpf_run(const or_rb_model* m, const or_proposal* prop, const or_resample
     double* Qt = malloc(sizeof(double) * dz * dz);
 #pragma omp for schedule(static)
     for (long i = 0; i < N; ++i) {
-      double e[64], mx[64], v[64], xn[64], dif[64], tmpd[64], bt[64];
-      double* p = S + (size_t)i * width;
-      double *xo = p, *mu = p + dxo, *Sig = p + dxo + dz, *L = p + dxo + dz + dz * dz;
+      double e[64];
       draw_normals(noise, seed, dxo, N, t, i, e);
-      /* outer propogate (particles.jl:175-245) */
-      mv(dxo, dxo, m->A_o, xo, mx);
-      for (int d = 0; d < dxo; ++d) mx[d] += m->b_o[d];
       double inc = 0.0;
-      if (prop->kind == OR_PROP_BOOTSTRAP) {
-        mv(dxo, dxo, LQo, e, v);
-        for (int d = 0; d < dxo; ++d) xn[d] = mx[d] + v[d];
-      } else {
-        mv(dxo, dxo, Lqo, e, v);
-        for (int d = 0; d < dxo; ++d) xn[d] = mx[d] + v[d];
-        for (int d = 0; d < dxo; ++d) dif[d] = xn[d] - mx[d];
-        double lp = logpdf_chol(dxo, LQo, dif, tmpd);
-        double lq = logpdf_chol(dxo, Lqo, dif, tmpd);
-        inc = lp - lq;
-      }
-      /* inner predict with prev_outer = xo, new_outer = xn (rbpf.jl:45-55) */
-      mv(dz, dxo, m->C_z, xo, bt);
-      for (int d = 0; d < dz; ++d) bt[d] += m->b_z[d];
-      double qs = exp(m->q_gamma * xn[m->q_index]);
-      for (int k = 0; k < dz * dz; ++k) Qt[k] = m->Q_z[k] * qs;
-      int s1 = kf_predict(dz, m->A_z, bt, Qt, mu, Sig, L, &ws);
-      double lin = 0.0;
-      int s2 = s1 ? s1 : kf_update(dz, dy, m->H, m->c, m->R, LR, y, 0.0, 0, mu, Sig, L, &lin, &ws);
-      if (s2) fail |= 1;
-      memcpy(xo, xn, 8 * dxo);
-      logw[i] = logw[i] + inc + lin;
+      if (rb_particle_step(m, prop, LQo, Lqo, LR, y, e, S + (size_t)i * width, Qt, &ws, &inc))
+        fail |= 1;
+      logw[i] = logw[i] + inc;
     }
     free(Qt);
     kf_ws_free(&ws);
@@ -1092,6 +1105,64 @@ done:
   *ll = tot;
   free(S); free(Stmp); free(logw); free(wbuf); free(ubuf);
   free(Lo0); free(LQo); free(Lqo); free(LZ0); free(LR);
+  return st;
+}
+
+/* One bootstrap RBPF step from a given state (teacher forcing for the FP32
+ * bank's parity checks): maybe_resample with this step's uniforms u, then
+ * rb_particle_step for every particle with noise_t ([dxo][N]), the baseline and
+ * LSE accounting of or_rbpf_run.  state: [N][dxo + dz + dz*dz] (x, mu, Sigma
+ * column-major) in and out; logw [N] normalised, in and out; `uniform` marks
+ * the initial TypelessZero weights. */
+int or_rbpf_step(const or_rb_model* m, const or_resample_cfg* rc, long N, const double* y,
+                 const double* noise_t, const double* u, int uniform, double* state,
+                 double* logw, int32_t* anc, double* margins, double* ess, int8_t* resampled,
+                 double* ll_inc) {
+  int dxo = m->dxo, dz = m->dz, dy = m->dy;
+  int w_in = dxo + dz + dz * dz, width = w_in + dz * dz;
+  double* S = malloc(sizeof(double) * N * width);
+  double* Stmp = malloc(sizeof(double) * N * width);
+  double* wbuf = malloc(sizeof(double) * N);
+  double* ubuf = malloc(sizeof(double) * N);
+  double *LQo = calloc(dxo * dxo, 8), *LR = calloc(dy * dy, 8);
+  or_proposal boot = {OR_PROP_BOOTSTRAP, 1.0};
+  int st = OR_OK, fail = 0;
+  long clamps = 0;
+  if ((st = or_chol_lower(dxo, m->Q_o, LQo)) || (st = or_chol_lower(dy, m->R, LR))) goto done;
+  for (long i = 0; i < N && !st; ++i) {
+    double* p = S + (size_t)i * width;
+    memcpy(p, state + (size_t)i * w_in, sizeof(double) * w_in);
+    st = or_chol_lower(dz, p + dxo + dz, p + w_in);
+  }
+  if (st) goto done;
+  {
+    or_resample_cfg rc1 = *rc;
+    int8_t sch = rc->schedule ? rc->schedule[0] : -1;
+    rc1.schedule = &sch;
+    int was_uniform = uniform;
+    int res = maybe_resample(&rc1, 1, N, width, S, Stmp, logw, &uniform, wbuf, ubuf, u, 0, anc,
+                             margins, ess, &clamps);
+    *resampled = (int8_t)res;
+    double baseline = (was_uniform && !res) ? log((double)N) : or_logsumexp(logw, N);
+    kf_ws ws = kf_ws_alloc(dz, dy);
+    double* Qt = malloc(sizeof(double) * dz * dz);
+    for (long i = 0; i < N; ++i) {
+      double e[64], inc = 0.0;
+      for (int d = 0; d < dxo; ++d) e[d] = noise_t[(size_t)d * N + i];
+      if (rb_particle_step(m, &boot, LQo, NULL, LR, y, e, S + (size_t)i * width, Qt, &ws, &inc))
+        fail = 1;
+      logw[i] += inc;
+    }
+    free(Qt);
+    kf_ws_free(&ws);
+    if (fail) { st = OR_NOT_PD; goto done; }
+    double lse = or_logsumexp(logw, N);
+    for (long i = 0; i < N; ++i) logw[i] -= lse;
+    *ll_inc = lse - baseline;
+    for (long i = 0; i < N; ++i) memcpy(state + (size_t)i * w_in, S + (size_t)i * width, sizeof(double) * w_in);
+  }
+done:
+  free(S); free(Stmp); free(wbuf); free(ubuf); free(LQo); free(LR);
   return st;
 }
 

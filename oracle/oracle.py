@@ -364,6 +364,38 @@ def rbpf_run(m: RBModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshol
     return out
 
 
+def rbpf_step(m: RBModel, x, mu, Sigma, logw, y, noise_t, u, *, uniform=False,
+              resampler=SYSTEMATIC, conv=CONV_CPU, threshold=0.5, decision=-1):
+    """One bootstrap RBPF step from a given state (teacher forcing).  x [N, dxo],
+    mu [N, dz], Sigma [N, dz, dz]; logw [N] normalised; noise_t [dxo, N]; u this
+    step's uniforms.  Returns the new x, mu, Sigma, logw and the step's
+    ancestors (1-based), margins, ESS, decision and ll increment."""
+    N, dxo, dz = x.shape[0], m.dxo, m.dz
+    w_in = dxo + dz + dz * dz
+    S = np.empty((N, w_in))
+    S[:, :dxo] = x
+    S[:, dxo:dxo + dz] = mu
+    S[:, dxo + dz:] = np.asarray(Sigma, np.float64).transpose(0, 2, 1).reshape(N, dz * dz)
+    S = np.ascontiguousarray(S)
+    logw = np.ascontiguousarray(logw, np.float64).copy()
+    anc = np.zeros(N, np.int32)
+    mar = np.zeros(N)
+    ess, res, inc = C.c_double(), C.c_int8(), C.c_double()
+    sched = np.array([decision], np.int8)
+    rc = _RC(resampler, conv, threshold, sched.ctypes.data_as(C.POINTER(C.c_int8)))
+    un = _f64(np.atleast_1d(u))
+    st = lib().or_rbpf_step(C.byref(m._struct()), C.byref(rc), C.c_long(N),
+                            _p(_f64(y).ravel()), _p(_f64(noise_t)), _p(un), int(uniform), _p(S),
+                            _p(logw), anc.ctypes.data_as(C.POINTER(C.c_int32)), _p(mar),
+                            C.byref(ess), C.byref(res), C.byref(inc))
+    if st:
+        raise np.linalg.LinAlgError(f"oracle RBPF step status {st}")
+    Sig = S[:, dxo + dz:].reshape(N, dz, dz).transpose(0, 2, 1)
+    return dict(x=S[:, :dxo].copy(), mu=S[:, dxo:dxo + dz].copy(), Sigma=Sig.copy(), logw=logw,
+                ancestors=anc, margins=mar, ess=ess.value, resampled=bool(res.value),
+                ll_inc=inc.value)
+
+
 # --------------------------------------------------------------------------- #
 # numpy restatements of the reference's test fixtures                          #
 # --------------------------------------------------------------------------- #

@@ -292,3 +292,40 @@ def test_two_filter_smoother_equals_rts(Dy):
     _, mr, Sr = O.rts_smooth(m, ys)
     np.testing.assert_allclose(mus, mr, rtol=1e-7, atol=1e-9)
     np.testing.assert_allclose(Ss, Sr, rtol=1e-7, atol=1e-9)
+
+
+@pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.MULTINOMIAL])
+def test_rbpf_step_chain_equals_rbpf_run(kind):
+    """The teacher-forcing step (or_rbpf_step) chained from the prior draw
+    reproduces the full oracle RBPF run (or_rbpf_run) with ESS-triggered
+    resampling: same decisions, ancestors, ll increments and final state."""
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                    "ssmproblems.jl_b200"))
+    from gfb200 import workloads as W
+    from helpers import to_oracle_rb
+    hier, ys = W.rb_trend(seed=4, T=25, dz=4, dy=2)
+    om = to_oracle_rb(hier)
+    N, T = 400, 25
+    rng = np.random.default_rng(3)
+    noise = rng.standard_normal((T + 1, om.dxo, N))
+    unif = rng.random(T) if kind == O.SYSTEMATIC else rng.random((T, N))
+    ref = O.rbpf_run(om, N, ys, resampler=kind, threshold=0.9, noise=noise, uniforms=unif,
+                     want_ancestors=True)
+    x = (om.mu_o[:, None] + np.linalg.cholesky(om.Sigma_o) @ noise[0]).T
+    mu = np.tile(om.mu_z, (N, 1))
+    Sig = np.tile(om.Sigma_z, (N, 1, 1))
+    logw = np.zeros(N)
+    for t in range(1, T + 1):
+        r = O.rbpf_step(om, x, mu, Sig, logw, ys[t - 1], noise[t], unif[t - 1], uniform=t == 1,
+                        resampler=kind, threshold=0.9)
+        assert r["resampled"] == bool(ref["resampled"][t - 1])
+        np.testing.assert_array_equal(r["ancestors"], ref["ancestors"][t - 1])
+        assert abs(r["ll_inc"] - ref["ll_steps"][t - 1]) < 1e-10
+        x, mu, Sig, logw = r["x"], r["mu"], r["Sigma"], r["logw"]
+    assert ref["resampled"].sum() >= 3
+    dz = om.dz
+    xf = ref["x_final"]
+    np.testing.assert_allclose(x, xf[:, :om.dxo], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(mu, xf[:, om.dxo:om.dxo + dz], rtol=1e-10, atol=1e-12)
+    np.testing.assert_allclose(logw, ref["logw_final"], atol=1e-10)
