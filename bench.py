@@ -4,7 +4,12 @@ Default workload (the large bootstrap-PF configuration): LGSSM with Dx=16,
 Dy=8, A random orthogonal * 0.95, Q = 0.1 I, H_ij ~ N(0, 1/Dx), R = 0.2 I,
 N = 2^20 particles in FP32 SoA, T = 1000, systematic resampling when
 ESS < 0.5 N, FP64 normaliser and cumulative weights, in-kernel Philox noise.
-One step = one full filter run (N * T particle-steps).
+One step = one full filter run (N * T particle-steps).  The line also carries
+`parity` (the estimate against the exact Kalman log-likelihood in Monte-Carlo
+standard deviations; a full-N teacher-forced check of the first steps against
+the FP64 oracle with ancestor boundary counts), the 16-thread and
+single-thread CPU baselines, and `secondary`: the batched Kalman bank (65,536
+uneven filters) and the serving loop at 200 and 1000 req/s from the same process.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
                     [--workload pf|pf1d|kf|smooth|rbpf|serve|csmc|kfgrad]
@@ -142,6 +147,100 @@ def cpu_baseline_pf(model, ys, N, seconds=12.0, threads=None):
                       f"{threads} OpenMP threads (serial cumsum/LSE as in the reference)"}
 
 
+def pf_parity(ctx, model, ys, N, ll_timed, seeds=8, tf_steps=4):
+    """Accuracy of the headline configuration against FP64 (outside the timed
+    region): (1) the log-likelihood estimate against the exact Kalman value, in
+    Monte-Carlo standard deviations of the estimate over `seeds` independent
+    runs; (2) teacher forcing at full N: one run of the first `tf_steps` steps
+    records every state, then each step is re-done by the FP64 oracle from the
+    GPU's own previous state with the same injected noise and uniforms."""
+    import torch
+    import gfb200 as G
+    from gfb200.plans import PfPlan
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle as O
+    O.build()
+    om = O.LGModel(model.prior.mu0, model.prior.Sigma0, model.dyn.A, model.dyn.b, model.dyn.Q,
+                   model.obs.H, model.obs.c, model.obs.R)
+    T = len(ys)
+    ll_kf = O.kf_filter(om, ys)[0]
+    algo = G.BF(N, threshold=0.5)
+    ys_dev = torch.tensor(ys, dtype=torch.float64, device=f"cuda:{ctx.device}")
+    lls = []
+    for s in range(seeds):
+        p = PfPlan(model, algo, T, seed=5000 + s, ctx=ctx, graph=True)
+        p.run(ys_dev)
+        ctx.synchronize()
+        lls.append(float(p.ll.item()))
+        p.close()
+    lls = np.array(lls)
+    sd = float(lls.std(ddof=1))
+    # teacher forcing at full N
+    rng = np.random.default_rng(77)
+    Tt = tf_steps
+    dx = model.dyn.A.shape[0]
+    noise = rng.standard_normal((Tt + 1, dx, N)).astype(np.float32)
+    unif = rng.random(Tt)
+    cb = G.DenseAncestorCallback()
+    st, _ = G.filter(model, algo, ys[:Tt], noise=noise, uniforms=unif, callback=cb, ctx=ctx)
+    hist, lwh, anc = cb.container._hist, cb.container.weights, cb.container.ancestors
+    err_x = err_ll = 0.0
+    bad = boundary = slots = n_res = 0
+    for t in range(1, Tt + 1):
+        ref = O.pf_step(om, hist[t - 1].T.astype(np.float64), np.zeros(N) if t == 1 else lwh[t - 2],
+                        ys[t - 1], noise[t].astype(np.float64), unif[t - 1], uniform=t == 1,
+                        threshold=0.5)
+        n_res += int(ref["resampled"])
+        diff = anc[t - 1] != ref["ancestors"]
+        inside = ref["margins"] <= 1e-8
+        bad += int(np.sum(diff & ~inside))
+        boundary += int(np.sum(diff & inside))
+        slots += N if ref["resampled"] else 0
+        if not diff.any():
+            err_x = max(err_x, float(np.max(np.abs(hist[t].T - ref["x"]) / (np.abs(ref["x"]) + 1.0))))
+        err_ll = max(err_ll, abs(float(st.ll_steps[t - 1]) - ref["ll_inc"]))
+    return {
+        "ll_kf_exact": ll_kf, "ll_timed_run": ll_timed,
+        "ll_pf_mean": float(lls.mean()), "ll_pf_sd": sd, "ll_runs": seeds,
+        "ll_dev_in_sd": (ll_timed - ll_kf) / sd if sd > 0 else None,
+        "ll_mean_dev_in_se": (float(lls.mean()) - ll_kf) / (sd / np.sqrt(seeds)) if sd > 0 else None,
+        # log Z-hat is biased low by about Var(log Z-hat) / 2 (Z-hat unbiased and
+        # near log-normal): the mean's deviation after that correction
+        "ll_mean_dev_bias_corrected_in_se":
+            (float(lls.mean()) + sd * sd / 2 - ll_kf) / (sd / np.sqrt(seeds)) if sd > 0 else None,
+        "teacher_forced": {"N": N, "steps": Tt, "resampling_steps": n_res,
+                           "state_max_err_rel_plus_1": err_x, "ll_inc_max_abs_err": err_ll,
+                           "ancestor_mismatches_outside_1e-8_band": bad,
+                           "ancestor_boundary_cases": boundary, "ancestor_slots_checked": slots,
+                           "oracle": "FP64 C restatement of the reference PF step"},
+    }
+
+
+def _secondary(args, world, rank, local):
+    """The other halves of the metric, from the same process: the batched
+    Kalman bank (config 3) and the serving loop at stated request rates."""
+    import copy
+    out = {}
+    a = copy.copy(args)
+    a.steps, a.warmup = 2, 3
+    kf = bench_kf(a, world, rank, local, accuracy_sample=32)
+    out["kf_bank"] = {k: kf[k] for k in ("metric", "value", "unit", "ms_per_step", "config",
+                                          "roofline", "plain_form_kf_steps_per_s",
+                                          "batched_over_plain", "accuracy", "clocks")}
+    out["serving"] = []
+    for rate, reqs in ((200.0, 1000), (1000.0, 2000)):
+        a = copy.copy(args)
+        a.steps, a.warmup, a.serve_rate, a.serve_requests = 1, 1, rate, reqs
+        sv = bench_serve(a, world, rank, local)
+        out["serving"].append({"offered_req_s": sv["config"]["offered_req_s"],
+                               "served_req_s": sv["value"], "latency_ms": sv["latency_ms"],
+                               "completed": sv["completed"], "failed": sv["failed"],
+                               "kf_steps_per_s": sv["kf_steps_per_s"],
+                               "particle_steps_per_s": sv["particle_steps_per_s"],
+                               "workload": sv["config"]["workload"]})
+    return out
+
+
 def bench_pf(args, world, rank, local):
     import torch
     import gfb200 as G
@@ -263,13 +362,19 @@ def bench_pf(args, world, rank, local):
         "clocks": clk.summary(),
     }
     plan.close()
+    if rank == 0 and not args.no_parity:
+        line["parity"] = pf_parity(ctx, model, ys, N, ll)
     if rank == 0 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline_pf(model, ys, N, seconds=args.cpu_seconds)
+        line["cpu_baseline_single_thread"] = cpu_baseline_pf(model, ys, N, seconds=args.cpu_seconds,
+                                                             threads=1)
     ctx.close()
+    if not args.no_secondary:
+        line["secondary"] = _secondary(args, world, rank, local)
     return line
 
 
-def bench_kf(args, world, rank, local):
+def bench_kf(args, world, rank, local, accuracy_sample=0):
     """Batched Kalman filters: 65536 uneven LGSSMs (Dx 2..32, Dy 1..Dx, T 64..2048),
     per-step ll / mean / covariance outputs, one graph-captured persistent plan
     with autotuned block sizes; the plain one-launch-per-filter form is timed on a
@@ -329,6 +434,26 @@ def bench_kf(args, world, rank, local):
     p1.synchronize()
     plain_value = pplan.n_steps / (p0.elapsed_time(p1) / 1e3)
     pplan.close()
+    accuracy = None
+    if accuracy_sample and rank == 0:
+        # the timed run's own outputs for a sample of filters against the FP64
+        # oracle fed the same observations
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import oracle as O
+        ys_h = ys.cpu().numpy()
+        ll_h = plan.ll.cpu().numpy()
+        offs = np.concatenate([[0], np.cumsum([t * m.dy for t, m in zip(Ts, models)])])
+        worst = 0.0
+        pick = np.random.default_rng(1).choice(B, min(accuracy_sample, B), replace=False)
+        for f in pick:
+            m = models[f]
+            om = O.LGModel(m.prior.mu0, m.prior.Sigma0, m.dyn.A, m.dyn.b, m.dyn.Q, m.obs.H,
+                           m.obs.c, m.obs.R)
+            yf = ys_h[offs[f]:offs[f + 1]].reshape(Ts[f], m.dy)
+            rll = O.kf_filter(om, yf, algo=args.kf_algo)[0]
+            worst = max(worst, abs(ll_h[f] - rll) / max(1.0, abs(rll)))
+        accuracy = {"filters_checked": int(len(pick)), "max_rel_ll_err_vs_fp64": worst,
+                    "bar": "|d ll| / max(1, |ll|) <= 1e-4"}
     line = {
         "metric": "KF-steps/s", "value": value, "unit": "KF-steps/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms / args.steps,
@@ -341,9 +466,11 @@ def bench_kf(args, world, rank, local):
         "roofline": {"bound": "hbm", "achieved": bytes_run / run_s / 1e9, "peak": peak, "unit": "GB/s",
                      "frac": bytes_run / run_s / 1e9 / peak, "traffic": None,
                      "fp32_tflops": flops_run / run_s / 1e12, "fp32_nominal_tflops": 74.4,
+                     "fp32_frac_of_nominal": flops_run / run_s / 1e12 / 74.4,
                      "peak_source": peak_kind},
         "plain_form_kf_steps_per_s": plain_value,
         "batched_over_plain": value / world / plain_value,
+        "accuracy": accuracy,
         "clocks": clk.summary(),
     }
     plan.close()
@@ -1011,6 +1138,10 @@ def main():
                     help="time steps of the PF workload (smaller only for profiler captures)")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-parity", action="store_true",
+                    help="skip the accuracy block of the PF line (profiler captures)")
+    ap.add_argument("--no-secondary", action="store_true",
+                    help="skip the KF-bank and serving entries of the PF line")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3)
     world, rank, local = _dist_setup(args)
