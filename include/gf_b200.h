@@ -174,6 +174,22 @@ gf_status gf_kf_batch(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int3
                       const int32_t* T, const double* ys, double jitter, int32_t use_jitter,
                       int32_t memspace, gf_kf_out* out);
 
+/* Time-varying (non-homogeneous) models: calc_params(dyn, t) and
+ * calc_params(obs, t) of models/linear_gaussian.jl:44-63 changing with t, as
+ * GFTest's NonHomogeneousLinearGaussianLatentDynamics / ObservationProcess
+ * (GFTest/models/linear_gaussian.jl:42-95).  param_steps[f] = 1 runs model f as
+ * gf_kf_batch does; param_steps[f] >= T[f] means the A, b, Q, H, c, R pointers
+ * of models[f] each hold param_steps[f] consecutive per-step blocks (block t-1
+ * = step t, each column-major) and step t uses block t-1.  Time-varying models
+ * run with GF_ALGO_KF (GF_ALGO_SRKF returns GF_ERR_UNSUPPORTED); the smoother's
+ * prediction from t to t+1 uses step t+1's parameters (kalman.jl:89-126). */
+gf_status gf_kf_batch_tv(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
+                         const int32_t* T, const int32_t* param_steps, const double* ys,
+                         double jitter, int32_t use_jitter, int32_t memspace, gf_kf_out* out);
+gf_status gf_kf_smooth_tv(gf_ctx* ctx, const gf_lg_model* models, int32_t B, const int32_t* T,
+                          const int32_t* param_steps, const double* ys, int32_t memspace,
+                          gf_kf_out* out);
+
 /* Gradients of kf_loglikelihood (integrations/logdensity.jl:136-161) for B
  * homogeneous models: the ChainRules pullback (integrations/kalman_rrule.jl:
  * 22-107, step rules kalman_gradient.jl:89-263) with Delta ll = 1, summed over
@@ -234,6 +250,10 @@ typedef struct gf_kf_plan gf_kf_plan;
 gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
                             const int32_t* T, double jitter, int32_t use_jitter,
                             int32_t flags, gf_kf_plan** out);
+/* The same over time-varying models (param_steps as in gf_kf_batch_tv). */
+gf_status gf_kf_plan_create_tv(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
+                               const int32_t* T, const int32_t* param_steps, double jitter,
+                               int32_t use_jitter, int32_t flags, gf_kf_plan** out);
 gf_status gf_kf_plan_run(gf_kf_plan* plan, const double* ys_dev, gf_kf_out* out_dev);
 /* Forward run plus the RTS pass (as gf_kf_smooth) on a KalmanFilter() plan
  * without jitter; out_dev->means and covs receive the smoothed moments. */
@@ -244,8 +264,11 @@ gf_status gf_kf_plan_destroy(gf_kf_plan* plan);
  * (KF: one launch per filter, the unbatched baseline form), SIMT (PF: keep the
  * CUDA-core propagation even where the tensor-core path applies), NO_FUSE (PF:
  * run filters of N <= 1024 as separate kernels per step instead of one block
- * for the whole filter). */
-enum { GF_PLAN_AUTOTUNE = 1, GF_PLAN_NO_GRAPH = 2, GF_PLAN_PLAIN = 4, GF_PLAN_SIMT = 8, GF_PLAN_NO_FUSE = 16 };
+ * for the whole filter), STAGED_GATHER (PF, Dx <= 16 on the tensor-core path:
+ * copy each 128-particle sub-tile's sorted ancestor range into shared memory
+ * with bulk async copies, one sub-tile ahead, instead of per-thread loads). */
+enum { GF_PLAN_AUTOTUNE = 1, GF_PLAN_NO_GRAPH = 2, GF_PLAN_PLAIN = 4, GF_PLAN_SIMT = 8, GF_PLAN_NO_FUSE = 16,
+       GF_PLAN_STAGED_GATHER = 32 };
 
 /* -------------------------------------------------------- particle filters */
 /* filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys)

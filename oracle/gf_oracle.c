@@ -311,10 +311,28 @@ static double ess_of(const double* w, long n) { return 1.0 / pairwise_sum(w, 0, 
 
 /* ------------------------------------------------------------------------ */
 /* Kalman filter (kalman.jl:23-79, kalman_gradient.jl:12-29), FP64.         */
+/* tv = 0: homogeneous (one A, b, Q, H, c, R).  tv = 1: non-homogeneous, the
+ * parameters calc_params(dyn, t), calc_params(obs, t) of every step t = 1..T
+ * (models/linear_gaussian.jl:44-63; GFTest NonHomogeneousLinearGaussian*,
+ * GFTest/models/linear_gaussian.jl:42-95) stored step-major, block t-1 of
+ * each array column-major. */
 typedef struct {
   int dx, dy;
   const double *mu0, *Sigma0, *A, *b, *Q, *H, *c, *R;
+  int tv;
 } or_lg_model;
+
+/* Parameters of 0-based step s (1-based step s + 1). */
+typedef struct {
+  const double *A, *b, *Q, *H, *c, *R;
+} or_step_params;
+static or_step_params step_params(const or_lg_model* m, int s) {
+  const size_t k = m->tv ? (size_t)s : 0;
+  const size_t dx = m->dx, dy = m->dy;
+  or_step_params p = {m->A + k * dx * dx, m->b + k * dx, m->Q + k * dx * dx,
+                      m->H + k * dy * dx, m->c + k * dy, m->R + k * dy * dy};
+  return p;
+}
 
 typedef struct { /* workspace for one KF step */
   double *L, *Lp, *LR, *LS, *tmp, *tmp2, *Sp, *PHt, *S, *K, *IKH, *Sraw, *z, *w;
@@ -406,8 +424,10 @@ int or_kf_filter(const or_lg_model* m, int T, const double* ys, double jitter, i
   if ((st = or_chol_lower(dx, Sig, L)) || (st = or_chol_lower(dy, m->R, LR))) goto done;
   for (int t = 0; t < T; ++t) {
     double l = 0.0;
-    if ((st = kf_predict(dx, m->A, m->b, m->Q, mu, Sig, L, &ws))) break;
-    if ((st = kf_update(dx, dy, m->H, m->c, m->R, LR, ys + (size_t)t * dy, jitter, use_jitter,
+    const or_step_params P = step_params(m, t);
+    if (m->tv && t > 0 && (st = or_chol_lower(dy, P.R, LR))) break;
+    if ((st = kf_predict(dx, P.A, P.b, P.Q, mu, Sig, L, &ws))) break;
+    if ((st = kf_update(dx, dy, P.H, P.c, P.R, LR, ys + (size_t)t * dy, jitter, use_jitter,
                         mu, Sig, L, &l, &ws)))
       break;
     tot += l;
@@ -440,8 +460,10 @@ int or_rts_smooth(const or_lg_model* m, int T, const double* ys, double* ll, dou
   double *mp = malloc(8 * dx), *d = malloc(8 * dx), *ms = malloc(8 * dx);
   double *T1 = malloc(8 * n2), *Sp = malloc(8 * n2), *L = malloc(8 * n2), *X = malloc(8 * n2);
   double *D = malloc(8 * n2), *T2 = malloc(8 * n2), *Ss = malloc(8 * n2);
-  const double *A = m->A, *b = m->b, *Q = m->Q;
   for (int t = T - 2; t >= 0 && !st; --t) {
+    /* the prediction from t to t + 1 uses the parameters of step t + 1 */
+    const or_step_params P = step_params(m, t + 1);
+    const double *A = P.A, *b = P.b, *Q = P.Q;
     const double* mf = mus + (size_t)t * dx;
     const double* Sf = Sigmas + (size_t)t * n2;
     const double* mn = mus + (size_t)(t + 1) * dx;   /* smoothed at t+1 */
@@ -671,6 +693,19 @@ static void draw_normals(const double* noise, uint64_t seed, int dx, long N, int
     }
   }
 }
+/* The linear-Gaussian particle filter's noise: as draw_normals, except that a
+ * one-dimensional state takes normal i % 4 of the call (i / 4, t, 0) (the
+ * library's 1-D layout: one Philox call serves four particles). */
+static void draw_normals_lg(const double* noise, uint64_t seed, int dx, long N, int t, long i,
+                            double* e) {
+  if (noise || dx != 1) {
+    draw_normals(noise, seed, dx, N, t, i, e);
+  } else {
+    double buf[4];
+    or_philox_normals4(seed, (uint32_t)(i >> 2), (uint32_t)t, 0u, buf);
+    e[0] = buf[i & 3];
+  }
+}
 static void draw_uniforms(const double* uniforms, uint64_t seed, int kind, long N, int t,
                           double* u) {
   /* t is 1-based step index; injected layout: systematic [T], else [T][N] */
@@ -770,7 +805,7 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
   /* initialise (particles.jl:36-50): x ~ MvNormal(mu0, Sigma0) */
   for (long i = 0; i < N; ++i) {
     double e[64], v[64];
-    draw_normals(noise, seed, dx, N, 0, i, e);
+    draw_normals_lg(noise, seed, dx, N, 0, i, e);
     mv(dx, dx, L0, e, v);
     for (int d = 0; d < dx; ++d) x[(size_t)i * dx + d] = m->mu0[d] + v[d];
   }
@@ -849,7 +884,7 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
     for (long i = 0; i < N; ++i) {
       double e[64], mx[64], v[64], xn[64], tmpd[64], dif[64];
       double* xi = x + (size_t)i * dx;
-      draw_normals(noise, seed, dx, N, t, i, e);
+      draw_normals_lg(noise, seed, dx, N, t, i, e);
       mv(dx, dx, m->A, xi, mx);
       for (int d = 0; d < dx; ++d) mx[d] += m->b[d]; /* A x + b */
       double inc = 0.0;

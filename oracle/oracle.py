@@ -73,7 +73,7 @@ def _fortran(a):
 
 class _LG(C.Structure):
     _fields_ = [("dx", C.c_int), ("dy", C.c_int)] + [
-        (n, _dp) for n in ("mu0", "Sigma0", "A", "b", "Q", "H", "c", "R")]
+        (n, _dp) for n in ("mu0", "Sigma0", "A", "b", "Q", "H", "c", "R")] + [("tv", C.c_int)]
 
 
 class _RC(C.Structure):
@@ -109,10 +109,40 @@ class LGModel:
         self.Sigma0, self.A, self.Q = _fortran(Sigma0), _fortran(A), _fortran(Q)
         self.H, self.R = _fortran(np.atleast_2d(H)), _fortran(np.atleast_2d(R))
         self.dx, self.dy = self.A.shape[0], self.H.shape[0]
+        self.tv = False
+
+    @classmethod
+    def time_varying(cls, mu0, Sigma0, As, bs, Qs, Hs, cs, Rs):
+        """Non-homogeneous model (GFTest/models/linear_gaussian.jl:42-95): the
+        parameters of steps 1..T as sequences; params(t) returns step t's."""
+        m = cls(mu0, Sigma0, As[0], bs[0], Qs[0], Hs[0], cs[0], Rs[0])
+        m.tv = True
+        m.steps = len(As)
+        m.As = [_fortran(a) for a in As]
+        m.bs = [_f64(v).ravel() for v in bs]
+        m.Qs = [_fortran(q) for q in Qs]
+        m.Hs = [_fortran(np.atleast_2d(h)) for h in Hs]
+        m.cs = [_f64(v).ravel() for v in cs]
+        m.Rs = [_fortran(np.atleast_2d(r)) for r in Rs]
+        # step-major blocks, each column-major (the C oracle's tv layout)
+        m._stk = {n: np.ascontiguousarray(np.concatenate([np.asarray(x).ravel(order="F")
+                                                          for x in getattr(m, n + "s")]))
+                  for n in ("A", "b", "Q", "H", "c", "R")}
+        return m
+
+    def params(self, t):
+        """(A, b, Q, H, c, R) of 1-based step t (calc_params(dyn, t), calc_params(obs, t))."""
+        if not self.tv:
+            return self.A, self.b, self.Q, self.H, self.c, self.R
+        k = t - 1
+        return self.As[k], self.bs[k], self.Qs[k], self.Hs[k], self.cs[k], self.Rs[k]
 
     def _struct(self):
+        if self.tv:
+            arrs = [self.mu0, self.Sigma0] + [self._stk[n] for n in ("A", "b", "Q", "H", "c", "R")]
+            return _LG(self.dx, self.dy, *[_p(a) for a in arrs], 1)
         s = _LG(self.dx, self.dy, *[_p(getattr(self, n)) for n in
-                                    ("mu0", "Sigma0", "A", "b", "Q", "H", "c", "R")])
+                                    ("mu0", "Sigma0", "A", "b", "Q", "H", "c", "R")], 0)
         return s
 
 
@@ -289,9 +319,17 @@ def ancestors_to_offspring(ancestors):
 
 
 def philox_normals(seed, N, dx, t):
-    """[dx, N] normals of step t from the shared Philox stream (FP64 Box-Muller)."""
+    """[dx, N] normals of step t from the shared Philox stream (FP64 Box-Muller).
+    A one-dimensional state takes normal i % 4 of the call (i // 4, t, 0)."""
     out = np.zeros((dx, N))
     buf = (C.c_double * 4)()
+    if dx == 1:
+        for g in range((N + 3) // 4):
+            lib().or_philox_normals4(C.c_uint64(seed), g, t, 0, buf)
+            for r in range(4):
+                if 4 * g + r < N:
+                    out[0, 4 * g + r] = buf[r]
+        return out
     for i in range(N):
         for q in range((dx + 3) // 4):
             lib().or_philox_normals4(C.c_uint64(seed), i, t, q, buf)
@@ -457,20 +495,37 @@ def create_linear_gaussian_model(rng, Dx, Dy, process_noise_scale=0.1, obs_noise
     return LGModel(mu0, S0, A, b, Q, H, c, R)
 
 
+def create_nonhomogeneous_linear_gaussian_model(rng, Dx, Dy, T_max, process_noise_scale=0.1,
+                                                obs_noise_scale=1.0):
+    """GFTest/models/linear_gaussian.jl:97-119 (numpy RNG): a prior and one
+    (A, b, Q, H, c, R) per step t = 1..T_max."""
+    mu0 = rng.random(Dx)
+    S0 = rand_cov(rng, Dx)
+    As = [rng.random((Dx, Dx)) for _ in range(T_max)]
+    bs = [rng.random(Dx) for _ in range(T_max)]
+    Qs = [rand_cov(rng, Dx, scale=process_noise_scale) for _ in range(T_max)]
+    Hs = [rng.random((Dy, Dx)) for _ in range(T_max)]
+    cs = [rng.random(Dy) for _ in range(T_max)]
+    Rs = [rand_cov(rng, Dy, scale=obs_noise_scale) for _ in range(T_max)]
+    return LGModel.time_varying(mu0, S0, As, bs, Qs, Hs, cs, Rs)
+
+
 def sample(rng, m: LGModel, T):
     """SSMProblems forward simulation (utils/forward_simulation.jl:14-26)."""
     x = rng.multivariate_normal(m.mu0, m.Sigma0)
     xs, ys = [], []
-    for _ in range(T):
-        x = m.A @ x + m.b + rng.multivariate_normal(np.zeros(m.dx), m.Q)
+    for t in range(1, T + 1):
+        A, b, Q, H, c, R = m.params(t)
+        x = A @ x + b + rng.multivariate_normal(np.zeros(m.dx), Q)
         xs.append(x)
-        ys.append(m.H @ x + m.c + rng.multivariate_normal(np.zeros(m.dy), m.R))
+        ys.append(H @ x + c + rng.multivariate_normal(np.zeros(m.dy), R))
     return np.array(xs), np.array(ys).reshape(T, m.dy)
 
 
 def compute_joint(m: LGModel, T):
-    """GFTest/models/linear_gaussian.jl:171-215: Z = [X0..XT, Y1..YT] ~ N(mu_Z,
-    Sigma_Z) from (I - P) Z = eps."""
+    """GFTest/models/linear_gaussian.jl:171-215 (and :121-169,
+    _compute_joint_nonhomogeneous, for time-varying models): Z = [X0..XT, Y1..YT]
+    ~ N(mu_Z, Sigma_Z) from (I - P) Z = eps."""
     Dx, Dy = m.dx, m.dy
     n = Dx + T * (Dx + Dy)
     P = np.zeros((n, n))
@@ -479,14 +534,15 @@ def compute_joint(m: LGModel, T):
     mu_e[:Dx] = m.mu0
     S_e[:Dx, :Dx] = m.Sigma0
     for t in range(1, T + 1):
+        A, b, Q, H, c, R = m.params(t)   # _compute_joint_nonhomogeneous for tv models
         iA, jA = t * Dx, (t - 1) * Dx
-        P[iA:iA + Dx, jA:jA + Dx] = m.A
+        P[iA:iA + Dx, jA:jA + Dx] = A
         iH, jH = Dx * (T + 1) + (t - 1) * Dy, Dx * t
-        P[iH:iH + Dy, jH:jH + Dx] = m.H
-        mu_e[iA:iA + Dx] = m.b
-        mu_e[iH:iH + Dy] = m.c
-        S_e[iA:iA + Dx, iA:iA + Dx] = m.Q
-        S_e[iH:iH + Dy, iH:iH + Dy] = m.R
+        P[iH:iH + Dy, jH:jH + Dx] = H
+        mu_e[iA:iA + Dx] = b
+        mu_e[iH:iH + Dy] = c
+        S_e[iA:iA + Dx, iA:iA + Dx] = Q
+        S_e[iH:iH + Dy, iH:iH + Dy] = R
     IP = np.eye(n) - P
     mu_Z = np.linalg.solve(IP, mu_e)
     Sigma_Z = np.linalg.solve(IP, np.linalg.solve(IP, S_e).T).T

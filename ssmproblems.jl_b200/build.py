@@ -32,11 +32,25 @@ def _headers():
         glob.glob(os.path.join(INCLUDE, "*.h"))
 
 
+def _deps(dep_file):
+    """Headers listed in an nvcc -MD dependency file (None if absent)."""
+    if not os.path.exists(dep_file):
+        return None
+    text = open(dep_file).read().replace("\\\n", " ")
+    parts = text.split(":", 1)
+    return parts[1].split() if len(parts) == 2 else None
+
+
 def _stale(obj, src, hdr_mtime):
     if not os.path.exists(obj):
         return True
     m = os.path.getmtime(obj)
-    return m < os.path.getmtime(src) or m < hdr_mtime
+    if m < os.path.getmtime(src):
+        return True
+    deps = _deps(obj[:-2] + ".d")
+    if deps is None:
+        return m < hdr_mtime
+    return any(not os.path.exists(d) or m < os.path.getmtime(d) for d in deps)
 
 
 def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -> str:
@@ -54,7 +68,7 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
 
     def compile_one(so):
         s, o = so
-        cmd = [NVCC] + ARCH + FLAGS + ["-c", s, "-o", o]
+        cmd = [NVCC] + ARCH + FLAGS + ["-MD", "-MF", o[:-2] + ".d", "-c", s, "-o", o]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed for {s}:\n{r.stdout}\n{r.stderr}")

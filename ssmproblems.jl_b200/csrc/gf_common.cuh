@@ -14,7 +14,10 @@ namespace gf {
 
 // ---------------------------------------------------------------- Philox ---
 // Counter layout (shared with the FP64 oracle so it can regenerate the noise):
-//   normals : ctr = (particle i, step t, block q, 'NORM'), 4 normals per call
+//   normals : ctr = (particle i, step t, block q, 'NORM'), 4 normals per call;
+//             a one-dimensional linear-Gaussian state takes normal i % 4 of the
+//             call (i / 4, t, 0, 'NORM'), so no draw is discarded
+
 //   uniforms: ctr = (slot j, step t, 0, 'UNIF'), one FP64 uniform per call
 constexpr uint32_t kTagNormal = 0x4E4F524Du;
 constexpr uint32_t kTagUnif = 0x554E4946u;
@@ -94,26 +97,38 @@ __device__ __forceinline__ double warp_sum(double v) {
   for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
   return v;
 }
-// Block-wide reductions over blockDim.x threads (multiple of 32, <= 1024).
-// `sh` is shared scratch of >= 32 doubles; ends with all threads holding the result.
-__device__ __forceinline__ double block_max(double v, double* sh) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// The threads that reduce and synchronise together (the block); the
+// reductions and the step finalise are written against this interface.
+struct BlockSync {
+  __device__ __forceinline__ int tid() const { return (int)threadIdx.x; }
+  __device__ __forceinline__ int size() const { return (int)blockDim.x; }
+  __device__ __forceinline__ void sync() const { __syncthreads(); }
+};
+
+// Reductions over the threads of S (a multiple of 32, <= 1024). `sh` is shared
+// scratch of >= 32 doubles owned by S; every thread ends holding the result.
+template <class S>
+__device__ __forceinline__ double sync_max(const S& g, double v, double* sh) {
+  const int lane = g.tid() & 31, wid = g.tid() >> 5, nw = g.size() >> 5;
   v = warp_max(v);
-  __syncthreads();
+  g.sync();
   if (lane == 0) sh[wid] = v;
-  __syncthreads();
+  g.sync();
   v = lane < nw ? sh[lane] : -INFINITY;
   return warp_max(v);
 }
-__device__ __forceinline__ double block_sum(double v, double* sh) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+template <class S>
+__device__ __forceinline__ double sync_sum(const S& g, double v, double* sh) {
+  const int lane = g.tid() & 31, wid = g.tid() >> 5, nw = g.size() >> 5;
   v = warp_sum(v);
-  __syncthreads();
+  g.sync();
   if (lane == 0) sh[wid] = v;
-  __syncthreads();
+  g.sync();
   v = lane < nw ? sh[lane] : 0.0;
   return warp_sum(v);
 }
+__device__ __forceinline__ double block_max(double v, double* sh) { return sync_max(BlockSync(), v, sh); }
+__device__ __forceinline__ double block_sum(double v, double* sh) { return sync_sum(BlockSync(), v, sh); }
 
 // ---------------------------------------------------------- job scalars ----
 // Device-resident per-filter scalars of a particle filter.  The last block of

@@ -31,29 +31,38 @@ namespace gf {
 
 template <int DXP, int DYP>
 struct KfSmem {
-  static constexpr int LD = DXP + 1;   // row stride of dx-wide matrices
-  static constexpr int LY = DYP + 1;   // row stride of dy-wide matrices
+  // Float matrices are row-major with 16-byte rows (stride a multiple of 4 and
+  // at least 4 past the width): the products read four k at a time, so every
+  // row an operand of a product is zero in its columns [k, ceil4(k)).
+  static constexpr int LD = DXP + 4;   // row stride of dx-wide matrices
+  static constexpr int LY = DYP + 4;   // row stride of dy-wide matrices
+  static constexpr int LS = DYP + 1;   // row stride of S (FP64)
   static constexpr int LW = DXP + 1;   // row stride of the FP64 solve buffer (dx RHS + z)
+  double S[DYP * LS], dinv[DYP], z[DYP], w[DYP], red[32];
   // Buffers shared by values whose lifetimes within a step do not overlap:
-  //   Sig : filtered covariance; from step 2 to 8 it holds the prediction Sp
-  //   XZ  : X = A Sig (steps 1-2), then I - KH (steps 7-9); Z = (I - KH) Sp
-  //         (steps 8-9); during the gain solve (steps 4-6) both hold the FP64
-  //         right-hand sides Wm (dy rows of LW doubles fit in 2 * DXP * LD floats)
-  //   PK  : P H' (steps 3-6), then K R (steps 7-9)
-  double S[DYP * LY], dinv[DYP], z[DYP], w[DYP], red[32];
-  alignas(16) float XZ[2 * DXP * LD];
-  float A[DXP * LD], Q[DXP * LD], Sig[DXP * LD];
-  float H[DYP * LD], PK[DXP * LY], K[DXP * LY], R[DYP * LY];
+  //   Sig : filtered covariance; from phase 2 to 8 it holds the prediction Sp
+  //   T1  : A Sig (phases 1-2), then I - K H (phases 7-9)
+  //   W2  : (I - K H) Sp | K R (phases 7-9); the FP64 solve buffer Wm (5-6)
+  alignas(16) float A[DXP * LD];
+  alignas(16) float Q[DXP * LD];
+  alignas(16) float Sig[DXP * LD];
+  alignas(16) float T1[DXP * LD];
+  alignas(16) float H[DYP * LD];
+  alignas(16) float HS[DYP * LD];  // H Sp (phases 3-6)
+  alignas(16) float K[DXP * LY];
+  alignas(16) float R[DYP * LY];
+  alignas(16) float W2[DXP * LD + DXP * LY];
   float mu[DXP], mup[DXP], b[DXP], c[DYP];
   int fid, fail;
-  static_assert(DYP * LW * sizeof(double) <= 2 * DXP * LD * sizeof(float), "Wm must fit in XZ");
+  static_assert(DYP * LW * sizeof(double) <= sizeof(W2), "Wm must fit in W2");
 };
 
 __device__ __forceinline__ void group_sync() { __syncthreads(); }
 
-// y (m x n, row-major, ld) = op over all elements, strided over the block
+// One step's parameters (A b Q H c R, column-major) into shared memory (the
+// valid entries only: padding stays as kf_load left it).
 template <int DXP, int DYP>
-__device__ void kf_load(KfSmem<DXP, DYP>& s, const float* P, int dx, int dy) {
+__device__ void kf_load_step(KfSmem<DXP, DYP>& s, const float* P, int dx, int dy) {
   const int G = blockDim.x;
   const float* pA = P;
   const float* pb = pA + dx * dx;
@@ -61,14 +70,11 @@ __device__ void kf_load(KfSmem<DXP, DYP>& s, const float* P, int dx, int dy) {
   const float* pH = pQ + dx * dx;
   const float* pc = pH + dy * dx;
   const float* pR = pc + dy;
-  const float* pm = pR + dy * dy;
-  const float* pS = pm + dx;
   constexpr int LD = KfSmem<DXP, DYP>::LD, LY = KfSmem<DXP, DYP>::LY;
   for (int e = threadIdx.x; e < dx * dx; e += G) {
     int i = e % dx, j = e / dx;  // column-major source
     s.A[i * LD + j] = pA[e];
     s.Q[i * LD + j] = pQ[e];
-    s.Sig[i * LD + j] = pS[e];
   }
   for (int e = threadIdx.x; e < dy * dx; e += G) {
     int i = e % dy, j = e / dy;
@@ -78,11 +84,111 @@ __device__ void kf_load(KfSmem<DXP, DYP>& s, const float* P, int dx, int dy) {
     int i = e % dy, j = e / dy;
     s.R[i * LY + j] = pR[e];
   }
-  for (int e = threadIdx.x; e < dx; e += G) {
-    s.b[e] = pb[e];
-    s.mu[e] = pm[e];
-  }
+  for (int e = threadIdx.x; e < dx; e += G) s.b[e] = pb[e];
   for (int e = threadIdx.x; e < dy; e += G) s.c[e] = pc[e];
+}
+
+// A filter's first-step parameters from P and its prior (mu0, Sigma0) from P0.
+template <int DXP, int DYP>
+__device__ void kf_load(KfSmem<DXP, DYP>& s, const float* P, const float* P0, int dx, int dy) {
+  const int G = blockDim.x;
+  constexpr int LD = KfSmem<DXP, DYP>::LD;
+  // zero every float matrix first: the product operands' k-padding must be 0
+  using SM = KfSmem<DXP, DYP>;
+  constexpr int nzero = (int)((offsetof(SM, mu) - offsetof(SM, A)) / sizeof(float));
+  for (int e = threadIdx.x; e < nzero; e += G) s.A[e] = 0.f;
+  __syncthreads();
+  kf_load_step<DXP, DYP>(s, P, dx, dy);
+  const float* pm = P0;
+  const float* pS = pm + dx;
+  for (int e = threadIdx.x; e < dx * dx; e += G) s.Sig[(e % dx) * LD + e / dx] = pS[e];
+  for (int e = threadIdx.x; e < dx; e += G) s.mu[e] = pm[e];
+}
+
+// ------------------------------------------------------------ small products
+// C(i, j) = init(i, j) + sum_k A[i][k] B[j][k] for i < m, j < n (both operands
+// row-major with k contiguous, 16-byte rows, zero in columns [kk, ceil4(kk))).
+// Each thread of the block takes 2x2 outputs and reads four k per 128-bit
+// shared-memory load (two A rows, two B rows: 16 FMAs per 4 loads).  Every
+// output accumulates its FMAs in k order, so the result does not depend on
+// the block size.  SYM: only tiles on or above the diagonal, each output with
+// j >= i written to (i, j) and (j, i).  A second operand pair (A2, B2, kk2) is
+// accumulated after the first into the same sums.  Acc = float or double
+// (double: FP64 FMAs of the FP32 products' operands).
+template <typename Acc, bool SYM, typename Init, typename Store>
+__device__ __forceinline__ void mm_abt(const float* A, int lda, const float* B, int ldb, int kk,
+                                       const float* A2, int lda2, const float* B2, int ldb2, int kk2,
+                                       int m, int n, Init init, Store store) {
+  const int tm = (m + 1) >> 1, tn = (n + 1) >> 1;
+  for (int t = threadIdx.x; t < tm * tn; t += blockDim.x) {
+    const int ti = t / tn, tj = t - ti * tn;
+    if (SYM && tj < ti) continue;
+    const int i0 = 2 * ti, j0 = 2 * tj;
+    const int i1 = min(i0 + 1, m - 1), j1 = min(j0 + 1, n - 1);
+    Acc c00 = init(i0, j0), c01 = init(i0, j1), c10 = init(i1, j0), c11 = init(i1, j1);
+    auto run = [&](const float* X, int ldx, const float* Y, int ldy, int k) {
+      const float4* a0 = reinterpret_cast<const float4*>(X + i0 * ldx);
+      const float4* a1 = reinterpret_cast<const float4*>(X + i1 * ldx);
+      const float4* b0 = reinterpret_cast<const float4*>(Y + j0 * ldy);
+      const float4* b1 = reinterpret_cast<const float4*>(Y + j1 * ldy);
+      const int k4 = (k + 3) >> 2;
+#pragma unroll 1
+      for (int q = 0; q < k4; ++q) {
+        const float4 x0 = a0[q], x1 = a1[q], y0 = b0[q], y1 = b1[q];
+        auto step = [&](float u0, float u1, float v0, float v1) {
+          c00 = fma((Acc)u0, (Acc)v0, c00);
+          c01 = fma((Acc)u0, (Acc)v1, c01);
+          c10 = fma((Acc)u1, (Acc)v0, c10);
+          c11 = fma((Acc)u1, (Acc)v1, c11);
+        };
+        step(x0.x, x1.x, y0.x, y1.x);
+        step(x0.y, x1.y, y0.y, y1.y);
+        step(x0.z, x1.z, y0.z, y1.z);
+        step(x0.w, x1.w, y0.w, y1.w);
+      }
+    };
+    run(A, lda, B, ldb, kk);
+    if (A2) run(A2, lda2, B2, ldb2, kk2);
+    if (!SYM || j0 >= i0) store(i0, j0, c00);
+    if (j1 > j0 && (!SYM || j1 >= i0)) store(i0, j1, c01);
+    if (i1 > i0 && (!SYM || j0 >= i1)) store(i1, j0, c10);
+    if (i1 > i0 && j1 > j0 && (!SYM || j1 >= i1)) store(i1, j1, c11);
+  }
+}
+
+// C(i, j) = init(i, j) - sum_{k < kk} A[i][k] B[k][j] (B row-major, j contiguous,
+// rows 8-byte aligned), 2x2 outputs per thread, FMAs in k order.
+template <typename Init, typename Store>
+__device__ __forceinline__ void mm_ab_neg(const float* A, int lda, const float* B, int ldb, int kk,
+                                          int m, int n, Init init, Store store) {
+  const int tm = (m + 1) >> 1, tn = (n + 1) >> 1;
+  for (int t = threadIdx.x; t < tm * tn; t += blockDim.x) {
+    const int ti = t / tn, tj = t - ti * tn;
+    const int i0 = 2 * ti, j0 = 2 * tj;
+    const int i1 = min(i0 + 1, m - 1);
+    float c00 = init(i0, j0), c01 = init(i0, j0 + 1), c10 = init(i1, j0), c11 = init(i1, j0 + 1);
+    for (int k = 0; k < kk; ++k) {
+      const float a0 = -A[i0 * lda + k], a1 = -A[i1 * lda + k];
+      const float2 y = *reinterpret_cast<const float2*>(B + k * ldb + j0);
+      c00 = fmaf(a0, y.x, c00);
+      c01 = fmaf(a0, y.y, c01);
+      c10 = fmaf(a1, y.x, c10);
+      c11 = fmaf(a1, y.y, c11);
+    }
+    store(i0, j0, c00);
+    if (j0 + 1 < n) store(i0, j0 + 1, c01);
+    if (i1 > i0) {
+      store(i1, j0, c10);
+      if (j0 + 1 < n) store(i1, j0 + 1, c11);
+    }
+  }
+}
+
+// Zeroes columns [n, ceil4(n)) of rows [0, m) (k-padding of a product operand
+// written into a buffer that held other data).
+__device__ __forceinline__ void zero_pad(float* C, int ldc, int m, int n) {
+  const int p = ((n + 3) & ~3) - n;
+  for (int e = threadIdx.x; e < m * p; e += blockDim.x) C[(e / p) * ldc + n + e % p] = 0.f;
 }
 
 // FP64 Cholesky of s.S (dy x dy, lower triangle, in place) by warp 0 with one
@@ -90,11 +196,11 @@ __device__ void kf_load(KfSmem<DXP, DYP>& s, const float* P, int dx, int dy) {
 // Returns false if S is not positive definite.
 template <int DXP, int DYP>
 __device__ bool kf_chol(KfSmem<DXP, DYP>& s, int dy) {
-  constexpr int LY = KfSmem<DXP, DYP>::LY;
+  constexpr int LS = KfSmem<DXP, DYP>::LS;
   if (threadIdx.x < 32) {
     const int r = threadIdx.x;
     for (int j = 0; j < dy; ++j) {
-      const double djj = s.S[j * LY + j];
+      const double djj = s.S[j * LS + j];
       if (!(djj > 0.0)) {
         if (r == 0) s.fail = 1;
         break;
@@ -102,16 +208,16 @@ __device__ bool kf_chol(KfSmem<DXP, DYP>& s, int dy) {
       const double d = sqrt(djj), inv = 1.0 / d;
       double lrj = 0.0;
       if (r > j && r < dy) {
-        lrj = s.S[r * LY + j] * inv;
-        s.S[r * LY + j] = lrj;
+        lrj = s.S[r * LS + j] * inv;
+        s.S[r * LS + j] = lrj;
       }
       if (r == j) {
-        s.S[j * LY + j] = d;
+        s.S[j * LS + j] = d;
         s.dinv[j] = inv;
       }
       __syncwarp();
       if (r > j && r < dy)
-        for (int k = j + 1; k <= r; ++k) s.S[r * LY + k] -= lrj * s.S[k * LY + j];
+        for (int k = j + 1; k <= r; ++k) s.S[r * LS + k] -= lrj * s.S[k * LS + j];
       __syncwarp();
     }
   }
@@ -124,14 +230,14 @@ __device__ bool kf_chol(KfSmem<DXP, DYP>& s, int dy) {
 // take interleaved column sets; dy <= 32.
 template <int DXP, int DYP>
 __device__ void kf_solves(KfSmem<DXP, DYP>& s, double* Wm, int dy, int nf, int nb) {
-  constexpr int LY = KfSmem<DXP, DYP>::LY, LW = KfSmem<DXP, DYP>::LW;
+  constexpr int LS = KfSmem<DXP, DYP>::LS, LW = KfSmem<DXP, DYP>::LW;
   const int r = threadIdx.x & 31, w = threadIdx.x >> 5, nw = blockDim.x >> 5;
   for (int i = 0; i < dy; ++i) {
     if (r == i)
       for (int c = w; c < nf; c += nw) Wm[i * LW + c] *= s.dinv[i];
     __syncwarp();
     if (r > i && r < dy) {
-      const double l = s.S[r * LY + i];
+      const double l = s.S[r * LS + i];
       for (int c = w; c < nf; c += nw) Wm[r * LW + c] -= l * Wm[i * LW + c];
     }
     __syncwarp();
@@ -141,7 +247,7 @@ __device__ void kf_solves(KfSmem<DXP, DYP>& s, double* Wm, int dy, int nf, int n
       for (int c = w; c < nb; c += nw) Wm[i * LW + c] *= s.dinv[i];
     __syncwarp();
     if (r < i) {
-      const double l = s.S[i * LY + r];
+      const double l = s.S[i * LS + r];
       for (int c = w; c < nb; c += nw) Wm[r * LW + c] -= l * Wm[i * LW + c];
     }
     __syncwarp();
@@ -166,20 +272,22 @@ __device__ void kf_srv_publish(const KfDesc& D, const float* mu, CovF cov, doubl
   }
 }
 
+// 64 registers: four blocks of 256 threads (the dx <= 32 bucket's shared memory
+// also allows four)
 template <int DXP, int DYP>
-__global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
+__global__ void __launch_bounds__(256, 4) kf_batch_kernel(KfRun run) {
   using SM = KfSmem<DXP, DYP>;
-  constexpr int LD = SM::LD, LY = SM::LY;
+  constexpr int LD = SM::LD, LY = SM::LY, LS = SM::LS, LW = SM::LW;
   extern __shared__ __align__(16) unsigned char smraw[];
   SM& s = *reinterpret_cast<SM*>(smraw);
   const int G = blockDim.x;
-  float* const T1 = s.XZ;                      // A Sig
-  float* const IKH = s.XZ;                     // I - K H
-  float* const T2 = s.XZ + DXP * LD;           // (I - K H) Sp
-  float* const Sp = s.Sig;                     // predicted covariance
-  float* const PHt = s.PK;
-  float* const KR = s.PK;
-  double* const Wm = reinterpret_cast<double*>(s.XZ);
+  float* const Sp = s.Sig;        // predicted covariance (phases 2-8)
+  float* const IKH = s.T1;        // I - K H (phases 7-9)
+  float* const T2 = s.W2;         // (I - K H) Sp (phases 8-9)
+  float* const KR = s.W2 + DXP * LD;  // K R (phases 7-9)
+  double* const Wm = reinterpret_cast<double*>(s.W2);
+  const float* const nul = nullptr;
+  auto zero = [](int, int) { return 0.f; };
   while (true) {
     if (threadIdx.x == 0) {
       unsigned k = atomicAdd(run.counter, 1u);
@@ -191,25 +299,22 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
     if (f < 0) return;
     const KfDesc D = run.desc[f];
     const int dx = D.dx, dy = D.dy;
-    kf_load<DXP, DYP>(s, run.params + D.poff, dx, dy);
+    const float* P = run.params + D.poff;
+    kf_load<DXP, DYP>(s, P, P + (D.p0 ? D.p0 : kf_step_block_len(dx, dy)), dx, dy);
     group_sync();
-    // 2-D thread maps without integer division: rows of width dx / dy are
-    // covered by 2^lx / 2^ly lanes, the remaining threads step over rows
-    const int lx = dx <= 4 ? 2 : (dx <= 8 ? 3 : (dx <= 16 ? 4 : 5));
-    const int ly = dy <= 4 ? 2 : (dy <= 8 ? 3 : (dy <= 16 ? 4 : 5));
-    const int tx = threadIdx.x & ((1 << lx) - 1), ty = threadIdx.x >> lx, nx = 1 << lx, ny = G >> lx;
-    const int ux = threadIdx.x & ((1 << ly) - 1), uy = threadIdx.x >> ly, mx = 1 << ly, my = G >> ly;
     double lltot = 0.0;
     int status = GF_OK;
     for (int t = 0; t < D.T; ++t) {
       const double* y = run.ys + D.yoff + (int64_t)t * dy;
-      // 1. T1 = A Sigma ; mup = A mu + b
-      for (int i = ty; i < dx; i += ny)
-      for (int j = tx; j < dx; j += nx) {
-        float acc = 0.f;
-        for (int k = 0; k < dx; ++k) acc = fmaf(s.A[i * LD + k], s.Sig[k * LD + j], acc);
-        T1[i * LD + j] = acc;
+      // 0. time-varying model: this step's A, b, Q, H, c, R (calc_params(dyn, t),
+      //    calc_params(obs, t), models/linear_gaussian.jl:44-63)
+      if (D.pstep && t > 0) {
+        kf_load_step<DXP, DYP>(s, P + (int64_t)t * D.pstep, dx, dy);
+        group_sync();
       }
+      // 1. T1 = A Sigma (Sigma symmetric: rows of Sigma are its columns) ; mup = A mu + b
+      mm_abt<float, false>(s.A, LD, s.Sig, LD, dx, nul, 0, nul, 0, 0, dx, dx, zero,
+                                  [&](int i, int j, float v) { s.T1[i * LD + j] = v; });
       for (int i = threadIdx.x; i < dx; i += G) {
         float acc = s.b[i];
         for (int k = 0; k < dx; ++k) acc = fmaf(s.A[i * LD + k], s.mu[k], acc);
@@ -217,103 +322,88 @@ __global__ void __launch_bounds__(256) kf_batch_kernel(KfRun run) {
       }
       group_sync();
       // 2. Sp = T1 A' + Q (upper triangle, mirrored)
-      for (int i = ty; i < dx; i += ny)
-      for (int j = tx; j < dx; j += nx) {
-        if (j < i) continue;
-        float acc = s.Q[i * LD + j];
-        for (int k = 0; k < dx; ++k) acc = fmaf(T1[i * LD + k], s.A[j * LD + k], acc);
-        Sp[i * LD + j] = acc;
-        Sp[j * LD + i] = acc;
-      }
+      mm_abt<float, true>(s.T1, LD, s.A, LD, dx, nul, 0, nul, 0, 0, dx, dx,
+                                 [&](int i, int j) { return s.Q[i * LD + j]; },
+                                 [&](int i, int j, float v) {
+                                   Sp[i * LD + j] = v;
+                                   Sp[j * LD + i] = v;
+                                 });
       group_sync();
-      // 3. PHt = Sp H' ; z = y - H mup - c
-      for (int i = uy; i < dx; i += my)
-      for (int j = ux; j < dy; j += mx) {
-        float acc = 0.f;
-        for (int k = 0; k < dx; ++k) acc = fmaf(Sp[i * LD + k], s.H[j * LD + k], acc);
-        PHt[i * LY + j] = acc;
-      }
+      // 3. HS = H Sp (= (Sp H')') ; z = y - H mup - c
+      mm_abt<float, false>(s.H, LD, Sp, LD, dx, nul, 0, nul, 0, 0, dy, dx, zero,
+                                  [&](int i, int j, float v) { s.HS[i * LD + j] = v; });
       for (int i = threadIdx.x; i < dy; i += G) {
         double acc = y[i] - (double)s.c[i];
         for (int k = 0; k < dx; ++k) acc -= (double)s.H[i * LD + k] * (double)s.mup[k];
         s.z[i] = acc;
       }
       group_sync();
-      // 4. S = H PHt + R in FP64 (lower triangle is all the Cholesky reads)
-      for (int i = uy; i < dy; i += my)
-      for (int j = ux; j <= i; j += mx) {
-        double acc = (double)s.R[i * LY + j];
-        for (int k = 0; k < dx; ++k) acc += (double)s.H[i * LD + k] * (double)PHt[k * LY + j];
-        s.S[i * LY + j] = acc;
-      }
+      // 4. S = H HS' + R in FP64 (lower triangle is all the Cholesky reads)
+      mm_abt<double, false>(s.H, LD, s.HS, LD, dx, nul, 0, nul, 0, 0, dy, dy,
+                                   [&](int i, int j) { return (double)s.R[i * LY + j]; },
+                                   [&](int i, int j, double v) {
+                                     if (j <= i) s.S[i * LS + j] = v;
+                                   });
       group_sync();
       // 5. Cholesky of S (FP64)
       if (!kf_chol<DXP, DYP>(s, dy)) {
         status = GF_ERR_NOT_PD;
         break;
       }
-      // 6. RHS = [PHt' | z]; forward solve gives w = L^-1 z (last column),
-      //    back solve of the first dx columns gives K' = S^-1 PHt'
-      constexpr int LW = SM::LW;
-      for (int c = ty; c <= dx; c += ny)
-        for (int i = tx; i < dy; i += nx) Wm[i * LW + c] = c < dx ? (double)PHt[c * LY + i] : s.z[i];
+      // 6. RHS = [HS | z]; forward solve gives w = L^-1 z (last column),
+      //    back solve of the first dx columns gives K' = S^-1 HS
+      for (int e = threadIdx.x; e < dy * (dx + 1); e += G) {
+        const int i = e / (dx + 1), cc = e - i * (dx + 1);
+        Wm[i * LW + cc] = cc < dx ? (double)s.HS[i * LD + cc] : s.z[i];
+      }
       __syncthreads();
       kf_solves<DXP, DYP>(s, Wm, dy, dx + 1, dx);
       for (int i = threadIdx.x; i < dy; i += G) s.w[i] = Wm[i * LW + dx];
-      for (int i = uy; i < dx; i += my)
-        for (int j = ux; j < dy; j += mx) s.K[i * LY + j] = (float)Wm[j * LW + i];
+      for (int e = threadIdx.x; e < dx * dy; e += G) {
+        const int i = e / dy, j = e - i * dy;
+        s.K[i * LY + j] = (float)Wm[j * LW + i];
+      }
       group_sync();
-      // 7. mu = mup + K z ; IKH = I - K H ; KR = K R
+      // 7. mu = mup + K z ; IKH = I - K H ; KR = K R (R symmetric)
       for (int i = threadIdx.x; i < dx; i += G) {
         double acc = (double)s.mup[i];
         for (int k = 0; k < dy; ++k) acc += (double)s.K[i * LY + k] * s.z[k];
         s.mu[i] = (float)acc;
       }
-      for (int i = ty; i < dx; i += ny)
-      for (int j = tx; j < dx; j += nx) {
-        float acc = (i == j) ? 1.f : 0.f;
-        for (int k = 0; k < dy; ++k) acc = fmaf(-s.K[i * LY + k], s.H[k * LD + j], acc);
-        IKH[i * LD + j] = acc;
-      }
-      for (int i = uy; i < dx; i += my)
-      for (int j = ux; j < dy; j += mx) {
-        float acc = 0.f;
-        for (int k = 0; k < dy; ++k) acc = fmaf(s.K[i * LY + k], s.R[k * LY + j], acc);
-        KR[i * LY + j] = acc;
-      }
+      mm_ab_neg(s.K, LY, s.H, LD, dy, dx, dx, [](int i, int j) { return i == j ? 1.f : 0.f; },
+                [&](int i, int j, float v) { IKH[i * LD + j] = v; });
+      mm_abt<float, false>(s.K, LY, s.R, LY, dy, nul, 0, nul, 0, 0, dx, dy, zero,
+                                  [&](int i, int j, float v) { KR[i * LY + j] = v; });
+      zero_pad(KR, LY, dx, dy);
       group_sync();
-      // 8. T1 = IKH Sp
-      for (int i = ty; i < dx; i += ny)
-      for (int j = tx; j < dx; j += nx) {
-        float acc = 0.f;
-        for (int k = 0; k < dx; ++k) acc = fmaf(IKH[i * LD + k], Sp[k * LD + j], acc);
-        T2[i * LD + j] = acc;
-      }
+      // 8. T2 = IKH Sp
+      mm_abt<float, false>(IKH, LD, Sp, LD, dx, nul, 0, nul, 0, 0, dx, dx, zero,
+                                  [&](int i, int j, float v) { T2[i * LD + j] = v; });
+      zero_pad(T2, LD, dx, dx);
       group_sync();
-      // 9. Sig = T1 IKH' + KR K' (+ jitter I), upper triangle mirrored
-      float* cov_out = run.covs ? run.covs + D.coff + (int64_t)t * dx * dx : nullptr;
-      for (int i = ty; i < dx; i += ny)
-      for (int j = tx; j < dx; j += nx) {
-        if (j < i) continue;
-        float acc = 0.f;
-        for (int k = 0; k < dx; ++k) acc = fmaf(T2[i * LD + k], IKH[j * LD + k], acc);
-        for (int k = 0; k < dy; ++k) acc = fmaf(KR[i * LY + k], s.K[j * LY + k], acc);
-        if (run.use_jitter && i == j) acc += (float)run.jitter;
-        s.Sig[i * LD + j] = acc;
-        s.Sig[j * LD + i] = acc;
-      }
+      // 9. Sig = T2 IKH' + KR K' (+ jitter I), upper triangle mirrored
+      const float jit = run.use_jitter ? (float)run.jitter : 0.f;
+      mm_abt<float, true>(T2, LD, IKH, LD, dx, KR, LY, s.K, LY, dy, dx, dx, zero,
+                                 [&](int i, int j, float v) {
+                                   if (run.use_jitter && i == j) v += jit;
+                                   s.Sig[i * LD + j] = v;
+                                   s.Sig[j * LD + i] = v;
+                                 });
       group_sync();
       // 10. outputs
+      float* cov_out = run.covs ? run.covs + D.coff + (int64_t)t * dx * dx : nullptr;
       if (cov_out)
-        for (int j = ty; j < dx; j += ny)
-          for (int i = tx; i < dx; i += nx) cov_out[i + j * dx] = s.Sig[i * LD + j];
+        for (int e = threadIdx.x; e < dx * dx; e += G) {
+          const int j = e / dx, i = e - j * dx;
+          cov_out[e] = s.Sig[i * LD + j];
+        }
       if (run.means)
         for (int i = threadIdx.x; i < dx; i += G) run.means[D.moff + (int64_t)t * dx + i] = s.mu[i];
       if (threadIdx.x < 32) {
         double q = 0.0, ld = 0.0;
         for (int i = threadIdx.x; i < dy; i += 32) {
           q += s.w[i] * s.w[i];
-          ld += log(s.S[i * LY + i]);
+          ld += log(s.S[i * LS + i]);
         }
         q = warp_sum(q);
         ld = warp_sum(ld);
@@ -601,20 +691,26 @@ __global__ void __launch_bounds__(256) rts_smooth_kernel(KfRun run) {
       continue;
     }
     const float* P = run.params + D.poff;  // A dx*dx | b dx | Q dx*dx | ...
-    for (int e = threadIdx.x; e < dx * dx; e += G) {
-      const int i = e % dx, j = e / dx;  // column-major source
-      s.A[i * LD + j] = P[e];
-      s.Q[i * LD + j] = P[dx * dx + dx + e];
-      s.Sn[i * LD + j] = run.covs[D.coff + (int64_t)(T - 1) * dx * dx + e];
-    }
-    for (int e = threadIdx.x; e < dx; e += G) {
-      s.b[e] = P[dx * dx + e];
-      s.mn[e] = run.means[D.moff + (int64_t)(T - 1) * dx + e];
-    }
+    // the parameters of 0-based step k (a time-varying model's block k)
+    auto load_params = [&](int k) {
+      const float* Pk = P + (int64_t)k * D.pstep;
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        const int i = e % dx, j = e / dx;  // column-major source
+        s.A[i * LD + j] = Pk[e];
+        s.Q[i * LD + j] = Pk[dx * dx + dx + e];
+      }
+      for (int e = threadIdx.x; e < dx; e += G) s.b[e] = Pk[dx * dx + e];
+    };
+    load_params(0);
+    for (int e = threadIdx.x; e < dx * dx; e += G)
+      s.Sn[(e % dx) * LD + e / dx] = run.covs[D.coff + (int64_t)(T - 1) * dx * dx + e];
+    for (int e = threadIdx.x; e < dx; e += G) s.mn[e] = run.means[D.moff + (int64_t)(T - 1) * dx + e];
     __syncthreads();
     for (int t = T - 2; t >= 0; --t) {
       float* cov = run.covs + D.coff + (int64_t)t * dx * dx;
       float* mean = run.means + D.moff + (int64_t)t * dx;
+      // the prediction from t to t + 1 uses the parameters of step t + 1
+      if (D.pstep) load_params(t + 1);
       for (int e = threadIdx.x; e < dx * dx; e += G) s.Sf[(e % dx) * LD + e / dx] = cov[e];
       for (int e = threadIdx.x; e < dx; e += G) s.mf[e] = mean[e];
       __syncthreads();
@@ -1064,9 +1160,33 @@ static gf_status kf_autotune_bucket(gf_kf_plan* p, gf_kf_plan::Bucket& bk) {
   return GF_OK;
 }
 
-extern "C" gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_model* models,
-                                       int32_t B, const int32_t* T, double jitter,
-                                       int32_t use_jitter, int32_t flags, gf_kf_plan** out) {
+// A time-varying model's pool entry: T step blocks (A b Q H c R) then mu0, S0.
+static gf_status kf_pack_model_tv(gf_ctx* ctx, const gf_lg_model& m, int f, int T,
+                                  std::vector<float>& pool) {
+  const int dx = m.dx, dy = m.dy;
+  std::vector<double> L(std::max(dx, dy) * std::max(dx, dy));
+  if (chol_lower(dx, m.Sigma0, L.data())) return set_err(ctx, GF_ERR_NOT_PD, "filter %d: Sigma0 not PD", f);
+  auto put = [&](const double* a, int64_t n) {
+    for (int64_t i = 0; i < n; ++i) pool.push_back((float)a[i]);
+  };
+  for (int t = 0; t < T; ++t) {
+    if (chol_lower(dy, m.R + (size_t)t * dy * dy, L.data()))
+      return set_err(ctx, GF_ERR_NOT_PD, "filter %d: R of step %d not PD", f, t + 1);
+    put(m.A + (size_t)t * dx * dx, (int64_t)dx * dx);
+    put(m.b + (size_t)t * dx, dx);
+    put(m.Q + (size_t)t * dx * dx, (int64_t)dx * dx);
+    put(m.H + (size_t)t * dy * dx, (int64_t)dy * dx);
+    put(m.c + (size_t)t * dy, dy);
+    put(m.R + (size_t)t * dy * dy, (int64_t)dy * dy);
+  }
+  put(m.mu0, dx);
+  put(m.Sigma0, (int64_t)dx * dx);
+  return GF_OK;
+}
+
+static gf_status kf_plan_create_impl(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
+                                     const int32_t* T, const int32_t* param_steps, double jitter,
+                                     int32_t use_jitter, int32_t flags, gf_kf_plan** out) {
   if (!ctx || !out || !models || !T || B < 1) return ctx ? set_err(ctx, GF_ERR_ARG, "bad arguments") : GF_ERR_ARG;
   if (algo != GF_ALGO_KF && algo != GF_ALGO_SRKF) return set_err(ctx, GF_ERR_ARG, "unknown algo");
   *out = nullptr;
@@ -1103,9 +1223,22 @@ extern "C" gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_mo
     d.coff = coff;
     d.index = f;
     const int dx = m.dx, dy = m.dy;
-    gf_status pst = kf_pack_model(ctx, algo, m, f, pool);
-    if (pst) return pst;
-    poff += kf_param_len(dx, dy);
+    const int ps = param_steps ? param_steps[f] : 1;
+    if (ps != 1 && ps < T[f])
+      return set_err(ctx, GF_ERR_ARG, "filter %d: %d parameter steps for T = %d", f, ps, T[f]);
+    if (ps != 1) {
+      if (algo != GF_ALGO_KF)
+        return set_err(ctx, GF_ERR_UNSUPPORTED, "filter %d: time-varying parameters run with KalmanFilter()", f);
+      gf_status pst = kf_pack_model_tv(ctx, m, f, T[f], pool);
+      if (pst) return pst;
+      d.pstep = kf_step_block_len(dx, dy);
+      d.p0 = T[f] * d.pstep;
+      poff += (int64_t)d.p0 + dx + (int64_t)dx * dx;
+    } else {
+      gf_status pst = kf_pack_model(ctx, algo, m, f, pool);
+      if (pst) return pst;
+      poff += kf_param_len(dx, dy);
+    }
     yoff += (int64_t)T[f] * dy;
     soff += T[f];
     moff += (int64_t)T[f] * dx;
@@ -1167,6 +1300,19 @@ extern "C" gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_mo
   }
   *out = p.release();
   return GF_OK;
+}
+
+extern "C" gf_status gf_kf_plan_create(gf_ctx* ctx, int32_t algo, const gf_lg_model* models,
+                                       int32_t B, const int32_t* T, double jitter,
+                                       int32_t use_jitter, int32_t flags, gf_kf_plan** out) {
+  return kf_plan_create_impl(ctx, algo, models, B, T, nullptr, jitter, use_jitter, flags, out);
+}
+
+extern "C" gf_status gf_kf_plan_create_tv(gf_ctx* ctx, int32_t algo, const gf_lg_model* models,
+                                          int32_t B, const int32_t* T, const int32_t* param_steps,
+                                          double jitter, int32_t use_jitter, int32_t flags,
+                                          gf_kf_plan** out) {
+  return kf_plan_create_impl(ctx, algo, models, B, T, param_steps, jitter, use_jitter, flags, out);
 }
 
 extern "C" gf_status gf_kf_plan_run(gf_kf_plan* p, const double* ys_dev, gf_kf_out* out) {
@@ -1244,13 +1390,15 @@ static gf_status kf_smooth_enqueue(gf_kf_plan* p, const gf_kf_out* out) {
 }
 
 static gf_status kf_batch_impl(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
-                               const int32_t* T, const double* ys, double jitter, int32_t use_jitter,
-                               int32_t memspace, gf_kf_out* out, bool smooth) {
+                               const int32_t* T, const int32_t* param_steps, const double* ys,
+                               double jitter, int32_t use_jitter, int32_t memspace, gf_kf_out* out,
+                               bool smooth) {
   if (!ctx || !out || !ys) return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
   if (smooth && (!out->means || !out->covs))
     return set_err(ctx, GF_ERR_ARG, "smoothing needs out->means and out->covs");
   gf_kf_plan* p = nullptr;
-  gf_status st = gf_kf_plan_create(ctx, algo, models, B, T, jitter, use_jitter, GF_PLAN_NO_GRAPH, &p);
+  gf_status st = kf_plan_create_impl(ctx, algo, models, B, T, param_steps, jitter, use_jitter,
+                                     GF_PLAN_NO_GRAPH, &p);
   if (st) return st;
   std::unique_ptr<gf_kf_plan, gf_status (*)(gf_kf_plan*)> guard(p, gf_kf_plan_destroy);
   if (memspace == GF_MEM_DEVICE) {
@@ -1303,12 +1451,25 @@ static gf_status kf_batch_impl(gf_ctx* ctx, int32_t algo, const gf_lg_model* mod
 extern "C" gf_status gf_kf_batch(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
                                  const int32_t* T, const double* ys, double jitter,
                                  int32_t use_jitter, int32_t memspace, gf_kf_out* out) {
-  return kf_batch_impl(ctx, algo, models, B, T, ys, jitter, use_jitter, memspace, out, false);
+  return kf_batch_impl(ctx, algo, models, B, T, nullptr, ys, jitter, use_jitter, memspace, out, false);
 }
 
 extern "C" gf_status gf_kf_smooth(gf_ctx* ctx, const gf_lg_model* models, int32_t B, const int32_t* T,
                                   const double* ys, int32_t memspace, gf_kf_out* out) {
-  return kf_batch_impl(ctx, GF_ALGO_KF, models, B, T, ys, 0.0, 0, memspace, out, true);
+  return kf_batch_impl(ctx, GF_ALGO_KF, models, B, T, nullptr, ys, 0.0, 0, memspace, out, true);
+}
+
+extern "C" gf_status gf_kf_batch_tv(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
+                                    const int32_t* T, const int32_t* param_steps, const double* ys,
+                                    double jitter, int32_t use_jitter, int32_t memspace,
+                                    gf_kf_out* out) {
+  return kf_batch_impl(ctx, algo, models, B, T, param_steps, ys, jitter, use_jitter, memspace, out, false);
+}
+
+extern "C" gf_status gf_kf_smooth_tv(gf_ctx* ctx, const gf_lg_model* models, int32_t B, const int32_t* T,
+                                     const int32_t* param_steps, const double* ys, int32_t memspace,
+                                     gf_kf_out* out) {
+  return kf_batch_impl(ctx, GF_ALGO_KF, models, B, T, param_steps, ys, 0.0, 0, memspace, out, true);
 }
 
 extern "C" gf_status gf_kf_plan_smooth(gf_kf_plan* p, const double* ys_dev, gf_kf_out* out) {

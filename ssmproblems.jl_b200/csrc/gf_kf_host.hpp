@@ -19,14 +19,17 @@ struct KfSrvRec {
 };
 
 struct KfDesc {
-  int32_t dx, dy, T, pad;
+  // pstep: floats per step of a time-varying model's parameter blocks (0: one
+  // block for every step); p0: float offset of the prior (mu0, Sigma0) from the
+  // filter's first block (0: right after the single block)
+  int32_t dx, dy, T, pstep;
   int64_t poff;    // float offset into the parameter pool
   int64_t yoff;    // double offset into ys
   int64_t soff;    // step offset (ll_steps)
   int64_t moff;    // float offset of means
   int64_t coff;    // float offset of covs
   int32_t index;   // caller's filter index
-  int32_t pad2;
+  int32_t p0;
   // serving only (null in plans): host-mapped destinations of this filter
   KfSrvRec* srv;
   float* srv_mu;       // [dx] final filtered mean
@@ -54,8 +57,13 @@ struct KfRun {
 // parameter pool layout per filter (column-major, unpadded):
 //   A dx*dx | b dx | Q dx*dx | H dy*dx | c dy | R dy*dy | mu0 dx | S0 dx*dx |
 //   UQ dx*dx | UR dy*dy | U0 dx*dx     (upper Cholesky factors, used by the SRKF)
+// A time-varying model (KF only) holds T step blocks (A b Q H c R) followed
+// by mu0 | S0.
 __host__ __device__ inline int64_t kf_param_len(int dx, int dy) {
   return (int64_t)5 * dx * dx + 2 * dx + dy * dx + dy + 2 * dy * dy;
+}
+__host__ __device__ inline int32_t kf_step_block_len(int dx, int dy) {
+  return 2 * dx * dx + dx + dy * dx + dy + dy * dy;
 }
 
 // Dimension buckets: index of the smallest compiled (DXP, DYP) holding (dx, dy),

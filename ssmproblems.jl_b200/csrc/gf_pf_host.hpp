@@ -24,6 +24,9 @@ struct PfLgKernels {
   size_t tc_smem = 0;
   int tc_nm = 0;
   int tc_split = 1;  // blocks per tile of the tensor-core kernel
+  // the same with the staged (bulk-copy) ancestor gather, Dx = 16; null if none
+  void (*prop_tc_staged)(const PfJob*, int) = nullptr;
+  size_t tc_staged_smem = 0;
 };
 
 // FP64 model factors computed once per plan (column-major).

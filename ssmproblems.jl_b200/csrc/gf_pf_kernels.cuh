@@ -211,21 +211,23 @@ __device__ __forceinline__ OffspringRule make_rule(const PfJob& J, const PfScala
 }
 
 
-// Block-wide exclusive scan of unsigned 64-bit values (exact, associative);
-// returns the exclusive prefix of this thread's value, *total gets the sum.
-__device__ __forceinline__ unsigned long long block_excl_scan_u64(unsigned long long v,
-                                                                  unsigned long long* sh,
-                                                                  unsigned long long* total) {
-  const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+// Exclusive scan of unsigned 64-bit values over the threads of S (exact,
+// associative); returns the exclusive prefix of this thread's value, *total
+// gets the sum.  `sh` holds >= 32 values owned by S.
+template <class S>
+__device__ __forceinline__ unsigned long long sync_excl_scan_u64(const S& g, unsigned long long v,
+                                                                 unsigned long long* sh,
+                                                                 unsigned long long* total) {
+  const int lane = g.tid() & 31, wid = g.tid() >> 5, nw = g.size() >> 5;
   unsigned long long x = v;
 #pragma unroll
   for (int o = 1; o < 32; o <<= 1) {
     const unsigned long long y = __shfl_up_sync(0xffffffffu, x, o);
     if (lane >= o) x += y;
   }
-  __syncthreads();
+  g.sync();
   if (lane == 31) sh[wid] = x;
-  __syncthreads();
+  g.sync();
   unsigned long long pre = 0ull, tot = 0ull;
   for (int w = 0; w < nw; ++w) {
     const unsigned long long tw = sh[w];
@@ -234,6 +236,11 @@ __device__ __forceinline__ unsigned long long block_excl_scan_u64(unsigned long 
   }
   *total = tot;
   return pre + x - v;
+}
+__device__ __forceinline__ unsigned long long block_excl_scan_u64(unsigned long long v,
+                                                                  unsigned long long* sh,
+                                                                  unsigned long long* total) {
+  return sync_excl_scan_u64(BlockSync(), v, sh, total);
 }
 
 // Per-thread online accumulation of (max, sum exp, sum exp^2) in FP64.
@@ -281,14 +288,15 @@ static __device__ bool fold_partials(const PfJob& J, int tile, LseAcc a, double*
 }
 
 // Last block: (max, sum e, sum e^2) over every partial, in a fixed order.
-static __device__ void global_stats(const PfJob& J, int nparts, double* red, double* GM_out,
-                                    double* GS1_out, double* GS2_out) {
+template <class S>
+static __device__ void global_stats(const S& g, const PfJob& J, int nparts, double* red,
+                                    double* GM_out, double* GS1_out, double* GS2_out) {
   const int nall = J.ntiles * nparts;
   double m = -INFINITY;
-  for (int bb = threadIdx.x; bb < nall; bb += blockDim.x) m = fmax(m, __ldcg(J.part + (size_t)bb * PF_PW));
-  double GM = block_max(m, red);
+  for (int bb = g.tid(); bb < nall; bb += g.size()) m = fmax(m, __ldcg(J.part + (size_t)bb * PF_PW));
+  double GM = sync_max(g, m, red);
   double s1 = 0.0, s2 = 0.0;
-  for (int bb = threadIdx.x; bb < nall; bb += blockDim.x) {
+  for (int bb = g.tid(); bb < nall; bb += g.size()) {
     const double* p = J.part + (size_t)bb * PF_PW;
     double mb = __ldcg(p);
     if (mb > -INFINITY) {
@@ -298,19 +306,20 @@ static __device__ void global_stats(const PfJob& J, int nparts, double* red, dou
     }
   }
   *GM_out = GM;
-  *GS1_out = block_sum(s1, red);
-  *GS2_out = block_sum(s2, red);
+  *GS1_out = sync_sum(g, s1, red);
+  *GS2_out = sync_sum(g, s2, red);
 }
 
 // Last block: cumulative normalised weight at every tile start,
 // P_b = sum_{b'<b} S1_b' e^{M_b' - lse}, summed in 64-bit fixed point (2^-62
 // units): integer sums are exact, so the parallel scan gives the same monotone
-// prefixes in any order.
-static __device__ void write_tile_prefixes(const PfJob& J, int nparts, double lse) {
+// prefixes in any order.  `wsum` is shared scratch of >= 32 values owned by S.
+template <class S>
+static __device__ void write_tile_prefixes(const S& g, const PfJob& J, int nparts, double lse,
+                                           unsigned long long* wsum) {
   PfScalars* sc = J.sc;
-  __shared__ unsigned long long s_wsum[32];
-  const int per = (J.ntiles + blockDim.x - 1) / blockDim.x;
-  const int b0 = min((int)threadIdx.x * per, J.ntiles), b1 = min(b0 + per, J.ntiles);
+  const int per = (J.ntiles + g.size() - 1) / g.size();
+  const int b0 = min(g.tid() * per, J.ntiles), b1 = min(b0 + per, J.ntiles);
   unsigned long long tot = 0ull;
   auto tile_fix = [&](int bb) {  // fixed-point normalised weight of tile bb
     unsigned long long w = 0ull;
@@ -323,39 +332,36 @@ static __device__ void write_tile_prefixes(const PfJob& J, int nparts, double ls
   };
   for (int bb = b0; bb < b1; ++bb) tot += tile_fix(bb);
   unsigned long long all = 0ull;
-  unsigned long long run = block_excl_scan_u64(tot, s_wsum, &all);
+  unsigned long long run = sync_excl_scan_u64(g, tot, wsum, &all);
   for (int bb = b0; bb < b1; ++bb) {
     J.tprefix[bb] = (double)run * kInvFix;
     run += tile_fix(bb);
   }
-  if (threadIdx.x == 0) {
+  if (g.tid() == 0) {
     J.tprefix[J.ntiles] = (double)all * kInvFix;
     sc->wn = (double)all * kInvFix;
   }
 }
 
-// Folds the block's accumulators into part[tile] and lets the last block of
-// the job finalise the step (containers.jl:160-173 marginalise!,
-// particles.jl:70-73 baseline, resamplers.jl:179-183 ESS decision).
-// Baseline: log N after a resample or for the initial TypelessZero weights
-// (plus the auxiliary filter's first-stage shift sc->base_adj after one of its
-// resamples, resamplers.jl:118-138); otherwise logsumexp of the normalised
-// log-weights, which is 0 up to the rounding of the normalisation (below
-// 1e-15), so it is taken as 0.
-// A tile may be covered by `nparts` blocks (block `part` of tile `tile`); the
-// partials are then kept per part, folded in part order and summed per tile
-// for the tile prefixes.
-static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh, LseAcc a,
-                                    double* red, int part = 0, int nparts = 1) {
+// The step's finalise, run by the threads of S in the job's last block (or
+// group) once every partial of the step is in J.part (containers.jl:160-173
+// marginalise!, particles.jl:70-73 baseline, resamplers.jl:179-183 ESS
+// decision).  Baseline: log N after a resample or for the initial
+// TypelessZero weights (plus the auxiliary filter's first-stage shift
+// sc->base_adj after one of its resamples, resamplers.jl:118-138); otherwise
+// logsumexp of the normalised log-weights, which is 0 up to the rounding of the
+// normalisation (below 1e-15), so it is taken as 0.  `red`, `wsum` and `s_res`
+// are shared scratch owned by S.
+template <class S>
+static __device__ void finish_step(const S& g, const PfJob& J, int t, bool fresh, int nparts,
+                                   double* red, unsigned long long* wsum, int* s_res) {
   PfScalars* sc = J.sc;
-  if (!fold_partials(J, tile, a, red, part, nparts)) return;
-  // ---- last block: fold all partials in a fixed order (deterministic) ----
+  // fold all partials in a fixed order (deterministic)
   double GM, GS1, GS2;
-  global_stats(J, nparts, red, &GM, &GS1, &GS2);
+  global_stats(g, J, nparts, red, &GM, &GS1, &GS2);
   const double base = fresh ? J.log_n + sc->base_adj : 0.0;
-  __shared__ int s_res;
   const double lse = GM + log(GS1);
-  if (threadIdx.x == 0) {
+  if (g.tid() == 0) {
     double inc = lse - base;
     double ess = GS1 * GS1 / GS2;
     if (!(lse > -INFINITY) || isnan(lse)) sc->status = GF_ERR_ARG;  // all weights vanished
@@ -373,19 +379,31 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
     sc->ess = ess;
     sc->resample = res;
     sc->base_adj = 0.0;
-    s_res = res;
+    *s_res = res;
   }
-  __syncthreads();
+  g.sync();
   // the auxiliary filter decides in its lookahead kernel instead
-  if (s_res && !J.eta) write_tile_prefixes(J, nparts, lse);
-  __syncthreads();
-  if (threadIdx.x == 0) {
+  if (*s_res && !J.eta) write_tile_prefixes(g, J, nparts, lse, wsum);
+  g.sync();
+  if (g.tid() == 0) {
     sc->uniform = 0;
     sc->scan_tile = 0u;
     sc->counter = 0u;
     __threadfence();
     sc->t = t;
   }
+}
+
+// Folds the block's accumulators into part[tile] and lets the last block of
+// the job finalise the step (finish_step).  A tile may be covered by `nparts`
+// blocks (block `part` of tile `tile`); the partials are then kept per part,
+// folded in part order and summed per tile for the tile prefixes.
+static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh, LseAcc a,
+                                    double* red, int part = 0, int nparts = 1) {
+  if (!fold_partials(J, tile, a, red, part, nparts)) return;
+  __shared__ unsigned long long s_wsum[32];
+  __shared__ int s_res;
+  finish_step(BlockSync(), J, t, fresh, nparts, red, s_wsum, &s_res);
 }
 
 // Auxiliary particle filter, last block of the lookahead launch of step t:
@@ -398,9 +416,10 @@ static __device__ void apf_finish(const PfJob& J, int tile, int t, LseAcc a, dou
   PfScalars* sc = J.sc;
   if (!fold_partials(J, tile, a, red, 0, 1)) return;
   double GM, GS1, GS2;
-  global_stats(J, 1, red, &GM, &GS1, &GS2);
+  global_stats(BlockSync(), J, 1, red, &GM, &GS1, &GS2);
   const double lse1 = GM + log(GS1);
   __shared__ int s_res;
+  __shared__ unsigned long long s_wsum[32];
   if (threadIdx.x == 0) {
     const double ess = GS1 * GS1 / GS2;
     const int s = J.schedule ? (int)J.schedule[t - 1] : -1;
@@ -414,7 +433,7 @@ static __device__ void apf_finish(const PfJob& J, int tile, int t, LseAcc a, dou
     s_res = res;
   }
   __syncthreads();
-  if (s_res) write_tile_prefixes(J, 1, lse1);
+  if (s_res) write_tile_prefixes(BlockSync(), J, 1, lse1, s_wsum);
   __syncthreads();
   if (threadIdx.x == 0) {
     sc->counter = 0u;

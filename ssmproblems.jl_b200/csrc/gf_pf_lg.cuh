@@ -35,6 +35,10 @@ __device__ __forceinline__ void draw_noise(const PfJob& J, const Real* noise, in
   if (noise) {
 #pragma unroll
     for (int d = 0; d < DXP; ++d) e[d] = d < dx ? noise[(size_t)d * N + i] : Real(0);
+  } else if (DXP == 1) {
+    Real tmp[4];  // 1-D: particle i takes normal i % 4 of call i / 4
+    philox_normals4<Real>(J.seed, (uint32_t)(i >> 2), (uint32_t)t, 0u, tmp);
+    e[0] = tmp[i & 3];
   } else {
 #pragma unroll
     for (int q = 0; q < (DXP + 3) / 4; ++q) {
@@ -44,6 +48,29 @@ __device__ __forceinline__ void draw_noise(const PfJob& J, const Real* noise, in
       for (int r = 0; r < 4; ++r)
         if (4 * q + r < DXP) e[4 * q + r] = tmp[r];
     }
+  }
+}
+
+// 1-D noise of a thread's PF_PPT particles (i = tile * PF_TILE + p * PF_THREADS
+// + threadIdx.x): lane l of each warp runs Philox call (i / 4) for the group of
+// four consecutive particles at p = l / 8, slot l % 8, and the warp hands each
+// particle normal i % 4 by shuffles -- one call per four particles.  All 32
+// lanes take part (calls beyond N are unused).
+template <typename Real>
+__device__ __forceinline__ void noise_1d_tile(uint64_t seed, int tile, int t, Real* ep) {
+  static_assert(PF_PPT * PF_THREADS == PF_TILE && PF_PPT == 4, "four particles per thread");
+  const int lane = threadIdx.x & 31;
+  const int64_t wbase = (int64_t)tile * PF_TILE + (threadIdx.x & ~31);
+  const int64_t mine = wbase + (lane >> 3) * PF_THREADS + 4 * (lane & 7);
+  Real r4[4];
+  philox_normals4<Real>(seed, (uint32_t)(mine >> 2), (uint32_t)t, 0u, r4);
+#pragma unroll
+  for (int p = 0; p < PF_PPT; ++p) {
+    const int src = p * 8 + (lane >> 2);
+    const Real v0 = __shfl_sync(0xffffffffu, r4[0], src), v1 = __shfl_sync(0xffffffffu, r4[1], src);
+    const Real v2 = __shfl_sync(0xffffffffu, r4[2], src), v3 = __shfl_sync(0xffffffffu, r4[3], src);
+    const int k = lane & 3;
+    ep[p] = k == 0 ? v0 : (k == 1 ? v1 : (k == 2 ? v2 : v3));
   }
 }
 
@@ -95,6 +122,10 @@ __device__ __forceinline__ void lg_propagate_tile(const PfJob& J, int tile) {
   const Real* eta = reinterpret_cast<const Real*>(J.eta);
   const bool apf = resamp && eta != nullptr;
   LseAcc acc;
+  Real ep1[DXP == 1 ? PF_PPT : 1];
+  if constexpr (DXP == 1) {
+    if (!noise) noise_1d_tile<Real>(seed, tile, t, ep1);
+  }
 
   for (int p = 0; p < PF_PPT; ++p) {
     const int64_t i = (int64_t)tile * PF_TILE + p * PF_THREADS + threadIdx.x;
@@ -140,6 +171,8 @@ __device__ __forceinline__ void lg_propagate_tile(const PfJob& J, int tile) {
           const int c = 4 * q + cc;
           e4[cc] = (c < DXP && c < dx) ? noise[(size_t)c * N + i] : Real(0);
         }
+      } else if constexpr (DXP == 1) {
+        e4[0] = ep1[p];
       } else {
         philox_normals4<Real>(seed, (uint32_t)i, (uint32_t)t, (uint32_t)q, e4);
       }
@@ -316,8 +349,26 @@ struct TcLayout {
   static constexpr int min_blocks = by_smem < 1 ? 1 : (by_smem > 5 ? 5 : by_smem);
 };
 
-template <int DXP, int DYP>
-__global__ void __launch_bounds__(TC_THREADS, (TcLayout<DXP, DYP>::min_blocks)) pf_lg_propagate_tc(const PfJob* __restrict__ jobs,
+// Staged ancestor gather (STAGED instances of pf_lg_propagate_tc): while the
+// MMA and epilogue of sub-tile s run, one thread copies the contiguous source
+// range [a_first, a_last] of sub-tile s+1 (sorted ancestors: the CPU-rule
+// systematic and stratified resamplers, or a = i without a resample) from every
+// state dimension into shared memory with cp.async.bulk (16-byte aligned, size
+// a multiple of 16), completing on an mbarrier; the threads then read their
+// gathered states from shared memory.  Ranges longer than TC_GCAP particles,
+// the multinomial search and N % 4 != 0 take the per-thread gather.
+constexpr int TC_GCAP = 192;
+template <int DXP, int DYP, bool STAGED>
+struct TcSmem {
+  static constexpr size_t gather_off = (TcLayout<DXP, DYP>::smem_bytes + 127) / 128 * 128;
+  static constexpr size_t bytes = STAGED ? gather_off + sizeof(float) * DXP * TC_GCAP
+                                         : TcLayout<DXP, DYP>::smem_bytes;
+  static constexpr int by_smem = (int)((228u * 1024u) / (bytes + 2048u));
+  static constexpr int min_blocks = by_smem < 1 ? 1 : (by_smem > 5 ? 5 : by_smem);
+};
+
+template <int DXP, int DYP, bool STAGED = false>
+__global__ void __launch_bounds__(TC_THREADS, (TcSmem<DXP, DYP, STAGED>::min_blocks)) pf_lg_propagate_tc(const PfJob* __restrict__ jobs,
                                                                int njobs) {
   using Lay = LgLayout<DXP, DYP>;
   using TL = TcLayout<DXP, DYP>;
@@ -330,8 +381,10 @@ __global__ void __launch_bounds__(TC_THREADS, (TcLayout<DXP, DYP>::min_blocks)) 
   float* sb = sBl + NM * K;
   float* sHb = sb + DXP;
   float* sy = sHb + DYP;
+  float* sG = reinterpret_cast<float*>(smraw + TcSmem<DXP, DYP, STAGED>::gather_off);  // [DXP][TC_GCAP]
   __shared__ double red[32];
-  __shared__ uint64_t mbar;
+  __shared__ uint64_t mbar, gbar;
+  __shared__ int64_t glo[2];  // staged sub-tile: first copied source particle, -1 = per-thread gather
   __shared__ uint32_t tmem_slot;
 
   const int jb = find_job(jobs, njobs, blockIdx.x / TC_SPLIT, false);
@@ -364,6 +417,7 @@ __global__ void __launch_bounds__(TC_THREADS, (TcLayout<DXP, DYP>::min_blocks)) 
   }
   if (tid == 0) {
     umma::mbar_init(&mbar, 1);
+    if (STAGED) umma::mbar_init(&gbar, 1);
     umma::fence_mbar_init();
   }
   if (tid < 32) umma::tmem_alloc(&tmem_slot, TL::NCOLS);
@@ -395,6 +449,29 @@ __global__ void __launch_bounds__(TC_THREADS, (TcLayout<DXP, DYP>::min_blocks)) 
   const int64_t ib = (int64_t)tile * PF_TILE + part * TC_SUB_BLOCK * TC_THREADS + tid;
   const bool pref = resamp && !searched;
   int32_t a_nx = (pref && ib < N) ? ancv[ib] : 0;
+  // staged gather of sub-tile s (thread 0): bulk copies of the source range,
+  // or glo = -1 (per-thread gather); the gbar phase completes either way
+  const bool can_stage = STAGED && !searched && (N & 3) == 0;
+  auto stage = [&](int s) {
+    const int64_t f = ib - tid + (int64_t)s * TC_THREADS;
+    const int64_t l = min(f + TC_THREADS - 1, N - 1);
+    int64_t lo = -1, cnt = 0;
+    if (can_stage && f < N) {
+      const int64_t a0 = resamp ? (int64_t)ancv[f] : f, a1 = resamp ? (int64_t)ancv[l] : l;
+      lo = a0 & ~(int64_t)3;
+      cnt = min((a1 | 3) + 1, N) - lo;
+      if (cnt > TC_GCAP) lo = -1;
+    }
+    glo[s & 1] = lo;
+    if (lo >= 0) {
+      umma::mbar_arrive_expect_tx(&gbar, (uint32_t)(dx * cnt * 4));
+      for (int d = 0; d < dx; ++d)
+        umma::bulk_copy_g2s(sG + d * TC_GCAP, Xs + (size_t)d * N + lo, (uint32_t)(cnt * 4), &gbar);
+    } else {
+      umma::mbar_arrive(&gbar);
+    }
+  };
+  if (STAGED && tid == 0) stage(0);
   for (int s = 0; s < TC_SUB_BLOCK; ++s) {
     const int64_t i = ib + (int64_t)s * TC_THREADS;
     const bool valid = i < N;
@@ -402,8 +479,19 @@ __global__ void __launch_bounds__(TC_THREADS, (TcLayout<DXP, DYP>::min_blocks)) 
     if (valid && resamp) a = searched ? find_ancestor(J, sc, t, i, 0, N) : (int64_t)a_nx;
     if (pref && s + 1 < TC_SUB_BLOCK) a_nx = i + TC_THREADS < N ? ancv[i + TC_THREADS] : 0;
     float xe[K];
+    int64_t g0 = -1;
+    if (STAGED) {
+      ok = umma::mbar_wait(&gbar, (uint32_t)(s & 1), TC_WAIT) && ok;
+      g0 = glo[s & 1];
+    }
+    if (g0 >= 0) {
+      const float* src = sG + (a - g0);
 #pragma unroll
-    for (int d = 0; d < DXP; ++d) xe[d] = (valid && d < dx) ? Xs[(size_t)d * N + a] : 0.f;
+      for (int d = 0; d < DXP; ++d) xe[d] = (valid && d < dx) ? src[d * TC_GCAP] : 0.f;
+    } else {
+#pragma unroll
+      for (int d = 0; d < DXP; ++d) xe[d] = (valid && d < dx) ? Xs[(size_t)d * N + a] : 0.f;
+    }
 #pragma unroll
     for (int q = 0; q < DXP / 4; ++q) {
       float e4[4];
@@ -435,6 +523,8 @@ __global__ void __launch_bounds__(TC_THREADS, (TcLayout<DXP, DYP>::min_blocks)) 
     umma::fence_async_smem();
     __syncthreads();
     if (tid == 0) {
+      // every thread has read sub-tile s's staged states: stage s + 1
+      if (STAGED && s + 1 < TC_SUB_BLOCK) stage(s + 1);
       umma::fence_after_sync();
 #pragma unroll
       for (int ks = 0; ks < K / 8; ++ks) {
@@ -475,6 +565,7 @@ __global__ void __launch_bounds__(TC_THREADS, (TcLayout<DXP, DYP>::min_blocks)) 
     __syncthreads();
   }
   if (!ok && tid == 0) sc->status = GF_ERR_TIMEOUT;
+  if (STAGED && !ok) umma::mbar_wait(&gbar, (uint32_t)((TC_SUB_BLOCK - 1) & 1), TC_WAIT);  // copies in flight
   if (tid < 32) umma::tmem_dealloc(tbase, TL::NCOLS);
   block_finish(J, tile, t, fresh, acc, red, part, TC_SPLIT);
 }
@@ -574,6 +665,10 @@ PfLgKernels make_lg() {
     k.tc_smem = TcLayout<DXP, DYP>::smem_bytes;
     k.tc_nm = TcLayout<DXP, DYP>::NM;
     k.tc_split = TC_SPLIT;
+    if constexpr (DXP == 16) {
+      k.prop_tc_staged = pf_lg_propagate_tc<DXP, DYP, true>;
+      k.tc_staged_smem = TcSmem<DXP, DYP, true>::bytes;
+    }
   }
   return k;
 }

@@ -97,9 +97,10 @@ gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cf
   o->pp.insert(o->pp.end(), f.K.begin(), f.K.end());
   o->pp.insert(o->pp.end(), f.vb.begin(), f.vb.end());
   if (o->k.prop_tc && !(flags & GF_PLAN_SIMT)) {
-    o->prop = o->k.prop_tc;
+    const bool staged = (flags & GF_PLAN_STAGED_GATHER) && o->k.prop_tc_staged;
+    o->prop = staged ? o->k.prop_tc_staged : o->k.prop_tc;
     o->threads = 128;
-    o->smem = o->k.tc_smem;
+    o->smem = staged ? o->k.tc_staged_smem : o->k.tc_smem;
     o->split = o->k.tc_split;
   } else {
     o->prop = o->k.prop;

@@ -91,6 +91,12 @@ __global__ void a2o_kernel(const int64_t* __restrict__ anc, int64_t n, unsigned 
 template <typename Real>
 __global__ void rng_normals_kernel(uint64_t seed, int t, int dx, int64_t n, Real* __restrict__ out) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+    if (dx == 1) {  // 1-D layout: normal i % 4 of call i / 4
+      Real tmp[4];
+      philox_normals4<Real>(seed, (uint32_t)(i >> 2), (uint32_t)t, 0u, tmp);
+      out[i] = tmp[i & 3];
+      continue;
+    }
     for (int q = 0; q * 4 < dx; ++q) {
       Real tmp[4];
       philox_normals4<Real>(seed, (uint32_t)i, (uint32_t)t, (uint32_t)q, tmp);

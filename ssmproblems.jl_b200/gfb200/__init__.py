@@ -21,8 +21,10 @@ from .filtering import (MvNormal, ParticleDistribution, ancestors_to_offspring, 
 from .models import (HierarchicalSSM, HomogeneousGaussianPrior,  # noqa: F401
                      HomogeneousLinearGaussianLatentDynamics,
                      HomogeneousLinearGaussianObservationProcess, InnerDynamics,
-                     LatentDynamics, ObservationProcess, StatePrior, StateSpaceModel,
-                     create_homogeneous_linear_gaussian_model)
+                     LatentDynamics, NonHomogeneousLinearGaussianLatentDynamics,
+                     NonHomogeneousLinearGaussianObservationProcess, ObservationProcess,
+                     StatePrior, StateSpaceModel, create_homogeneous_linear_gaussian_model,
+                     create_nonhomogeneous_linear_gaussian_model)
 from .serving import Server  # noqa: F401,E402
 from .csmc import (AncestorSampling, BackwardSimulation, ConditionalSMC, CSMCModel,  # noqa: F401,E402
                    CSMCState, NoRefreshment)

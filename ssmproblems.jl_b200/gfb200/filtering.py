@@ -290,6 +290,19 @@ def _rbpf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sch
     return state, float(out["ll"][0])
 
 
+def _param_steps(models, T):
+    """Per-model parameter blocks for the time-varying entry points, or None
+    when every model is homogeneous.  A time-varying model needs a block for
+    every observed step (calc_params(dyn, t) for t = 1..T)."""
+    if not any(m.is_time_varying() for m in models):
+        return None
+    ps = np.array([m.param_steps() for m in models], dtype=np.int32)
+    for f, m in enumerate(models):
+        if m.is_time_varying() and ps[f] < T[f]:
+            raise ValueError(f"model {f}: {ps[f]} parameter steps for {T[f]} observations")
+    return ps
+
+
 def filter_batch(models, algo, observations, *, ctx=None, want_steps=True, want_covs=True):
     """Many independent Kalman / square-root Kalman filters in one batched launch.
     Returns a list of (MvNormal(final mu, Sigma), ll) with per-step outputs
@@ -301,6 +314,7 @@ def filter_batch(models, algo, observations, *, ctx=None, want_steps=True, want_
     mcs = (L.LGModelC * B)(*[m._c_struct() for m in models])
     ys_list = [L.f64(y).reshape(-1, m.dy) for y, m in zip(observations, models)]
     T = np.array([y.shape[0] for y in ys_list], dtype=np.int32)
+    psteps = _param_steps(models, T)
     ys = np.concatenate([y.ravel() for y in ys_list]) if B else np.zeros(0)
     dxs = np.array([m.dx for m in models])
     tot_steps = int(T.sum())
@@ -310,10 +324,16 @@ def filter_batch(models, algo, observations, *, ctx=None, want_steps=True, want_
                status=np.zeros(B, np.int32))
     o = L.KFOutC(*[L.ptr(out[k]) for k in ("ll", "ll_steps", "means", "covs", "status")])
     jit = algo.jitter
-    L.check(ctx.h, L.load().gf_kf_batch(ctx.h, algo.algo, mcs,  B,
-                                        T.ctypes.data_as(C.POINTER(C.c_int32)), L.ptr(ys),
-                                        float(jit or 0.0), int(jit is not None), L.GF_MEM_HOST,
-                                        C.byref(o)))
+    i32 = C.POINTER(C.c_int32)
+    if psteps is None:
+        L.check(ctx.h, L.load().gf_kf_batch(ctx.h, algo.algo, mcs,  B, T.ctypes.data_as(i32),
+                                            L.ptr(ys), float(jit or 0.0), int(jit is not None),
+                                            L.GF_MEM_HOST, C.byref(o)))
+    else:
+        L.check(ctx.h, L.load().gf_kf_batch_tv(ctx.h, algo.algo, mcs, B, T.ctypes.data_as(i32),
+                                               psteps.ctypes.data_as(i32), L.ptr(ys),
+                                               float(jit or 0.0), int(jit is not None),
+                                               L.GF_MEM_HOST, C.byref(o)))
     res = []
     so = mo = co = 0
     for f, m in enumerate(models):
@@ -341,6 +361,7 @@ def smooth_batch(models, observations, *, ctx=None):
     mcs = (L.LGModelC * B)(*[m._c_struct() for m in models])
     ys_list = [L.f64(y).reshape(-1, m.dy) for y, m in zip(observations, models)]
     T = np.array([y.shape[0] for y in ys_list], dtype=np.int32)
+    psteps = _param_steps(models, T)
     ys = np.concatenate([y.ravel() for y in ys_list]) if B else np.zeros(0)
     dxs = np.array([m.dx for m in models])
     out = dict(ll=np.zeros(B), ll_steps=None,
@@ -348,8 +369,14 @@ def smooth_batch(models, observations, *, ctx=None):
                covs=np.zeros(int((T * dxs * dxs).sum()), np.float32),
                status=np.zeros(B, np.int32))
     o = L.KFOutC(*[L.ptr(out[k]) for k in ("ll", "ll_steps", "means", "covs", "status")])
-    L.check(ctx.h, L.load().gf_kf_smooth(ctx.h, mcs, B, T.ctypes.data_as(C.POINTER(C.c_int32)),
-                                         L.ptr(ys), L.GF_MEM_HOST, C.byref(o)))
+    i32 = C.POINTER(C.c_int32)
+    if psteps is None:
+        L.check(ctx.h, L.load().gf_kf_smooth(ctx.h, mcs, B, T.ctypes.data_as(i32),
+                                             L.ptr(ys), L.GF_MEM_HOST, C.byref(o)))
+    else:
+        L.check(ctx.h, L.load().gf_kf_smooth_tv(ctx.h, mcs, B, T.ctypes.data_as(i32),
+                                                psteps.ctypes.data_as(i32), L.ptr(ys),
+                                                L.GF_MEM_HOST, C.byref(o)))
     res = []
     mo = co = 0
     for f, m in enumerate(models):

@@ -51,6 +51,33 @@ class HomogeneousLinearGaussianObservationProcess(ObservationProcess):
         self.R = fortran64(np.atleast_2d(R))
 
 
+class NonHomogeneousLinearGaussianLatentDynamics(LatentDynamics):
+    """Time-varying linear-Gaussian dynamics: calc_params(dyn, t) = (As[t], bs[t],
+    Qs[t]) for 1-based step t (models/linear_gaussian.jl:44-52; GFTest's
+    NonHomogeneousLinearGaussianLatentDynamics, GFTest/models/linear_gaussian.jl:42-66)."""
+
+    def __init__(self, As, bs, Qs):
+        if not (len(As) == len(bs) == len(Qs)) or len(As) < 1:
+            raise ValueError("As, bs, Qs need one entry per step")
+        self.As = [fortran64(np.atleast_2d(a)) for a in As]
+        self.bs = [f64(v).ravel() for v in bs]
+        self.Qs = [fortran64(np.atleast_2d(q)) for q in Qs]
+        self.A = self.As[0]
+
+
+class NonHomogeneousLinearGaussianObservationProcess(ObservationProcess):
+    """Time-varying observations: calc_params(obs, t) = (Hs[t], cs[t], Rs[t])
+    (models/linear_gaussian.jl:54-63; GFTest/models/linear_gaussian.jl:68-95)."""
+
+    def __init__(self, Hs, cs, Rs):
+        if not (len(Hs) == len(cs) == len(Rs)) or len(Hs) < 1:
+            raise ValueError("Hs, cs, Rs need one entry per step")
+        self.Hs = [fortran64(np.atleast_2d(h)) for h in Hs]
+        self.cs = [f64(v).ravel() for v in cs]
+        self.Rs = [fortran64(np.atleast_2d(r)) for r in Rs]
+        self.H = self.Hs[0]
+
+
 class StateSpaceModel:
     """SSMProblems.StateSpaceModel{PT,LD,OP} (SSMProblems.jl:264-272)."""
 
@@ -63,6 +90,23 @@ class StateSpaceModel:
                 and isinstance(self.dyn, HomogeneousLinearGaussianLatentDynamics)
                 and isinstance(self.obs, HomogeneousLinearGaussianObservationProcess))
 
+    def is_time_varying(self):
+        """A linear-Gaussian model whose dynamics or observations vary with t."""
+        return (isinstance(self.prior, HomogeneousGaussianPrior)
+                and isinstance(self.dyn, (HomogeneousLinearGaussianLatentDynamics,
+                                          NonHomogeneousLinearGaussianLatentDynamics))
+                and isinstance(self.obs, (HomogeneousLinearGaussianObservationProcess,
+                                          NonHomogeneousLinearGaussianObservationProcess))
+                and not self.is_linear_gaussian())
+
+    def param_steps(self):
+        """Per-step parameter blocks the model carries (1 if homogeneous)."""
+        if not self.is_time_varying():
+            return 1
+        n = [len(x.As) for x in (self.dyn,) if hasattr(x, "As")] + \
+            [len(x.Hs) for x in (self.obs,) if hasattr(x, "Hs")]
+        return min(n)
+
     @property
     def dx(self):
         return self.dyn.A.shape[0]
@@ -72,19 +116,42 @@ class StateSpaceModel:
         return self.obs.H.shape[0]
 
     def _c_struct(self):
-        """gf_lg_model view; keeps references to the arrays alive on self."""
-        if not self.is_linear_gaussian():
-            raise TypeError("filter on the GPU needs a homogeneous linear-Gaussian model")
+        """gf_lg_model view; keeps references to the arrays alive on self.  For a
+        time-varying model the A, b, Q, H, c, R pointers hold param_steps()
+        step-major blocks (each column-major)."""
+        import ctypes as C
+        dp = C.POINTER(C.c_double)
         p, d, o = self.prior, self.dyn, self.obs
+        dx, dy = self.dx, self.dy
+        if self.is_time_varying():
+            n = self.param_steps()
+            dl = [(getattr(d, "As", None), d.A), (getattr(d, "bs", None), getattr(d, "b", None)),
+                  (getattr(d, "Qs", None), getattr(d, "Q", None))]
+            ol = [(getattr(o, "Hs", None), o.H), (getattr(o, "cs", None), getattr(o, "c", None)),
+                  (getattr(o, "Rs", None), getattr(o, "R", None))]
+            shapes = [(dx, dx), (dx,), (dx, dx), (dy, dx), (dy,), (dy, dy)]
+            stk = []
+            for (seq, one), shp in zip(dl + ol, shapes):
+                blocks = seq[:n] if seq is not None else [one] * n
+                for blk in blocks:
+                    if blk.shape != shp:
+                        raise ValueError(f"DimensionMismatch: expected {shp}, got {blk.shape}")
+                stk.append(np.ascontiguousarray(np.concatenate([np.asarray(b).ravel(order="F")
+                                                                for b in blocks])))
+            arrs = [p.mu0, p.Sigma0] + stk
+            for a, s in zip(arrs[:2], [(dx,), (dx, dx)]):
+                if a.shape != s:
+                    raise ValueError(f"DimensionMismatch: expected {s}, got {a.shape}")
+            self._keep = arrs
+            return LGModelC(dx, dy, *[a.ctypes.data_as(dp) for a in arrs])
+        if not self.is_linear_gaussian():
+            raise TypeError("filter on the GPU needs a linear-Gaussian model")
         arrs = [p.mu0, p.Sigma0, d.A, d.b, d.Q, o.H, o.c, o.R]
         self._keep = arrs
-        dx, dy = self.dx, self.dy
         shapes = [(dx,), (dx, dx), (dx, dx), (dx,), (dx, dx), (dy, dx), (dy,), (dy, dy)]
         for a, s in zip(arrs, shapes):
             if a.shape != s:
                 raise ValueError(f"DimensionMismatch: expected {s}, got {a.shape}")
-        import ctypes as C
-        dp = C.POINTER(C.c_double)
         return LGModelC(dx, dy, *[a.ctypes.data_as(dp) for a in arrs])
 
 
@@ -93,6 +160,15 @@ def create_homogeneous_linear_gaussian_model(mu0, Sigma0, A, b, Q, H, c, R):
     return StateSpaceModel(HomogeneousGaussianPrior(mu0, Sigma0),
                            HomogeneousLinearGaussianLatentDynamics(A, b, Q),
                            HomogeneousLinearGaussianObservationProcess(H, c, R))
+
+
+def create_nonhomogeneous_linear_gaussian_model(mu0, Sigma0, As, bs, Qs, Hs, cs, Rs):
+    """A time-varying linear-Gaussian model from per-step parameter sequences
+    (entry t-1 = step t), the model of GFTest's
+    create_nonhomogeneous_linear_gaussian_model (GFTest/models/linear_gaussian.jl:97-119)."""
+    return StateSpaceModel(HomogeneousGaussianPrior(mu0, Sigma0),
+                           NonHomogeneousLinearGaussianLatentDynamics(As, bs, Qs),
+                           NonHomogeneousLinearGaussianObservationProcess(Hs, cs, Rs))
 
 
 class InnerDynamics(LatentDynamics):

@@ -17,7 +17,8 @@ using GeneralisedFilters: KalmanFilter, SRKalmanFilter, ParticleFilter, ESSResam
     Systematic, Stratified, Multinomial, LatentProposal, RBPF, HierarchicalSSM,
     ParticleDistribution, Particle, TypelessZero, AuxiliaryParticleFilter, MeanPredictive,
     ModePredictive, DrawPredictive, ConditionalSMC, NoRefreshment, AncestorSampling,
-    BackwardSimulation
+    BackwardSimulation, AbstractProposal
+using GeneralisedFilters.GFTest: OptimalProposal, OverdispersedProposal, InnerDynamics
 using SSMProblems
 using Distributions: MvNormal
 using LinearAlgebra
@@ -29,7 +30,7 @@ const GF_OK = Int32(0)
 const GF_ERR_NOT_PD = Int32(1)
 const GF_MEM_HOST = Int32(0)
 const GF_PREC_F32, GF_PREC_F64 = Int32(0), Int32(1)
-const GF_PROP_BOOTSTRAP = Int32(0)
+const GF_PROP_BOOTSTRAP, GF_PROP_OPTIMAL, GF_PROP_OVERDISPERSED = Int32(0), Int32(1), Int32(2)
 
 # --- C structs (field order and types match include/gf_b200.h) ---------------
 struct GfLgModel
@@ -40,6 +41,28 @@ struct GfLgModel
     A::Ptr{Float64}
     b::Ptr{Float64}
     Q::Ptr{Float64}
+    H::Ptr{Float64}
+    c::Ptr{Float64}
+    R::Ptr{Float64}
+end
+
+struct GfRbModel          # gf_rb_model
+    dxo::Int32
+    dz::Int32
+    dy::Int32
+    mu_o::Ptr{Float64}
+    Sigma_o::Ptr{Float64}
+    A_o::Ptr{Float64}
+    b_o::Ptr{Float64}
+    Q_o::Ptr{Float64}
+    mu_z::Ptr{Float64}
+    Sigma_z::Ptr{Float64}
+    A_z::Ptr{Float64}
+    b_z::Ptr{Float64}
+    C_z::Ptr{Float64}
+    Q_z::Ptr{Float64}
+    q_gamma::Float64
+    q_index::Int32
     H::Ptr{Float64}
     c::Ptr{Float64}
     R::Ptr{Float64}
@@ -214,14 +237,38 @@ function GeneralisedFilters.filter(
     return _bf(rng, model, algo, observations, Int32(0); kwargs...)
 end
 
-function _bf(rng, model, algo, observations, lookahead::Int32; callback=nothing, precision::Symbol=:f32,
-             kwargs...)
+# Guided filters (particles.jl:175-195) with the linear-Gaussian proposals the
+# reference tests use: OptimalProposal (q = p(x_t | x_{t-1}, y_t), a Kalman update
+# of N(A x + b, Q)) and OverdispersedProposal (N(A x + b, k Q)), GFTest/proposals.jl.
+# The proposal's own dyn/obs must be the model's (as GFTest builds them).
+function GeneralisedFilters.filter(
+    rng::AbstractRNG,
+    model::GeneralisedFilters.LinearGaussianStateSpaceModel,
+    algo::ParticleFilter{<:ESSResampler,<:Union{OptimalProposal,OverdispersedProposal}},
+    observations::AbstractVector;
+    kwargs...,
+)
+    q = algo.proposal
+    code = q isa OptimalProposal ? GF_PROP_OPTIMAL : GF_PROP_OVERDISPERSED
+    k = q isa OverdispersedProposal ? Float64(q.k) : 1.0
+    return _bf(rng, model, algo, observations, Int32(0); proposal=code, proposal_k=k, kwargs...)
+end
+
+# The reference's particles carry the model's element type: FP64 unless the
+# model is Float32 (then the FP32-state / FP64-normaliser kernels run).
+default_precision(model) = eltype(GeneralisedFilters.calc_params(SSMProblems.dyn(model), 1)[1]) === Float32 ?
+                           :f32 : :f64
+
+function _bf(rng, model, algo, observations, lookahead::Int32; callback=nothing,
+             precision::Union{Symbol,Nothing}=nothing, proposal::Int32=GF_PROP_BOOTSTRAP,
+             proposal_k::Float64=1.0, kwargs...)
     isnothing(callback) || throw(ArgumentError("GFB200 supports callback=nothing only"))
+    precision = isnothing(precision) ? default_precision(model) : precision
     N, T = algo.N, length(observations)
     ys = reduce(vcat, [Float64.(collect(y)) for y in observations])
     cfg = Ref(GfPfConfig(N, resampler_code(algo.resampler.resampler), 0,
                          algo.resampler.threshold,
-                         precision === :f64 ? GF_PREC_F64 : GF_PREC_F32, GF_PROP_BOOTSTRAP, 1.0,
+                         precision === :f64 ? GF_PREC_F64 : GF_PREC_F32, proposal, proposal_k,
                          rand(rng, UInt64), C_NULL, lookahead))
     return with_lg_model(model) do m
         dx = Int(m.dx)
@@ -240,6 +287,114 @@ function _bf(rng, model, algo, observations, lookahead::Int32; callback=nothing,
         particles = [Particle(Vector{ET}(states[i, :]), logw[i], 0) for i in 1:N]
         return ParticleDistribution(particles, zero(Float64)), ll[1]
     end
+end
+
+# --- filter_batch(models, KalmanFilter() | SRKF(), yss) -----------------------------
+"""
+    filter_batch(models, algo::Union{KalmanFilter,SRKalmanFilter}, yss) -> Vector{(MvNormal, ll)}
+
+B independent homogeneous linear-Gaussian models of uneven dx, dy and length,
+filtered in one batched launch (gf_kf_batch); element f equals
+`filter(models[f], algo, yss[f])`.
+"""
+function filter_batch(models::AbstractVector, algo::Union{KalmanFilter,SRKalmanFilter},
+                      yss::AbstractVector)
+    B = length(models)
+    length(yss) == B || throw(ArgumentError("one observation sequence per model"))
+    arrs = [lg_arrays(m) for m in models]
+    Ts = Int32[length(y) for y in yss]
+    ys = reduce(vcat, [reduce(vcat, [Float64.(collect(y)) for y in ysf]) for ysf in yss])
+    dxs = [size(a[3], 1) for a in arrs]
+    ll = zeros(Float64, B)
+    means = zeros(Float32, sum(Int.(Ts) .* dxs))
+    covs = zeros(Float32, sum(Int.(Ts) .* dxs .^ 2))
+    status = zeros(Int32, B)
+    jit = algo.jitter
+    GC.@preserve arrs ll means covs status ys begin
+        ms = [GfLgModel(Int32(size(a[3], 1)), Int32(size(a[6], 1)), map(pointer, a)...) for a in arrs]
+        out = Ref(GfKfOut(pointer(ll), C_NULL, pointer(means), pointer(covs), pointer(status)))
+        check(ccall((:gf_kf_batch, libgfb200), Int32,
+                    (Ptr{Cvoid}, Int32, Ptr{GfLgModel}, Int32, Ptr{Int32}, Ptr{Float64},
+                     Float64, Int32, Int32, Ref{GfKfOut}),
+                    context(), algo isa KalmanFilter ? 0 : 1, ms, Int32(B), Ts, ys,
+                    isnothing(jit) ? 0.0 : Float64(jit), isnothing(jit) ? 0 : 1, GF_MEM_HOST, out))
+    end
+    res = Vector{Any}(undef, B)
+    mo, co = 0, 0
+    for f in 1:B
+        dx, T = dxs[f], Int(Ts[f])
+        mo += T * dx
+        co += T * dx * dx
+        μ = Float64.(means[(mo - dx + 1):mo])
+        Σ = reshape(Float64.(covs[(co - dx * dx + 1):co]), dx, dx)
+        res[f] = (MvNormal(μ, Symmetric(Σ)), ll[f])
+    end
+    return res
+end
+
+# --- filter(rng, ::HierarchicalSSM, RBPF(BF(N; ...), KalmanFilter()), ys) ----------------
+# rbpf.jl:8-84 on a conditionally linear-Gaussian HierarchicalSSM (models/hierarchical.jl):
+# homogeneous linear-Gaussian outer prior and dynamics, inner prior N(mu_z, Sigma_z),
+# inner dynamics GFTest.InnerDynamics (z' = A z + b + C x_prev + N(0, Q)) or any
+# homogeneous linear-Gaussian dynamics (C = 0), linear-Gaussian observations of z.
+# q_scale = (gamma, i) multiplies the inner Q by exp(gamma * x_t[i]) (the
+# stochastic-volatility form of the trend-inflation example); (0, 1) = off.
+function GeneralisedFilters.filter(
+    rng::AbstractRNG,
+    model::HierarchicalSSM,
+    algo::RBPF{<:ParticleFilter{<:ESSResampler,LatentProposal},<:KalmanFilter},
+    observations::AbstractVector;
+    callback=nothing,
+    q_scale::Tuple{Real,Integer}=(0.0, 1),
+    kwargs...,
+)
+    isnothing(callback) || throw(ArgumentError("GFB200 supports callback=nothing only"))
+    pf = algo.pf
+    N, T = pf.N, length(observations)
+    mat(x) = Matrix{Float64}(x isa AbstractVector ? reshape(x, :, 1) : Matrix(x))
+    μo, Σo = GeneralisedFilters.calc_initial(model.outer_prior)
+    Ao, bo, Qo = GeneralisedFilters.calc_params(model.outer_dyn, 1)
+    μz, Σz = GeneralisedFilters.calc_initial(GeneralisedFilters.inner_prior(model))
+    idyn = GeneralisedFilters.inner_dyn(model)
+    Az, bz, Cz, Qz = if idyn isa InnerDynamics
+        idyn.A, idyn.b, idyn.C, idyn.Q
+    else
+        A_, b_, Q_ = GeneralisedFilters.calc_params(idyn, 1)
+        A_, b_, zeros(size(A_, 1), length(μo)), Q_
+    end
+    H, c, R = GeneralisedFilters.calc_params(SSMProblems.obs(model), 1)
+    arrs = map(mat, (μo, Σo, Ao, bo, Qo, μz, Σz, Az, bz, Cz, Qz, H, c, R))
+    dxo, dz, dy = size(arrs[3], 1), size(arrs[8], 1), size(arrs[12], 1)
+    ys = reduce(vcat, [Float64.(collect(y)) for y in observations])
+    cfg = Ref(GfPfConfig(N, resampler_code(pf.resampler.resampler), 0, pf.resampler.threshold,
+                         GF_PREC_F32, GF_PROP_BOOTSTRAP, 1.0, rand(rng, UInt64), C_NULL, Int32(0)))
+    width = dxo + dz + dz * (dz + 1) ÷ 2    # packed device state: x, mu, Sigma upper by rows
+    ll = zeros(Float64, 1)
+    states = zeros(Float32, N, width)
+    logw = zeros(Float64, N)
+    GC.@preserve arrs ll states logw ys begin
+        p = map(pointer, arrs)
+        m = Ref(GfRbModel(Int32(dxo), Int32(dz), Int32(dy), p[1:11]..., Float64(q_scale[1]),
+                          Int32(q_scale[2] - 1), p[12:14]...))
+        out = Ref(GfPfOut(pointer(ll), C_NULL, C_NULL, C_NULL, C_NULL, C_NULL,
+                          Ptr{Cvoid}(pointer(states)), pointer(logw), C_NULL, C_NULL, C_NULL, C_NULL))
+        check(ccall((:gf_rbpf_run, libgfb200), Int32,
+                    (Ptr{Cvoid}, Ref{GfRbModel}, Ref{GfPfConfig}, Int32, Ptr{Float64}, Ptr{Cvoid},
+                     Ptr{Float64}, Int32, Ref{GfPfOut}, Ptr{Float64}),
+                    context(), m, cfg, Int32(T), ys, C_NULL, C_NULL, GF_MEM_HOST, out, C_NULL))
+    end
+    particles = map(1:N) do i
+        x = Vector{Float64}(states[i, 1:dxo])
+        μ = Vector{Float64}(states[i, (dxo + 1):(dxo + dz)])
+        Σ = zeros(dz, dz)
+        k = dxo + dz
+        for r in 1:dz, q in r:dz
+            k += 1
+            Σ[r, q] = Σ[q, r] = states[i, k]
+        end
+        Particle(GeneralisedFilters.RBState(x, MvNormal(μ, Symmetric(Σ))), logw[i], 0)
+    end
+    return ParticleDistribution(particles, zero(Float64)), ll[1]
 end
 
 # --- kf_loglikelihood and its gradients (integrations/logdensity.jl:136-161) -------

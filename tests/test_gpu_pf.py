@@ -111,14 +111,20 @@ def test_bf_f32_teacher_forced_steps(ctx):
 
 
 @pytest.mark.parametrize("prec", ["f32", "f64"])
-def test_fused_rng_equals_exported_noise(ctx, prec):
-    """Noise drawn in-kernel == the same stream exported by gf_rng_normals and injected."""
-    m, ys = W.lgssm_rot(seed=2, dx=4, dy=4, T=20)
-    N, T, seed = 3000, 20, 99
+@pytest.mark.parametrize("dx,N", [(4, 3000), (1, 3001), (1, 1000)])
+def test_fused_rng_equals_exported_noise(ctx, prec, dx, N):
+    """Noise drawn in-kernel == the same stream exported by gf_rng_normals and injected
+    (the 1-D layout shares one Philox call between four particles; N = 1000 runs
+    the whole filter in one block)."""
+    m, ys = W.lgssm_rot(seed=2, dx=dx, dy=dx, T=20)
+    T, seed = 20, 99
     a, lla = G.filter(m, G.BF(N, threshold=0.7, precision=prec), ys, seed=seed, ctx=ctx,
                       want_ancestors=True)
-    noise = np.stack([G.rng_normals(seed, t, 4, N, prec, ctx=ctx).cpu().numpy()
+    noise = np.stack([G.rng_normals(seed, t, dx, N, prec, ctx=ctx).cpu().numpy()
                       for t in range(T + 1)])
+    if dx == 1:
+        np.testing.assert_allclose(noise[3], O.philox_normals(seed, N, 1, 3),
+                                   rtol=0, atol=1e-5 if prec == "f32" else 1e-12)
     unif = np.array([O.philox_uniform(seed, 0, t) for t in range(1, T + 1)])
     b, llb = G.filter(m, G.BF(N, threshold=0.7, precision=prec), ys, noise=noise, uniforms=unif,
                       ctx=ctx, want_ancestors=True)
@@ -232,6 +238,39 @@ def test_tensor_core_path_matches_simt(ctx, dims):
     # per-step ll is a log-sum-exp of the log-weights: its error is bounded by
     # theirs (FP32 sums of up to 32 squared residuals per particle)
     np.testing.assert_allclose(l0, l1, rtol=1e-5, atol=1e-5)
+
+
+@pytest.mark.parametrize("kind,N,threshold", [(O.SYSTEMATIC, 2 ** 16, 0.5), (O.STRATIFIED, 5000, 0.7),
+                                              (O.SYSTEMATIC, 5001, 0.5), (O.MULTINOMIAL, 4096, 0.5),
+                                              (O.SYSTEMATIC, 3000, 0.0)])
+def test_staged_gather_equals_per_thread_gather(ctx, kind, N, threshold):
+    """The bulk-copy (TMA-engine) staged ancestor gather reads the same states as
+    the per-thread gather: identical ll, ancestors and final states.  Covers
+    resampling and non-resampling steps (threshold 0), ragged N, N % 4 != 0 and
+    the multinomial search (both of which take the per-thread path)."""
+    import torch
+    from gfb200.plans import PfPlan
+    m, ys = W.lgssm_rot(seed=5, dx=16, dy=8, T=12)
+    T = 12
+    ysd = torch.tensor(ys, device="cuda:0")
+    algo = G.BF(N, threshold=threshold, resampler={O.SYSTEMATIC: G.Systematic(), O.STRATIFIED: G.Stratified(),
+                                                  O.MULTINOMIAL: G.Multinomial()}[kind])
+    out = {}
+    for staged in (False, True):
+        plan = PfPlan(m, algo, T, seed=9, ctx=ctx, graph=False, staged_gather=staged)
+        states = torch.zeros((16, N), dtype=torch.float32, device="cuda:0")
+        anc = torch.zeros((T, N), dtype=torch.int32, device="cuda:0")
+        plan.run(ysd, states=states, ancestors=anc)
+        ctx.synchronize()
+        out[staged] = (plan.ll.item(), states.cpu().numpy(), anc.cpu().numpy(),
+                       plan.resampled.cpu().numpy())
+        plan.close()
+    assert out[False][0] == out[True][0]
+    np.testing.assert_array_equal(out[False][1], out[True][1])
+    np.testing.assert_array_equal(out[False][2], out[True][2])
+    np.testing.assert_array_equal(out[False][3], out[True][3])
+    if threshold > 0:
+        assert out[True][3].sum() >= 3
 
 
 @pytest.mark.parametrize("kind,threshold,T", [(O.SYSTEMATIC, 0.5, 6), (O.STRATIFIED, 1.0, 5),

@@ -26,6 +26,31 @@ def test_kf_matches_joint_gaussian(Dy, T):
 
 
 @pytest.mark.parametrize("Dy", [1, 2, 3])
+@pytest.mark.parametrize("T", [1, 4])
+def test_nonhomogeneous_kf_and_smoother_match_joint_gaussian(Dy, T):
+    """Time-varying parameters (calc_params(dyn, t), models/linear_gaussian.jl:44-63):
+    the filter and the RTS smoother of a non-homogeneous model equal Gaussian
+    conditioning of _compute_joint_nonhomogeneous (GFTest/models/linear_gaussian.jl:
+    121-169), as test/algorithms/kalman.jl:263-300 checks for the smoother."""
+    rng = np.random.default_rng(77 + Dy + 10 * T)
+    m = O.create_nonhomogeneous_linear_gaussian_model(rng, 2, Dy, T)
+    _, ys = O.sample(rng, m, T)
+    ll, _, mus, S = O.kf_filter(m, ys)
+    mu, St, lt = O.joint_filter_truth(m, ys)
+    assert abs(ll - lt) <= 1e-10 * max(1.0, abs(lt))
+    np.testing.assert_allclose(mus[-1], mu, rtol=1e-9, atol=1e-12)
+    np.testing.assert_allclose(S[-1], St, rtol=1e-8, atol=1e-12)
+    _, ms, Ss = O.rts_smooth(m, ys)
+    mj, Sj = O.joint_smooth_truth(m, ys)
+    np.testing.assert_allclose(ms, mj, rtol=1e-8, atol=1e-11)
+    np.testing.assert_allclose(Ss, Sj, rtol=1e-8, atol=1e-11)
+    # a homogeneous model written as per-step copies is the homogeneous model
+    h = O.create_linear_gaussian_model(rng, 2, Dy)
+    hv = O.LGModel.time_varying(h.mu0, h.Sigma0, *[[x] * T for x in (h.A, h.b, h.Q, h.H, h.c, h.R)])
+    np.testing.assert_array_equal(O.kf_filter(h, ys)[2], O.kf_filter(hv, ys)[2])
+
+
+@pytest.mark.parametrize("Dy", [1, 2, 3])
 @pytest.mark.parametrize("T", [1, 5])
 def test_rts_smoother_matches_joint_gaussian(Dy, T):
     """smooth(model, KalmanSmoother(), ys) (kalman.jl:89-126,206-234): every
