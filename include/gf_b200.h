@@ -266,9 +266,11 @@ gf_status gf_kf_plan_destroy(gf_kf_plan* plan);
  * run filters of N <= 1024 as separate kernels per step instead of one block
  * for the whole filter), STAGED_GATHER (PF, Dx <= 16 on the tensor-core path:
  * copy each 128-particle sub-tile's sorted ancestor range into shared memory
- * with bulk async copies, one sub-tile ahead, instead of per-thread loads). */
+ * with bulk async copies, one sub-tile ahead, instead of per-thread loads),
+ * UNITS (PF, tensor-core path: a grid of resident blocks striding over
+ * 128-particle units instead of one block per 1024-particle tile). */
 enum { GF_PLAN_AUTOTUNE = 1, GF_PLAN_NO_GRAPH = 2, GF_PLAN_PLAIN = 4, GF_PLAN_SIMT = 8, GF_PLAN_NO_FUSE = 16,
-       GF_PLAN_STAGED_GATHER = 32 };
+       GF_PLAN_STAGED_GATHER = 32, GF_PLAN_UNITS = 64 };
 
 /* -------------------------------------------------------- particle filters */
 /* filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys)
@@ -281,12 +283,23 @@ enum { GF_PLAN_AUTOTUNE = 1, GF_PLAN_NO_GRAPH = 2, GF_PLAN_PLAIN = 4, GF_PLAN_SI
 gf_status gf_pf_run(gf_ctx* ctx, const gf_lg_model* model, const gf_pf_config* cfg, int32_t T,
                     const double* ys, const void* noise, const double* uniforms,
                     int32_t memspace, gf_pf_out* out);
+/* The same for a time-varying model (calc_params(dyn, t), calc_params(obs, t),
+ * models/linear_gaussian.jl:44-63): param_steps = 1 is gf_pf_run; param_steps
+ * >= T means the A, b, Q, H, c, R pointers of `model` each hold param_steps
+ * per-step blocks (block t-1 = step t, column-major).  Bootstrap proposal
+ * (GF_ERR_UNSUPPORTED otherwise); the auxiliary lookahead uses step t's
+ * parameters for step t. */
+gf_status gf_pf_run_tv(gf_ctx* ctx, const gf_lg_model* model, int32_t param_steps,
+                       const gf_pf_config* cfg, int32_t T, const double* ys, const void* noise,
+                       const double* uniforms, int32_t memspace, gf_pf_out* out);
 
 /* Reusable PF plan: device buffers sized once, the T-step loop captured in a
  * CUDA graph; gf_pf_plan_run takes device-resident inputs and outputs. */
 typedef struct gf_pf_plan gf_pf_plan;
 gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* model, const gf_pf_config* cfg,
                             int32_t T, int32_t flags, gf_pf_plan** out);
+gf_status gf_pf_plan_create_tv(gf_ctx* ctx, const gf_lg_model* model, int32_t param_steps,
+                               const gf_pf_config* cfg, int32_t T, int32_t flags, gf_pf_plan** out);
 gf_status gf_pf_plan_run(gf_pf_plan* plan, const double* ys_dev, const void* noise_dev,
                          const double* uniforms_dev, gf_pf_out* out_dev);
 gf_status gf_pf_plan_destroy(gf_pf_plan* plan);

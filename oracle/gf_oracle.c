@@ -773,6 +773,7 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
   if ((st = or_chol_lower(dx, m->Sigma0, L0)) || (st = or_chol_lower(dx, m->Q, LQ)) ||
       (st = or_chol_lower(dy, m->R, LR)))
     goto done;
+  if (m->tv && prop->kind != OR_PROP_BOOTSTRAP) { st = OR_ARG; goto done; } /* bootstrap only */
   if (prop->kind == OR_PROP_OVERDISPERSED) {
     /* GFTest/proposals.jl:39-50: MvNormal(A x + b, k Q) */
     double* kQ = malloc(sizeof(double) * dx * dx);
@@ -815,6 +816,10 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
     double* mar_t = out && out->margins ? out->margins + (size_t)(t - 1) * N : NULL;
     double ess = 0.0, baseline;
     int res;
+    /* this step's parameters (calc_params(dyn, t), calc_params(obs, t)) */
+    const or_step_params SP = step_params(m, t - 1);
+    if (m->tv && ((st = or_chol_lower(dx, SP.Q, LQ)) || (st = or_chol_lower(dy, SP.R, LR)))) goto done;
+    const double *mA = SP.A, *mb = SP.b, *mH = SP.H, *mc = SP.c;
     if (prop->lookahead) {
       /* AuxiliaryParticleFilter step (particles.jl:311-345): log eta_i =
        * logpdf(obs, A x_i + b, y_t) (MeanPredictive, :359-365; predictive_loglik
@@ -823,8 +828,8 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
       const double* yl = ys + (size_t)(t - 1) * dy;
       for (long i = 0; i < N; ++i) {
         double mx[64], hx[64], dif[64], tmpd[64];
-        mv(dx, dx, m->A, x + (size_t)i * dx, mx);
-        for (int d = 0; d < dx; ++d) mx[d] += m->b[d];
+        mv(dx, dx, mA, x + (size_t)i * dx, mx);
+        for (int d = 0; d < dx; ++d) mx[d] += mb[d];
         if (prop->lookahead == 2) {
           /* DrawPredictive (particles.jl:377-384): x* ~ MvNormal(A x + b, Q), the draw
            * from the Philox stream tagged TAG_LOOKAHEAD with counters (i, t, q) */
@@ -836,8 +841,8 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
           mv(dx, dx, LQ, e, v);
           for (int d = 0; d < dx; ++d) mx[d] += v[d];
         }
-        mv(dy, dx, m->H, mx, hx);
-        for (int k = 0; k < dy; ++k) dif[k] = yl[k] - hx[k] - m->c[k];
+        mv(dy, dx, mH, mx, hx);
+        for (int k = 0; k < dy; ++k) dif[k] = yl[k] - hx[k] - mc[k];
         eta[i] = logpdf_chol(dy, LR, dif, tmpd);
         aux[i] = (uniform ? 0.0 : logw[i]) + eta[i];
       }
@@ -885,8 +890,8 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
       double e[64], mx[64], v[64], xn[64], tmpd[64], dif[64];
       double* xi = x + (size_t)i * dx;
       draw_normals_lg(noise, seed, dx, N, t, i, e);
-      mv(dx, dx, m->A, xi, mx);
-      for (int d = 0; d < dx; ++d) mx[d] += m->b[d]; /* A x + b */
+      mv(dx, dx, mA, xi, mx);
+      for (int d = 0; d < dx; ++d) mx[d] += mb[d]; /* A x + b */
       double inc = 0.0;
       if (prop->kind == OR_PROP_BOOTSTRAP) {
         mv(dx, dx, LQ, e, v);
@@ -914,8 +919,8 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
       memcpy(xi, xn, sizeof(double) * dx);
       /* update (particles.jl:133-145): += logpdf(MvNormal(H x + c, R), y) */
       double hx[64];
-      mv(dy, dx, m->H, xn, hx);
-      for (int k = 0; k < dy; ++k) dif[k] = y[k] - hx[k] - m->c[k];
+      mv(dy, dx, mH, xn, hx);
+      for (int k = 0; k < dy; ++k) dif[k] = y[k] - hx[k] - mc[k];
       double lo = logpdf_chol(dy, LR, dif, tmpd);
       logw[i] = logw[i] + inc + lo;
     }

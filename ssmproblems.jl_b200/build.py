@@ -12,6 +12,7 @@ import glob
 import os
 import subprocess
 import sys
+import time
 from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
@@ -68,10 +69,14 @@ def build(force: bool = False, jobs: int | None = None, verbose: bool = False) -
 
     def compile_one(so):
         s, o = so
+        t0 = time.time()
         cmd = [NVCC] + ARCH + FLAGS + ["-MD", "-MF", o[:-2] + ".d", "-c", s, "-o", o]
         r = subprocess.run(cmd, capture_output=True, text=True)
         if r.returncode != 0:
             raise RuntimeError(f"nvcc failed for {s}:\n{r.stdout}\n{r.stderr}")
+        # date the object at the compile's start: a source or header edited while
+        # nvcc ran then still counts as newer, and the next build recompiles it
+        os.utime(o, (t0, t0))
         if verbose:
             print(f"compiled {os.path.basename(s)}", flush=True)
         return o

@@ -24,11 +24,12 @@ __global__ void pf_prep_ystep(const PfJob* __restrict__ job, int T, int dx, int 
                               int dyp, const double* __restrict__ pp, Real* __restrict__ out) {
   // pp: LRinv[dy*dy] | c[dy] | K[dx*dy] | vb[dx]
   const double* ys = job->ys;
-  const double* LRi = pp;
-  const double* c = LRi + dy * dy;
-  const double* K = c + dy;
-  const double* vb = K + dx * dy;
+  const int32_t pps = job->ppstride;  // time-varying model: per-step factor blocks
   for (int t = blockIdx.x * blockDim.x + threadIdx.x; t < T; t += gridDim.x * blockDim.x) {
+    const double* LRi = pp + (size_t)t * pps;
+    const double* c = LRi + dy * dy;
+    const double* K = c + dy;
+    const double* vb = K + dx * dy;
     const double* y = ys + (size_t)t * dy;
     Real* o = out + (size_t)t * (dyp + dxp);
     for (int k = 0; k < dyp; ++k) {
@@ -133,6 +134,36 @@ __global__ void pf_dense_ancestry_kernel(int T, int64_t N, int dx, const Real* _
       if (t > 0) a = (int64_t)anc[(size_t)(t - 1) * N + a] - 1;
     }
   }
+}
+
+// The step's finalise after pf_lg_propagate_tc_units: one block of 1024
+// threads per job folds the job's unit partials (finish_step, as the last
+// propagate block does in the tile kernels), keeping each partial's
+// exponential in shared memory between the fold and the tile prefixes when
+// they fit (UNITS_ECACHE partials).
+constexpr int UNITS_FINISH_THREADS = 1024;
+constexpr int UNITS_ECACHE = 16384;
+__global__ void __launch_bounds__(UNITS_FINISH_THREADS) pf_finish_units_kernel(const PfJob* __restrict__ jobs,
+                                                                               int njobs) {
+  extern __shared__ double ecache[];
+  __shared__ double red[32];
+  __shared__ unsigned long long s_wsum[32];
+  __shared__ int s_res;
+  const PfJob& J = jobs[blockIdx.x];
+  PfScalars* sc = J.sc;
+  const int t = sc->t + 1;
+  if (t > J.T || sc->status != 0) return;
+  const bool fresh = sc->resample != 0 || sc->uniform != 0;
+  const bool cache = J.ntiles * TC_SUB <= UNITS_ECACHE;
+  finish_step(BlockSync(), J, t, fresh, TC_SUB, red, s_wsum, &s_res, cache ? ecache : nullptr);
+}
+
+void launch_finish_units(gf_ctx* ctx, const PfJob* jobs_dev, int njobs) {
+  // the cache's dynamic shared memory (128 KB) needs the opt-in (current device)
+  cudaFuncSetAttribute((const void*)pf_finish_units_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)(sizeof(double) * UNITS_ECACHE));
+  pf_finish_units_kernel<<<njobs, UNITS_FINISH_THREADS, sizeof(double) * UNITS_ECACHE, ctx->stream>>>(jobs_dev,
+                                                                                                   njobs);
 }
 
 void launch_record(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int64_t N) {
@@ -401,8 +432,10 @@ static void pack_lg_params(const LgFactors& f, int DXP, int DYP, std::vector<cha
     v.insert(v.end(), B.begin(), B.end());
     v.insert(v.end(), Hb.begin(), Hb.end());
   }
-  out.resize(sizeof(Real) * v.size());
-  std::memcpy(out.data(), v.data(), out.size());
+  // appended: a time-varying model packs one block per step
+  const size_t off = out.size();
+  out.resize(off + sizeof(Real) * v.size());
+  std::memcpy(out.data() + off, v.data(), sizeof(Real) * v.size());
 }
 
 void pack_params(const LgFactors& f, bool dbl, int dxp, int dyp, std::vector<char>& out) {

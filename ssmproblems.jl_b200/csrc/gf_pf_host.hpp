@@ -27,6 +27,9 @@ struct PfLgKernels {
   // the same with the staged (bulk-copy) ancestor gather, Dx = 16; null if none
   void (*prop_tc_staged)(const PfJob*, int) = nullptr;
   size_t tc_staged_smem = 0;
+  // the same over 128-particle units with a grid of resident blocks
+  void (*prop_tc_units)(const PfJob*, int) = nullptr;
+  int tc_units_blocks = 0;  // resident blocks per SM
 };
 
 // FP64 model factors computed once per plan (column-major).
@@ -50,6 +53,8 @@ void launch_means(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int njobs, int t
                   double* mpart, int mdim);
 void launch_finish(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int64_t N);
 void launch_record(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int64_t N);
+// the step's finalise after the unit-grid tensor-core propagation
+void launch_finish_units(gf_ctx* ctx, const PfJob* jobs_dev, int njobs);
 void launch_prep(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int T, int dx, int dy, int dxp,
                  int dyp, const double* pp, void* out);
 
@@ -59,6 +64,8 @@ namespace gf {
 
 // Largest number of blocks per tile of any propagate kernel (sizes `part`).
 constexpr int PF_MAX_SPLIT = 8;
+// 128-particle units per 1024-particle tile (pf_lg_propagate_tc_units)
+constexpr int TC_SUB_UNITS = 8;
 
 // Rao-Blackwellised PF propagation: one particle per thread, RB_SPLIT blocks of
 // RB_THREADS threads per 1024-particle tile (its log-sum-exp partials are kept
@@ -93,15 +100,21 @@ struct LgJobSetup {
   void (*prop)(const PfJob*, int) = nullptr;
   int threads = 0;
   int split = 1;  // propagate blocks per tile (grid = tiles * split)
+  int units_blocks = 0;  // > 0: unit kernel, grid = min(units, SMs * units_blocks)
   size_t smem = 0;
-  std::vector<char> params;
-  std::vector<double> pp;
+  std::vector<char> params;      // parameter blocks (one per step if time-varying)
+  std::vector<double> pp;        // observation-prep factors (likewise)
+  std::vector<double> obs_consts;  // time-varying: the observation constant of every step
+  int64_t pstride = 0;           // time-varying: elements between parameter blocks
+  int32_t ppstride = 0;          // time-varying: doubles between prep blocks
   double ess1 = 0.0;
   int8_t res1 = 0;
   PfJob J;
 };
+// param_steps: 1 for a homogeneous model, >= T when the A, b, Q, H, c, R
+// pointers of m hold one block per step (bootstrap proposal only).
 gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg, int32_t T,
-                       int32_t flags, LgJobSetup* out);
+                       int32_t flags, LgJobSetup* out, int32_t param_steps = 1);
 
 }  // namespace gf
 

@@ -40,6 +40,13 @@ struct PfJob {
   const void* ystep;         // per-step vectors [T][ystride]
   int32_t ystride;
   int32_t lookahead_draw;    // auxiliary filter: DrawPredictive (x* drawn from the transition)
+  // time-varying model: step t's parameter block is params + (t-1) * pstride
+  // elements and its observation constant obs_consts[t-1]; the observation
+  // prep reads its factors pp + t * ppstride (0 / null: one block for all steps)
+  int64_t pstride;
+  const double* obs_consts;
+  int32_t ppstride;
+  int32_t pad_tv;
   void* X[2];                // SoA state ping-pong [width][N]
   void* lw;                  // stored log-weights [N]
   double* key;               // cumulative normalised weights [N]
@@ -68,6 +75,11 @@ struct PfJob {
   void* hist;                // nullable [T+1][dx][N] dense state history
   double* lwh;               // nullable [T][N] normalised log-weight history
 };
+
+// Observation constant of step t (time-varying models carry one per step).
+__device__ __forceinline__ double step_obs_const(const PfJob& J, int t) {
+  return J.obs_consts ? J.obs_consts[t - 1] : J.obs_const;
+}
 
 __device__ __forceinline__ int find_job(const PfJob* jobs, int njobs, int block, bool scan) {
   int lo = 0, hi = njobs - 1;
@@ -288,9 +300,12 @@ static __device__ bool fold_partials(const PfJob& J, int tile, LseAcc a, double*
 }
 
 // Last block: (max, sum e, sum e^2) over every partial, in a fixed order.
+// ecache (nullable, shared, nall entries): keeps exp(M_b - GM) of every
+// partial for write_tile_prefixes.
 template <class S>
 static __device__ void global_stats(const S& g, const PfJob& J, int nparts, double* red,
-                                    double* GM_out, double* GS1_out, double* GS2_out) {
+                                    double* GM_out, double* GS1_out, double* GS2_out,
+                                    double* ecache = nullptr) {
   const int nall = J.ntiles * nparts;
   double m = -INFINITY;
   for (int bb = g.tid(); bb < nall; bb += g.size()) m = fmax(m, __ldcg(J.part + (size_t)bb * PF_PW));
@@ -299,11 +314,13 @@ static __device__ void global_stats(const S& g, const PfJob& J, int nparts, doub
   for (int bb = g.tid(); bb < nall; bb += g.size()) {
     const double* p = J.part + (size_t)bb * PF_PW;
     double mb = __ldcg(p);
+    double ff = 0.0;
     if (mb > -INFINITY) {
-      double ff = exp(mb - GM);
+      ff = exp(mb - GM);
       s1 += __ldcg(p + 1) * ff;
       s2 += __ldcg(p + 2) * ff * ff;
     }
+    if (ecache) ecache[bb] = ff;
   }
   *GM_out = GM;
   *GS1_out = sync_sum(g, s1, red);
@@ -314,9 +331,12 @@ static __device__ void global_stats(const S& g, const PfJob& J, int nparts, doub
 // P_b = sum_{b'<b} S1_b' e^{M_b' - lse}, summed in 64-bit fixed point (2^-62
 // units): integer sums are exact, so the parallel scan gives the same monotone
 // prefixes in any order.  `wsum` is shared scratch of >= 32 values owned by S.
+// ecache (nullable): global_stats' exp(M_b - GM) of every partial, with
+// inv_gs1 = 1 / sum: exp(M_b - lse) is then ecache[b] * inv_gs1.
 template <class S>
 static __device__ void write_tile_prefixes(const S& g, const PfJob& J, int nparts, double lse,
-                                           unsigned long long* wsum) {
+                                           unsigned long long* wsum, const double* ecache = nullptr,
+                                           double inv_gs1 = 0.0) {
   PfScalars* sc = J.sc;
   const int per = (J.ntiles + g.size() - 1) / g.size();
   const int b0 = min(g.tid() * per, J.ntiles), b1 = min(b0 + per, J.ntiles);
@@ -326,7 +346,10 @@ static __device__ void write_tile_prefixes(const S& g, const PfJob& J, int npart
     for (int q = 0; q < nparts; ++q) {
       const double* p = J.part + ((size_t)bb * nparts + q) * PF_PW;
       const double mb = __ldcg(p);
-      if (mb > -INFINITY) w += __double2ull_rn(__ldcg(p + 1) * exp(mb - lse) * kFix);
+      if (mb > -INFINITY) {
+        const double e = ecache ? ecache[(size_t)bb * nparts + q] * inv_gs1 : exp(mb - lse);
+        w += __double2ull_rn(__ldcg(p + 1) * e * kFix);
+      }
     }
     return w;
   };
@@ -354,11 +377,12 @@ static __device__ void write_tile_prefixes(const S& g, const PfJob& J, int npart
 // are shared scratch owned by S.
 template <class S>
 static __device__ void finish_step(const S& g, const PfJob& J, int t, bool fresh, int nparts,
-                                   double* red, unsigned long long* wsum, int* s_res) {
+                                   double* red, unsigned long long* wsum, int* s_res,
+                                   double* ecache = nullptr) {
   PfScalars* sc = J.sc;
   // fold all partials in a fixed order (deterministic)
   double GM, GS1, GS2;
-  global_stats(g, J, nparts, red, &GM, &GS1, &GS2);
+  global_stats(g, J, nparts, red, &GM, &GS1, &GS2, ecache);
   const double base = fresh ? J.log_n + sc->base_adj : 0.0;
   const double lse = GM + log(GS1);
   if (g.tid() == 0) {
@@ -383,7 +407,7 @@ static __device__ void finish_step(const S& g, const PfJob& J, int t, bool fresh
   }
   g.sync();
   // the auxiliary filter decides in its lookahead kernel instead
-  if (*s_res && !J.eta) write_tile_prefixes(g, J, nparts, lse, wsum);
+  if (*s_res && !J.eta) write_tile_prefixes(g, J, nparts, lse, wsum, ecache, 1.0 / GS1);
   g.sync();
   if (g.tid() == 0) {
     sc->uniform = 0;

@@ -99,7 +99,7 @@ __device__ __forceinline__ void lg_propagate_tile(const PfJob& J, int tile) {
   const double lse_prev = sc->lse;
   const bool searched = J.resampler == GF_RS_MULTINOMIAL;
 
-  const Real* P = reinterpret_cast<const Real*>(J.params);
+  const Real* P = reinterpret_cast<const Real*>(J.params) + (size_t)(t - 1) * J.pstride;
   for (int k = threadIdx.x; k < Lay::H + DYP * DXP; k += PF_THREADS) sA[k] = P[k];
   const Real* Y = reinterpret_cast<const Real*>(J.ystep) + (size_t)(t - 1) * J.ystride;
   for (int k = threadIdx.x; k < DYP + DXP; k += PF_THREADS) sy[k] = Y[k];
@@ -118,7 +118,7 @@ __device__ __forceinline__ void lg_propagate_tile(const PfJob& J, int tile) {
   int32_t* __restrict__ anc_out = J.anc_out;
   const uint64_t seed = J.seed;
   const bool diag = J.diag_l != 0;
-  const double obs_const = J.obs_const, prop_const = J.prop_const;
+  const double obs_const = step_obs_const(J, t), prop_const = J.prop_const;
   const Real* eta = reinterpret_cast<const Real*>(J.eta);
   const bool apf = resamp && eta != nullptr;
   LseAcc acc;
@@ -322,6 +322,7 @@ __global__ void __launch_bounds__(PF_THREADS) pf_lg_small_filter(const PfJob* __
 // (one lane per particle) and is read back for the weight and the state store.
 constexpr int TC_THREADS = 128;
 constexpr int TC_SUB = PF_TILE / TC_THREADS;
+static_assert(TC_SUB == TC_SUB_UNITS && TC_SUB <= PF_MAX_SPLIT, "unit partials per tile");
 // Blocks per tile (each TC_SUB / TC_SPLIT sub-tiles, partials kept per block).
 // One: the per-block prologue (operand-B staging, TMEM allocation) and the
 // partial reduction cost more than shorter waves save (at Dx=16, N=2^20 the
@@ -400,7 +401,7 @@ __global__ void __launch_bounds__(TC_THREADS, (TcSmem<DXP, DYP, STAGED>::min_blo
   const double lse_prev = sc->lse;
   const bool searched = J.resampler == GF_RS_MULTINOMIAL;
 
-  const float* P = reinterpret_cast<const float*>(J.params);
+  const float* P = reinterpret_cast<const float*>(J.params) + (size_t)(t - 1) * J.pstride;
   for (int e = tid; e < NM * K; e += TC_THREADS) {
     const int n = e / K, k = e - n * K;
     const float v = P[TL::B_off + e];
@@ -436,7 +437,7 @@ __global__ void __launch_bounds__(TC_THREADS, (TcSmem<DXP, DYP, STAGED>::min_blo
   const int32_t* __restrict__ ancv = J.anc;
   int32_t* __restrict__ anc_out = J.anc_out;
   const uint64_t seed = J.seed;
-  const double obs_const = J.obs_const;
+  const double obs_const = step_obs_const(J, t);
   const float* eta = reinterpret_cast<const float*>(J.eta);
   const bool apf = resamp && eta != nullptr;
   const uint32_t idesc = umma::idesc_tf32(128, NM);
@@ -570,6 +571,209 @@ __global__ void __launch_bounds__(TC_THREADS, (TcSmem<DXP, DYP, STAGED>::min_blo
   block_finish(J, tile, t, fresh, acc, red, part, TC_SPLIT);
 }
 
+// The same propagation over 128-particle units instead of whole tiles: a grid
+// of resident blocks (5 per SM at Dx=16) strides over the units of every job,
+// each unit exactly one sub-tile of pf_lg_propagate_tc, and writes one partial
+// per unit (TC_SUB per tile, in unit order, so the fold and tile prefixes do
+// not depend on the grid).  The step's finalise runs in pf_finish_units_kernel
+// after this launch, so no unit pays a device-wide fence or a counter atomic.
+// With 8192 units at N = 2^20 the last round of the grid is 92% full, against
+// 38% for the last wave of 1024 tile blocks; the operand-B staging and TMEM
+// allocation are paid once per block (again only when the job changes).
+template <int DXP, int DYP>
+__global__ void __launch_bounds__(TC_THREADS, (TcLayout<DXP, DYP>::min_blocks)) pf_lg_propagate_tc_units(
+    const PfJob* __restrict__ jobs, int njobs) {
+  using Lay = LgLayout<DXP, DYP>;
+  using TL = TcLayout<DXP, DYP>;
+  constexpr int K = TL::K, NM = TL::NM;
+  extern __shared__ __align__(128) unsigned char smraw[];
+  float* sAh = reinterpret_cast<float*>(smraw);
+  float* sAl = sAh + 128 * K;
+  float* sBh = sAl + 128 * K;
+  float* sBl = sBh + NM * K;
+  float* sb = sBl + NM * K;
+  float* sHb = sb + DXP;
+  float* sy = sHb + DYP;
+  __shared__ double red[32];
+  __shared__ uint64_t mbar;
+  __shared__ uint32_t tmem_slot;
+  const int tid = threadIdx.x;
+  const PfJob& JL = jobs[njobs - 1];
+  const int64_t nunits = (int64_t)TC_SUB * (JL.tile0 + JL.ntiles);
+  if ((int64_t)blockIdx.x >= nunits) return;
+  if (tid == 0) {
+    umma::mbar_init(&mbar, 1);
+    umma::fence_mbar_init();
+  }
+  if (tid < 32) umma::tmem_alloc(&tmem_slot, TL::NCOLS);
+  umma::fence_before_sync();
+  __syncthreads();
+  umma::fence_after_sync();
+  const uint32_t tbase = tmem_slot;
+  const uint32_t tlane = tbase + ((uint32_t)(32 * (tid >> 5)) << 16);
+  const uint32_t idesc = umma::idesc_tf32(128, NM);
+  const uint32_t kstride = 128, mstride = (uint32_t)(K / 4) * 128;
+  bool ok = true;
+  uint32_t nmma = 0;
+  int jcur = -1;
+  // the current job's step state (reloaded when a unit belongs to another job)
+  const PfJob* J = nullptr;
+  PfScalars* sc = nullptr;
+  int t = 0;
+  bool active = false, resamp = false, fresh = false, searched = false, apf = false;
+  double lse_prev = 0.0, obs_const = 0.0;
+  int64_t N = 0;
+  int dx = 0;
+  const float* Xs = nullptr;
+  float* Xd = nullptr;
+  float* lw = nullptr;
+  const float* noise = nullptr;
+  const int32_t* ancv = nullptr;
+  int32_t* anc_out = nullptr;
+  const float* eta = nullptr;
+  for (int64_t u = blockIdx.x; u < nunits; u += gridDim.x) {
+    const int gt = (int)(u / TC_SUB);
+    const int jb = find_job(jobs, njobs, gt, false);
+    if (jb != jcur) {
+      jcur = jb;
+      J = &jobs[jb];
+      sc = J->sc;
+      t = sc->t + 1;
+      active = t <= J->T && sc->status == 0;
+      if (active) {
+        resamp = sc->resample != 0;
+        fresh = resamp || sc->uniform != 0;
+        lse_prev = sc->lse;
+        searched = J->resampler == GF_RS_MULTINOMIAL;
+        N = J->N;
+        dx = J->dx;
+        Xs = reinterpret_cast<const float*>(J->X[(t - 1) & 1]);
+        Xd = reinterpret_cast<float*>(J->X[t & 1]);
+        lw = reinterpret_cast<float*>(J->lw);
+        noise = J->noise ? reinterpret_cast<const float*>(J->noise) + (size_t)t * dx * N : nullptr;
+        ancv = J->anc;
+        anc_out = J->anc_out;
+        obs_const = step_obs_const(*J, t);
+        eta = reinterpret_cast<const float*>(J->eta);
+        apf = resamp && eta != nullptr;
+        const float* P = reinterpret_cast<const float*>(J->params) + (size_t)(t - 1) * J->pstride;
+        for (int e = tid; e < NM * K; e += TC_THREADS) {
+          const int n = e / K, k = e - n * K;
+          const float v = P[TL::B_off + e];
+          const float h = umma::to_tf32(v);
+          const uint32_t off = umma::kmajor_offset(n, k, K) >> 2;
+          sBh[off] = h;
+          sBl[off] = umma::to_tf32(v - h);
+        }
+        for (int e = tid; e < DXP; e += TC_THREADS) sb[e] = P[Lay::b + e];
+        const float* Y = reinterpret_cast<const float*>(J->ystep) + (size_t)(t - 1) * J->ystride;
+        for (int e = tid; e < DYP; e += TC_THREADS) {
+          sHb[e] = P[TL::Hb_off + e];
+          sy[e] = Y[e];
+        }
+      }
+      __syncthreads();
+    }
+    if (!active) continue;
+    const int tile = gt - J->tile0;
+    const int sub = (int)(u % TC_SUB);
+    const int64_t i = (int64_t)tile * PF_TILE + sub * TC_THREADS + tid;
+    const bool valid = i < N;
+    int64_t a = i;
+    if (valid && resamp) a = searched ? find_ancestor(*J, sc, t, i, 0, N) : (int64_t)ancv[i];
+    float xe[K];
+#pragma unroll
+    for (int d = 0; d < DXP; ++d) xe[d] = (valid && d < dx) ? Xs[(size_t)d * N + a] : 0.f;
+#pragma unroll
+    for (int q = 0; q < DXP / 4; ++q) {
+      float e4[4];
+      if (noise) {
+#pragma unroll
+        for (int cc = 0; cc < 4; ++cc) {
+          const int c = 4 * q + cc;
+          e4[cc] = (valid && c < dx) ? noise[(size_t)c * N + i] : 0.f;
+        }
+      } else {
+        philox_normals4<float>(J->seed, (uint32_t)i, (uint32_t)t, (uint32_t)q, e4);
+      }
+#pragma unroll
+      for (int cc = 0; cc < 4; ++cc) xe[DXP + 4 * q + cc] = e4[cc];
+    }
+    const double lin = !valid ? 0.0 : fresh ? (apf ? -(double)eta[a] : 0.0) : (double)lw[i] - lse_prev;
+#pragma unroll
+    for (int k4 = 0; k4 < K / 4; ++k4) {
+      float4 h, l;
+      umma::split_tf32(xe[4 * k4 + 0], h.x, l.x);
+      umma::split_tf32(xe[4 * k4 + 1], h.y, l.y);
+      umma::split_tf32(xe[4 * k4 + 2], h.z, l.z);
+      umma::split_tf32(xe[4 * k4 + 3], h.w, l.w);
+      const uint32_t off = umma::kmajor_offset(tid, 4 * k4, K) >> 2;
+      *reinterpret_cast<float4*>(sAh + off) = h;
+      *reinterpret_cast<float4*>(sAl + off) = l;
+    }
+    umma::fence_async_smem();
+    __syncthreads();
+    if (tid == 0) {
+      umma::fence_after_sync();
+#pragma unroll
+      for (int ks = 0; ks < K / 8; ++ks) {
+        const uint32_t koff = (uint32_t)ks * 2 * kstride;
+        const uint64_t ah = umma::desc(umma::smem_u32(sAh) + koff, kstride, mstride);
+        const uint64_t al = umma::desc(umma::smem_u32(sAl) + koff, kstride, mstride);
+        const uint64_t bh = umma::desc(umma::smem_u32(sBh) + koff, kstride, mstride);
+        const uint64_t bl = umma::desc(umma::smem_u32(sBl) + koff, kstride, mstride);
+        umma::mma_tf32(tbase, ah, bh, idesc, ks > 0 ? 1u : 0u);
+        umma::mma_tf32(tbase, ah, bl, idesc, 1u);
+        umma::mma_tf32(tbase, al, bh, idesc, 1u);
+      }
+      umma::mma_commit(&mbar);
+    }
+    ok = umma::mbar_wait(&mbar, nmma & 1u, TC_WAIT) && ok;
+    ++nmma;
+    umma::fence_after_sync();
+    float accv[NM];
+#pragma unroll
+    for (int c = 0; c < NM; c += 16) umma::tmem_ld16(tlane + (uint32_t)c, accv + c);
+    umma::tmem_wait_ld();
+    LseAcc acc;
+    if (valid) {
+      float q = 0.f;
+#pragma unroll
+      for (int k = 0; k < DYP; ++k) {
+        const float r = sy[k] - accv[DXP + k] - sHb[k];
+        q = fmaf(r, r, q);
+      }
+      const double lout = lin + (obs_const - 0.5 * (double)q);
+      const float lst = (float)lout;
+      lw[i] = lst;
+#pragma unroll
+      for (int d = 0; d < DXP; ++d)
+        if (d < dx) Xd[(size_t)d * N + i] = accv[d] + sb[d];
+      if (anc_out) anc_out[(size_t)(t - 1) * N + i] = (int32_t)(a + 1);
+      acc.add((double)lst);
+    }
+    umma::fence_before_sync();
+    if (!ok && tid == 0) sc->status = GF_ERR_TIMEOUT;
+    // the unit's (max, sum e, sum e^2); pf_finish_units_kernel folds them
+    const double M = block_max(acc.m, red);
+    const double f = acc.m > -INFINITY ? exp(acc.m - M) : 0.0;
+    const double S1 = block_sum(acc.s1 * f, red);
+    const double S2 = block_sum(acc.s2 * f * f, red);
+    if (tid == 0) {
+      double* pp = J->part + ((size_t)tile * TC_SUB + sub) * PF_PW;
+      pp[0] = M;
+      pp[1] = S1;
+      pp[2] = S2;
+    }
+  }
+  umma::fence_before_sync();
+  __syncthreads();
+  if (tid < 32) {
+    umma::fence_after_sync();
+    umma::tmem_dealloc(tbase, TL::NCOLS);
+  }
+}
+
 // Auxiliary particle filter, first stage of step t (particles.jl:273-357):
 // log eta_i = log p(y_t | x*_i) with x*_i = A x_i + b, the mean and the mode of
 // the transition MvNormal(A x + b, Q) (MeanPredictive, ModePredictive), or a
@@ -587,7 +791,7 @@ __global__ void __launch_bounds__(PF_THREADS) pf_apf_lookahead(const PfJob* __re
   const int t = sc->t + 1;
   if (t > J.T || sc->status != 0) return;
   const int tile = blockIdx.x - J.tile0;
-  const Real* P = reinterpret_cast<const Real*>(J.params);
+  const Real* P = reinterpret_cast<const Real*>(J.params) + (size_t)(t - 1) * J.pstride;
   for (int k = threadIdx.x; k < DXP * DXP; k += PF_THREADS) {
     sA[k] = P[Lay::A + k];
     sL[k] = P[Lay::L + k];
@@ -602,7 +806,7 @@ __global__ void __launch_bounds__(PF_THREADS) pf_apf_lookahead(const PfJob* __re
   const Real* Xs = reinterpret_cast<const Real*>(J.X[(t - 1) & 1]);
   const Real* lw = reinterpret_cast<const Real*>(J.lw);
   Real* eta = reinterpret_cast<Real*>(J.eta);
-  const double obs_const = J.obs_const;
+  const double obs_const = step_obs_const(J, t);
   const bool draw = J.lookahead_draw != 0;
   LseAcc acc;
   for (int p = 0; p < PF_PPT; ++p) {
@@ -665,6 +869,8 @@ PfLgKernels make_lg() {
     k.tc_smem = TcLayout<DXP, DYP>::smem_bytes;
     k.tc_nm = TcLayout<DXP, DYP>::NM;
     k.tc_split = TC_SPLIT;
+    k.prop_tc_units = pf_lg_propagate_tc_units<DXP, DYP>;
+    k.tc_units_blocks = TcLayout<DXP, DYP>::min_blocks;
     if constexpr (DXP == 16) {
       k.prop_tc_staged = pf_lg_propagate_tc<DXP, DYP, true>;
       k.tc_staged_smem = TcSmem<DXP, DYP, true>::bytes;

@@ -1,6 +1,7 @@
 // gf_pf_plan.cu -- PF plans (device buffers + captured T-step graph) and the
 // particle-filter entry points of the C ABI.
 #include <cmath>
+#include <algorithm>
 #include <cstring>
 #include <memory>
 #include <vector>
@@ -27,6 +28,7 @@ struct gf_pf_plan {
   double* tprefix = nullptr;
   int32_t *ocum = nullptr, *mpk = nullptr, *anc = nullptr;
   void* eta = nullptr;  // auxiliary filter: lookahead log eta [N]
+  double* obs_consts = nullptr;  // time-varying model: observation constant per step
   unsigned long long* flags = nullptr;
   PfScalars* sc = nullptr;
   int8_t *sched_dev = nullptr, *res1 = nullptr;
@@ -35,6 +37,8 @@ struct gf_pf_plan {
   void (*prop_fn)(const PfJob*, int) = nullptr;  // chosen propagate kernel
   int prop_threads = 0;
   int prop_split = 1;
+  int prop_grid = 0;
+  bool units = false;  // unit-grid propagation: the step's finalise is a separate launch
   size_t prop_smem = 0;
   cudaGraphExec_t graph = nullptr;
   bool graph_means = false;
@@ -79,29 +83,60 @@ static gf_status validate_cfg(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_con
 namespace gf {
 
 gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg, int32_t T,
-                       int32_t flags, LgJobSetup* o) {
+                       int32_t flags, LgJobSetup* o, int32_t param_steps) {
   gf_status st = validate_cfg(ctx, m, cfg, T);
   if (st) return st;
   o->dbl = cfg->precision == GF_PREC_F64;
   const bool guided = cfg->proposal != GF_PROP_BOOTSTRAP;
+  const bool tv = param_steps != 1;
+  if (tv && param_steps < T)
+    return set_err(ctx, GF_ERR_ARG, "%d parameter steps for T = %d", param_steps, T);
+  if (tv && guided)
+    return set_err(ctx, GF_ERR_UNSUPPORTED, "time-varying parameters run with the bootstrap proposal");
   if (!pick_lg_kernels(o->dbl, guided, m->dx, m->dy, &o->k))
     return set_err(ctx, GF_ERR_DIM, "no kernel for dx=%d dy=%d in %s", m->dx, m->dy,
                    o->dbl ? "FP64 (max 16)" : "FP32 (max 64)");
-  LgFactors f;
-  if ((st = build_lg_factors(ctx, m, cfg, &f))) return st;
+  // one parameter block (and observation-prep block) per step of a
+  // time-varying model (calc_params(dyn, t), calc_params(obs, t)), else one
+  const int nblk = tv ? T : 1;
+  const int dx = m->dx, dy = m->dy;
   o->params.clear();
-  pack_params(f, o->dbl, o->k.dxp, o->k.dyp, o->params);
   o->pp.clear();
-  o->pp.insert(o->pp.end(), f.LRi.begin(), f.LRi.end());
-  o->pp.insert(o->pp.end(), f.c.begin(), f.c.end());
-  o->pp.insert(o->pp.end(), f.K.begin(), f.K.end());
-  o->pp.insert(o->pp.end(), f.vb.begin(), f.vb.end());
+  o->obs_consts.clear();
+  bool diag = true;
+  LgFactors f;
+  for (int sblk = 0; sblk < nblk; ++sblk) {
+    gf_lg_model ms = *m;
+    if (tv) {
+      ms.A = m->A + (size_t)sblk * dx * dx;
+      ms.b = m->b + (size_t)sblk * dx;
+      ms.Q = m->Q + (size_t)sblk * dx * dx;
+      ms.H = m->H + (size_t)sblk * dy * dx;
+      ms.c = m->c + (size_t)sblk * dy;
+      ms.R = m->R + (size_t)sblk * dy * dy;
+    }
+    if ((st = build_lg_factors(ctx, &ms, cfg, &f))) return st;
+    pack_params(f, o->dbl, o->k.dxp, o->k.dyp, o->params);
+    o->pp.insert(o->pp.end(), f.LRi.begin(), f.LRi.end());
+    o->pp.insert(o->pp.end(), f.c.begin(), f.c.end());
+    o->pp.insert(o->pp.end(), f.K.begin(), f.K.end());
+    o->pp.insert(o->pp.end(), f.vb.begin(), f.vb.end());
+    if (tv) o->obs_consts.push_back(f.obs_const);
+    for (int j = 0; j < dx; ++j)
+      for (int i = 0; i < dx; ++i)
+        if (i != j && f.L[i + j * dx] != 0.0) diag = false;
+  }
+  o->pstride = tv ? (int64_t)(o->params.size() / nblk) / (o->dbl ? 8 : 4) : 0;
+  o->ppstride = tv ? (int32_t)(o->pp.size() / nblk) : 0;
+  o->units_blocks = 0;
   if (o->k.prop_tc && !(flags & GF_PLAN_SIMT)) {
     const bool staged = (flags & GF_PLAN_STAGED_GATHER) && o->k.prop_tc_staged;
-    o->prop = staged ? o->k.prop_tc_staged : o->k.prop_tc;
+    const bool units = (flags & GF_PLAN_UNITS) && o->k.prop_tc_units && !staged;
+    o->prop = staged ? o->k.prop_tc_staged : (units ? o->k.prop_tc_units : o->k.prop_tc);
     o->threads = 128;
     o->smem = staged ? o->k.tc_staged_smem : o->k.tc_smem;
     o->split = o->k.tc_split;
+    if (units) o->units_blocks = o->k.tc_units_blocks;
   } else {
     o->prop = o->k.prop;
     o->threads = PF_THREADS;
@@ -125,10 +160,6 @@ gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cf
   J.resampler = cfg->resampler;
   J.conv = cfg->convention;
   J.prop = cfg->proposal;
-  bool diag = true;
-  for (int j = 0; j < m->dx; ++j)
-    for (int i = 0; i < m->dx; ++i)
-      if (i != j && f.L[i + j * m->dx] != 0.0) diag = false;
   J.diag_l = diag ? 1 : 0;
   J.threshold = cfg->threshold;
   J.log_n = std::log((double)N);
@@ -136,18 +167,20 @@ gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cf
   J.prop_const = f.prop_const;
   J.seed = cfg->seed;
   J.ystride = o->k.dyp + o->k.dxp;
+  J.pstride = o->pstride;
+  J.ppstride = o->ppstride;
   J.lookahead_draw = cfg->lookahead == GF_LOOKAHEAD_DRAW ? 1 : 0;
   return GF_OK;
 }
 
 }  // namespace gf
 
-extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg,
-                                       int32_t T, int32_t flags, gf_pf_plan** out) {
+static gf_status pf_plan_create_impl(gf_ctx* ctx, const gf_lg_model* m, int32_t param_steps,
+                                     const gf_pf_config* cfg, int32_t T, int32_t flags, gf_pf_plan** out) {
   if (!ctx || !out) return GF_ERR_ARG;
   *out = nullptr;
   LgJobSetup L;
-  gf_status st = lg_job_setup(ctx, m, cfg, T, flags, &L);
+  gf_status st = lg_job_setup(ctx, m, cfg, T, flags, &L, param_steps);
   if (st) return st;
   cudaSetDevice(ctx->device);
   auto p = std::make_unique<gf_pf_plan>();
@@ -191,6 +224,7 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   ALLOC(res1, 8);
   ALLOC(job_dev, sizeof(PfJob));
   if (!p->sched.empty()) { ALLOC(sched_dev, (size_t)T); }
+  if (!L.obs_consts.empty()) { ALLOC(obs_consts, sizeof(double) * L.obs_consts.size()); }
 #undef ALLOC
   cudaStream_t s = ctx->stream;
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->params, L.params.data(), L.params.size(), cudaMemcpyHostToDevice, s));
@@ -198,6 +232,9 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   if (p->sched_dev)
     GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->sched_dev, p->sched.data(), (size_t)T, cudaMemcpyHostToDevice, s));
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->ess1, &L.ess1, sizeof(double), cudaMemcpyHostToDevice, s));
+  if (p->obs_consts)
+    GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->obs_consts, L.obs_consts.data(), sizeof(double) * L.obs_consts.size(),
+                                       cudaMemcpyHostToDevice, s));
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(p->res1, &L.res1, 1, cudaMemcpyHostToDevice, s));
   GF_CHECK_CUDA(ctx, cudaStreamSynchronize(s));
   p->small = p->N <= PF_TILE && cfg->resampler != GF_RS_MULTINOMIAL && p->k.small && !(flags & GF_PLAN_NO_FUSE);
@@ -209,6 +246,10 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   p->prop_threads = L.threads;
   p->prop_split = L.split;
   p->prop_smem = L.smem;
+  p->units = L.units_blocks > 0;
+  p->prop_grid = L.units_blocks ? (int)std::min<int64_t>((int64_t)p->ntiles * TC_SUB_UNITS,
+                                                        (int64_t)ctx->num_sms * L.units_blocks)
+                                : p->ntiles * L.split;
   GF_CHECK_CUDA(ctx, cudaFuncSetAttribute((const void*)p->prop_fn,
                                           cudaFuncAttributeMaxDynamicSharedMemorySize, (int)p->prop_smem));
   // all of the SM's shared memory, so the tensor-core propagate reaches its
@@ -233,8 +274,20 @@ extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const 
   J.tprefix = p->tprefix;
   J.eta = p->eta;
   J.schedule = p->sched_dev;
+  J.obs_consts = p->obs_consts;
   *out = p.release();
   return GF_OK;
+}
+
+extern "C" gf_status gf_pf_plan_create(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg,
+                                       int32_t T, int32_t flags, gf_pf_plan** out) {
+  return pf_plan_create_impl(ctx, m, 1, cfg, T, flags, out);
+}
+
+extern "C" gf_status gf_pf_plan_create_tv(gf_ctx* ctx, const gf_lg_model* m, int32_t param_steps,
+                                          const gf_pf_config* cfg, int32_t T, int32_t flags,
+                                          gf_pf_plan** out) {
+  return pf_plan_create_impl(ctx, m, param_steps, cfg, T, flags, out);
 }
 
 // Enqueues one full filter run (prep, init, T steps, outputs) on the stream.
@@ -269,8 +322,9 @@ static void enqueue_run(gf_pf_plan* p, bool means, bool record) {
   for (int t = 1; t <= p->T; ++t) {
     {
       ProfScope ps(ctx, KC_PROPAGATE);
-      p->prop_fn<<<p->ntiles * p->prop_split, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
+      p->prop_fn<<<p->prop_grid, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
     }
+    if (p->units) launch_finish_units(ctx, p->job_dev, 1);
     if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);
     if (record) launch_record(ctx, p->dbl, p->job_dev, p->N);
     if (t < p->T) {
@@ -306,7 +360,8 @@ static gf_status enqueue_run_paths(gf_pf_plan* p, bool means, bool record, void*
       if ((st = tree_host_reserve(p->tree, steps * p->N))) return st;
     }
     tree_launch_step_pre(ctx, p->job_dev, p->N, p->tree.tree, p->cfg.resampler != GF_RS_MULTINOMIAL);
-    p->prop_fn<<<p->ntiles * p->prop_split, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
+    p->prop_fn<<<p->prop_grid, p->prop_threads, p->prop_smem, s>>>(p->job_dev, 1);
+    if (p->units) launch_finish_units(ctx, p->job_dev, 1);
     tree_launch_insert(ctx, p->dbl, p->job_dev, p->N, p->tree.tree, t);
     if (means) launch_means(ctx, p->dbl, p->job_dev, 1, p->ntiles, p->mpart, p->dx);
     if (record) launch_record(ctx, p->dbl, p->job_dev, p->N);
@@ -408,13 +463,13 @@ struct TmpDev {
 };
 }  // namespace
 
-extern "C" gf_status gf_pf_run(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg,
-                               int32_t T, const double* ys, const void* noise,
-                               const double* uniforms, int32_t memspace, gf_pf_out* out) {
+static gf_status pf_run_impl(gf_ctx* ctx, const gf_lg_model* m, int32_t param_steps,
+                             const gf_pf_config* cfg, int32_t T, const double* ys, const void* noise,
+                             const double* uniforms, int32_t memspace, gf_pf_out* out) {
   if (!ctx || !out || !ys) return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
   if (!out->ll) return set_err(ctx, GF_ERR_ARG, "out->ll is required");
   gf_pf_plan* p = nullptr;
-  gf_status st = gf_pf_plan_create(ctx, m, cfg, T, GF_PLAN_NO_GRAPH, &p);
+  gf_status st = pf_plan_create_impl(ctx, m, param_steps, cfg, T, GF_PLAN_NO_GRAPH, &p);
   if (st) return st;
   std::unique_ptr<gf_pf_plan, gf_status (*)(gf_pf_plan*)> guard(p, gf_pf_plan_destroy);
   if (memspace == GF_MEM_DEVICE) {
@@ -469,4 +524,17 @@ extern "C" gf_status gf_pf_run(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_co
   for (auto& mp : maps)
     GF_CHECK_CUDA(ctx, cudaMemcpyAsync(mp.host, *mp.dev, mp.bytes, cudaMemcpyDeviceToHost, s));
   return plan_status(p);
+}
+
+extern "C" gf_status gf_pf_run(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cfg,
+                               int32_t T, const double* ys, const void* noise,
+                               const double* uniforms, int32_t memspace, gf_pf_out* out) {
+  return pf_run_impl(ctx, m, 1, cfg, T, ys, noise, uniforms, memspace, out);
+}
+
+extern "C" gf_status gf_pf_run_tv(gf_ctx* ctx, const gf_lg_model* m, int32_t param_steps,
+                                  const gf_pf_config* cfg, int32_t T, const double* ys,
+                                  const void* noise, const double* uniforms, int32_t memspace,
+                                  gf_pf_out* out) {
+  return pf_run_impl(ctx, m, param_steps, cfg, T, ys, noise, uniforms, memspace, out);
 }

@@ -23,7 +23,7 @@ GF_PREC_F32, GF_PREC_F64 = 0, 1
 GF_PROP_BOOTSTRAP, GF_PROP_OPTIMAL, GF_PROP_OVERDISPERSED = 0, 1, 2
 GF_ALGO_KF, GF_ALGO_SRKF = 0, 1
 GF_PLAN_AUTOTUNE, GF_PLAN_NO_GRAPH, GF_PLAN_PLAIN, GF_PLAN_SIMT, GF_PLAN_NO_FUSE = 1, 2, 4, 8, 16
-GF_PLAN_STAGED_GATHER = 32
+GF_PLAN_STAGED_GATHER, GF_PLAN_UNITS = 32, 64
 GF_REQ_KF, GF_REQ_SRKF, GF_REQ_PF, GF_REQ_RBPF = 0, 1, 2, 3
 GF_CSMC_NONE, GF_CSMC_ANCESTOR, GF_CSMC_BACKWARD = 0, 1, 2
 GF_LOOKAHEAD_NONE, GF_LOOKAHEAD_MEAN, GF_LOOKAHEAD_DRAW = 0, 1, 2
@@ -33,7 +33,7 @@ EXPORTED = [
     "gf_ctx_synchronize", "gf_ctx_memory", "gf_ctx_profile", "gf_ctx_profile_read", "gf_version",
     "gf_kf_batch", "gf_kf_smooth", "gf_kf_batch_tv", "gf_kf_smooth_tv", "gf_kf_plan_create_tv",
     "gf_kf_plan_create", "gf_kf_plan_run", "gf_kf_plan_smooth", "gf_kf_plan_destroy",
-    "gf_pf_run", "gf_pf_plan_create", "gf_pf_plan_run", "gf_pf_plan_destroy", "gf_rbpf_run",
+    "gf_pf_run", "gf_pf_run_tv", "gf_pf_plan_create_tv", "gf_pf_plan_create", "gf_pf_plan_run", "gf_pf_plan_destroy", "gf_rbpf_run",
     "gf_sample_ancestors", "gf_offspring_to_ancestors", "gf_ancestors_to_offspring",
     "gf_rng_normals", "gf_sample_ancestors_noalloc", "gf_sample_ancestors_noalloc_max_n",
     "gf_srv_create", "gf_srv_submit", "gf_srv_poll", "gf_srv_drain", "gf_srv_stats",
@@ -178,6 +178,10 @@ def load(path: str | None = None):
                             _vp, i32, C.POINTER(PFOutC)]),
         "gf_pf_plan_create": (i32, [ctxp, C.POINTER(LGModelC), C.POINTER(PFConfigC), i32, i32,
                                     C.POINTER(_vp)]),
+        "gf_pf_run_tv": (i32, [ctxp, C.POINTER(LGModelC), i32, C.POINTER(PFConfigC), i32, _vp, _vp,
+                               _vp, i32, C.POINTER(PFOutC)]),
+        "gf_pf_plan_create_tv": (i32, [ctxp, C.POINTER(LGModelC), i32, C.POINTER(PFConfigC), i32, i32,
+                                       C.POINTER(_vp)]),
         "gf_pf_plan_run": (i32, [_vp, _vp, _vp, _vp, C.POINTER(PFOutC)]),
         "gf_pf_plan_destroy": (i32, [_vp]),
         "gf_rbpf_run": (i32, [ctxp, C.POINTER(RBModelC), C.POINTER(PFConfigC), i32, _vp, _vp,

@@ -234,8 +234,15 @@ def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sched
                                            "clamps", "paths", "history", "log_weight_history")])
     nz = None if noise is None else np.ascontiguousarray(noise, dtype=rdt)
     un = None if uniforms is None else L.f64(uniforms)
-    L.check(ctx.h, L.load().gf_pf_run(ctx.h, C.byref(mc), C.byref(cfg), T, L.ptr(ys),
-                                      L.ptr(nz), L.ptr(un), L.GF_MEM_HOST, C.byref(o)))
+    if model.is_time_varying():
+        ps = model.param_steps()
+        if ps < T:
+            raise ValueError(f"{ps} parameter steps for {T} observations")
+        L.check(ctx.h, L.load().gf_pf_run_tv(ctx.h, C.byref(mc), ps, C.byref(cfg), T, L.ptr(ys),
+                                             L.ptr(nz), L.ptr(un), L.GF_MEM_HOST, C.byref(o)))
+    else:
+        L.check(ctx.h, L.load().gf_pf_run(ctx.h, C.byref(mc), C.byref(cfg), T, L.ptr(ys),
+                                          L.ptr(nz), L.ptr(un), L.GF_MEM_HOST, C.byref(o)))
     state = ParticleDistribution(out["states"].T, out["log_weights"], ll_steps=out["ll_steps"],
                                  ess_steps=out["ess_steps"], resampled=out["resampled"],
                                  ancestors=out["ancestors"], means=out["means"],

@@ -171,6 +171,28 @@ function with_lg_model(f, model)
     end
 end
 
+# Time-varying models (any LinearGaussianLatentDynamics / ObservationProcess that
+# is not the homogeneous type): calc_params(dyn, t), calc_params(obs, t) for
+# t = 1..T stacked step-major (block t = step t, column-major) for the _tv entry
+# points; f(m, param_steps).
+is_homogeneous(model) = SSMProblems.dyn(model) isa GeneralisedFilters.HomogeneousLinearGaussianLatentDynamics &&
+                        SSMProblems.obs(model) isa GeneralisedFilters.HomogeneousLinearGaussianObservationProcess
+
+function with_lg_model_steps(f, model, T::Integer)
+    is_homogeneous(model) && return with_lg_model(m -> f(m, Int32(1)), model)
+    pr, dy, ob = SSMProblems.prior(model), SSMProblems.dyn(model), SSMProblems.obs(model)
+    μ0, Σ0 = GeneralisedFilters.calc_initial(pr)
+    col(x) = Float64.(vec(collect(x)))
+    steps = [(GeneralisedFilters.calc_params(dy, t)..., GeneralisedFilters.calc_params(ob, t)...) for t in 1:T]
+    stack(k) = reduce(vcat, [col(st[k]) for st in steps])
+    arrs = (col(μ0), col(Matrix(Σ0)), stack(1), stack(2), stack(3), stack(4), stack(5), stack(6))
+    dx, dyo = length(μ0), length(steps[1][5])
+    GC.@preserve arrs begin
+        m = GfLgModel(Int32(dx), Int32(dyo), map(pointer, arrs)...)
+        return f(m, Int32(T))
+    end
+end
+
 resampler_code(::Systematic) = Int32(0)
 resampler_code(::Stratified) = Int32(1)
 resampler_code(::Multinomial) = Int32(2)
@@ -187,7 +209,7 @@ function GeneralisedFilters.filter(
     isnothing(callback) || throw(ArgumentError("GFB200 supports callback=nothing only"))
     T = length(observations)
     ys = reduce(vcat, [Float64.(collect(y)) for y in observations])
-    return with_lg_model(model) do m
+    return with_lg_model_steps(model, T) do m, psteps
         dx = Int(m.dx)
         ll = zeros(Float64, 1)
         means = zeros(Float32, dx * T)
@@ -196,10 +218,11 @@ function GeneralisedFilters.filter(
         out = Ref(GfKfOut(pointer(ll), C_NULL, pointer(means), pointer(covs), pointer(status)))
         jit = algo.jitter
         GC.@preserve ll means covs status ys begin
-            check(ccall((:gf_kf_batch, libgfb200), Int32,
-                        (Ptr{Cvoid}, Int32, Ref{GfLgModel}, Int32, Ref{Int32}, Ptr{Float64},
+            # gf_kf_batch_tv with param_steps = 1 is gf_kf_batch
+            check(ccall((:gf_kf_batch_tv, libgfb200), Int32,
+                        (Ptr{Cvoid}, Int32, Ref{GfLgModel}, Int32, Ref{Int32}, Ref{Int32}, Ptr{Float64},
                          Float64, Int32, Int32, Ref{GfKfOut}),
-                        context(), algo isa KalmanFilter ? 0 : 1, m, 1, Int32(T), ys,
+                        context(), algo isa KalmanFilter ? 0 : 1, m, 1, Int32(T), psteps, ys,
                         isnothing(jit) ? 0.0 : Float64(jit), isnothing(jit) ? 0 : 1,
                         GF_MEM_HOST, out))
         end
@@ -270,7 +293,7 @@ function _bf(rng, model, algo, observations, lookahead::Int32; callback=nothing,
                          algo.resampler.threshold,
                          precision === :f64 ? GF_PREC_F64 : GF_PREC_F32, proposal, proposal_k,
                          rand(rng, UInt64), C_NULL, lookahead))
-    return with_lg_model(model) do m
+    return with_lg_model_steps(model, T) do m, psteps
         dx = Int(m.dx)
         ET = precision === :f64 ? Float64 : Float32
         ll = zeros(Float64, 1)
@@ -279,10 +302,11 @@ function _bf(rng, model, algo, observations, lookahead::Int32; callback=nothing,
         out = Ref(GfPfOut(pointer(ll), C_NULL, C_NULL, C_NULL, C_NULL, C_NULL,
                           Ptr{Cvoid}(pointer(states)), pointer(logw), C_NULL, C_NULL, C_NULL, C_NULL))
         GC.@preserve ll states logw ys begin
-            check(ccall((:gf_pf_run, libgfb200), Int32,
-                        (Ptr{Cvoid}, Ref{GfLgModel}, Ref{GfPfConfig}, Int32, Ptr{Float64},
+            # gf_pf_run_tv with param_steps = 1 is gf_pf_run
+            check(ccall((:gf_pf_run_tv, libgfb200), Int32,
+                        (Ptr{Cvoid}, Ref{GfLgModel}, Int32, Ref{GfPfConfig}, Int32, Ptr{Float64},
                          Ptr{Cvoid}, Ptr{Float64}, Int32, Ref{GfPfOut}),
-                        context(), m, cfg, Int32(T), ys, C_NULL, C_NULL, GF_MEM_HOST, out))
+                        context(), m, psteps, cfg, Int32(T), ys, C_NULL, C_NULL, GF_MEM_HOST, out))
         end
         particles = [Particle(Vector{ET}(states[i, :]), logw[i], 0) for i in 1:N]
         return ParticleDistribution(particles, zero(Float64)), ll[1]

@@ -273,6 +273,73 @@ def test_staged_gather_equals_per_thread_gather(ctx, kind, N, threshold):
         assert out[True][3].sum() >= 3
 
 
+@pytest.mark.parametrize("dims,N", [((16, 8), 5000), ((16, 16), 2 ** 16 + 77), ((32, 16), 3000)])
+def test_unit_grid_propagation_matches_tile_blocks(ctx, dims, N):
+    """The unit-grid tensor-core propagation (resident blocks striding over
+    128-particle units, one log-sum-exp partial per unit) computes the same MMA
+    chain as one block per tile: identical states on the same injected noise; the
+    log-weights and ll differ only through the fold order of the partials."""
+    import torch
+    from gfb200.plans import PfPlan
+    dx, dy = dims
+    m, ys = W.lgssm_rot(seed=dx + dy, dx=dx, dy=dy, T=5)
+    T = 5
+    rng = np.random.default_rng(4)
+    noise = torch.tensor(rng.standard_normal((T + 1, dx, N)).astype(np.float32), device="cuda:0")
+    ysd = torch.tensor(ys, device="cuda:0")
+    out = {}
+    for units in (False, True):
+        plan = PfPlan(m, G.BF(N, threshold=0.0), T, ctx=ctx, graph=False, units=units)
+        states = torch.zeros((dx, N), dtype=torch.float32, device="cuda:0")
+        lw = torch.zeros(N, dtype=torch.float64, device="cuda:0")
+        plan.run(ysd, noise_dev=noise, states=states, log_weights=lw)
+        ctx.synchronize()
+        out[units] = (states.cpu().numpy(), lw.cpu().numpy(), plan.ll_steps.cpu().numpy())
+        plan.close()
+    (s0, w0, l0), (s1, w1, l1) = out[False], out[True]
+    np.testing.assert_array_equal(s0, s1)
+    np.testing.assert_allclose(w0, w1, rtol=0, atol=1e-5)
+    np.testing.assert_allclose(l0, l1, rtol=0, atol=1e-9)
+
+
+def test_unit_grid_resampling_run_matches_oracle_steps(ctx):
+    """Unit-grid propagation with ESS-triggered systematic resampling, teacher-forced
+    against the FP64 oracle step by step (as test_bf_f32_teacher_forced_steps)."""
+    from gfb200.plans import PfPlan
+    import torch
+    m, ys = W.lgssm_rot(seed=7, dx=16, dy=8, T=8)
+    N, T = 4096, 8
+    rng = np.random.default_rng(8)
+    noise = rng.standard_normal((T + 1, 16, N)).astype(np.float32)
+    unif = rng.random(T)
+    om = to_oracle(m)
+    prev = None
+    n_res = 0
+    for t in range(1, T + 1):
+        plan = PfPlan(m, G.BF(N, threshold=0.9), t, ctx=ctx, graph=False, units=True)
+        states = torch.zeros((16, N), dtype=torch.float32, device="cuda:0")
+        lw = torch.zeros(N, dtype=torch.float64, device="cuda:0")
+        anc = torch.zeros((t, N), dtype=torch.int32, device="cuda:0")
+        plan.run(torch.tensor(ys[:t], device="cuda:0"), noise_dev=torch.tensor(noise[:t + 1], device="cuda:0"),
+                 unif_dev=torch.tensor(unif[:t], device="cuda:0"), states=states, log_weights=lw,
+                 ancestors=anc)
+        ctx.synchronize()
+        cur = (states.cpu().numpy().T.copy(), lw.cpu().numpy(), anc.cpu().numpy(),
+               plan.resampled.cpu().numpy(), plan.ll_steps.cpu().numpy())
+        plan.close()
+        if prev is not None:
+            ref = O.pf_step(om, prev[0].astype(np.float64), prev[1], ys[t - 1],
+                            noise[t].astype(np.float64), unif[t - 1], threshold=0.9)
+            assert bool(cur[3][t - 1]) == ref["resampled"]
+            n_res += ref["resampled"]
+            bad, _ = ancestors_match(cur[2][t - 1], ref["ancestors"], ref["margins"], 1e-8)
+            assert bad == 0
+            np.testing.assert_allclose(cur[0], ref["x"], rtol=2e-5, atol=2e-5)
+            assert abs(cur[4][t - 1] - ref["ll_inc"]) < 1e-4
+        prev = cur
+    assert n_res >= 3
+
+
 @pytest.mark.parametrize("kind,threshold,T", [(O.SYSTEMATIC, 0.5, 6), (O.STRATIFIED, 1.0, 5),
                                               (O.MULTINOMIAL, 0.7, 5), (O.SYSTEMATIC, 0.0, 70)])
 def test_path_storage_matches_dense_ancestry(ctx, kind, threshold, T):

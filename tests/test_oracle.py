@@ -50,6 +50,18 @@ def test_nonhomogeneous_kf_and_smoother_match_joint_gaussian(Dy, T):
     np.testing.assert_array_equal(O.kf_filter(h, ys)[2], O.kf_filter(hv, ys)[2])
 
 
+def test_nonhomogeneous_pf_oracle_converges_to_kf():
+    """The oracle's bootstrap PF on a time-varying model uses step t's
+    parameters: its ll converges to the exact time-varying KF (N = 2e5)."""
+    rng = np.random.default_rng(5)
+    m = O.create_nonhomogeneous_linear_gaussian_model(rng, 2, 2, 5)
+    m = O.LGModel.time_varying(m.mu0, m.Sigma0, [O.random_orthogonal(rng, 2) * 0.8 for _ in range(5)],
+                               m.bs, m.Qs, m.Hs, m.cs, m.Rs)
+    _, ys = O.sample(rng, m, 5)
+    lls = [O.pf_run(m, 200000, ys, threshold=0.5, seed=s, threads=4)["ll"] for s in range(2)]
+    assert abs(np.mean(lls) - O.kf_filter(m, ys)[0]) < 2e-2
+
+
 @pytest.mark.parametrize("Dy", [1, 2, 3])
 @pytest.mark.parametrize("T", [1, 5])
 def test_rts_smoother_matches_joint_gaussian(Dy, T):
