@@ -161,6 +161,7 @@ gf_status gf_ctx_destroy(gf_ctx* ctx) {
   if (!ctx) return GF_OK;
   cudaSetDevice(ctx->device);
   cudaStreamSynchronize(ctx->stream);
+  gf::pf_plan_cache_release(ctx);
   for (auto& p : ctx->pending) {
     cudaEventDestroy(p.a);
     cudaEventDestroy(p.b);

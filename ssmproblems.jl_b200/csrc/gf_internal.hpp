@@ -30,6 +30,9 @@ struct gf_ctx {
   std::vector<cudaEvent_t> event_pool;
   double prof_ms[8] = {0};
   long long prof_n[8] = {0};
+  // plans kept by the one-shot particle-filter calls (gf_pf_run, gf_pf_run_tv),
+  // most recently used first: (model / configuration key, gf_pf_plan*)
+  std::vector<std::pair<std::vector<char>, void*>> pf_plans;
 };
 
 namespace gf {
@@ -37,6 +40,7 @@ namespace gf {
 enum KernelClass { KC_PROPAGATE = 0, KC_SCAN = 1, KC_KF = 2, KC_RBPF = 3, KC_PREP = 4, KC_FILL = 5 };
 
 gf_status set_err(gf_ctx* ctx, gf_status code, const char* fmt, ...);
+void pf_plan_cache_release(gf_ctx* ctx);  // frees the plans kept in ctx->pf_plans
 gf_status cuda_err(gf_ctx* ctx, cudaError_t e, const char* where);
 gf_status dev_alloc(gf_ctx* ctx, size_t bytes, void** p);
 void dev_free(gf_ctx* ctx, void* p, size_t bytes);

@@ -463,15 +463,90 @@ struct TmpDev {
 };
 }  // namespace
 
+// One-shot calls keep their plans in the context: a call with the same model,
+// configuration (all but the seed), T and parameter steps as a kept plan reuses
+// its device buffers and its captured CUDA graph instead of building them again
+// (PF_PLAN_CACHE plans per context, least recently used dropped; models whose
+// key exceeds PF_PLAN_KEY_MAX bytes are not kept).
+constexpr size_t PF_PLAN_CACHE = 4;
+constexpr size_t PF_PLAN_KEY_MAX = 1 << 20;
+
+namespace gf {
+void pf_plan_cache_release(gf_ctx* ctx) {
+  for (auto& e : ctx->pf_plans) gf_pf_plan_destroy(static_cast<gf_pf_plan*>(e.second));
+  ctx->pf_plans.clear();
+}
+}  // namespace gf
+
+static bool pf_plan_key(const gf_lg_model* m, int32_t param_steps, const gf_pf_config* cfg, int32_t T,
+                        std::vector<char>& key) {
+  if (!m || !cfg || m->dx < 1 || m->dy < 1 || T < 1) return false;
+  const size_t dx = m->dx, dy = m->dy, nb = param_steps > 1 ? (size_t)param_steps : 1;
+  const size_t bytes = 8 * (dx + dx * dx + nb * (2 * dx * dx + dx + dy * dx + dy + dy * dy)) + T + 128;
+  if (bytes > PF_PLAN_KEY_MAX) return false;
+  key.clear();
+  key.reserve(bytes);
+  auto put = [&](const void* p, size_t n) {
+    const char* c = static_cast<const char*>(p);
+    key.insert(key.end(), c, c + n);
+  };
+  gf_pf_config c = *cfg;
+  c.seed = 0;
+  c.schedule = nullptr;
+  const int32_t hdr[4] = {m->dx, m->dy, T, param_steps};
+  put(hdr, sizeof hdr);
+  put(&c, sizeof c);
+  const int8_t has_sched = cfg->schedule ? 1 : 0;
+  put(&has_sched, 1);
+  if (cfg->schedule) put(cfg->schedule, (size_t)T);
+  put(m->mu0, 8 * dx);
+  put(m->Sigma0, 8 * dx * dx);
+  put(m->A, 8 * nb * dx * dx);
+  put(m->b, 8 * nb * dx);
+  put(m->Q, 8 * nb * dx * dx);
+  put(m->H, 8 * nb * dy * dx);
+  put(m->c, 8 * nb * dy);
+  put(m->R, 8 * nb * dy * dy);
+  return true;
+}
+
 static gf_status pf_run_impl(gf_ctx* ctx, const gf_lg_model* m, int32_t param_steps,
                              const gf_pf_config* cfg, int32_t T, const double* ys, const void* noise,
                              const double* uniforms, int32_t memspace, gf_pf_out* out) {
   if (!ctx || !out || !ys) return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
   if (!out->ll) return set_err(ctx, GF_ERR_ARG, "out->ll is required");
   gf_pf_plan* p = nullptr;
-  gf_status st = pf_plan_create_impl(ctx, m, param_steps, cfg, T, GF_PLAN_NO_GRAPH, &p);
-  if (st) return st;
-  std::unique_ptr<gf_pf_plan, gf_status (*)(gf_pf_plan*)> guard(p, gf_pf_plan_destroy);
+  gf_status st = GF_OK;
+  std::vector<char> key;
+  const bool keep = pf_plan_key(m, param_steps, cfg, T, key);
+  for (size_t k = 0; keep && k < ctx->pf_plans.size(); ++k)
+    if (ctx->pf_plans[k].first == key) {
+      p = static_cast<gf_pf_plan*>(ctx->pf_plans[k].second);
+      std::rotate(ctx->pf_plans.begin(), ctx->pf_plans.begin() + k, ctx->pf_plans.begin() + k + 1);
+      break;
+    }
+  std::unique_ptr<gf_pf_plan, gf_status (*)(gf_pf_plan*)> guard(nullptr, gf_pf_plan_destroy);
+  if (!p) {
+    st = pf_plan_create_impl(ctx, m, param_steps, cfg, T, keep ? 0 : GF_PLAN_NO_GRAPH, &p);
+    if (st && !ctx->pf_plans.empty() && (st == GF_ERR_OOM_BUDGET || st == GF_ERR_CUDA)) {
+      // the kept plans hold device memory: drop them and try once more
+      pf_plan_cache_release(ctx);
+      cudaGetLastError();
+      st = pf_plan_create_impl(ctx, m, param_steps, cfg, T, keep ? 0 : GF_PLAN_NO_GRAPH, &p);
+    }
+    if (st) return st;
+    if (keep) {
+      ctx->pf_plans.insert(ctx->pf_plans.begin(), {std::move(key), p});
+      while (ctx->pf_plans.size() > PF_PLAN_CACHE) {
+        gf_pf_plan_destroy(static_cast<gf_pf_plan*>(ctx->pf_plans.back().second));
+        ctx->pf_plans.pop_back();
+      }
+    } else {
+      guard.reset(p);
+    }
+  }
+  p->cfg.seed = cfg->seed;
+  p->job.seed = cfg->seed;
   if (memspace == GF_MEM_DEVICE) {
     if ((st = gf_pf_plan_run(p, ys, noise, uniforms, out))) return st;
     return plan_status(p);

@@ -133,6 +133,22 @@ def test_fused_rng_equals_exported_noise(ctx, prec, dx, N):
     np.testing.assert_array_equal(a.particles, b.particles)
 
 
+def test_kept_plans_take_each_calls_seed_and_inputs(ctx):
+    """gf_pf_run keeps its plan for calls with the same model and configuration:
+    a later call with another seed or other observations must still see them
+    (and give what a fresh context gives)."""
+    m, ys = W.lgssm_rot(seed=3, dx=16, dy=8, T=30)
+    algo = G.BF(50000, threshold=0.5)
+    a = G.filter(m, algo, ys, seed=1, ctx=ctx)[1]
+    b = G.filter(m, algo, ys, seed=2, ctx=ctx)[1]
+    c = G.filter(m, algo, ys, seed=1, ctx=ctx)[1]
+    d = G.filter(m, algo, ys[::-1].copy(), seed=1, ctx=ctx)[1]
+    fresh = G.Context(0)
+    e = G.filter(m, algo, ys[::-1].copy(), seed=1, ctx=fresh)[1]
+    fresh.close()
+    assert a == c and a != b and d != a and d == e
+
+
 def test_runs_are_deterministic(ctx):
     m, ys = W.lgssm_rot(seed=4, dx=16, dy=8, T=40)
     algo = G.BF(200_000, threshold=0.5)
