@@ -316,6 +316,11 @@ gf_status gf_pf_dense_ancestry(gf_ctx* ctx, int32_t T, int64_t N, int32_t dx, in
 
 /* filter(rng, hier_model, RBPF(PF(N, ...), KalmanFilter()), ys) (rbpf.jl:8-84).
  * Supports GF_PROP_BOOTSTRAP and GF_PROP_OVERDISPERSED outer proposals.
+ * cfg->lookahead != GF_LOOKAHEAD_NONE runs AuxiliaryParticleFilter(RBPF(...),
+ * pp) (rbpf.jl:86-124): log eta_i is the inner update log-likelihood of y_t
+ * after predicting particle i's inner Gaussian to x*, the mean of its outer
+ * transition (GF_LOOKAHEAD_MEAN) or one draw from it (GF_LOOKAHEAD_DRAW, from
+ * the lookahead Philox stream with counters (i, t, 0)).
  * noise: nullable [(T+1)][dxo][N] FP32.  states out: GF_MEM_HOST gives
  * [dxo + dz + dz*dz][N] (x, mu, Sigma column-major); GF_MEM_DEVICE gives the
  * device layout [dxo + dz + dz*(dz+1)/2][N] (Sigma packed upper, row by row).

@@ -1051,6 +1051,39 @@ static int rb_particle_step(const or_rb_model* m, const or_proposal* prop, const
   return s2;
 }
 
+/* First-stage score of the auxiliary RBPF (rbpf.jl:86-124 through
+ * compute_logeta, particles.jl:283-296): x* = A_o x + b_o, the mean / mode of
+ * the outer transition, or (lookahead == 2, DrawPredictive) one draw
+ * A_o x + b_o + chol(Q_o) e' with e' from the Philox stream tagged
+ * TAG_LOOKAHEAD, counters (i, t, 0); the inner Gaussian predicted with
+ * (prev_outer x, new_outer x*) and log eta = the update log-likelihood of y
+ * (predictive_loglik).  p = [x | mu | Sigma | L] is left unchanged; q is
+ * scratch of the same width. */
+static int rb_logeta(const or_rb_model* m, int lookahead, const double* LQo, const double* LR,
+                     const double* y, const double* p, uint64_t seed, long i, int t, double* q,
+                     double* Qt, kf_ws* ws, double* eta) {
+  int dxo = m->dxo, dz = m->dz, dy = m->dy;
+  double xs[64], bt[64], e[64], v[64], buf[4];
+  mv(dxo, dxo, m->A_o, p, xs);
+  for (int d = 0; d < dxo; ++d) xs[d] += m->b_o[d];
+  if (lookahead == 2) {
+    philox_normals4_tag(seed, (uint32_t)i, (uint32_t)t, 0u, TAG_LOOKAHEAD, buf);
+    for (int d = 0; d < dxo; ++d) e[d] = buf[d];
+    mv(dxo, dxo, LQo, e, v);
+    for (int d = 0; d < dxo; ++d) xs[d] += v[d];
+  }
+  mv(dz, dxo, m->C_z, p, bt);
+  for (int d = 0; d < dz; ++d) bt[d] += m->b_z[d];
+  double qs = exp(m->q_gamma * xs[m->q_index]);
+  for (int k = 0; k < dz * dz; ++k) Qt[k] = m->Q_z[k] * qs;
+  double *mu = q, *Sig = q + dz, *L = q + dz + dz * dz;
+  memcpy(mu, p + dxo, sizeof(double) * dz);
+  memcpy(Sig, p + dxo + dz, sizeof(double) * dz * dz);
+  memcpy(L, p + dxo + dz + dz * dz, sizeof(double) * dz * dz);
+  int st = kf_predict(dz, m->A_z, bt, Qt, mu, Sig, L, ws);
+  return st ? st : kf_update(dz, dy, m->H, m->c, m->R, LR, y, 0.0, 0, mu, Sig, L, eta, ws);
+}
+
 int or_rbpf_run(const or_rb_model* m, const or_proposal* prop, const or_resample_cfg* rc, long N,
                 int T, const double* ys, const double* noise, const double* uniforms,
                 uint64_t seed, double* ll, or_pf_out* out, double* zmeans /* T*dz */) {
@@ -1061,6 +1094,8 @@ int or_rbpf_run(const or_rb_model* m, const or_proposal* prop, const or_resample
   double* logw = calloc(N, 8);
   double* wbuf = malloc(sizeof(double) * N);
   double* ubuf = malloc(sizeof(double) * N);
+  double* eta = malloc(sizeof(double) * N);
+  double* aux = malloc(sizeof(double) * N);
   double *Lo0 = calloc(dxo * dxo, 8), *LQo = calloc(dxo * dxo, 8), *Lqo = calloc(dxo * dxo, 8);
   double *LZ0 = calloc(dz * dz, 8), *LR = calloc(dy * dy, 8);
   int st = OR_OK, uniform = 1;
@@ -1090,14 +1125,64 @@ int or_rbpf_run(const or_rb_model* m, const or_proposal* prop, const or_resample
   for (int t = 1; t <= T; ++t) {
     int32_t* anc_t = out && out->ancestors ? out->ancestors + (size_t)(t - 1) * N : NULL;
     double* mar_t = out && out->margins ? out->margins + (size_t)(t - 1) * N : NULL;
-    double ess = 0.0;
-    int was_uniform = uniform;
-    int res = maybe_resample(rc, t, N, width, S, Stmp, logw, &uniform, wbuf, ubuf, uniforms,
-                             seed, anc_t, mar_t, &ess, &clamps);
+    double ess = 0.0, baseline;
+    int res;
+    const double* y = ys + (size_t)(t - 1) * dy;
+    if (prop->lookahead) {
+      /* AuxiliaryParticleFilter(RBPF(...), pp) step (particles.jl:311-345):
+       * resample on softmax(logw + log eta) (resamplers.jl:109-116), new weights
+       * -log eta[a] and the ll_baseline of construct_new_state (:118-143), as
+       * in or_pf_run. */
+      int bad = 0;
+#pragma omp parallel num_threads(g_threads) reduction(| : bad)
+      {
+      kf_ws ws = kf_ws_alloc(dz, dy);
+      double* Qt = malloc(sizeof(double) * dz * dz);
+      double* q = malloc(sizeof(double) * width);
+#pragma omp for schedule(static)
+      for (long i = 0; i < N; ++i) {
+        if (rb_logeta(m, prop->lookahead, LQo, LR, y, S + (size_t)i * width, seed, i, t, q, Qt, &ws,
+                      &eta[i]))
+          bad |= 1;
+        aux[i] = (uniform ? 0.0 : logw[i]) + eta[i];
+      }
+      free(q); free(Qt);
+      kf_ws_free(&ws);
+      }
+      if (bad) { st = OR_NOT_PD; break; }
+      softmax(aux, N, wbuf);
+      ess = ess_of(wbuf, N);
+      int sched = rc->schedule ? rc->schedule[t - 1] : -1;
+      res = sched >= 0 ? sched : (rc->threshold * (double)N >= ess);
+      if (res) {
+        draw_uniforms(uniforms, seed, rc->kind, N, t, ubuf);
+        int32_t* a = anc_t ? anc_t : (int32_t*)malloc(sizeof(int32_t) * N);
+        clamps += or_sample_ancestors(rc->kind, rc->conv, N, wbuf, ubuf, a, mar_t);
+        memcpy(Stmp, S, sizeof(double) * N * width);
+        for (long i = 0; i < N; ++i)
+          memcpy(S + (size_t)i * width, Stmp + (size_t)(a[i] - 1) * width, sizeof(double) * width);
+        const double lse1 = or_logsumexp(aux, N);
+        const double lse2 = uniform ? log((double)N) : or_logsumexp(logw, N);
+        for (long i = 0; i < N; ++i) logw[i] = -eta[a[i] - 1];
+        const double lse3 = or_logsumexp(logw, N), lse4 = log((double)N);
+        baseline = lse3 - ((lse1 - lse2) + (lse3 - lse4));
+        uniform = 0;
+        if (!anc_t) free(a);
+      } else {
+        if (anc_t)
+          for (long i = 0; i < N; ++i) anc_t[i] = (int32_t)(i + 1);
+        if (mar_t)
+          for (long i = 0; i < N; ++i) mar_t[i] = 0.0;
+        baseline = uniform ? log((double)N) : or_logsumexp(logw, N);
+      }
+    } else {
+      int was_uniform = uniform;
+      res = maybe_resample(rc, t, N, width, S, Stmp, logw, &uniform, wbuf, ubuf, uniforms,
+                           seed, anc_t, mar_t, &ess, &clamps);
+      baseline = (was_uniform && !res) ? log((double)N) : or_logsumexp(logw, N);
+    }
     if (out && out->ess) out->ess[t - 1] = ess;
     if (out && out->resampled) out->resampled[t - 1] = (int8_t)res;
-    double baseline = (was_uniform && !res) ? log((double)N) : or_logsumexp(logw, N);
-    const double* y = ys + (size_t)(t - 1) * dy;
     int fail = 0;
 #pragma omp parallel num_threads(g_threads) reduction(| : fail)
     {
@@ -1143,7 +1228,7 @@ int or_rbpf_run(const or_rb_model* m, const or_proposal* prop, const or_resample
 done:
   if (out && out->clamps) *out->clamps = clamps;
   *ll = tot;
-  free(S); free(Stmp); free(logw); free(wbuf); free(ubuf);
+  free(S); free(Stmp); free(logw); free(wbuf); free(ubuf); free(eta); free(aux);
   free(Lo0); free(LQo); free(Lqo); free(LZ0); free(LR);
   return st;
 }

@@ -369,8 +369,10 @@ class RBModel:
 
 def rbpf_run(m: RBModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=0.5,
              schedule=None, noise=None, uniforms=None, seed=0, proposal=PROP_BOOTSTRAP,
-             k=1.0, want_ancestors=False, threads=1):
-    """filter(rng, hier_model, RBPF(PF(N, ...), KalmanFilter()), ys)."""
+             k=1.0, want_ancestors=False, want_margins=False, threads=1, lookahead=0):
+    """filter(rng, hier_model, RBPF(PF(N, ...), KalmanFilter()), ys); lookahead=1
+    (MeanPredictive) or 2 (DrawPredictive) runs AuxiliaryParticleFilter(RBPF(...),
+    pp) (rbpf.jl:86-124)."""
     ys = _f64(ys).reshape(-1, m.dy)
     T = ys.shape[0]
     width = m.dxo + m.dz + m.dz * m.dz
@@ -379,11 +381,12 @@ def rbpf_run(m: RBModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshol
                logw_final=np.zeros(N))
     zmeans = np.zeros((T, m.dz))
     anc = np.zeros((T, N), np.int32) if want_ancestors else None
+    mar = np.zeros((T, N)) if want_margins else None
     clamps = C.c_long(0)
     o = _PFOut(_p(out["ll_steps"]), _p(out["ess"]),
                out["resampled"].ctypes.data_as(C.POINTER(C.c_int8)),
                None if anc is None else anc.ctypes.data_as(C.POINTER(C.c_int32)),
-               None, _p(out["means"]), _p(out["x_final"]), _p(out["logw_final"]),
+               _p(mar), _p(out["means"]), _p(out["x_final"]), _p(out["logw_final"]),
                C.pointer(clamps))
     sched = None if schedule is None else np.ascontiguousarray(schedule, np.int8)
     rc = _RC(resampler, conv, threshold,
@@ -392,13 +395,13 @@ def rbpf_run(m: RBModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshol
     un = None if uniforms is None else _f64(uniforms)
     ll = C.c_double()
     lib().or_set_threads(int(threads))
-    st = lib().or_rbpf_run(C.byref(m._struct()), C.byref(_Prop(proposal, k)), C.byref(rc),
+    st = lib().or_rbpf_run(C.byref(m._struct()), C.byref(_Prop(proposal, k, int(lookahead))), C.byref(rc),
                            C.c_long(N), T, _p(ys), _p(nz), _p(un), C.c_uint64(seed),
                            C.byref(ll), C.byref(o), _p(zmeans))
     lib().or_set_threads(1)
     if st:
         raise np.linalg.LinAlgError(f"oracle RBPF status {st}")
-    out.update(ll=ll.value, ancestors=anc, zmeans=zmeans, clamps=clamps.value)
+    out.update(ll=ll.value, ancestors=anc, margins=mar, zmeans=zmeans, clamps=clamps.value)
     return out
 
 

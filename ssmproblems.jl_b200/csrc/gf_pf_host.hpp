@@ -78,6 +78,7 @@ struct RbKernels {
   int dxo, dz, dy;
   void (*prop)(const PfJob*, int, float, int, int);
   void (*init)(const PfJob*, int);
+  void (*lookahead)(const PfJob*, int, float, int);  // auxiliary RBPF first stage
 };
 bool pick_rb(int dxo, int dz, int dy, RbKernels* out);
 gf_status rb_pack_params(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_config* cfg,

@@ -435,12 +435,14 @@ static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh,
 // resamplers.jl:109-116, 179-183), and after a resample the tile prefixes of
 // those weights and the baseline shift LSE(logw) - LSE(logw + log eta) that
 // construct_new_state folds into ll_baseline (resamplers.jl:118-138; with the
-// particles' new log-weights -log eta[a], LSE_3 cancels in predict).
-static __device__ void apf_finish(const PfJob& J, int tile, int t, LseAcc a, double* red) {
+// particles' new log-weights -log eta[a], LSE_3 cancels in predict).  A tile
+// may be scored by `nparts` blocks (block `part` of tile `tile`).
+static __device__ void apf_finish(const PfJob& J, int tile, int t, LseAcc a, double* red, int part = 0,
+                                  int nparts = 1) {
   PfScalars* sc = J.sc;
-  if (!fold_partials(J, tile, a, red, 0, 1)) return;
+  if (!fold_partials(J, tile, a, red, part, nparts)) return;
   double GM, GS1, GS2;
-  global_stats(BlockSync(), J, 1, red, &GM, &GS1, &GS2);
+  global_stats(BlockSync(), J, nparts, red, &GM, &GS1, &GS2);
   const double lse1 = GM + log(GS1);
   __shared__ int s_res;
   __shared__ unsigned long long s_wsum[32];
@@ -457,7 +459,7 @@ static __device__ void apf_finish(const PfJob& J, int tile, int t, LseAcc a, dou
     s_res = res;
   }
   __syncthreads();
-  if (s_res) write_tile_prefixes(BlockSync(), J, 1, lse1, s_wsum);
+  if (s_res) write_tile_prefixes(BlockSync(), J, nparts, lse1, s_wsum);
   __syncthreads();
   if (threadIdx.x == 0) {
     sc->counter = 0u;

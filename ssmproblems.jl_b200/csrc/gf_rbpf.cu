@@ -38,6 +38,119 @@ __host__ __device__ constexpr int pk(int i, int j, int n) {  // packed upper ind
 static_assert(RB_SPLIT * RB_THREADS == PF_TILE, "RBPF blocks must tile a propagate tile exactly");
 static_assert(RB_SPLIT <= PF_MAX_SPLIT, "part buffers hold PF_MAX_SPLIT partials per tile");
 
+// Inner KF predict of one particle (kalman.jl:42-49 with prev_outer x and
+// new_outer xn, rbpf.jl:45-55): mp = Az mu + bz + Cz x and the packed upper
+// Sp = Az S Az' + Qz exp(gamma xn[q_index]).
+template <int DXO, int DZ, int DY>
+__device__ __forceinline__ void rb_inner_predict(const float* sp, const float (&x)[DXO], const float (&xn)[DXO],
+                                                 float q_gamma, int q_index, const float (&mu)[DZ],
+                                                 const float (&S)[DZ * (DZ + 1) / 2], float (&mp)[DZ],
+                                                 float (&Sp)[DZ * (DZ + 1) / 2]) {
+  using L = RbLayout<DXO, DZ, DY>;
+#pragma unroll
+  for (int r = 0; r < DZ; ++r) {
+    float v = sp[L::bz + r];
+#pragma unroll
+    for (int c = 0; c < DXO; ++c) v = fmaf(sp[L::Cz + c * DZ + r], x[c], v);
+#pragma unroll
+    for (int c = 0; c < DZ; ++c) v = fmaf(sp[L::Az + c * DZ + r], mu[c], v);
+    mp[r] = v;
+  }
+  const float qs = q_gamma != 0.f ? __expf(q_gamma * xn[q_index]) : 1.f;
+  // T = Az S (row r), then Sp[r][j] = T_r . Az[j,:] for j >= r
+#pragma unroll
+  for (int r = 0; r < DZ; ++r) {
+    float Tr[DZ];
+#pragma unroll
+    for (int k = 0; k < DZ; ++k) {
+      float v = 0.f;
+#pragma unroll
+      for (int m = 0; m < DZ; ++m) {
+        const float Smk = m <= k ? S[pk(m, k, DZ)] : S[pk(k, m, DZ)];
+        v = fmaf(sp[L::Az + m * DZ + r], Smk, v);
+      }
+      Tr[k] = v;
+    }
+#pragma unroll
+    for (int j = r; j < DZ; ++j) {
+      float v = sp[L::Qz + pk(r, j, DZ)] * qs;
+#pragma unroll
+      for (int k = 0; k < DZ; ++k) v = fmaf(Tr[k], sp[L::Az + k * DZ + j], v);
+      Sp[pk(r, j, DZ)] = v;
+    }
+  }
+}
+
+// Innovation of the inner update (kalman_gradient.jl:12-23): PHt = Sp H' and
+// the FP64 Cholesky factor (lower, in place) of S = H Sp H' + R.  Returns
+// false if S is not positive definite.
+template <int DXO, int DZ, int DY>
+__device__ __forceinline__ bool rb_innovation(const float* sp, const float (&Sp)[DZ * (DZ + 1) / 2],
+                                              float (&PHt)[DZ][DY], double (&Sd)[DY][DY]) {
+  using L = RbLayout<DXO, DZ, DY>;
+#pragma unroll
+  for (int r = 0; r < DZ; ++r)
+#pragma unroll
+    for (int j = 0; j < DY; ++j) {
+      float v = 0.f;
+#pragma unroll
+      for (int k = 0; k < DZ; ++k) {
+        const float Srk = r <= k ? Sp[pk(r, k, DZ)] : Sp[pk(k, r, DZ)];
+        v = fmaf(Srk, sp[L::H + k * DY + j], v);
+      }
+      PHt[r][j] = v;
+    }
+#pragma unroll
+  for (int i2 = 0; i2 < DY; ++i2)
+#pragma unroll
+    for (int j = 0; j <= i2; ++j) {
+      double v = (double)sp[L::R + j * DY + i2];
+#pragma unroll
+      for (int k = 0; k < DZ; ++k) v += (double)sp[L::H + k * DY + i2] * (double)PHt[k][j];
+      Sd[i2][j] = v;
+    }
+  bool pd = true;
+#pragma unroll
+  for (int j = 0; j < DY; ++j) {
+    double d = Sd[j][j];
+#pragma unroll
+    for (int k = 0; k < j; ++k) d -= Sd[j][k] * Sd[j][k];
+    pd = pd && (d > 0.0);
+    d = sqrt(fmax(d, 1e-300));
+    Sd[j][j] = d;
+#pragma unroll
+    for (int i2 = j + 1; i2 < DY; ++i2) {
+      double v = Sd[i2][j];
+#pragma unroll
+      for (int k = 0; k < j; ++k) v -= Sd[i2][k] * Sd[j][k];
+      Sd[i2][j] = v / d;
+    }
+  }
+  return pd;
+}
+
+// Whitened innovation w = L^-1 (y - H mp - c), its squared norm and
+// log det L: the update's log-likelihood is -(qf + 2 ldet + dy log 2 pi) / 2.
+template <int DXO, int DZ, int DY>
+__device__ __forceinline__ void rb_whiten(const float* sp, const double* sy, const float (&mp)[DZ],
+                                          const double (&Sd)[DY][DY], double (&w)[DY], double& qf,
+                                          double& ldet) {
+  using L = RbLayout<DXO, DZ, DY>;
+  qf = 0.0;
+  ldet = 0.0;
+#pragma unroll
+  for (int i2 = 0; i2 < DY; ++i2) {
+    double v = sy[i2] - (double)sp[L::c + i2];
+#pragma unroll
+    for (int k = 0; k < DZ; ++k) v -= (double)sp[L::H + k * DY + i2] * (double)mp[k];
+#pragma unroll
+    for (int k = 0; k < i2; ++k) v -= Sd[i2][k] * w[k];
+    w[i2] = v / Sd[i2][i2];
+    qf += w[i2] * w[i2];
+    ldet += log(Sd[i2][i2]);
+  }
+}
+
 // One particle per thread: a particle's Kalman update needs ~250 registers, so
 // a 1024-particle tile is spread over RB_SPLIT blocks of RB_THREADS threads
 // (grid = RB_SPLIT * tiles) to keep every SM busy at moderate N.
@@ -69,6 +182,9 @@ __global__ void __launch_bounds__(RB_THREADS) rbpf_propagate(const PfJob* __rest
   float* Xd = reinterpret_cast<float*>(J.X[t & 1]);
   float* lw = reinterpret_cast<float*>(J.lw);
   const float* noise = J.noise ? reinterpret_cast<const float*>(J.noise) + (size_t)t * DXO * N : nullptr;
+  // auxiliary filter: after a resample the new weights are -log eta[a]
+  const float* eta = reinterpret_cast<const float*>(J.eta);
+  const bool apf = resamp && eta != nullptr;
   LseAcc acc;
   int fail = 0;
   for (int p = 0; p < 1; ++p) {
@@ -83,7 +199,7 @@ __global__ void __launch_bounds__(RB_THREADS) rbpf_propagate(const PfJob* __rest
     for (int d = 0; d < DZ; ++d) mu[d] = Xs[(size_t)(DXO + d) * N + a];
 #pragma unroll
     for (int d = 0; d < NS; ++d) S[d] = Xs[(size_t)(DXO + DZ + d) * N + a];
-    const double lin = fresh ? 0.0 : (double)lw[i] - lse_prev;
+    const double lin = !fresh ? (double)lw[i] - lse_prev : apf ? -(double)eta[a] : 0.0;
     // ---- outer propagate
     float e[DXO];
     if (noise) {
@@ -131,99 +247,14 @@ __global__ void __launch_bounds__(RB_THREADS) rbpf_propagate(const PfJob* __rest
       }
       inc = -0.5 * (double)qz + 0.5 * (double)qe + J.prop_const;
     }
-    // ---- inner predict: mu^ = Az mu + bz + Cz x_prev ; Sp = Az S Az' + Qz exp(gamma x'[qi])
-    float mp[DZ];
-#pragma unroll
-    for (int r = 0; r < DZ; ++r) {
-      float v = sp[L::bz + r];
-#pragma unroll
-      for (int c = 0; c < DXO; ++c) v = fmaf(sp[L::Cz + c * DZ + r], x[c], v);
-#pragma unroll
-      for (int c = 0; c < DZ; ++c) v = fmaf(sp[L::Az + c * DZ + r], mu[c], v);
-      mp[r] = v;
-    }
-    const float qs = q_gamma != 0.f ? __expf(q_gamma * xn[q_index]) : 1.f;
-    float Sp[NS];
-    {
-      // T = Az S (row r), then Sp[r][j] = T_r . Az[j,:] for j >= r
-#pragma unroll
-      for (int r = 0; r < DZ; ++r) {
-        float Tr[DZ];
-#pragma unroll
-        for (int k = 0; k < DZ; ++k) {
-          float v = 0.f;
-#pragma unroll
-          for (int m = 0; m < DZ; ++m) {
-            const float Smk = m <= k ? S[pk(m, k, DZ)] : S[pk(k, m, DZ)];
-            v = fmaf(sp[L::Az + m * DZ + r], Smk, v);
-          }
-          Tr[k] = v;
-        }
-#pragma unroll
-        for (int j = r; j < DZ; ++j) {
-          float v = sp[L::Qz + pk(r, j, DZ)] * qs;
-#pragma unroll
-          for (int k = 0; k < DZ; ++k) v = fmaf(Tr[k], sp[L::Az + k * DZ + j], v);
-          Sp[pk(r, j, DZ)] = v;
-        }
-      }
-    }
-    // ---- inner update
+    // ---- inner predict, then the update's innovation and log-likelihood
+    float mp[DZ], Sp[NS];
+    rb_inner_predict<DXO, DZ, DY>(sp, x, xn, q_gamma, q_index, mu, S, mp, Sp);
     float PHt[DZ][DY];
-#pragma unroll
-    for (int r = 0; r < DZ; ++r)
-#pragma unroll
-      for (int j = 0; j < DY; ++j) {
-        float v = 0.f;
-#pragma unroll
-        for (int k = 0; k < DZ; ++k) {
-          const float Srk = r <= k ? Sp[pk(r, k, DZ)] : Sp[pk(k, r, DZ)];
-          v = fmaf(Srk, sp[L::H + k * DY + j], v);
-        }
-        PHt[r][j] = v;
-      }
     double Sd[DY][DY];
-#pragma unroll
-    for (int i2 = 0; i2 < DY; ++i2)
-#pragma unroll
-      for (int j = 0; j <= i2; ++j) {
-        double v = (double)sp[L::R + j * DY + i2];
-#pragma unroll
-        for (int k = 0; k < DZ; ++k) v += (double)sp[L::H + k * DY + i2] * (double)PHt[k][j];
-        Sd[i2][j] = v;
-      }
-    // FP64 Cholesky (lower) in place
-    bool pd = true;
-#pragma unroll
-    for (int j = 0; j < DY; ++j) {
-      double d = Sd[j][j];
-#pragma unroll
-      for (int k = 0; k < j; ++k) d -= Sd[j][k] * Sd[j][k];
-      pd = pd && (d > 0.0);
-      d = sqrt(fmax(d, 1e-300));
-      Sd[j][j] = d;
-#pragma unroll
-      for (int i2 = j + 1; i2 < DY; ++i2) {
-        double v = Sd[i2][j];
-#pragma unroll
-        for (int k = 0; k < j; ++k) v -= Sd[i2][k] * Sd[j][k];
-        Sd[i2][j] = v / d;
-      }
-    }
-    if (!pd) fail = 1;
-    // z = y - H mp - c ; w = L^-1 z
-    double w[DY], ldet = 0.0, qf = 0.0;
-#pragma unroll
-    for (int i2 = 0; i2 < DY; ++i2) {
-      double v = sy[i2] - (double)sp[L::c + i2];
-#pragma unroll
-      for (int k = 0; k < DZ; ++k) v -= (double)sp[L::H + k * DY + i2] * (double)mp[k];
-#pragma unroll
-      for (int k = 0; k < i2; ++k) v -= Sd[i2][k] * w[k];
-      w[i2] = v / Sd[i2][i2];
-      qf += w[i2] * w[i2];
-      ldet += log(Sd[i2][i2]);
-    }
+    if (!rb_innovation<DXO, DZ, DY>(sp, Sp, PHt, Sd)) fail = 1;
+    double w[DY], ldet, qf;
+    rb_whiten<DXO, DZ, DY>(sp, sy, mp, Sd, w, qf, ldet);
     // K = PHt S^-1: rows solve L L' k' = PHt_r'
     float K[DZ][DY];
 #pragma unroll
@@ -312,6 +343,76 @@ __global__ void __launch_bounds__(RB_THREADS) rbpf_propagate(const PfJob* __rest
   block_finish(J, tile, t, fresh, acc, red, part, RB_SPLIT);
 }
 
+// Auxiliary RBPF, first stage of step t (rbpf.jl:86-124 through compute_logeta,
+// particles.jl:283-296): each particle's representative outer state x* is the
+// mean (MeanPredictive, ModePredictive) of its outer transition, A_o x + b_o, or
+// one draw A_o x + b_o + chol(Q_o) e' from it (DrawPredictive; e' from the
+// Philox stream tagged kTagLookahead, counters (i, t, 0)); its inner Gaussian is
+// predicted with (prev_outer x, new_outer x*) and log eta_i is that prediction's
+// update log-likelihood of y_t (predictive_loglik, rbpf.jl:113-124).  The last
+// block takes the resampling decision on softmax(logw + log eta) (apf_finish).
+template <int DXO, int DZ, int DY>
+__global__ void __launch_bounds__(RB_THREADS) rbpf_lookahead(const PfJob* __restrict__ jobs, int njobs,
+                                                            float q_gamma, int q_index) {
+  using L = RbLayout<DXO, DZ, DY>;
+  constexpr int NS = L::NS;
+  static_assert(DXO <= 4, "one Philox block draws the outer state");
+  __shared__ float sp[L::total];
+  __shared__ double sy[DY];
+  __shared__ double red[32];
+  const int jb = find_job(jobs, njobs, blockIdx.x / RB_SPLIT, false);
+  const PfJob& J = jobs[jb];
+  PfScalars* sc = J.sc;
+  const int t = sc->t + 1;
+  if (t > J.T || sc->status != 0) return;
+  const int tile = blockIdx.x / RB_SPLIT - J.tile0;
+  const int part = blockIdx.x % RB_SPLIT;
+  const float* P = reinterpret_cast<const float*>(J.params);
+  for (int k = threadIdx.x; k < L::total; k += RB_THREADS) sp[k] = P[k];
+  if (threadIdx.x < DY) sy[threadIdx.x] = J.ys[(size_t)(t - 1) * DY + threadIdx.x];
+  __syncthreads();
+  const int64_t N = J.N;
+  const float* Xs = reinterpret_cast<const float*>(J.X[(t - 1) & 1]);
+  const float* lw = reinterpret_cast<const float*>(J.lw);
+  float* eta = reinterpret_cast<float*>(J.eta);
+  LseAcc acc;
+  int fail = 0;
+  const int64_t i = (int64_t)tile * PF_TILE + part * RB_THREADS + threadIdx.x;
+  if (i < N) {
+    float x[DXO], mu[DZ], S[NS];
+#pragma unroll
+    for (int d = 0; d < DXO; ++d) x[d] = Xs[(size_t)d * N + i];
+#pragma unroll
+    for (int d = 0; d < DZ; ++d) mu[d] = Xs[(size_t)(DXO + d) * N + i];
+#pragma unroll
+    for (int d = 0; d < NS; ++d) S[d] = Xs[(size_t)(DXO + DZ + d) * N + i];
+    float e[4] = {0.f, 0.f, 0.f, 0.f};
+    if (J.lookahead_draw) philox_normals4<float>(J.seed, (uint32_t)i, (uint32_t)t, 0u, e, kTagLookahead);
+    float xs[DXO];
+#pragma unroll
+    for (int r = 0; r < DXO; ++r) {
+      float v = sp[L::bo + r];
+#pragma unroll
+      for (int c = 0; c < DXO; ++c) v = fmaf(sp[L::Ao + c * DXO + r], x[c], v);
+#pragma unroll
+      for (int c = 0; c <= r; ++c) v = fmaf(sp[L::Lo + c * DXO + r], e[c], v);
+      xs[r] = v;
+    }
+    float mp[DZ], Sp[NS];
+    rb_inner_predict<DXO, DZ, DY>(sp, x, xs, q_gamma, q_index, mu, S, mp, Sp);
+    float PHt[DZ][DY];
+    double Sd[DY][DY];
+    if (!rb_innovation<DXO, DZ, DY>(sp, Sp, PHt, Sd)) fail = 1;
+    double w[DY], ldet, qf;
+    rb_whiten<DXO, DZ, DY>(sp, sy, mp, Sd, w, qf, ldet);
+    const float le = (float)(-0.5 * (qf + 2.0 * ldet + DY * GF_LOG2PI));
+    eta[i] = le;
+    acc.add((double)lw[i] + (double)le);
+  }
+  if (fail) sc->status = GF_ERR_NOT_PD;
+  apf_finish(J, tile, t, acc, red, part, RB_SPLIT);
+}
+
 template <int DXO, int DZ, int DY>
 __global__ void __launch_bounds__(PF_THREADS) rbpf_init(const PfJob* __restrict__ jobs, int njobs) {
   using L = RbLayout<DXO, DZ, DY>;
@@ -354,7 +455,7 @@ __global__ void __launch_bounds__(PF_THREADS) rbpf_init(const PfJob* __restrict_
 
 template <int A, int B, int C>
 static RbKernels make_rb() {
-  return {A, B, C, rbpf_propagate<A, B, C>, rbpf_init<A, B, C>};
+  return {A, B, C, rbpf_propagate<A, B, C>, rbpf_init<A, B, C>, rbpf_lookahead<A, B, C>};
 }
 
 bool pick_rb(int dxo, int dz, int dy, RbKernels* out) {
@@ -423,8 +524,8 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   if (!ctx || !m || !cfg || !out || !ys || !out->ll)
     return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
   if (cfg->precision != GF_PREC_F32) return set_err(ctx, GF_ERR_UNSUPPORTED, "RBPF runs in FP32 only");
-  if (cfg->lookahead != GF_LOOKAHEAD_NONE)
-    return set_err(ctx, GF_ERR_UNSUPPORTED, "the auxiliary filter is built for the linear-Gaussian PF");
+  if (cfg->lookahead < GF_LOOKAHEAD_NONE || cfg->lookahead > GF_LOOKAHEAD_DRAW)
+    return set_err(ctx, GF_ERR_ARG, "unknown lookahead");
   if (cfg->proposal == GF_PROP_OPTIMAL)
     return set_err(ctx, GF_ERR_UNSUPPORTED, "RBPF supports bootstrap and overdispersed outer proposals");
   if (cfg->n_particles < 1 || T < 1) return set_err(ctx, GF_ERR_ARG, "bad N or T");
@@ -474,6 +575,8 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   if ((st = get(8, &res1))) return st;
   if ((st = get(sizeof(PfJob), &jobv))) return st;
   if (cfg->schedule && (st = get((size_t)T, &schedv))) return st;
+  void* etav = nullptr;  // auxiliary filter: first-stage log eta [N]
+  if (cfg->lookahead != GF_LOOKAHEAD_NONE && (st = get(sizeof(float) * (size_t)N, &etav))) return st;
   cudaStream_t s = ctx->stream;
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(d_params, P.data(), sizeof(float) * P.size(), cudaMemcpyHostToDevice, s));
   if (schedv) GF_CHECK_CUDA(ctx, cudaMemcpyAsync(schedv, cfg->schedule, (size_t)T, cudaMemcpyHostToDevice, s));
@@ -577,6 +680,8 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   J.means_out = d_means;
   J.hist = d.history;
   J.lwh = d.log_weight_history;
+  J.eta = etav;
+  J.lookahead_draw = cfg->lookahead == GF_LOOKAHEAD_DRAW ? 1 : 0;
   PfJob* jd = (PfJob*)jobv;
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(jd, &J, sizeof J, cudaMemcpyHostToDevice, s));
   launch_init_scalars(ctx, jd, 1, (const double*)ess1, (const int8_t*)res1);
@@ -604,6 +709,14 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
     tree_launch_init(ctx, false, jd, N, th.tree);
   }
   if (record) launch_record(ctx, false, jd, N);
+  // auxiliary filter: first-stage scores and the resampling decision of the
+  // coming step, before its resample
+  auto lookahead = [&]() {
+    if (!etav) return;
+    ProfScope ps(ctx, KC_SCAN);
+    K.lookahead<<<ntiles * RB_SPLIT, RB_THREADS, 0, s>>>(jd, 1, (float)m->q_gamma, m->q_index);
+  };
+  lookahead();
   launch_resample(ctx, false, jd, 1, ntiles);
   const int guided = cfg->proposal == GF_PROP_OVERDISPERSED;
   for (int t = 1; t <= T; ++t) {
@@ -621,7 +734,10 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
     if (paths) tree_launch_insert(ctx, false, jd, N, th.tree, t);
     if (want_means) launch_means(ctx, false, jd, 1, ntiles, (double*)mpart, dxo + dz);
     if (record) launch_record(ctx, false, jd, N);
-    if (t < T) launch_resample(ctx, false, jd, 1, ntiles);
+    if (t < T) {
+      lookahead();
+      launch_resample(ctx, false, jd, 1, ntiles);
+    }
   }
   launch_finish(ctx, false, jd, N);
   if (paths) tree_launch_paths(ctx, false, jd, N, th.tree, T, d.paths);

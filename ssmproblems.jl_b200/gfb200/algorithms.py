@@ -164,8 +164,9 @@ class ModePredictive(PredictiveStatistic):
 
 
 class DrawPredictive(PredictiveStatistic):
-    """A draw from the transition, A x + b + chol(Q) e' (bootstrap proposal; e' from its
-    own in-kernel Philox stream)."""
+    """A draw from the transition, A x + b + chol(Q) e' (the linear-Gaussian PF with the
+    bootstrap proposal, or the outer transition of an RBPF; e' from its own in-kernel
+    Philox stream)."""
     lookahead = 2
 
 
@@ -178,9 +179,12 @@ class AuxiliaryParticleFilter(AbstractFilter):
     """AuxiliaryParticleFilter(pf, pp) (particles.jl:270-357): first-stage weights
     log p(y_t | x*) with x* the predictive statistic `pp` of each particle's
     transition, resampling on softmax(logw + log eta) (AuxiliaryResampler,
-    resamplers.jl:85-143), second-stage weights corrected by -log eta[a]."""
+    resamplers.jl:85-143), second-stage weights corrected by -log eta[a].  ``pf`` is a
+    ParticleFilter on a linear-Gaussian model, or an RBPF on a HierarchicalSSM, whose
+    x* is the outer predictive statistic and log eta the inner Kalman update's
+    log-likelihood after predicting to x* (rbpf.jl:86-124)."""
 
-    def __init__(self, pf: "ParticleFilter", pp):
+    def __init__(self, pf, pp):
         if isinstance(pp, RepresentativeStateLookAhead):
             pp = pp.pp
         if not isinstance(pp, PredictiveStatistic):

@@ -166,6 +166,22 @@ def filter(model, algo, observations, *, seed: int = 0, noise=None, uniforms=Non
     """
     ctx = _resolve_ctx(ctx)
     ys = L.f64(observations)
+    if isinstance(algo, AuxiliaryParticleFilter) and isinstance(algo.pf, RBPF):
+        # AuxiliaryParticleFilter(RBPF(pf, KalmanFilter()), pp) (rbpf.jl:86-124)
+        la = algo.weight_strategy.pp.lookahead
+        if callback is not None:
+            if not isinstance(callback, (AncestorCallback, DenseAncestorCallback)):
+                raise TypeError(f"unsupported callback {type(callback).__name__}")
+            dense = isinstance(callback, DenseAncestorCallback)
+            st, ll = _rbpf(model, algo.pf, ys, seed, noise, uniforms, ctx, True, want_means, schedule,
+                           want_paths=not dense, want_history=dense, lookahead=la)
+            if dense:
+                callback.container = DenseParticleContainer(st._history, st._lw_history, st.ancestors, ctx)
+            else:
+                callback.tree = ParticleTree(st.paths)
+            return st, ll
+        return _rbpf(model, algo.pf, ys, seed, noise, uniforms, ctx, want_ancestors, want_means,
+                     schedule, lookahead=la)
     if callback is not None and isinstance(algo, RBPF):
         if not isinstance(callback, (AncestorCallback, DenseAncestorCallback)):
             raise TypeError(f"unsupported callback {type(callback).__name__}")
@@ -253,7 +269,7 @@ def _pf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sched
 
 
 def _rbpf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, schedule,
-          want_paths=False, want_history=False):
+          want_paths=False, want_history=False, lookahead=0):
     """RBPF run; paths and history hold the packed device state per particle
     [x (dxo) | mu (dz) | Sigma upper triangle by rows (dz (dz + 1) / 2)]."""
     if not isinstance(model, HierarchicalSSM):
@@ -262,7 +278,7 @@ def _rbpf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sch
     ys = ys.reshape(-1, model.dy)
     T = ys.shape[0]
     pf = algo.pf
-    cfg, sched, prec = _pf_config(pf, T, seed, schedule)
+    cfg, sched, prec = _pf_config(pf, T, seed, schedule, lookahead)
     N, dxo, dz = pf.N, model.dxo, model.dz
     width = dxo + dz + dz * dz
     out = dict(ll=np.zeros(1), ll_steps=np.zeros(T), ess_steps=np.zeros(T),

@@ -372,6 +372,31 @@ function GeneralisedFilters.filter(
     q_scale::Tuple{Real,Integer}=(0.0, 1),
     kwargs...,
 )
+    return _rbpf(rng, model, algo, observations, Int32(0); callback, q_scale)
+end
+
+# AuxiliaryParticleFilter(RBPF(BF(N; ...), KalmanFilter()), pp) (rbpf.jl:86-124):
+# x* is the mean / mode (MeanPredictive, ModePredictive) or a draw (DrawPredictive,
+# from the library's lookahead Philox stream) of each particle's outer transition,
+# and log eta the inner Kalman update's log-likelihood of y_t after predicting to x*.
+function GeneralisedFilters.filter(
+    rng::AbstractRNG,
+    model::HierarchicalSSM,
+    algo::AuxiliaryParticleFilter{<:RBPF{<:ParticleFilter{<:ESSResampler,LatentProposal},<:KalmanFilter}},
+    observations::AbstractVector;
+    callback=nothing,
+    q_scale::Tuple{Real,Integer}=(0.0, 1),
+    kwargs...,
+)
+    pp = algo.weight_strategy.pp
+    pp isa Union{MeanPredictive,ModePredictive,DrawPredictive} ||
+        throw(ArgumentError("GFB200 builds the mean / mode / draw lookahead only"))
+    return _rbpf(rng, model, algo.pf, observations, pp isa DrawPredictive ? Int32(2) : Int32(1);
+                 callback, q_scale)
+end
+
+function _rbpf(rng, model, algo, observations, lookahead::Int32; callback=nothing,
+               q_scale::Tuple{Real,Integer}=(0.0, 1))
     isnothing(callback) || throw(ArgumentError("GFB200 supports callback=nothing only"))
     pf = algo.pf
     N, T = pf.N, length(observations)
@@ -391,7 +416,7 @@ function GeneralisedFilters.filter(
     dxo, dz, dy = size(arrs[3], 1), size(arrs[8], 1), size(arrs[12], 1)
     ys = reduce(vcat, [Float64.(collect(y)) for y in observations])
     cfg = Ref(GfPfConfig(N, resampler_code(pf.resampler.resampler), 0, pf.resampler.threshold,
-                         GF_PREC_F32, GF_PROP_BOOTSTRAP, 1.0, rand(rng, UInt64), C_NULL, Int32(0)))
+                         GF_PREC_F32, GF_PROP_BOOTSTRAP, 1.0, rand(rng, UInt64), C_NULL, lookahead))
     width = dxo + dz + dz * (dz + 1) ÷ 2    # packed device state: x, mu, Sigma upper by rows
     ll = zeros(Float64, 1)
     states = zeros(Float32, N, width)

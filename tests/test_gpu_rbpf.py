@@ -100,3 +100,66 @@ def test_rbpf_ancestry_callbacks(ctx, kind):
     last = dcb.container.states[-1]  # [N, width]: x (1), mu (2), Sigma packed (3)
     np.testing.assert_array_equal(last[:, :1], np.asarray(st2.particles["x"]).reshape(N, 1))
     np.testing.assert_array_equal(last[:, 1:3], np.asarray(st2.particles["mu"]).reshape(N, 2))
+
+
+@pytest.mark.parametrize("pp", ["mean", "draw"])
+@pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.MULTINOMIAL])
+def test_auxiliary_rbpf_matches_oracle(ctx, pp, kind):
+    """AuxiliaryParticleFilter(RBPF(BF(N), KalmanFilter()), pp) (rbpf.jl:86-124) on the
+    stochastic-volatility model, whose inner Q scales with exp(x*[1]), so the mean and
+    the draw of the outer transition give different first-stage scores.  Resamples are
+    forced at steps 1 and 4 (the second on non-uniform weights); the FP32 bank against
+    the FP64 oracle on the same injected noise, uniforms and lookahead seed: ESS of
+    softmax(logw + log eta) within 1e-4, ancestors exact outside a 1e-6 band around
+    the cumulative-weight boundaries (band cases counted), per-step ll within 1e-4."""
+    from helpers import ancestors_match
+    model, ys = W.rb_trend(seed=9, T=8, dz=4, dy=2)
+    T, N = 8, 2048
+    rng = np.random.default_rng(31 + kind)
+    noise = rng.standard_normal((T + 1, 2, N)).astype(np.float32)
+    unif = rng.random(T) if kind == O.SYSTEMATIC else rng.random((T, N))
+    sched = [1, 0, 0, 1, 0, 0, 0, 0]
+    rs = {O.SYSTEMATIC: G.Systematic(), O.MULTINOMIAL: G.Multinomial()}[kind]
+    p = G.MeanPredictive() if pp == "mean" else G.DrawPredictive()
+    algo = G.APF(G.RBPF(G.BF(N, resampler=rs), G.KalmanFilter()), p)
+    st, ll = G.filter(model, algo, ys, noise=noise, uniforms=unif, schedule=sched, seed=17,
+                      want_ancestors=True, want_means=True, ctx=ctx)
+    la = 1 if pp == "mean" else 2
+    om = to_oracle_rb(model)
+    ref = O.rbpf_run(om, N, ys, resampler=kind, schedule=sched, noise=noise.astype(np.float64),
+                     uniforms=unif, seed=17, want_ancestors=True, want_margins=True, lookahead=la)
+    plain = O.rbpf_run(om, N, ys, resampler=kind, schedule=sched, noise=noise.astype(np.float64),
+                       uniforms=unif, seed=17, lookahead=0)
+    assert abs(ref["ll"] - plain["ll"]) > 1e-6, "the first stage must change the estimate"
+    np.testing.assert_array_equal(st.resampled, ref["resampled"])
+    np.testing.assert_allclose(st.ess_steps, ref["ess"], rtol=1e-4)
+    bad, boundary = ancestors_match(st.ancestors, ref["ancestors"], ref["margins"], 1e-6)
+    print(f"auxiliary RBPF ({pp}, resampler {kind}): ancestor boundary cases {boundary}")
+    assert bad == 0
+    np.testing.assert_allclose(st.ll_steps, ref["ll_steps"], rtol=1e-4, atol=1e-4)
+    np.testing.assert_allclose(st.means, ref["means"], rtol=1e-3, atol=1e-4)
+
+
+def test_auxiliary_rbpf_converges_to_kf(ctx):
+    """The auxiliary RBPF's log-evidence at N = 2^22, resampling at every step, within
+    the reference's 1e-3 of the joint Kalman filter (test/algorithms/rbpf.jl:5-34)."""
+    rng = np.random.default_rng(1234)
+    full, hier = dummy_rb_model(rng, 1, 1, 1)
+    _, ys = simulate(rng, full, 4)
+    algo = G.APF(G.RBPF(G.BF(2**22, threshold=1.0), G.KalmanFilter()), G.MeanPredictive())
+    st, ll = G.filter(hier, algo, ys, seed=31, ctx=ctx)
+    llkf = O.kf_filter(to_oracle(full), ys)[0]
+    assert st.resampled.all()
+    assert abs(ll - llkf) <= 1e-3
+
+
+def test_auxiliary_rbpf_without_resampling_is_the_rbpf(ctx):
+    """threshold 0: the first-stage scores are computed but never used, so the run is
+    the plain RBPF's bit for bit."""
+    model, ys = W.rb_trend(seed=5, T=6, dz=4, dy=2)
+    bf = G.BF(4096, threshold=0.0)
+    s0, l0 = G.filter(model, G.RBPF(bf, G.KalmanFilter()), ys, seed=5, ctx=ctx)
+    s1, l1 = G.filter(model, G.APF(G.RBPF(bf, G.KalmanFilter()), G.DrawPredictive()), ys, seed=5,
+                      ctx=ctx)
+    assert l0 == l1
+    np.testing.assert_array_equal(s0.particles["x"], s1.particles["x"])

@@ -366,3 +366,43 @@ def test_rbpf_step_chain_equals_rbpf_run(kind):
     np.testing.assert_allclose(x, xf[:, :om.dxo], rtol=1e-10, atol=1e-12)
     np.testing.assert_allclose(mu, xf[:, om.dxo:om.dxo + dz], rtol=1e-10, atol=1e-12)
     np.testing.assert_allclose(logw, ref["logw_final"], atol=1e-10)
+
+
+def _rb_helpers():
+    import sys
+    sys.path.insert(0, os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))),
+                                    "ssmproblems.jl_b200"))
+    from helpers import dummy_rb_model, to_oracle, to_oracle_rb
+    return dummy_rb_model, to_oracle, to_oracle_rb
+
+
+@pytest.mark.parametrize("lookahead", [1, 2])
+def test_rbpf_apf_oracle_without_resampling_is_the_rbpf(lookahead):
+    """AuxiliaryParticleFilter(RBPF(...), pp): the first-stage scores only act through
+    a resample, so with threshold 0 the run equals the plain RBPF's exactly."""
+    dummy_rb_model, _, to_oracle_rb = _rb_helpers()
+    rng = np.random.default_rng(13)
+    full, hier = dummy_rb_model(rng, 1, 2, 1)
+    ys = rng.standard_normal((5, 1))
+    om = to_oracle_rb(hier)
+    a = O.rbpf_run(om, 500, ys, threshold=0.0, seed=4, lookahead=lookahead)
+    b = O.rbpf_run(om, 500, ys, threshold=0.0, seed=4, lookahead=0)
+    assert a["ll"] == b["ll"]
+    assert not a["resampled"].any()
+
+
+@pytest.mark.parametrize("lookahead", [1, 2])
+def test_rbpf_apf_oracle_converges_to_kf(lookahead):
+    """test/algorithms/rbpf.jl:5-34 with the auxiliary first stage and a resample at
+    every step: the log-evidence estimate is unbiased for the joint Kalman filter's
+    (the dummy hierarchical model is jointly linear-Gaussian)."""
+    dummy_rb_model, to_oracle, to_oracle_rb = _rb_helpers()
+    rng = np.random.default_rng(1234)
+    full, hier = dummy_rb_model(rng, 1, 1, 1)
+    from helpers import simulate
+    _, ys = simulate(rng, full, 4)
+    kll = O.kf_filter(to_oracle(full), ys)[0]
+    r = O.rbpf_run(to_oracle_rb(hier), 100_000, ys, threshold=1.0, seed=2, lookahead=lookahead,
+                   threads=4)
+    assert r["resampled"].all()
+    assert abs(r["ll"] - kll) < 2e-3
