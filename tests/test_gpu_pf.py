@@ -44,6 +44,37 @@ def test_bf_f64_injected_matches_oracle(ctx, kind, conv):
     assert st.clamps == ref["clamps"] == 0
 
 
+@pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.STRATIFIED])
+@pytest.mark.parametrize("conv", ["cpu", "cudaext"])
+def test_degenerate_weights_ancestors_match_oracle(ctx, kind, conv):
+    """An observation far more precise than the prior piles the weight on a few
+    particles, so one tile of 1024 particles owns more than 8192 of the slots: the
+    merge-path fill still gives every block the same number of items, and the
+    ancestors stay bit-exact with the FP64 oracle on the same injected noise."""
+    from gfb200 import create_homogeneous_linear_gaussian_model
+    dx = 2
+    m = create_homogeneous_linear_gaussian_model(np.zeros(dx), 4.0 * np.eye(dx), 0.9 * np.eye(dx),
+                                                 np.zeros(dx), np.eye(dx), np.eye(dx), np.zeros(dx),
+                                                 1e-4 * np.eye(dx))
+    rng = np.random.default_rng(19)
+    T, N = 4, 32768
+    _, ys = simulate(rng, m, T)
+    noise, unif = injected(rng, T, dx, N, kind)
+    algo = G.BF(N, threshold=0.5, resampler=RS[kind], precision="f64", convention=conv)
+    st, ll = G.filter(m, algo, ys, noise=noise, uniforms=unif, want_ancestors=True, ctx=ctx)
+    ref = O.pf_run(to_oracle(m), N, ys, resampler=kind,
+                   conv=O.CONV_CUDAEXT if conv == "cudaext" else O.CONV_CPU, threshold=0.5,
+                   noise=noise, uniforms=unif, want_ancestors=True, want_margins=True)
+    np.testing.assert_array_equal(st.resampled, ref["resampled"])
+    res = np.flatnonzero(st.resampled)
+    # slots owned by the busiest tile of 1024 particles on a resampling step
+    busiest = max(np.bincount((st.ancestors[t] - 1) // 1024).max() for t in res)
+    assert busiest > 8192, "workload must pile the offspring on one tile"
+    bad, boundary = ancestors_match(st.ancestors, ref["ancestors"], ref["margins"], 1e-9)
+    assert bad == 0 and boundary == 0
+    np.testing.assert_allclose(st.ll_steps, ref["ll_steps"], atol=1e-7, rtol=1e-9)
+
+
 @pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.STRATIFIED, O.MULTINOMIAL])
 def test_bf_f64_in_kernel_philox_matches_oracle(ctx, kind):
     """In-kernel Philox noise and uniforms: the oracle regenerates the same stream."""
