@@ -62,8 +62,6 @@ void launch_prep(gf_ctx* ctx, bool dbl, const PfJob* job_dev, int T, int dx, int
 
 namespace gf {
 
-// Largest number of blocks per tile of any propagate kernel (sizes `part`).
-constexpr int PF_MAX_SPLIT = 8;
 // 128-particle units per 1024-particle tile (pf_lg_propagate_tc_units)
 constexpr int TC_SUB_UNITS = 8;
 

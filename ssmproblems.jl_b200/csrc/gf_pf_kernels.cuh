@@ -21,7 +21,8 @@ constexpr int PF_TILE = PF_THREADS * PF_PPT;   // particles per propagate block
 constexpr int SCAN_THREADS = 256;
 constexpr int SCAN_IPT = 16;
 constexpr int SCAN_TILE = SCAN_THREADS * SCAN_IPT;
-constexpr int PF_PW = 6;                       // doubles per block partial
+constexpr int PF_PW = 3;                       // doubles per block partial (M, S1, S2)
+constexpr int PF_MAX_SPLIT = 8;                // largest number of partials per tile (sizes `part`)
 constexpr int FILL_D = 2 * PF_TILE;            // merge items (particles + slots) per fill block
 constexpr int FILL_IPT = FILL_D / PF_THREADS;  // merge items per fill thread
 constexpr unsigned long long kReady = 1ull << 63;
@@ -50,7 +51,7 @@ struct PfJob {
   void* X[2];                // SoA state ping-pong [width][N]
   void* lw;                  // stored log-weights [N]
   double* key;               // cumulative normalised weights [N]
-  double* part;              // [ntiles][PF_PW]
+  double* part;              // [PF_PW][ntiles * PF_MAX_SPLIT] partial fields, one array each
   unsigned long long* flags; // [2][nstiles] lookback aggregate / inclusive prefix
   PfScalars* sc;
   const void* noise;         // nullable [(T+1)][nz][N]
@@ -273,8 +274,15 @@ struct LseAcc {
   }
 };
 
-// Folds the block's accumulators into part[tile * nparts + part]; true in the
-// job's last block to arrive (which then folds every partial).
+// The block partials are kept field by field (structure of arrays): M, S1
+// and S2 of partial b at part[f * part_stride(J) + b], so the last block's
+// reads of one field are contiguous across its threads.
+__host__ __device__ __forceinline__ size_t part_stride(const PfJob& J) {
+  return (size_t)J.ntiles * PF_MAX_SPLIT;
+}
+
+// Folds the block's accumulators into partial tile * nparts + part; true in
+// the job's last block to arrive (which then folds every partial).
 static __device__ bool fold_partials(const PfJob& J, int tile, LseAcc a, double* red, int part,
                                      int nparts) {
   PfScalars* sc = J.sc;
@@ -285,10 +293,11 @@ static __device__ bool fold_partials(const PfJob& J, int tile, LseAcc a, double*
   double S1 = block_sum(a.s1 * f, red);
   double S2 = block_sum(a.s2 * f * f, red);
   if (threadIdx.x == 0) {
-    double* p = J.part + ((size_t)tile * nparts + part) * PF_PW;
+    const size_t ps = part_stride(J);
+    double* p = J.part + (size_t)tile * nparts + part;
     p[0] = M;
-    p[1] = S1;
-    p[2] = S2;
+    p[ps] = S1;
+    p[2 * ps] = S2;
     __threadfence();
     unsigned prev = atomicAdd(&sc->counter, 1u);
     s_last = (prev == (unsigned)(nall - 1));
@@ -306,19 +315,23 @@ template <class S>
 static __device__ void global_stats(const S& g, const PfJob& J, int nparts, double* red,
                                     double* GM_out, double* GS1_out, double* GS2_out,
                                     double* ecache = nullptr) {
+  // job fields are read once: a store through ecache (or any pointer) may
+  // alias the job table, and every later J.x would be another L2 round trip
   const int nall = J.ntiles * nparts;
+  const size_t ps = part_stride(J);
+  const double* __restrict__ part = J.part;
   double m = -INFINITY;
-  for (int bb = g.tid(); bb < nall; bb += g.size()) m = fmax(m, __ldcg(J.part + (size_t)bb * PF_PW));
+  for (int bb = g.tid(); bb < nall; bb += g.size()) m = fmax(m, __ldcg(part + bb));
   double GM = sync_max(g, m, red);
   double s1 = 0.0, s2 = 0.0;
   for (int bb = g.tid(); bb < nall; bb += g.size()) {
-    const double* p = J.part + (size_t)bb * PF_PW;
+    const double* p = part + bb;
     double mb = __ldcg(p);
     double ff = 0.0;
     if (mb > -INFINITY) {
       ff = exp(mb - GM);
-      s1 += __ldcg(p + 1) * ff;
-      s2 += __ldcg(p + 2) * ff * ff;
+      s1 += __ldcg(p + ps) * ff;
+      s2 += __ldcg(p + 2 * ps) * ff * ff;
     }
     if (ecache) ecache[bb] = ff;
   }
@@ -337,18 +350,23 @@ template <class S>
 static __device__ void write_tile_prefixes(const S& g, const PfJob& J, int nparts, double lse,
                                            unsigned long long* wsum, const double* ecache = nullptr,
                                            double inv_gs1 = 0.0) {
-  PfScalars* sc = J.sc;
-  const int per = (J.ntiles + g.size() - 1) / g.size();
-  const int b0 = min(g.tid() * per, J.ntiles), b1 = min(b0 + per, J.ntiles);
+  // job fields in registers (the tprefix stores may alias the job table)
+  PfScalars* const sc = J.sc;
+  const int ntiles = J.ntiles;
+  const double* __restrict__ part = J.part;
+  const size_t ps = part_stride(J);
+  double* __restrict__ tprefix = J.tprefix;
+  const int per = (ntiles + g.size() - 1) / g.size();
+  const int b0 = min(g.tid() * per, ntiles), b1 = min(b0 + per, ntiles);
   unsigned long long tot = 0ull;
   auto tile_fix = [&](int bb) {  // fixed-point normalised weight of tile bb
     unsigned long long w = 0ull;
     for (int q = 0; q < nparts; ++q) {
-      const double* p = J.part + ((size_t)bb * nparts + q) * PF_PW;
+      const double* p = part + (size_t)bb * nparts + q;
       const double mb = __ldcg(p);
       if (mb > -INFINITY) {
         const double e = ecache ? ecache[(size_t)bb * nparts + q] * inv_gs1 : exp(mb - lse);
-        w += __double2ull_rn(__ldcg(p + 1) * e * kFix);
+        w += __double2ull_rn(__ldcg(p + ps) * e * kFix);
       }
     }
     return w;
@@ -357,11 +375,11 @@ static __device__ void write_tile_prefixes(const S& g, const PfJob& J, int npart
   unsigned long long all = 0ull;
   unsigned long long run = sync_excl_scan_u64(g, tot, wsum, &all);
   for (int bb = b0; bb < b1; ++bb) {
-    J.tprefix[bb] = (double)run * kInvFix;
+    tprefix[bb] = (double)run * kInvFix;
     run += tile_fix(bb);
   }
   if (g.tid() == 0) {
-    J.tprefix[J.ntiles] = (double)all * kInvFix;
+    tprefix[ntiles] = (double)all * kInvFix;
     sc->wn = (double)all * kInvFix;
   }
 }
@@ -379,25 +397,40 @@ template <class S>
 static __device__ void finish_step(const S& g, const PfJob& J, int t, bool fresh, int nparts,
                                    double* red, unsigned long long* wsum, int* s_res,
                                    double* ecache = nullptr) {
-  PfScalars* sc = J.sc;
+  PfScalars* const sc = J.sc;
+  const bool aux = J.eta != nullptr;
   // fold all partials in a fixed order (deterministic)
   double GM, GS1, GS2;
   global_stats(g, J, nparts, red, &GM, &GS1, &GS2, ecache);
   const double base = fresh ? J.log_n + sc->base_adj : 0.0;
   const double lse = GM + log(GS1);
   if (g.tid() == 0) {
+    // the job's fields are loaded together before the stores through sc and
+    // the output pointers (which may alias the job table) would force each
+    // one after the previous store: one L2 round trip instead of a chain
+    const int T = J.T;
+    const int64_t N = J.N;
+    const double threshold = J.threshold;
+    const int8_t* const schedule = J.schedule;
+    double* const ll_steps = J.ll_steps;
+    double* const ess_steps = J.ess_steps;
+    int8_t* const res_steps = J.res_steps;
+    const double* const unif = J.unif;
+    const uint64_t seed = J.seed;
+    const int sch = (t < T && schedule) ? (int)schedule[t] : -1;
+    const double u_next = (t < T && unif) ? unif[t] : 0.0;
+    const double ll_prev = sc->ll;
     double inc = lse - base;
     double ess = GS1 * GS1 / GS2;
     if (!(lse > -INFINITY) || isnan(lse)) sc->status = GF_ERR_ARG;  // all weights vanished
-    sc->ll += inc;
-    if (J.ll_steps) J.ll_steps[t - 1] = inc;
+    sc->ll = ll_prev + inc;
+    if (ll_steps) ll_steps[t - 1] = inc;
     int res = 0;
-    if (t < J.T) {
-      int s = J.schedule ? (int)J.schedule[t] : -1;
-      res = s >= 0 ? (s != 0) : (J.threshold * (double)J.N >= ess);
-      if (J.ess_steps) J.ess_steps[t] = ess;
-      if (J.res_steps) J.res_steps[t] = (int8_t)res;
-      sc->u0 = J.unif ? J.unif[t] : philox_uniform(J.seed, 0u, (uint32_t)(t + 1));
+    if (t < T) {
+      res = sch >= 0 ? (sch != 0) : (threshold * (double)N >= ess);
+      if (ess_steps) ess_steps[t] = ess;
+      if (res_steps) res_steps[t] = (int8_t)res;
+      sc->u0 = unif ? u_next : philox_uniform(seed, 0u, (uint32_t)(t + 1));
     }
     sc->lse = lse;
     sc->ess = ess;
@@ -407,7 +440,7 @@ static __device__ void finish_step(const S& g, const PfJob& J, int t, bool fresh
   }
   g.sync();
   // the auxiliary filter decides in its lookahead kernel instead
-  if (*s_res && !J.eta) write_tile_prefixes(g, J, nparts, lse, wsum, ecache, 1.0 / GS1);
+  if (*s_res && !aux) write_tile_prefixes(g, J, nparts, lse, wsum, ecache, 1.0 / GS1);
   g.sync();
   if (g.tid() == 0) {
     sc->uniform = 0;
@@ -674,7 +707,21 @@ __device__ __forceinline__ void fill_block(const PfJob& J, int m) {
   const int64_t j0 = d0 - k0, j1 = d1 - k1;
   const int nk = (int)(min(k1, N - 1) - k0 + 1);  // counts ocum[k0 .. min(k1, N-1)]
   const int32_t* __restrict__ oc = J.ocum;
-  for (int q = threadIdx.x; q < nk; q += PF_THREADS) s_oc[q] = COHERENT ? __ldcg(oc + k0 + q) : oc[k0 + q];
+  int32_t* __restrict__ anc = J.anc;
+  // all of a thread's counts are loaded before any is stored to shared memory:
+  // one L2 round trip instead of one per count (nk <= FILL_D + 1)
+  constexpr int kPer = (FILL_D + 1 + PF_THREADS - 1) / PF_THREADS;
+  int32_t cv[kPer];
+#pragma unroll
+  for (int r = 0; r < kPer; ++r) {
+    const int q = threadIdx.x + r * PF_THREADS;
+    cv[r] = q < nk ? (COHERENT ? __ldcg(oc + k0 + q) : oc[k0 + q]) : 0;
+  }
+#pragma unroll
+  for (int r = 0; r < kPer; ++r) {
+    const int q = threadIdx.x + r * PF_THREADS;
+    if (q < nk) s_oc[q] = cv[r];
+  }
   __syncthreads();
   const int64_t d = d0 + (int64_t)threadIdx.x * FILL_IPT;
   if (d < d1) {
@@ -697,7 +744,6 @@ __device__ __forceinline__ void fill_block(const PfJob& J, int m) {
     }
   }
   __syncthreads();
-  int32_t* __restrict__ anc = J.anc;
   for (int q = threadIdx.x; q < (int)(j1 - j0); q += PF_THREADS) anc[j0 + q] = s_anc[q];
 }
 

@@ -760,10 +760,11 @@ __global__ void __launch_bounds__(TC_THREADS, (TcLayout<DXP, DYP>::min_blocks)) 
     const double S1 = block_sum(acc.s1 * f, red);
     const double S2 = block_sum(acc.s2 * f * f, red);
     if (tid == 0) {
-      double* pp = J->part + ((size_t)tile * TC_SUB + sub) * PF_PW;
+      const size_t ps = part_stride(*J);
+      double* pp = J->part + (size_t)tile * TC_SUB + sub;
       pp[0] = M;
-      pp[1] = S1;
-      pp[2] = S2;
+      pp[ps] = S1;
+      pp[2 * ps] = S2;
     }
   }
   umma::fence_before_sync();
