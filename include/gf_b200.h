@@ -233,6 +233,16 @@ gf_status gf_kf_backward_information(gf_ctx* ctx, const gf_lg_model* models, int
                                      const double* ys, double initial_jitter, int32_t use_initial_jitter,
                                      double jitter, int32_t use_jitter, int32_t memspace,
                                      gf_kf_backward_out* out);
+/* The same for time-varying models (test/algorithms/kalman.jl:139-190 runs the
+ * backward predictor on a non-homogeneous model): param_steps[f] = 1 for a
+ * homogeneous model, else >= T[f] stacked step blocks as for gf_kf_batch_tv;
+ * backward_predict from x_{t+1} to x_t uses the dynamics of step t+1
+ * (calc_params(dyn, iter + 1), kalman.jl:294-320) and backward_update /
+ * backward_initialise the observation model of step t. */
+gf_status gf_kf_backward_information_tv(gf_ctx* ctx, const gf_lg_model* models, int32_t B, const int32_t* T,
+                                        const int32_t* param_steps, const double* ys, double initial_jitter,
+                                        int32_t use_initial_jitter, double jitter, int32_t use_jitter,
+                                        int32_t memspace, gf_kf_backward_out* out);
 
 /* smooth(model, KalmanSmoother(), ys) for B models (kalman.jl:206-234): the
  * forward Kalman filter (no jitter), then the Rauch-Tung-Striebel pass of

@@ -649,16 +649,18 @@ def backward_information(m: LGModel, ys, initial_jitter=None, jitter=None):
     backward_initialise / backward_update."""
     ys = _f64(ys).reshape(-1, m.dy)
     T = ys.shape[0]
-    A, b, Q, H, c, R = (np.asarray(v, np.float64) for v in (m.A, m.b, m.Q, m.H, m.c, m.R))
-    dx = A.shape[0]
-    Ri = np.linalg.inv(R)
-    F = np.linalg.cholesky(Q)
+    dx = m.dx
     lp, Op = np.zeros((T, dx)), np.zeros((T, dx, dx))
     lu, Ou = np.zeros((T, dx)), np.zeros((T, dx, dx))
+
+    def step(k):  # calc_params(dyn, k), calc_params(obs, k) (1-based), FP64
+        return tuple(np.asarray(v, np.float64) for v in m.params(k))
 
     def sym(M):  # PDMat(Symmetric(M)): the upper triangle mirrored
         return np.triu(M) + np.triu(M, 1).T
 
+    _, _, _, H, c, R = step(T)
+    Ri = np.linalg.inv(R)
     lam = H.T @ Ri @ (ys[T - 1] - c)
     Om = H.T @ Ri @ H
     if initial_jitter is not None:
@@ -666,6 +668,9 @@ def backward_information(m: LGModel, ys, initial_jitter=None, jitter=None):
     Om = sym(Om)
     lu[T - 1], Ou[T - 1] = lam, Om
     for t in range(T - 2, -1, -1):
+        # backward_predict at iter t+1 uses calc_params(dyn, iter + 1) (kalman.jl:294-320)
+        A, b, Q, _, _, _ = step(t + 2)
+        F = np.linalg.cholesky(Q)
         mvec = lam - Om @ b
         Lam = F.T @ Om @ F + np.eye(dx)
         FLF = F @ np.linalg.solve(Lam, F.T)
@@ -676,6 +681,8 @@ def backward_information(m: LGModel, ys, initial_jitter=None, jitter=None):
             Om_h = Om_h + jitter * np.eye(dx)
         Om_h = sym(Om_h)
         lp[t], Op[t] = lam_h, Om_h
+        _, _, _, H, c, R = step(t + 1)  # backward_update at iter t+1
+        Ri = np.linalg.inv(R)
         lam = lam_h + H.T @ Ri @ (ys[t] - c)
         Om = sym(Om_h + H.T @ Ri @ H)
         lu[t], Ou[t] = lam, Om

@@ -26,9 +26,10 @@ constexpr int BI_THREADS = 256;
 constexpr int BI_MATS = 30;  // shared LD x LD matrices, vectors included
 
 struct BiDesc {
-  int32_t dx, dy, T, pad;
+  int32_t dx, dy, T;
+  int32_t pstep;   // time-varying: doubles per step block (block k = calc_params(., k+1)); 0 = one block
   int64_t y_off;   // into ys: [T][dy]
-  int64_t p_off;   // into params: A | b | F | G = H'R^-1 | W = H'R^-1 H | Q | H | c | R | mu0 | Sigma0
+  int64_t p_off;   // into params: blocks A | b | F | G = H'R^-1 | W = H'R^-1 H | Q | H | c | R, then mu0 | Sigma0
   int64_t ck_off;  // forward scratch: T * (dx + dx*dx)
   int64_t v_off;   // outputs: sum of T*dx
   int64_t m_off;   // sum of T*dx*dx
@@ -74,34 +75,40 @@ __global__ void __launch_bounds__(BI_THREADS) kf_backinfo_kernel(BiArgs a) {
   double *ym = V + 11 * LD;
 
   const double* P = a.params + D.p_off;
-  const double* Pb = P + dx * dx;
-  const double* PF = Pb + dx;
-  const double* PG = PF + dx * dx;
-  const double* PW = PG + dx * dy;
-  const double* PQ = PW + dx * dx;
-  const double* PH = PQ + dx * dx;
-  const double* Pc = PH + dy * dx;
-  const double* PR = Pc + dy;
-  const double* Pmu0 = PR + dy * dy;
+  // one step block: A | b | F | G | W | Q | H | c | R (time-varying models: T of
+  // them, block k holding calc_params(dyn, k+1) and calc_params(obs, k+1))
+  const int blen = 4 * dx * dx + dx + 2 * dx * dy + dy + dy * dy;
+  const double* Pmu0 = P + (D.pstep ? (int64_t)T * D.pstep : (int64_t)blen);
   const double* PS0 = Pmu0 + dx;
+  auto load_dyn = [&](int k) {  // A, b, F = chol(Q), Q of block k
+    const double* B = P + (int64_t)k * D.pstep;
+    for (int e = tid; e < dx * dx; e += bd) {
+      const int o = e % dx + (e / dx) * LD;
+      A[o] = B[e];
+      F[o] = B[dx * dx + dx + e];
+      Q[o] = B[3 * dx * dx + dx + dx * dy + e];
+    }
+    for (int i = tid; i < dx; i += bd) b[i] = B[dx * dx + i];
+  };
+  auto load_obs = [&](int k) {  // G = H'R^-1, W = H'R^-1 H, H, c, R of block k
+    const double* B = P + (int64_t)k * D.pstep;
+    const double* PG = B + 2 * dx * dx + dx;
+    const double* PW = PG + dx * dy;
+    const double* PH = PW + 2 * dx * dx;
+    const double* Pc = PH + dy * dx;
+    const double* PR = Pc + dy;
+    for (int e = tid; e < dx * dx; e += bd) W[e % dx + (e / dx) * LD] = PW[e];
+    for (int e = tid; e < dx * dy; e += bd) G[e % dx + (e / dx) * LD] = PG[e];
+    for (int e = tid; e < dy * dx; e += bd) H[e % dy + (e / dy) * LD] = PH[e];
+    for (int e = tid; e < dy * dy; e += bd) R[e % dy + (e / dy) * LD] = PR[e];
+    for (int i = tid; i < dy; i += bd) c[i] = Pc[i];
+  };
   for (int e = tid; e < MS * (BI_MATS - 2); e += bd) sm[e] = 0.0;
   __syncthreads();
-  for (int e = tid; e < dx * dx; e += bd) {
-    const int i = e % dx, j = e / dx, o = i + j * LD;
-    A[o] = P[e];
-    F[o] = PF[e];
-    W[o] = PW[e];
-    Q[o] = PQ[e];
-    Sig[o] = PS0[e];
-  }
-  for (int e = tid; e < dx * dy; e += bd) G[e % dx + (e / dx) * LD] = PG[e];
-  for (int e = tid; e < dy * dx; e += bd) H[e % dy + (e / dy) * LD] = PH[e];
-  for (int e = tid; e < dy * dy; e += bd) R[e % dy + (e / dy) * LD] = PR[e];
-  for (int i = tid; i < dx; i += bd) {
-    b[i] = Pb[i];
-    mu[i] = Pmu0[i];
-  }
-  for (int i = tid; i < dy; i += bd) c[i] = Pc[i];
+  load_dyn(0);
+  load_obs(0);
+  for (int e = tid; e < dx * dx; e += bd) Sig[e % dx + (e / dx) * LD] = PS0[e];
+  for (int i = tid; i < dx; i += bd) mu[i] = Pmu0[i];
   __syncthreads();
   const double* Y = a.ys + D.y_off;
   double* CK = a.ck + D.ck_off;
@@ -112,6 +119,11 @@ __global__ void __launch_bounds__(BI_THREADS) kf_backinfo_kernel(BiArgs a) {
   // ---- forward filter (kalman.jl:42-79, Joseph form) when smoothing: filtered moments to CK
   for (int t = 0; smooth && t < T; ++t) {
     const double* y = Y + (size_t)t * dy;
+    if (D.pstep && t > 0) {  // step t's model
+      load_dyn(t);
+      load_obs(t);
+      __syncthreads();
+    }
     mv(mp, A, false, mu, dx, dx);
     for (int i = tid; i < dx; i += bd) mp[i] += b[i];
     mm(T1, A, false, Sig, false, dx, dx, dx, 1.0, 0.0);
@@ -162,8 +174,12 @@ __global__ void __launch_bounds__(BI_THREADS) kf_backinfo_kernel(BiArgs a) {
     __syncthreads();
   };
 
-  // ---- backward_initialise at T
+  // ---- backward_initialise at T (calc_params(obs, T))
   if (!status) {
+    if (D.pstep) {
+      load_obs(T - 1);
+      __syncthreads();
+    }
     for (int i = tid; i < dx; i += bd) lam[i] = 0.0;
     for (int e = tid; e < dx * dx; e += bd) {
       const int i = e % dx, j = e / dx;
@@ -193,7 +209,13 @@ __global__ void __launch_bounds__(BI_THREADS) kf_backinfo_kernel(BiArgs a) {
   }
 
   for (int t = T - 2; t >= 0 && !status; --t) {
-    // ---- backward_predict: p(y_{t+2:T} | x_{t+1}) -> p(y_{t+2:T} | x_t) (0-based t)
+    // ---- backward_predict: p(y_{t+2:T} | x_{t+1}) -> p(y_{t+2:T} | x_t) (0-based t),
+    //      the transition x_t -> x_{t+1} of block t + 1 (calc_params(dyn, iter + 1))
+    if (D.pstep) {
+      __syncthreads();
+      load_dyn(t + 1);
+      __syncthreads();
+    }
     mv(u, Om, false, b, dx, dx);
     for (int i = tid; i < dx; i += bd) mv_[i] = lam[i] - u[i];
     mm(T1, Om, false, F, false, dx, dx, dx, 1.0, 0.0);
@@ -252,7 +274,12 @@ __global__ void __launch_bounds__(BI_THREADS) kf_backinfo_kernel(BiArgs a) {
           a.Sig_s[D.m_off + (int64_t)t * dx * dx + e] = Ss[e % dx + (e / dx) * LD];
       __syncthreads();
     }
-    // ---- backward_update with y_t
+    // ---- backward_update with y_t (calc_params(obs, t + 1), block t)
+    if (D.pstep) {
+      __syncthreads();
+      load_obs(t);
+      __syncthreads();
+    }
     for (int i = tid; i < dx; i += bd) lam[i] = lamh[i];
     for (int e = tid; e < dx * dx; e += bd) {
       const int o = e % dx + (e / dx) * LD;
@@ -271,10 +298,10 @@ __global__ void __launch_bounds__(BI_THREADS) kf_backinfo_kernel(BiArgs a) {
 }  // namespace
 }  // namespace gf
 
-extern "C" gf_status gf_kf_backward_information(gf_ctx* ctx, const gf_lg_model* models, int32_t B,
-                                                const int32_t* T, const double* ys, double initial_jitter,
-                                                int32_t use_initial_jitter, double jitter, int32_t use_jitter,
-                                                int32_t memspace, gf_kf_backward_out* out) {
+static gf_status backward_impl(gf_ctx* ctx, const gf_lg_model* models, int32_t B, const int32_t* T,
+                               const int32_t* param_steps, const double* ys, double initial_jitter,
+                               int32_t use_initial_jitter, double jitter, int32_t use_jitter, int32_t memspace,
+                               gf_kf_backward_out* out) {
   using namespace gf;
   if (!ctx) return GF_ERR_ARG;
   if (!models || !T || !ys || !out || B < 1) return set_err(ctx, GF_ERR_ARG, "null argument or B < 1");
@@ -290,47 +317,57 @@ extern "C" gf_status gf_kf_backward_information(gf_ctx* ctx, const gf_lg_model* 
     if (dx < 1 || dy < 1 || dx > SM_MAXD || dy > SM_MAXD)
       return set_err(ctx, GF_ERR_DIM, "model %d: the backward filter needs 1 <= dx, dy <= %d", f, SM_MAXD);
     if (T[f] < 1) return set_err(ctx, GF_ERR_ARG, "model %d: T must be >= 1", f);
-    std::vector<double> LQ(dx * dx), LR(dy * dy), LRi(dy * dy), Ri(dy * dy), G(dx * dy), W(dx * dx);
-    if (chol_lower(dx, m.Q, LQ.data())) return set_err(ctx, GF_ERR_NOT_PD, "model %d: Q is not positive definite", f);
-    if (chol_lower(dy, m.R, LR.data())) return set_err(ctx, GF_ERR_NOT_PD, "model %d: R is not positive definite", f);
-    tri_inv_lower(dy, LR.data(), LRi.data());
-    for (int i = 0; i < dy; ++i)  // R^-1 = L^-T L^-1
-      for (int j = 0; j < dy; ++j) {
-        double acc = 0.0;
-        for (int p = 0; p < dy; ++p) acc += LRi[p + i * dy] * LRi[p + j * dy];
-        Ri[i + j * dy] = acc;
-      }
-    for (int i = 0; i < dx; ++i)  // G = H' R^-1
-      for (int j = 0; j < dy; ++j) {
-        double acc = 0.0;
-        for (int p = 0; p < dy; ++p) acc += m.H[p + i * dy] * Ri[p + j * dy];
-        G[i + j * dx] = acc;
-      }
-    for (int i = 0; i < dx; ++i)  // W = G H
-      for (int j = 0; j < dx; ++j) {
-        double acc = 0.0;
-        for (int p = 0; p < dy; ++p) acc += G[i + p * dx] * m.H[p + j * dy];
-        W[i + j * dx] = acc;
-      }
+    const int ps = param_steps ? param_steps[f] : 1;
+    if (ps != 1 && ps < T[f])
+      return set_err(ctx, GF_ERR_ARG, "model %d: %d parameter steps for T = %d", f, ps, T[f]);
+    const int nblk = ps == 1 ? 1 : T[f];
     BiDesc& d = desc[f];
     d.dx = dx;
     d.dy = dy;
     d.T = T[f];
-    d.pad = 0;
+    d.pstep = ps == 1 ? 0 : 4 * dx * dx + dx + 2 * dx * dy + dy + dy * dy;
     d.y_off = ny;
     d.p_off = (int64_t)params.size();
     d.ck_off = nck;
     d.v_off = nv;
     d.m_off = nm;
-    params.insert(params.end(), m.A, m.A + dx * dx);
-    params.insert(params.end(), m.b, m.b + dx);
-    params.insert(params.end(), LQ.begin(), LQ.end());
-    params.insert(params.end(), G.begin(), G.end());
-    params.insert(params.end(), W.begin(), W.end());
-    params.insert(params.end(), m.Q, m.Q + dx * dx);
-    params.insert(params.end(), m.H, m.H + dy * dx);
-    params.insert(params.end(), m.c, m.c + dy);
-    params.insert(params.end(), m.R, m.R + dy * dy);
+    for (int k = 0; k < nblk; ++k) {  // step block k: calc_params(dyn, k+1), calc_params(obs, k+1)
+      const double *mA = m.A + (size_t)k * dx * dx, *mb = m.b + (size_t)k * dx, *mQ = m.Q + (size_t)k * dx * dx;
+      const double *mH = m.H + (size_t)k * dy * dx, *mc = m.c + (size_t)k * dy, *mR = m.R + (size_t)k * dy * dy;
+      std::vector<double> LQ(dx * dx), LR(dy * dy), LRi(dy * dy), Ri(dy * dy), G(dx * dy), W(dx * dx);
+      if (chol_lower(dx, mQ, LQ.data()))
+        return set_err(ctx, GF_ERR_NOT_PD, "model %d: Q of step %d is not positive definite", f, k + 1);
+      if (chol_lower(dy, mR, LR.data()))
+        return set_err(ctx, GF_ERR_NOT_PD, "model %d: R of step %d is not positive definite", f, k + 1);
+      tri_inv_lower(dy, LR.data(), LRi.data());
+      for (int i = 0; i < dy; ++i)  // R^-1 = L^-T L^-1
+        for (int j = 0; j < dy; ++j) {
+          double acc = 0.0;
+          for (int p = 0; p < dy; ++p) acc += LRi[p + i * dy] * LRi[p + j * dy];
+          Ri[i + j * dy] = acc;
+        }
+      for (int i = 0; i < dx; ++i)  // G = H' R^-1
+        for (int j = 0; j < dy; ++j) {
+          double acc = 0.0;
+          for (int p = 0; p < dy; ++p) acc += mH[p + i * dy] * Ri[p + j * dy];
+          G[i + j * dx] = acc;
+        }
+      for (int i = 0; i < dx; ++i)  // W = G H
+        for (int j = 0; j < dx; ++j) {
+          double acc = 0.0;
+          for (int p = 0; p < dy; ++p) acc += G[i + p * dx] * mH[p + j * dy];
+          W[i + j * dx] = acc;
+        }
+      params.insert(params.end(), mA, mA + dx * dx);
+      params.insert(params.end(), mb, mb + dx);
+      params.insert(params.end(), LQ.begin(), LQ.end());
+      params.insert(params.end(), G.begin(), G.end());
+      params.insert(params.end(), W.begin(), W.end());
+      params.insert(params.end(), mQ, mQ + dx * dx);
+      params.insert(params.end(), mH, mH + dy * dx);
+      params.insert(params.end(), mc, mc + dy);
+      params.insert(params.end(), mR, mR + dy * dy);
+    }
     params.insert(params.end(), m.mu0, m.mu0 + dx);
     params.insert(params.end(), m.Sigma0, m.Sigma0 + dx * dx);
     ny += (int64_t)T[f] * dy;
@@ -409,4 +446,20 @@ extern "C" gf_status gf_kf_backward_information(gf_ctx* ctx, const gf_lg_model* 
   for (int f = 0; f < B; ++f)
     if (hs[f]) return set_err(ctx, hs[f], "model %d: a covariance or precision lost positive definiteness", f);
   return GF_OK;
+}
+
+extern "C" gf_status gf_kf_backward_information(gf_ctx* ctx, const gf_lg_model* models, int32_t B,
+                                                const int32_t* T, const double* ys, double initial_jitter,
+                                                int32_t use_initial_jitter, double jitter, int32_t use_jitter,
+                                                int32_t memspace, gf_kf_backward_out* out) {
+  return backward_impl(ctx, models, B, T, nullptr, ys, initial_jitter, use_initial_jitter, jitter, use_jitter,
+                       memspace, out);
+}
+
+extern "C" gf_status gf_kf_backward_information_tv(gf_ctx* ctx, const gf_lg_model* models, int32_t B,
+                                                   const int32_t* T, const int32_t* param_steps, const double* ys,
+                                                   double initial_jitter, int32_t use_initial_jitter, double jitter,
+                                                   int32_t use_jitter, int32_t memspace, gf_kf_backward_out* out) {
+  return backward_impl(ctx, models, B, T, param_steps, ys, initial_jitter, use_initial_jitter, jitter, use_jitter,
+                       memspace, out);
 }

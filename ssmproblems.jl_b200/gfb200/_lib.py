@@ -39,7 +39,7 @@ EXPORTED = [
     "gf_srv_create", "gf_srv_submit", "gf_srv_poll", "gf_srv_drain", "gf_srv_stats",
     "gf_srv_reset_stats", "gf_srv_last_error", "gf_srv_destroy",
     "gf_csmc_run", "gf_csmc_max_particles", "gf_pf_dense_ancestry", "gf_kf_loglikelihood_grad",
-    "gf_kf_backward_information",
+    "gf_kf_backward_information", "gf_kf_backward_information_tv",
 ]
 
 _dp = C.POINTER(C.c_double)
@@ -208,6 +208,9 @@ def load(path: str | None = None):
                                            i32, C.POINTER(KFGradOutC)]),
         "gf_kf_backward_information": (i32, [ctxp, C.POINTER(LGModelC), i32, C.POINTER(i32), _vp, dbl, i32,
                                              dbl, i32, i32, C.POINTER(KFBackOutC)]),
+        "gf_kf_backward_information_tv": (i32, [ctxp, C.POINTER(LGModelC), i32, C.POINTER(i32),
+                                                C.POINTER(i32), _vp, dbl, i32, dbl, i32, i32,
+                                                C.POINTER(KFBackOutC)]),
     }
     for name, (res, args) in sig.items():
         f = getattr(lib, name)

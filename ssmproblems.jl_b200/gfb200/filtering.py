@@ -551,10 +551,16 @@ def backward_information_batch(models, observations, *, initial_jitter=None, jit
         bufs["mu_smooth"] = bufs["Sigma_smooth"] = None
     status = np.zeros(B, np.int32)
     out = L.KFBackOutC(*[L.ptr(bufs[k]) for k in names], L.ptr(status))
-    L.check(ctx.h, L.load().gf_kf_backward_information(
-        ctx.h, mcs, B, Ts.ctypes.data_as(C.POINTER(C.c_int32)), L.ptr(ys),
-        float(initial_jitter or 0.0), int(initial_jitter is not None), float(jitter or 0.0),
-        int(jitter is not None), L.GF_MEM_HOST, C.byref(out)))
+    jit = (float(initial_jitter or 0.0), int(initial_jitter is not None), float(jitter or 0.0),
+           int(jitter is not None), L.GF_MEM_HOST, C.byref(out))
+    ps = _param_steps(models, Ts)
+    if ps is None:
+        L.check(ctx.h, L.load().gf_kf_backward_information(
+            ctx.h, mcs, B, Ts.ctypes.data_as(C.POINTER(C.c_int32)), L.ptr(ys), *jit))
+    else:
+        L.check(ctx.h, L.load().gf_kf_backward_information_tv(
+            ctx.h, mcs, B, Ts.ctypes.data_as(C.POINTER(C.c_int32)),
+            ps.ctypes.data_as(C.POINTER(C.c_int32)), L.ptr(ys), *jit))
     res, ov, om = [], 0, 0
     for f, m in enumerate(models):
         T, d = int(Ts[f]), m.dx

@@ -69,3 +69,35 @@ def test_backward_information_uneven_batch(ctx):
         _close(r["lam_upd"], lu, "lam_upd")
         mus, Ss = O.two_filter_smooth(to_oracle(m), ys, initial_jitter=1e-8, jitter=1e-12)
         _close(r["mu_smooth"], mus, "mu_smooth")
+
+
+def test_nonhomogeneous_backward_information_matches_oracle(ctx):
+    """Time-varying models (test/algorithms/kalman.jl:139-190 runs the backward
+    predictor on one): each step's dynamics and observation blocks are used where
+    the reference's calc_params(dyn, iter + 1) / calc_params(obs, iter) put them.
+    An uneven batch with a homogeneous model in the same launch; FP64 both sides."""
+    rng = np.random.default_rng(23)
+    oms, gms, yss = [], [], []
+    for dx, dy, T in [(2, 2, 4), (3, 1, 9), (5, 3, 12), (8, 8, 7)]:
+        om = O.create_nonhomogeneous_linear_gaussian_model(rng, dx, dy, T)
+        As = [O.random_orthogonal(rng, dx) * rng.uniform(0.5, 0.95) for _ in range(T)]
+        om = O.LGModel.time_varying(om.mu0, om.Sigma0, As, om.bs, om.Qs, om.Hs, om.cs, om.Rs)
+        gm = G.create_nonhomogeneous_linear_gaussian_model(om.mu0, om.Sigma0, om.As, om.bs, om.Qs,
+                                                           om.Hs, om.cs, om.Rs)
+        oms.append(om)
+        gms.append(gm)
+        yss.append(O.sample(rng, om, T)[1])
+    h = _stable_lg(rng, 4, 2)
+    oms.append(to_oracle(h))
+    gms.append(h)
+    yss.append(simulate(rng, h, 10)[1])
+    res = G.backward_information_batch(gms, yss, initial_jitter=1e-8, ctx=ctx)
+    for r, om, ys in zip(res, oms, yss):
+        lp, Op, lu, Ou = O.backward_information(om, ys, initial_jitter=1e-8)
+        _close(r["lam_pred"], lp, "lam_pred")
+        _close(r["Om_pred"], Op, "Om_pred")
+        _close(r["lam_upd"], lu, "lam_upd")
+        _close(r["Om_upd"], Ou, "Om_upd")
+        mus, Ss = O.two_filter_smooth(om, ys, initial_jitter=1e-8)
+        _close(r["mu_smooth"], mus, "mu_smooth")
+        _close(r["Sigma_smooth"], Ss, "Sigma_smooth")

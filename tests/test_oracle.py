@@ -319,6 +319,39 @@ def test_backward_information_matches_joint_gaussian(Dy):
 
 
 @pytest.mark.parametrize("Dy", [1, 2, 3])
+def test_nonhomogeneous_backward_information_matches_joint_gaussian(Dy):
+    """test/algorithms/kalman.jl:139-190 (T = 4, a non-homogeneous model): after
+    backward_initialise at T and two backward predict/update steps with each step's
+    own parameters (backward_predict at iter uses calc_params(dyn, iter + 1)), the
+    natural parameters of p(y_{T-2:T} | x_{T-2}) equal F' S^-1 (y - g) and
+    F' S^-1 F of the joint of (y_{T-2}, y_{T-1}, y_T) given x_{T-2}."""
+    rng = np.random.default_rng(1234 + Dy)
+    T = 4
+    m = O.create_nonhomogeneous_linear_gaussian_model(rng, 2, Dy, T)
+    _, ys = O.sample(rng, m, T)
+    _, _, lu, Ou = O.backward_information(m, ys, initial_jitter=1e-8)
+    _, _, _, H2, c2, R2 = m.params(T - 2)
+    A3, b3, Q3, H3, c3, R3 = m.params(T - 1)
+    A4, b4, Q4, H4, c4, R4 = m.params(T)
+    Z = np.zeros((Dy, Dy))
+    F = np.vstack([H2, H3 @ A3, H4 @ A4 @ A3])
+    g = np.concatenate([c2, H3 @ b3 + c3, H4 @ (A4 @ b3 + b4) + c4])
+    S = np.block([[R2, Z, Z],
+                  [Z, H3 @ Q3 @ H3.T + R3, H3 @ Q3 @ A4.T @ H4.T],
+                  [Z, H4 @ A4 @ Q3 @ H3.T, H4 @ (A4 @ Q3 @ A4.T + Q4) @ H4.T + R4]])
+    y = np.concatenate([ys[T - 3], ys[T - 2], ys[T - 1]])
+    lam_t = F.T @ np.linalg.solve(S, y - g)
+    Om_t = F.T @ np.linalg.solve(S, F)
+    np.testing.assert_allclose(lu[T - 3], lam_t, rtol=1e-7)
+    np.testing.assert_allclose(Ou[T - 3], Om_t, atol=1e-6)
+    # and the two-filter smoother of the time-varying model is the RTS smoother's
+    mus, Ss = O.two_filter_smooth(m, ys, initial_jitter=1e-10)
+    _, mr, Sr = O.rts_smooth(m, ys)
+    np.testing.assert_allclose(mus, mr, rtol=1e-6, atol=1e-9)
+    np.testing.assert_allclose(Ss, Sr, rtol=1e-6, atol=1e-9)
+
+
+@pytest.mark.parametrize("Dy", [1, 2, 3])
 def test_two_filter_smoother_equals_rts(Dy):
     """test/algorithms/kalman.jl:363-412: the two-filter smoother (forward filter x
     backward predictive likelihood) equals the RTS smoother at every time."""
