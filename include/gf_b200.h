@@ -180,9 +180,10 @@ gf_status gf_kf_batch(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int3
  * (GFTest/models/linear_gaussian.jl:42-95).  param_steps[f] = 1 runs model f as
  * gf_kf_batch does; param_steps[f] >= T[f] means the A, b, Q, H, c, R pointers
  * of models[f] each hold param_steps[f] consecutive per-step blocks (block t-1
- * = step t, each column-major) and step t uses block t-1.  Time-varying models
- * run with GF_ALGO_KF (GF_ALGO_SRKF returns GF_ERR_UNSUPPORTED); the smoother's
- * prediction from t to t+1 uses step t+1's parameters (kalman.jl:89-126). */
+ * = step t, each column-major) and step t uses block t-1, with GF_ALGO_KF or
+ * GF_ALGO_SRKF (whose step blocks carry the Cholesky factors of Q_t and R_t);
+ * the smoother's prediction from t to t+1 uses step t+1's parameters
+ * (kalman.jl:89-126). */
 gf_status gf_kf_batch_tv(gf_ctx* ctx, int32_t algo, const gf_lg_model* models, int32_t B,
                          const int32_t* T, const int32_t* param_steps, const double* ys,
                          double jitter, int32_t use_jitter, int32_t memspace, gf_kf_out* out);

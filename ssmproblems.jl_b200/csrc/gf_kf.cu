@@ -496,32 +496,56 @@ __global__ void __launch_bounds__(256) srkf_batch_kernel(KfRun run) {
     const KfDesc D = run.desc[f];
     const int dx = D.dx, dy = D.dy;
     const float* P = run.params + D.poff;
-    const float* pA = P;
-    const float* pb = pA + dx * dx;
-    const float* pH = pb + dx + dx * dx;
-    const float* pc = pH + dy * dx;
-    const float* pm = pc + dy + dy * dy;
-    const float* pUQ = pm + dx + dx * dx;
-    const float* pUR = pUQ + dx * dx;
-    const float* pU0 = pUR + dy * dy;
-    for (int e = threadIdx.x; e < dx * dx; e += G) {
-      int i = e % dx, j = e / dx;
-      s.A[i * LD + j] = pA[e];
-      s.UQ[i * LD + j] = pUQ[e];
-      s.U[i * LD + j] = pU0[e];
-    }
-    for (int e = threadIdx.x; e < dy * dx; e += G) s.H[(e % dy) * LD + e / dy] = pH[e];
-    for (int e = threadIdx.x; e < dy * dy; e += G) s.UR[(e % dy) * LY + e / dy] = pUR[e];
-    for (int e = threadIdx.x; e < dx; e += G) {
-      s.b[e] = pb[e];
-      s.mu[e] = pm[e];
-    }
-    for (int e = threadIdx.x; e < dy; e += G) s.c[e] = pc[e];
+    // homogeneous: A | b | Q | H | c | R | mu0 | S0 | UQ | UR | U0; time-varying:
+    // step blocks A | b | H | c | UQ | UR (calc_params(., t + 1)), then mu0 | U0
+    struct StepPtrs {
+      const float *A, *b, *H, *c, *UQ, *UR;
+    };
+    auto step_ptrs = [&](int t) {
+      StepPtrs q;
+      if (D.pstep) {
+        q.A = P + (int64_t)t * D.pstep;
+        q.b = q.A + dx * dx;
+        q.H = q.b + dx;
+        q.c = q.H + dy * dx;
+        q.UQ = q.c + dy;
+        q.UR = q.UQ + dx * dx;
+      } else {
+        q.A = P;
+        q.b = q.A + dx * dx;
+        q.H = q.b + dx + dx * dx;
+        q.c = q.H + dy * dx;
+        q.UQ = q.c + dy + dy * dy + dx + dx * dx;
+        q.UR = q.UQ + dx * dx;
+      }
+      return q;
+    };
+    auto load_step = [&](int t) {  // this step's A, b, H, c and the factors of Q and R
+      const StepPtrs q = step_ptrs(t);
+      for (int e = threadIdx.x; e < dx * dx; e += G) {
+        int i = e % dx, j = e / dx;
+        s.A[i * LD + j] = q.A[e];
+        s.UQ[i * LD + j] = q.UQ[e];
+      }
+      for (int e = threadIdx.x; e < dy * dx; e += G) s.H[(e % dy) * LD + e / dy] = q.H[e];
+      for (int e = threadIdx.x; e < dy * dy; e += G) s.UR[(e % dy) * LY + e / dy] = q.UR[e];
+      for (int e = threadIdx.x; e < dx; e += G) s.b[e] = q.b[e];
+      for (int e = threadIdx.x; e < dy; e += G) s.c[e] = q.c[e];
+    };
+    const float* pm = D.pstep ? P + D.p0 : step_ptrs(0).c + dy + dy * dy;
+    const float* pU0 = D.pstep ? pm + dx : step_ptrs(0).UR + dy * dy;
+    load_step(0);
+    for (int e = threadIdx.x; e < dx * dx; e += G) s.U[(e % dx) * LD + e / dx] = pU0[e];
+    for (int e = threadIdx.x; e < dx; e += G) s.mu[e] = pm[e];
     __syncthreads();
     double lltot = 0.0;
     int status = GF_OK;
     for (int t = 0; t < D.T; ++t) {
       const double* y = run.ys + D.yoff + (int64_t)t * dy;
+      if (D.pstep && t > 0) {  // time-varying model: step t's parameters
+        load_step(t);
+        __syncthreads();
+      }
       // predict: mu = A mu + b ; U = R(qr([UQ; U A']))
       float mnew = 0.f;
       if (threadIdx.x < dx) {
@@ -1160,8 +1184,9 @@ static gf_status kf_autotune_bucket(gf_kf_plan* p, gf_kf_plan::Bucket& bk) {
   return GF_OK;
 }
 
-// A time-varying model's pool entry: T step blocks (A b Q H c R) then mu0, S0.
-static gf_status kf_pack_model_tv(gf_ctx* ctx, const gf_lg_model& m, int f, int T,
+// A time-varying model's pool entry: T step blocks (A b Q H c R) then mu0, S0;
+// for the SRKF T blocks (A b H c UQ UR) then mu0, U0 (upper Cholesky factors).
+static gf_status kf_pack_model_tv(gf_ctx* ctx, int algo, const gf_lg_model& m, int f, int T,
                                   std::vector<float>& pool) {
   const int dx = m.dx, dy = m.dy;
   std::vector<double> L(std::max(dx, dy) * std::max(dx, dy));
@@ -1169,6 +1194,28 @@ static gf_status kf_pack_model_tv(gf_ctx* ctx, const gf_lg_model& m, int f, int 
   auto put = [&](const double* a, int64_t n) {
     for (int64_t i = 0; i < n; ++i) pool.push_back((float)a[i]);
   };
+  auto putU = [&](int n) {  // upper factor U = L' of the last chol_lower, column-major
+    for (int j = 0; j < n; ++j)
+      for (int i = 0; i < n; ++i) pool.push_back((float)L[j + i * n]);
+  };
+  if (algo == GF_ALGO_SRKF) {
+    for (int t = 0; t < T; ++t) {
+      put(m.A + (size_t)t * dx * dx, (int64_t)dx * dx);
+      put(m.b + (size_t)t * dx, dx);
+      put(m.H + (size_t)t * dy * dx, (int64_t)dy * dx);
+      put(m.c + (size_t)t * dy, dy);
+      if (chol_lower(dx, m.Q + (size_t)t * dx * dx, L.data()))
+        return set_err(ctx, GF_ERR_NOT_PD, "filter %d: Q of step %d not PD", f, t + 1);
+      putU(dx);
+      if (chol_lower(dy, m.R + (size_t)t * dy * dy, L.data()))
+        return set_err(ctx, GF_ERR_NOT_PD, "filter %d: R of step %d not PD", f, t + 1);
+      putU(dy);
+    }
+    put(m.mu0, dx);
+    chol_lower(dx, m.Sigma0, L.data());
+    putU(dx);
+    return GF_OK;
+  }
   for (int t = 0; t < T; ++t) {
     if (chol_lower(dy, m.R + (size_t)t * dy * dy, L.data()))
       return set_err(ctx, GF_ERR_NOT_PD, "filter %d: R of step %d not PD", f, t + 1);
@@ -1227,11 +1274,9 @@ static gf_status kf_plan_create_impl(gf_ctx* ctx, int32_t algo, const gf_lg_mode
     if (ps != 1 && ps < T[f])
       return set_err(ctx, GF_ERR_ARG, "filter %d: %d parameter steps for T = %d", f, ps, T[f]);
     if (ps != 1) {
-      if (algo != GF_ALGO_KF)
-        return set_err(ctx, GF_ERR_UNSUPPORTED, "filter %d: time-varying parameters run with KalmanFilter()", f);
-      gf_status pst = kf_pack_model_tv(ctx, m, f, T[f], pool);
+      gf_status pst = kf_pack_model_tv(ctx, algo, m, f, T[f], pool);
       if (pst) return pst;
-      d.pstep = kf_step_block_len(dx, dy);
+      d.pstep = algo == GF_ALGO_SRKF ? sr_step_block_len(dx, dy) : kf_step_block_len(dx, dy);
       d.p0 = T[f] * d.pstep;
       poff += (int64_t)d.p0 + dx + (int64_t)dx * dx;
     } else {

@@ -57,12 +57,15 @@ struct KfRun {
 // parameter pool layout per filter (column-major, unpadded):
 //   A dx*dx | b dx | Q dx*dx | H dy*dx | c dy | R dy*dy | mu0 dx | S0 dx*dx |
 //   UQ dx*dx | UR dy*dy | U0 dx*dx     (upper Cholesky factors, used by the SRKF)
-// A time-varying model (KF only) holds T step blocks (A b Q H c R) followed
-// by mu0 | S0.
+// A time-varying model holds T step blocks followed by the prior: for the KF
+// (A b Q H c R) then mu0 | S0; for the SRKF (A b H c UQ UR) then mu0 | U0.
 __host__ __device__ inline int64_t kf_param_len(int dx, int dy) {
   return (int64_t)5 * dx * dx + 2 * dx + dy * dx + dy + 2 * dy * dy;
 }
 __host__ __device__ inline int32_t kf_step_block_len(int dx, int dy) {
+  return 2 * dx * dx + dx + dy * dx + dy + dy * dy;
+}
+__host__ __device__ inline int32_t sr_step_block_len(int dx, int dy) {
   return 2 * dx * dx + dx + dy * dx + dy + dy * dy;
 }
 

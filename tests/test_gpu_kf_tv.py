@@ -95,5 +95,33 @@ def test_nonhomogeneous_needs_a_block_per_step(ctx):
     om, gm, ys = _tv_pair(rng, 3, 2, 5)
     with pytest.raises(ValueError):
         G.filter_batch([gm], G.KalmanFilter(), [np.vstack([ys, ys])], ctx=ctx)
-    with pytest.raises(Exception):
-        G.filter_batch([gm], G.SRKF(), [ys], ctx=ctx)
+    with pytest.raises(ValueError):
+        G.filter_batch([gm], G.SRKF(), [np.vstack([ys, ys])], ctx=ctx)
+
+
+def test_nonhomogeneous_srkf_matches_oracle(ctx):
+    """The square-root filter (srkf.jl:93-176) on time-varying models: each step's
+    A, b, H, c and the Cholesky factors of Q_t and R_t are that step's.  Uneven
+    batch with a homogeneous model mixed in; every step's ll, mean and covariance
+    against the FP64 oracle KF, at the bars of the time-varying KF test."""
+    rng = np.random.default_rng(29)
+    oms, gms, yss = [], [], []
+    for Dx, Dy, T in [(2, 2, 4), (3, 1, 30), (6, 3, 40), (16, 8, 25), (32, 16, 20)]:
+        om, gm, ys = _tv_pair(rng, Dx, Dy, T, stable=(Dx, T) != (2, 4))
+        oms.append(om)
+        gms.append(gm)
+        yss.append(ys)
+    h = O.create_linear_gaussian_model(rng, 4, 2)
+    h = O.LGModel(h.mu0, h.Sigma0, O.random_orthogonal(rng, 4) * 0.9, h.b, h.Q, h.H, h.c, h.R)
+    oms.append(h)
+    gms.append(G.create_homogeneous_linear_gaussian_model(h.mu0, h.Sigma0, h.A, h.b, h.Q, h.H, h.c, h.R))
+    yss.append(O.sample(rng, h, 17)[1])
+    res = G.filter_batch(gms, G.SRKF(), yss, ctx=ctx)
+    for (st, ll), om, ys in zip(res, oms, yss):
+        rll, rsteps, rmus, rsig = O.kf_filter(om, ys)
+        assert abs(ll - rll) <= 1e-4 * max(1.0, abs(rll)), (ll, rll)
+        scale_mu = np.abs(rmus).max(axis=1, keepdims=True) + 1e-3
+        assert np.all(np.abs(st.means - rmus) <= 1e-3 * scale_mu + 1e-5)
+        scale_s = np.abs(rsig).reshape(len(ys), -1).max(axis=1)[:, None, None]
+        assert np.all(np.abs(st.covs - rsig) <= 1e-3 * scale_s + 1e-6)
+        np.testing.assert_allclose(st.ll_steps, rsteps, rtol=1e-3, atol=1e-4)
