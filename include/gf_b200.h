@@ -297,9 +297,10 @@ gf_status gf_pf_run(gf_ctx* ctx, const gf_lg_model* model, const gf_pf_config* c
 /* The same for a time-varying model (calc_params(dyn, t), calc_params(obs, t),
  * models/linear_gaussian.jl:44-63): param_steps = 1 is gf_pf_run; param_steps
  * >= T means the A, b, Q, H, c, R pointers of `model` each hold param_steps
- * per-step blocks (block t-1 = step t, column-major).  Bootstrap proposal
- * (GF_ERR_UNSUPPORTED otherwise); the auxiliary lookahead uses step t's
- * parameters for step t. */
+ * per-step blocks (block t-1 = step t, column-major).  Every proposal; a
+ * guided proposal's factors (OptimalProposal's gain and covariance,
+ * OverdispersedProposal's k Q_t) are those of step t, as is the auxiliary
+ * lookahead. */
 gf_status gf_pf_run_tv(gf_ctx* ctx, const gf_lg_model* model, int32_t param_steps,
                        const gf_pf_config* cfg, int32_t T, const double* ys, const void* noise,
                        const double* uniforms, int32_t memspace, gf_pf_out* out);

@@ -751,6 +751,42 @@ static int maybe_resample(const or_resample_cfg* rc, int t, long N, int width, d
   return 1;
 }
 
+/* A guided proposal's factors for one step's (Q, H, c, R): OverdispersedProposal
+ * MvNormal(A x + b, k Q) (GFTest/proposals.jl:39-50) gives Lq = chol(k Q);
+ * OptimalProposal kalman_update(MvNormal(A x + b, Q), (H, c, R), y)
+ * (GFTest/proposals.jl:20-31) gives the gain Kq and covariance Sq = Lq Lq',
+ * which do not depend on x and are computed with the arithmetic kf_update
+ * applies to every particle.  Bootstrap: nothing. */
+static int guided_factors(int dx, int dy, const or_proposal* prop, const double* Q, const double* LQ,
+                          const double* H, const double* c, const double* R, const double* LR,
+                          double* Kq, double* Sq, double* Lq) {
+  int st = OR_OK;
+  if (prop->kind == OR_PROP_OVERDISPERSED) {
+    double* kQ = malloc(sizeof(double) * dx * dx);
+    for (int i = 0; i < dx * dx; ++i) kQ[i] = prop->k * Q[i];
+    st = or_chol_lower(dx, kQ, Lq);
+    free(kQ);
+  } else if (prop->kind == OR_PROP_OPTIMAL) {
+    kf_ws ws = kf_ws_alloc(dx, dy);
+    double* mu = calloc(dx, 8);
+    double* Sg = malloc(sizeof(double) * dx * dx);
+    double* Lg = malloc(sizeof(double) * dx * dx);
+    double* yz = calloc(dy, 8);
+    memcpy(Sg, Q, 8 * dx * dx);
+    memcpy(Lg, LQ, 8 * dx * dx);
+    double lldummy;
+    /* with mu = 0 and y = c the innovation is 0; K and Sigma_q are what we need */
+    memcpy(yz, c, 8 * dy);
+    st = kf_update(dx, dy, H, c, R, LR, yz, 0.0, 0, mu, Sg, Lg, &lldummy, &ws);
+    memcpy(Kq, ws.K, 8 * dx * dy);
+    memcpy(Sq, Sg, 8 * dx * dx);
+    memcpy(Lq, Lg, 8 * dx * dx);
+    free(mu); free(Sg); free(Lg); free(yz);
+    kf_ws_free(&ws);
+  }
+  return st;
+}
+
 /* filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys).
  * Returns status; *ll is the log-evidence. */
 int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_cfg* rc,
@@ -773,36 +809,7 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
   if ((st = or_chol_lower(dx, m->Sigma0, L0)) || (st = or_chol_lower(dx, m->Q, LQ)) ||
       (st = or_chol_lower(dy, m->R, LR)))
     goto done;
-  if (m->tv && prop->kind != OR_PROP_BOOTSTRAP) { st = OR_ARG; goto done; } /* bootstrap only */
-  if (prop->kind == OR_PROP_OVERDISPERSED) {
-    /* GFTest/proposals.jl:39-50: MvNormal(A x + b, k Q) */
-    double* kQ = malloc(sizeof(double) * dx * dx);
-    for (int i = 0; i < dx * dx; ++i) kQ[i] = prop->k * m->Q[i];
-    st = or_chol_lower(dx, kQ, Lq);
-    free(kQ);
-    if (st) goto done;
-  } else if (prop->kind == OR_PROP_OPTIMAL) {
-    /* GFTest/proposals.jl:20-31: kalman_update(MvNormal(A x + b, Q), (H,c,R), y).
-     * Gain and covariance do not depend on x; they are computed once with the
-     * same arithmetic kf_update applies to every particle. */
-    kf_ws ws = kf_ws_alloc(dx, dy);
-    double* mu = calloc(dx, 8);
-    double* Sg = malloc(sizeof(double) * dx * dx);
-    double* Lg = malloc(sizeof(double) * dx * dx);
-    double* yz = calloc(dy, 8);
-    memcpy(Sg, m->Q, 8 * dx * dx);
-    memcpy(Lg, LQ, 8 * dx * dx);
-    double lldummy;
-    /* with mu = 0 and y = c the innovation is 0; K and Sigma_q are what we need */
-    memcpy(yz, m->c, 8 * dy);
-    st = kf_update(dx, dy, m->H, m->c, m->R, LR, yz, 0.0, 0, mu, Sg, Lg, &lldummy, &ws);
-    memcpy(Kq, ws.K, 8 * dx * dy);
-    memcpy(Sq, Sg, 8 * dx * dx);
-    memcpy(Lq, Lg, 8 * dx * dx);
-    free(mu); free(Sg); free(Lg); free(yz);
-    kf_ws_free(&ws);
-    if (st) goto done;
-  }
+  if ((st = guided_factors(dx, dy, prop, m->Q, LQ, m->H, m->c, m->R, LR, Kq, Sq, Lq))) goto done;
   /* initialise (particles.jl:36-50): x ~ MvNormal(mu0, Sigma0) */
   for (long i = 0; i < N; ++i) {
     double e[64], v[64];
@@ -818,7 +825,9 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
     int res;
     /* this step's parameters (calc_params(dyn, t), calc_params(obs, t)) */
     const or_step_params SP = step_params(m, t - 1);
-    if (m->tv && ((st = or_chol_lower(dx, SP.Q, LQ)) || (st = or_chol_lower(dy, SP.R, LR)))) goto done;
+    if (m->tv && ((st = or_chol_lower(dx, SP.Q, LQ)) || (st = or_chol_lower(dy, SP.R, LR)) ||
+                  (st = guided_factors(dx, dy, prop, SP.Q, LQ, SP.H, SP.c, SP.R, LR, Kq, Sq, Lq))))
+      goto done;
     const double *mA = SP.A, *mb = SP.b, *mH = SP.H, *mc = SP.c;
     if (prop->lookahead) {
       /* AuxiliaryParticleFilter step (particles.jl:311-345): log eta_i =
@@ -900,8 +909,8 @@ int or_pf_run(const or_lg_model* m, const or_proposal* prop, const or_resample_c
         double mq[64];
         if (prop->kind == OR_PROP_OPTIMAL) {
           double z[64];
-          mv(dy, dx, m->H, mx, z);
-          for (int k = 0; k < dy; ++k) z[k] = y[k] - z[k] - m->c[k];
+          mv(dy, dx, mH, mx, z);
+          for (int k = 0; k < dy; ++k) z[k] = y[k] - z[k] - mc[k];
           mv(dx, dy, Kq, z, v);
           for (int d = 0; d < dx; ++d) mq[d] = mx[d] + v[d];
         } else {

@@ -103,7 +103,7 @@ struct LgJobSetup {
   size_t smem = 0;
   std::vector<char> params;      // parameter blocks (one per step if time-varying)
   std::vector<double> pp;        // observation-prep factors (likewise)
-  std::vector<double> obs_consts;  // time-varying: the observation constant of every step
+  std::vector<double> obs_consts;  // time-varying: observation and proposal constants of every step
   int64_t pstride = 0;           // time-varying: elements between parameter blocks
   int32_t ppstride = 0;          // time-varying: doubles between prep blocks
   double ess1 = 0.0;

@@ -42,8 +42,9 @@ struct PfJob {
   int32_t ystride;
   int32_t lookahead_draw;    // auxiliary filter: DrawPredictive (x* drawn from the transition)
   // time-varying model: step t's parameter block is params + (t-1) * pstride
-  // elements and its observation constant obs_consts[t-1]; the observation
-  // prep reads its factors pp + t * ppstride (0 / null: one block for all steps)
+  // elements, its observation and proposal constants obs_consts[2(t-1)] and
+  // obs_consts[2(t-1) + 1]; the observation prep reads its factors
+  // pp + t * ppstride (0 / null: one block for all steps)
   int64_t pstride;
   const double* obs_consts;
   int32_t ppstride;
@@ -79,7 +80,11 @@ struct PfJob {
 
 // Observation constant of step t (time-varying models carry one per step).
 __device__ __forceinline__ double step_obs_const(const PfJob& J, int t) {
-  return J.obs_consts ? J.obs_consts[t - 1] : J.obs_const;
+  return J.obs_consts ? J.obs_consts[2 * (t - 1)] : J.obs_const;
+}
+// log-normaliser difference of a guided proposal at step t (proposal vs transition)
+__device__ __forceinline__ double step_prop_const(const PfJob& J, int t) {
+  return J.obs_consts ? J.obs_consts[2 * (t - 1) + 1] : J.prop_const;
 }
 
 __device__ __forceinline__ int find_job(const PfJob* jobs, int njobs, int block, bool scan) {

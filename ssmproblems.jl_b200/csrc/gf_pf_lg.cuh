@@ -118,7 +118,7 @@ __device__ __forceinline__ void lg_propagate_tile(const PfJob& J, int tile) {
   int32_t* __restrict__ anc_out = J.anc_out;
   const uint64_t seed = J.seed;
   const bool diag = J.diag_l != 0;
-  const double obs_const = step_obs_const(J, t), prop_const = J.prop_const;
+  const double obs_const = step_obs_const(J, t), prop_const = step_prop_const(J, t);
   const Real* eta = reinterpret_cast<const Real*>(J.eta);
   const bool apf = resamp && eta != nullptr;
   LseAcc acc;

@@ -28,7 +28,7 @@ struct gf_pf_plan {
   double* tprefix = nullptr;
   int32_t *ocum = nullptr, *mpk = nullptr, *anc = nullptr;
   void* eta = nullptr;  // auxiliary filter: lookahead log eta [N]
-  double* obs_consts = nullptr;  // time-varying model: observation constant per step
+  double* obs_consts = nullptr;  // time-varying model: observation and proposal constants per step
   unsigned long long* flags = nullptr;
   PfScalars* sc = nullptr;
   int8_t *sched_dev = nullptr, *res1 = nullptr;
@@ -91,8 +91,6 @@ gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cf
   const bool tv = param_steps != 1;
   if (tv && param_steps < T)
     return set_err(ctx, GF_ERR_ARG, "%d parameter steps for T = %d", param_steps, T);
-  if (tv && guided)
-    return set_err(ctx, GF_ERR_UNSUPPORTED, "time-varying parameters run with the bootstrap proposal");
   if (!pick_lg_kernels(o->dbl, guided, m->dx, m->dy, &o->k))
     return set_err(ctx, GF_ERR_DIM, "no kernel for dx=%d dy=%d in %s", m->dx, m->dy,
                    o->dbl ? "FP64 (max 16)" : "FP32 (max 64)");
@@ -121,7 +119,10 @@ gf_status lg_job_setup(gf_ctx* ctx, const gf_lg_model* m, const gf_pf_config* cf
     o->pp.insert(o->pp.end(), f.c.begin(), f.c.end());
     o->pp.insert(o->pp.end(), f.K.begin(), f.K.end());
     o->pp.insert(o->pp.end(), f.vb.begin(), f.vb.end());
-    if (tv) o->obs_consts.push_back(f.obs_const);
+    if (tv) {  // step constants: observation, proposal
+      o->obs_consts.push_back(f.obs_const);
+      o->obs_consts.push_back(f.prop_const);
+    }
     for (int j = 0; j < dx; ++j)
       for (int i = 0; i < dx; ++i)
         if (i != j && f.L[i + j * dx] != 0.0) diag = false;

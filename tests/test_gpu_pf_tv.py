@@ -44,6 +44,29 @@ def test_tv_pf_f64_matches_oracle(ctx, kind, lookahead):
     assert st.resampled.sum() >= 2
 
 
+@pytest.mark.parametrize("prop", ["optimal", "overdispersed"])
+@pytest.mark.parametrize("kind", [O.SYSTEMATIC, O.MULTINOMIAL])
+def test_tv_guided_pf_f64_matches_oracle(ctx, prop, kind):
+    """Guided proposals (GFTest/proposals.jl:11-50) on a time-varying model: each
+    step's proposal factors and log-normaliser difference are that step's."""
+    rng = np.random.default_rng(40 + kind + (prop == "optimal"))
+    om, gm, ys = _tv(rng, 3, 2, 12)
+    N, T = 2000, 12
+    noise = rng.standard_normal((T + 1, 3, N))
+    unif = rng.random(T) if kind == O.SYSTEMATIC else rng.random((T, N))
+    rs = {O.SYSTEMATIC: G.Systematic(), O.MULTINOMIAL: G.Multinomial()}[kind]
+    q = G.OptimalProposal() if prop == "optimal" else G.OverdispersedProposal(k=1.6)
+    algo = G.PF(N, q, threshold=0.6, resampler=rs, precision="f64")
+    st, ll = G.filter(gm, algo, ys, noise=noise, uniforms=unif, want_ancestors=True, ctx=ctx)
+    ref = O.pf_run(om, N, ys, resampler=kind, threshold=0.6, noise=noise, uniforms=unif,
+                   want_ancestors=True,
+                   proposal=O.PROP_OPTIMAL if prop == "optimal" else O.PROP_OVERDISPERSED,
+                   k=1.0 if prop == "optimal" else 1.6)
+    np.testing.assert_allclose(st.ll_steps, ref["ll_steps"], rtol=0, atol=1e-9)
+    np.testing.assert_array_equal(st.ancestors, ref["ancestors"])
+    assert st.resampled.sum() >= 2
+
+
 @pytest.mark.parametrize("dx,dy", [(4, 3), (16, 8)])
 def test_tv_pf_f32_matches_oracle_without_resampling(ctx, dx, dy):
     """FP32 state (the tensor-core path at Dx = 16): every step's parameters reach

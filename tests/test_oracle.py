@@ -62,6 +62,21 @@ def test_nonhomogeneous_pf_oracle_converges_to_kf():
     assert abs(np.mean(lls) - O.kf_filter(m, ys)[0]) < 2e-2
 
 
+@pytest.mark.parametrize("proposal,k", [(O.PROP_OPTIMAL, 1.0), (O.PROP_OVERDISPERSED, 1.7)])
+def test_nonhomogeneous_guided_pf_oracle_converges_to_kf(proposal, k):
+    """Guided proposals on a time-varying model take step t's factors (the
+    optimal proposal's gain and covariance from Q_t, H_t, R_t; k Q_t for the
+    overdispersed one): the log-evidence converges to the exact time-varying KF."""
+    rng = np.random.default_rng(6)
+    m = O.create_nonhomogeneous_linear_gaussian_model(rng, 2, 2, 5)
+    m = O.LGModel.time_varying(m.mu0, m.Sigma0, [O.random_orthogonal(rng, 2) * 0.8 for _ in range(5)],
+                               m.bs, m.Qs, m.Hs, m.cs, m.Rs)
+    _, ys = O.sample(rng, m, 5)
+    lls = [O.pf_run(m, 200000, ys, threshold=0.5, seed=s, threads=4, proposal=proposal, k=k)["ll"]
+           for s in range(2)]
+    assert abs(np.mean(lls) - O.kf_filter(m, ys)[0]) < 2e-2
+
+
 @pytest.mark.parametrize("Dy", [1, 2, 3])
 @pytest.mark.parametrize("T", [1, 5])
 def test_rts_smoother_matches_joint_gaussian(Dy, T):
