@@ -340,6 +340,13 @@ gf_status gf_pf_dense_ancestry(gf_ctx* ctx, int32_t T, int64_t N, int32_t dx, in
 gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* model, const gf_pf_config* cfg, int32_t T,
                       const double* ys, const void* noise, const double* uniforms,
                       int32_t memspace, gf_pf_out* out, double* zmeans);
+/* The same for a time-varying hierarchical model: param_steps = 1 is
+ * gf_rbpf_run; param_steps >= T means A_o, b_o, Q_o, A_z, b_z, C_z, Q_z, H, c
+ * and R each hold param_steps per-step blocks (block t-1 = calc_params(., t),
+ * column-major); the priors and q_gamma, q_index are shared by all steps. */
+gf_status gf_rbpf_run_tv(gf_ctx* ctx, const gf_rb_model* model, int32_t param_steps,
+                         const gf_pf_config* cfg, int32_t T, const double* ys, const void* noise,
+                         const double* uniforms, int32_t memspace, gf_pf_out* out, double* zmeans);
 
 /* ---------------------------------------------------- resampling primitives */
 /* sample_ancestors(rng, resampler, weights) (resamplers.jl:206-238;

@@ -1021,7 +1021,28 @@ typedef struct {
   const double *mu_z, *Sigma_z, *A_z, *b_z, *C_z, *Q_z;  /* inner */
   double q_gamma; int q_index;
   const double *H, *c, *R;                               /* obs on inner */
+  int tv; /* 1: A_o, b_o, Q_o, A_z, b_z, C_z, Q_z, H, c, R hold one block per step */
 } or_rb_model;
+
+/* The model of 1-based step t+1 (calc_params(., t+1)): block t of a
+ * time-varying model, else the model itself. */
+static or_rb_model rb_step_model(const or_rb_model* m, int t) {
+  or_rb_model s = *m;
+  if (!m->tv) return s;
+  const int dxo = m->dxo, dz = m->dz, dy = m->dy;
+  s.A_o = m->A_o + (size_t)t * dxo * dxo;
+  s.b_o = m->b_o + (size_t)t * dxo;
+  s.Q_o = m->Q_o + (size_t)t * dxo * dxo;
+  s.A_z = m->A_z + (size_t)t * dz * dz;
+  s.b_z = m->b_z + (size_t)t * dz;
+  s.C_z = m->C_z + (size_t)t * dz * dxo;
+  s.Q_z = m->Q_z + (size_t)t * dz * dz;
+  s.H = m->H + (size_t)t * dy * dz;
+  s.c = m->c + (size_t)t * dy;
+  s.R = m->R + (size_t)t * dy * dy;
+  s.tv = 0;
+  return s;
+}
 
 /* One particle's RBPF move (rbpf.jl:24-84): outer propogate with noise e
  * (particles.jl:175-245), inner KF predict with (prev_outer, new_outer)
@@ -1137,6 +1158,16 @@ int or_rbpf_run(const or_rb_model* m, const or_proposal* prop, const or_resample
     double ess = 0.0, baseline;
     int res;
     const double* y = ys + (size_t)(t - 1) * dy;
+    /* this step's model (time-varying: calc_params(., t)) and its factors */
+    const or_rb_model ms = rb_step_model(m, t - 1);
+    if (m->tv) {
+      if ((st = or_chol_lower(dxo, ms.Q_o, LQo)) || (st = or_chol_lower(dy, ms.R, LR))) break;
+      if (prop->kind == OR_PROP_OVERDISPERSED) {
+        double kQ[64 * 64];
+        for (int i = 0; i < dxo * dxo; ++i) kQ[i] = prop->k * ms.Q_o[i];
+        if ((st = or_chol_lower(dxo, kQ, Lqo))) break;
+      }
+    }
     if (prop->lookahead) {
       /* AuxiliaryParticleFilter(RBPF(...), pp) step (particles.jl:311-345):
        * resample on softmax(logw + log eta) (resamplers.jl:109-116), new weights
@@ -1150,7 +1181,7 @@ int or_rbpf_run(const or_rb_model* m, const or_proposal* prop, const or_resample
       double* q = malloc(sizeof(double) * width);
 #pragma omp for schedule(static)
       for (long i = 0; i < N; ++i) {
-        if (rb_logeta(m, prop->lookahead, LQo, LR, y, S + (size_t)i * width, seed, i, t, q, Qt, &ws,
+        if (rb_logeta(&ms, prop->lookahead, LQo, LR, y, S + (size_t)i * width, seed, i, t, q, Qt, &ws,
                       &eta[i]))
           bad |= 1;
         aux[i] = (uniform ? 0.0 : logw[i]) + eta[i];
@@ -1202,7 +1233,7 @@ int or_rbpf_run(const or_rb_model* m, const or_proposal* prop, const or_resample
       double e[64];
       draw_normals(noise, seed, dxo, N, t, i, e);
       double inc = 0.0;
-      if (rb_particle_step(m, prop, LQo, Lqo, LR, y, e, S + (size_t)i * width, Qt, &ws, &inc))
+      if (rb_particle_step(&ms, prop, LQo, Lqo, LR, y, e, S + (size_t)i * width, Qt, &ws, &inc))
         fail |= 1;
       logw[i] = logw[i] + inc;
     }

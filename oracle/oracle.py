@@ -97,7 +97,8 @@ class _RB(C.Structure):
                 + [(n, _dp) for n in ("mu_o", "Sigma_o", "A_o", "b_o", "Q_o",
                                       "mu_z", "Sigma_z", "A_z", "b_z", "C_z", "Q_z")]
                 + [("q_gamma", C.c_double), ("q_index", C.c_int)]
-                + [(n, _dp) for n in ("H", "c", "R")])
+                + [(n, _dp) for n in ("H", "c", "R")]
+                + [("tv", C.c_int)])
 
 
 class LGModel:
@@ -360,11 +361,35 @@ class RBModel:
         self.q_gamma, self.q_index = float(q_gamma), int(q_index)
         self.dxo, self.dz, self.dy = self.mu_o.size, self.mu_z.size, self.H.shape[0]
 
+    STEP_NAMES = ("A_o", "b_o", "Q_o", "A_z", "b_z", "C_z", "Q_z", "H", "c", "R")
+
+    @classmethod
+    def time_varying(cls, mu_o, Sigma_o, mu_z, Sigma_z, steps, q_gamma=0.0, q_index=0):
+        """Non-homogeneous hierarchical model: `steps` is a list over t = 1..T of
+        dicts with the STEP_NAMES parameters of step t (calc_params(., t))."""
+        s0 = steps[0]
+        m = cls(mu_o, Sigma_o, s0["A_o"], s0["b_o"], s0["Q_o"], mu_z, Sigma_z, s0["A_z"], s0["b_z"],
+                s0["C_z"], s0["Q_z"], s0["H"], s0["c"], s0["R"], q_gamma, q_index)
+        m.tv = True
+        m.steps = [cls(mu_o, Sigma_o, d["A_o"], d["b_o"], d["Q_o"], mu_z, Sigma_z, d["A_z"], d["b_z"],
+                       d["C_z"], d["Q_z"], d["H"], d["c"], d["R"], q_gamma, q_index) for d in steps]
+        # step-major blocks, each column-major (the C oracle's tv layout)
+        m._stk = {n: np.concatenate([np.asarray(getattr(k, n)).ravel(order="F") for k in m.steps])
+                  for n in cls.STEP_NAMES}
+        return m
+
+    def step(self, t):
+        """The homogeneous model of 1-based step t."""
+        return self.steps[t - 1] if getattr(self, "tv", False) else self
+
     def _struct(self):
         names = ("mu_o", "Sigma_o", "A_o", "b_o", "Q_o", "mu_z", "Sigma_z", "A_z", "b_z",
                  "C_z", "Q_z")
-        return _RB(self.dxo, self.dz, self.dy, *[_p(getattr(self, n)) for n in names],
-                   self.q_gamma, self.q_index, _p(self.H), _p(self.c), _p(self.R))
+        tv = getattr(self, "tv", False)
+        get = (lambda n: self._stk[n] if n in self._stk else getattr(self, n)) if tv else \
+            (lambda n: getattr(self, n))
+        return _RB(self.dxo, self.dz, self.dy, *[_p(get(n)) for n in names],
+                   self.q_gamma, self.q_index, _p(get("H")), _p(get("c")), _p(get("R")), int(tv))
 
 
 def rbpf_run(m: RBModel, N, ys, *, resampler=SYSTEMATIC, conv=CONV_CPU, threshold=0.5,

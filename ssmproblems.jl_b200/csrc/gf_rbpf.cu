@@ -173,7 +173,8 @@ __global__ void __launch_bounds__(RB_THREADS) rbpf_propagate(const PfJob* __rest
   const bool fresh = resamp || sc->uniform != 0;
   const double lse_prev = sc->lse;
   const bool searched = J.resampler == GF_RS_MULTINOMIAL;
-  const float* P = reinterpret_cast<const float*>(J.params);
+  // step t's parameter block (time-varying models: calc_params(., t)), else the one block
+  const float* P = reinterpret_cast<const float*>(J.params) + (size_t)(t - 1) * J.pstride;
   for (int k = threadIdx.x; k < L::total; k += RB_THREADS) sp[k] = P[k];
   if (threadIdx.x < DY) sy[threadIdx.x] = J.ys[(size_t)(t - 1) * DY + threadIdx.x];
   __syncthreads();
@@ -367,7 +368,8 @@ __global__ void __launch_bounds__(RB_THREADS) rbpf_lookahead(const PfJob* __rest
   if (t > J.T || sc->status != 0) return;
   const int tile = blockIdx.x / RB_SPLIT - J.tile0;
   const int part = blockIdx.x % RB_SPLIT;
-  const float* P = reinterpret_cast<const float*>(J.params);
+  // step t's parameter block (time-varying models: calc_params(., t)), else the one block
+  const float* P = reinterpret_cast<const float*>(J.params) + (size_t)(t - 1) * J.pstride;
   for (int k = threadIdx.x; k < L::total; k += RB_THREADS) sp[k] = P[k];
   if (threadIdx.x < DY) sy[threadIdx.x] = J.ys[(size_t)(t - 1) * DY + threadIdx.x];
   __syncthreads();
@@ -517,10 +519,9 @@ gf_status rb_pack_params(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_config* 
 
 using namespace gf;
 
-extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_config* cfg,
-                                 int32_t T, const double* ys, const void* noise,
-                                 const double* uniforms, int32_t memspace, gf_pf_out* out,
-                                 double* zmeans) {
+static gf_status rbpf_run_impl(gf_ctx* ctx, const gf_rb_model* m, int32_t param_steps,
+                               const gf_pf_config* cfg, int32_t T, const double* ys, const void* noise,
+                               const double* uniforms, int32_t memspace, gf_pf_out* out, double* zmeans) {
   if (!ctx || !m || !cfg || !out || !ys || !out->ll)
     return ctx ? set_err(ctx, GF_ERR_ARG, "null argument") : GF_ERR_ARG;
   if (cfg->precision != GF_PREC_F32) return set_err(ctx, GF_ERR_UNSUPPORTED, "RBPF runs in FP32 only");
@@ -535,10 +536,33 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   cudaSetDevice(ctx->device);
   const int dxo = m->dxo, dz = m->dz, dy = m->dy;
   const int NS = dz * (dz + 1) / 2, width = dxo + dz + NS;
+  // one parameter block per step of a time-varying model (calc_params(., t)),
+  // else one; each block also carries the priors, which the initialisation
+  // reads from block 0
+  const bool tv = param_steps != 1;
+  if (tv && param_steps < T) return set_err(ctx, GF_ERR_ARG, "%d parameter steps for T = %d", param_steps, T);
+  const int nblk = tv ? T : 1;
   std::vector<float> P;
   double prop_const = 0.0;
   gf_status st;
-  if ((st = rb_pack_params(ctx, m, cfg, P, &prop_const))) return st;
+  for (int k = 0; k < nblk; ++k) {
+    gf_rb_model mk = *m;
+    if (tv) {
+      mk.A_o = m->A_o + (size_t)k * dxo * dxo;
+      mk.b_o = m->b_o + (size_t)k * dxo;
+      mk.Q_o = m->Q_o + (size_t)k * dxo * dxo;
+      mk.A_z = m->A_z + (size_t)k * dz * dz;
+      mk.b_z = m->b_z + (size_t)k * dz;
+      mk.C_z = m->C_z + (size_t)k * dz * dxo;
+      mk.Q_z = m->Q_z + (size_t)k * dz * dz;
+      mk.H = m->H + (size_t)k * dy * dz;
+      mk.c = m->c + (size_t)k * dy;
+      mk.R = m->R + (size_t)k * dy * dy;
+    }
+    // the proposal's log-normaliser difference, sum log sqrt(k), is the same every step
+    if ((st = rb_pack_params(ctx, &mk, cfg, P, &prop_const))) return st;
+  }
+  const int64_t pstride = tv ? (int64_t)(P.size() / nblk) : 0;
   const int64_t N = cfg->n_particles;
   const int ntiles = (int)((N + PF_TILE - 1) / PF_TILE);
   const int nstiles = (int)((N + SCAN_TILE - 1) / SCAN_TILE);
@@ -654,6 +678,7 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   J.prop_const = prop_const;
   J.seed = cfg->seed;
   J.params = d_params;
+  J.pstride = pstride;
   J.X[0] = X0;
   J.X[1] = X1;
   J.lw = lw;
@@ -792,4 +817,17 @@ extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_
   if (sc.status == GF_ERR_NOT_PD) return set_err(ctx, GF_ERR_NOT_PD, "inner innovation covariance not PD at step %d", sc.t + 1);
   if (sc.status) return set_err(ctx, sc.status, "RBPF failed at step %d (status %d)", sc.t + 1, sc.status);
   return GF_OK;
+}
+
+extern "C" gf_status gf_rbpf_run(gf_ctx* ctx, const gf_rb_model* m, const gf_pf_config* cfg, int32_t T,
+                                 const double* ys, const void* noise, const double* uniforms,
+                                 int32_t memspace, gf_pf_out* out, double* zmeans) {
+  return rbpf_run_impl(ctx, m, 1, cfg, T, ys, noise, uniforms, memspace, out, zmeans);
+}
+
+extern "C" gf_status gf_rbpf_run_tv(gf_ctx* ctx, const gf_rb_model* m, int32_t param_steps,
+                                    const gf_pf_config* cfg, int32_t T, const double* ys, const void* noise,
+                                    const double* uniforms, int32_t memspace, gf_pf_out* out,
+                                    double* zmeans) {
+  return rbpf_run_impl(ctx, m, param_steps, cfg, T, ys, noise, uniforms, memspace, out, zmeans);
 }

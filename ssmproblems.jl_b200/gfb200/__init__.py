@@ -20,7 +20,7 @@ from .filtering import (MvNormal, ParticleDistribution, ancestors_to_offspring, 
                         smooth, smooth_batch)
 from .models import (HierarchicalSSM, HomogeneousGaussianPrior,  # noqa: F401
                      HomogeneousLinearGaussianLatentDynamics,
-                     HomogeneousLinearGaussianObservationProcess, InnerDynamics,
+                     HomogeneousLinearGaussianObservationProcess, InnerDynamics, NonHomogeneousInnerDynamics,
                      LatentDynamics, NonHomogeneousLinearGaussianLatentDynamics,
                      NonHomogeneousLinearGaussianObservationProcess, ObservationProcess,
                      StatePrior, StateSpaceModel, create_homogeneous_linear_gaussian_model,

@@ -34,6 +34,7 @@ EXPORTED = [
     "gf_kf_batch", "gf_kf_smooth", "gf_kf_batch_tv", "gf_kf_smooth_tv", "gf_kf_plan_create_tv",
     "gf_kf_plan_create", "gf_kf_plan_run", "gf_kf_plan_smooth", "gf_kf_plan_destroy",
     "gf_pf_run", "gf_pf_run_tv", "gf_pf_plan_create_tv", "gf_pf_plan_create", "gf_pf_plan_run", "gf_pf_plan_destroy", "gf_rbpf_run",
+    "gf_rbpf_run_tv",
     "gf_sample_ancestors", "gf_offspring_to_ancestors", "gf_ancestors_to_offspring",
     "gf_rng_normals", "gf_sample_ancestors_noalloc", "gf_sample_ancestors_noalloc_max_n",
     "gf_srv_create", "gf_srv_submit", "gf_srv_poll", "gf_srv_drain", "gf_srv_stats",
@@ -186,6 +187,8 @@ def load(path: str | None = None):
         "gf_pf_plan_destroy": (i32, [_vp]),
         "gf_rbpf_run": (i32, [ctxp, C.POINTER(RBModelC), C.POINTER(PFConfigC), i32, _vp, _vp,
                               _vp, i32, C.POINTER(PFOutC), _vp]),
+        "gf_rbpf_run_tv": (i32, [ctxp, C.POINTER(RBModelC), i32, C.POINTER(PFConfigC), i32, _vp, _vp,
+                                 _vp, i32, C.POINTER(PFOutC), _vp]),
         "gf_sample_ancestors": (i32, [ctxp, i32, i32, i64, _vp, _vp, _vp]),
         "gf_offspring_to_ancestors": (i32, [ctxp, i64, _vp, _vp]),
         "gf_ancestors_to_offspring": (i32, [ctxp, i64, _vp, _vp]),

@@ -296,9 +296,17 @@ def _rbpf(model, algo, ys, seed, noise, uniforms, ctx, want_anc, want_means, sch
                                            "clamps", "paths", "history", "log_weight_history")])
     nz = None if noise is None else np.ascontiguousarray(noise, dtype=np.float32)
     un = None if uniforms is None else L.f64(uniforms)
-    L.check(ctx.h, L.load().gf_rbpf_run(ctx.h, C.byref(mc), C.byref(cfg), T, L.ptr(ys),
-                                        L.ptr(nz), L.ptr(un), L.GF_MEM_HOST, C.byref(o),
-                                        L.ptr(zmeans)))
+    if model.is_time_varying():
+        ps = model.param_steps()
+        if ps < T:
+            raise ValueError(f"{ps} parameter steps for {T} observations")
+        L.check(ctx.h, L.load().gf_rbpf_run_tv(ctx.h, C.byref(mc), ps, C.byref(cfg), T, L.ptr(ys),
+                                               L.ptr(nz), L.ptr(un), L.GF_MEM_HOST, C.byref(o),
+                                               L.ptr(zmeans)))
+    else:
+        L.check(ctx.h, L.load().gf_rbpf_run(ctx.h, C.byref(mc), C.byref(cfg), T, L.ptr(ys),
+                                            L.ptr(nz), L.ptr(un), L.GF_MEM_HOST, C.byref(o),
+                                            L.ptr(zmeans)))
     S = out["states"]
     x = S[:dxo].T
     mu = S[dxo:dxo + dz].T

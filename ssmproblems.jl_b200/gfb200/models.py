@@ -187,6 +187,23 @@ class InnerDynamics(LatentDynamics):
         self.q_index = int(q_index)
 
 
+class NonHomogeneousInnerDynamics(LatentDynamics):
+    """InnerDynamics with step-dependent parameters: calc_params(inner_dyn, t) =
+    (As[t], bs[t] + Cs[t] x_{t-1}, Qs[t] exp(q_gamma x_t[q_index])) for 1-based
+    step t (models/hierarchical.jl:96-137 with a time-varying inner model)."""
+
+    def __init__(self, As, bs, Cs, Qs, q_gamma=0.0, q_index=0):
+        if not (len(As) == len(bs) == len(Cs) == len(Qs)) or len(As) < 1:
+            raise ValueError("As, bs, Cs, Qs need one entry per step")
+        self.As = [fortran64(np.atleast_2d(a)) for a in As]
+        self.bs = [f64(v).ravel() for v in bs]
+        self.Cs = [fortran64(np.atleast_2d(c).reshape(self.bs[0].size, -1)) for c in Cs]
+        self.Qs = [fortran64(np.atleast_2d(q)) for q in Qs]
+        self.A, self.b = self.As[0], self.bs[0]
+        self.q_gamma = float(q_gamma)
+        self.q_index = int(q_index)
+
+
 class HierarchicalSSM:
     """models/hierarchical.jl:4-45: outer prior + outer dynamics + inner model."""
 
@@ -194,33 +211,62 @@ class HierarchicalSSM:
         self.outer_prior, self.outer_dyn = outer_prior, outer_dyn
         self.inner_model = StateSpaceModel(inner_prior, inner_dyn, obs)
 
+    _TV = (NonHomogeneousLinearGaussianLatentDynamics, NonHomogeneousInnerDynamics,
+           NonHomogeneousLinearGaussianObservationProcess)
+
+    def is_time_varying(self):
+        """Outer dynamics, inner dynamics or observations vary with t."""
+        return any(isinstance(x, self._TV) for x in (self.outer_dyn, self.inner_model.dyn,
+                                                     self.inner_model.obs))
+
+    def param_steps(self):
+        """Per-step parameter blocks the model carries (1 if homogeneous)."""
+        n = [len(getattr(x, a)) for x, a in ((self.outer_dyn, "As"), (self.inner_model.dyn, "As"),
+                                             (self.inner_model.obs, "Hs")) if hasattr(x, a)]
+        return min(n) if n else 1
+
     def _c_struct(self):
+        """gf_rb_model view; for a time-varying model the step parameters hold
+        param_steps() step-major blocks (each column-major)."""
         import ctypes as C
         op, od = self.outer_prior, self.outer_dyn
         ip, idyn, ob = self.inner_model.prior, self.inner_model.dyn, self.inner_model.obs
-        if not (isinstance(op, HomogeneousGaussianPrior)
-                and isinstance(od, HomogeneousLinearGaussianLatentDynamics)
-                and isinstance(ip, HomogeneousGaussianPrior)
-                and isinstance(ob, HomogeneousLinearGaussianObservationProcess)):
+        lgd = (HomogeneousLinearGaussianLatentDynamics, NonHomogeneousLinearGaussianLatentDynamics)
+        lgo = (HomogeneousLinearGaussianObservationProcess, NonHomogeneousLinearGaussianObservationProcess)
+        if not (isinstance(op, HomogeneousGaussianPrior) and isinstance(od, lgd)
+                and isinstance(ip, HomogeneousGaussianPrior) and isinstance(ob, lgo)):
             raise TypeError("RBPF on the GPU needs Gaussian priors, LG outer dynamics and LG obs")
+        dxo = od.A.shape[0]
         if isinstance(idyn, HomogeneousLinearGaussianLatentDynamics):
-            idyn = InnerDynamics(idyn.A, idyn.b, np.zeros((idyn.b.size, od.b.size)), idyn.Q)
-        arrs = [op.mu0, op.Sigma0, od.A, od.b, od.Q, ip.mu0, ip.Sigma0, idyn.A, idyn.b, idyn.C,
-                idyn.Q, ob.H, ob.c, ob.R]
+            idyn = InnerDynamics(idyn.A, idyn.b, np.zeros((idyn.b.size, dxo)), idyn.Q)
+        elif isinstance(idyn, NonHomogeneousLinearGaussianLatentDynamics):
+            idyn = NonHomogeneousInnerDynamics(idyn.As, idyn.bs, [np.zeros((idyn.bs[0].size, dxo))] *
+                                               len(idyn.As), idyn.Qs)
+        n = self.param_steps()
+
+        def stk(x, seq, one):  # the step parameter: n stacked blocks, or the single one
+            if not self.is_time_varying():
+                return getattr(x, one)
+            blocks = getattr(x, seq)[:n] if hasattr(x, seq) else [getattr(x, one)] * n
+            return np.concatenate([np.asarray(b, np.float64).ravel(order="F") for b in blocks])
+
+        arrs = [op.mu0, op.Sigma0, stk(od, "As", "A"), stk(od, "bs", "b"), stk(od, "Qs", "Q"),
+                ip.mu0, ip.Sigma0, stk(idyn, "As", "A"), stk(idyn, "bs", "b"), stk(idyn, "Cs", "C"),
+                stk(idyn, "Qs", "Q"), stk(ob, "Hs", "H"), stk(ob, "cs", "c"), stk(ob, "Rs", "R")]
         self._keep = arrs
         dp = C.POINTER(C.c_double)
         P = [a.ctypes.data_as(dp) for a in arrs]
-        return RBModelC(od.b.size, idyn.b.size, ob.c.size, *P[:11], idyn.q_gamma, idyn.q_index,
+        return RBModelC(dxo, idyn.b.size, ob.H.shape[0], *P[:11], idyn.q_gamma, idyn.q_index,
                         *P[11:])
 
     @property
     def dxo(self):
-        return self.outer_dyn.b.size
+        return self.outer_dyn.A.shape[0]
 
     @property
     def dz(self):
-        return self.inner_model.dyn.b.size
+        return self.inner_model.dyn.A.shape[0]
 
     @property
     def dy(self):
-        return self.inner_model.obs.c.size
+        return self.inner_model.obs.H.shape[0]

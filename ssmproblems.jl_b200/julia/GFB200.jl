@@ -402,18 +402,32 @@ function _rbpf(rng, model, algo, observations, lookahead::Int32; callback=nothin
     N, T = pf.N, length(observations)
     mat(x) = Matrix{Float64}(x isa AbstractVector ? reshape(x, :, 1) : Matrix(x))
     μo, Σo = GeneralisedFilters.calc_initial(model.outer_prior)
-    Ao, bo, Qo = GeneralisedFilters.calc_params(model.outer_dyn, 1)
     μz, Σz = GeneralisedFilters.calc_initial(GeneralisedFilters.inner_prior(model))
     idyn = GeneralisedFilters.inner_dyn(model)
-    Az, bz, Cz, Qz = if idyn isa InnerDynamics
-        idyn.A, idyn.b, idyn.C, idyn.Q
-    else
-        A_, b_, Q_ = GeneralisedFilters.calc_params(idyn, 1)
-        A_, b_, zeros(size(A_, 1), length(μo)), Q_
+    odyn, obs = model.outer_dyn, SSMProblems.obs(model)
+    # step t's parameters (calc_params(., t)); a model that is not of the
+    # homogeneous types runs time-varying, one block per step (gf_rbpf_run_tv)
+    function step_params(t)
+        Ao, bo, Qo = GeneralisedFilters.calc_params(odyn, t)
+        Az, bz, Cz, Qz = if idyn isa InnerDynamics
+            idyn.A, idyn.b, idyn.C, idyn.Q
+        else
+            A_, b_, Q_ = GeneralisedFilters.calc_params(idyn, t)
+            A_, b_, zeros(size(A_, 1), length(μo)), Q_
+        end
+        H, c, R = GeneralisedFilters.calc_params(obs, t)
+        return map(mat, (Ao, bo, Qo, Az, bz, Cz, Qz, H, c, R))
     end
-    H, c, R = GeneralisedFilters.calc_params(SSMProblems.obs(model), 1)
-    arrs = map(mat, (μo, Σo, Ao, bo, Qo, μz, Σz, Az, bz, Cz, Qz, H, c, R))
-    dxo, dz, dy = size(arrs[3], 1), size(arrs[8], 1), size(arrs[12], 1)
+    homog = odyn isa GeneralisedFilters.HomogeneousLinearGaussianLatentDynamics &&
+            (idyn isa InnerDynamics || idyn isa GeneralisedFilters.HomogeneousLinearGaussianLatentDynamics) &&
+            obs isa GeneralisedFilters.HomogeneousLinearGaussianObservationProcess
+    psteps = homog ? 1 : T
+    blocks = [step_params(t) for t in 1:psteps]
+    stk(k) = reduce(vcat, [vec(b[k]) for b in blocks])  # step-major, each column-major
+    sp = ntuple(stk, 10)
+    arrs = (mat(μo), mat(Σo), sp[1], sp[2], sp[3], mat(μz), mat(Σz), sp[4], sp[5], sp[6], sp[7], sp[8],
+            sp[9], sp[10])
+    dxo, dz, dy = size(blocks[1][1], 1), size(blocks[1][4], 1), size(blocks[1][8], 1)
     ys = reduce(vcat, [Float64.(collect(y)) for y in observations])
     cfg = Ref(GfPfConfig(N, resampler_code(pf.resampler.resampler), 0, pf.resampler.threshold,
                          GF_PREC_F32, GF_PROP_BOOTSTRAP, 1.0, rand(rng, UInt64), C_NULL, lookahead))
@@ -427,10 +441,11 @@ function _rbpf(rng, model, algo, observations, lookahead::Int32; callback=nothin
                           Int32(q_scale[2] - 1), p[12:14]...))
         out = Ref(GfPfOut(pointer(ll), C_NULL, C_NULL, C_NULL, C_NULL, C_NULL,
                           Ptr{Cvoid}(pointer(states)), pointer(logw), C_NULL, C_NULL, C_NULL, C_NULL))
-        check(ccall((:gf_rbpf_run, libgfb200), Int32,
-                    (Ptr{Cvoid}, Ref{GfRbModel}, Ref{GfPfConfig}, Int32, Ptr{Float64}, Ptr{Cvoid},
+        check(ccall((:gf_rbpf_run_tv, libgfb200), Int32,
+                    (Ptr{Cvoid}, Ref{GfRbModel}, Int32, Ref{GfPfConfig}, Int32, Ptr{Float64}, Ptr{Cvoid},
                      Ptr{Float64}, Int32, Ref{GfPfOut}, Ptr{Float64}),
-                    context(), m, cfg, Int32(T), ys, C_NULL, C_NULL, GF_MEM_HOST, out, C_NULL))
+                    context(), m, Int32(psteps), cfg, Int32(T), ys, C_NULL, C_NULL, GF_MEM_HOST, out,
+                    C_NULL))
     end
     particles = map(1:N) do i
         x = Vector{Float64}(states[i, 1:dxo])

@@ -63,6 +63,37 @@ def dummy_rb_model(rng, d_outer=1, d_inner=1, dy=1):
     return full, hier
 
 
+def tv_rb_oracle_pair(rng, T, d_outer=1, d_inner=1, dy=1):
+    """A time-varying hierarchical model built from T GFTest dummy models sharing
+    the first one's prior: (joint TV LGModel, TV RBModel), both oracle models."""
+    pairs = [dummy_rb_model(rng, d_outer, d_inner, dy) for _ in range(T)]
+    fulls = [to_oracle(f) for f, _ in pairs]
+    rbs = [to_oracle_rb(h) for _, h in pairs]
+    f0, r0 = fulls[0], rbs[0]
+    joint = O.LGModel.time_varying(f0.mu0, f0.Sigma0, *[[getattr(f, n) for f in fulls]
+                                                         for n in ("A", "b", "Q", "H", "c", "R")])
+    steps = [{n: getattr(r, n) for n in O.RBModel.STEP_NAMES} for r in rbs]
+    rb = O.RBModel.time_varying(r0.mu_o, r0.Sigma_o, r0.mu_z, r0.Sigma_z, steps)
+    return joint, rb
+
+
+def tv_rb_model(rb):
+    """The gfb200 HierarchicalSSM of a time-varying oracle RBModel."""
+    from gfb200 import (HierarchicalSSM, HomogeneousGaussianPrior, NonHomogeneousInnerDynamics,
+                        NonHomogeneousLinearGaussianLatentDynamics,
+                        NonHomogeneousLinearGaussianObservationProcess)
+    st = rb.steps
+    return HierarchicalSSM(
+        HomogeneousGaussianPrior(rb.mu_o, rb.Sigma_o),
+        NonHomogeneousLinearGaussianLatentDynamics([k.A_o for k in st], [k.b_o for k in st],
+                                                   [k.Q_o for k in st]),
+        HomogeneousGaussianPrior(rb.mu_z, rb.Sigma_z),
+        NonHomogeneousInnerDynamics([k.A_z for k in st], [k.b_z for k in st], [k.C_z for k in st],
+                                    [k.Q_z for k in st], rb.q_gamma, rb.q_index),
+        NonHomogeneousLinearGaussianObservationProcess([k.H for k in st], [k.c for k in st],
+                                                       [k.R for k in st]))
+
+
 def simulate(rng, m, T):
     return W.simulate_lg(rng, m, T)
 

@@ -163,3 +163,48 @@ def test_auxiliary_rbpf_without_resampling_is_the_rbpf(ctx):
                       ctx=ctx)
     assert l0 == l1
     np.testing.assert_array_equal(s0.particles["x"], s1.particles["x"])
+
+
+@pytest.mark.parametrize("apf", [False, True])
+def test_nonhomogeneous_rbpf_matches_oracle(ctx, apf):
+    """A time-varying hierarchical model (every outer, inner and observation
+    parameter of step t its own): the FP32 bank against the FP64 oracle on the
+    same injected noise and uniforms, resampling at steps 1 and 4 (plain RBPF and
+    AuxiliaryParticleFilter(RBPF, MeanPredictive())).  Bars as the homogeneous
+    parity test."""
+    from helpers import ancestors_match, tv_rb_model, tv_rb_oracle_pair
+    rng = np.random.default_rng(41 + apf)
+    T, N = 8, 2048
+    joint, rb = tv_rb_oracle_pair(rng, T, 2, 4, 2)
+    _, ys = O.sample(rng, joint, T)
+    hier = tv_rb_model(rb)
+    noise = rng.standard_normal((T + 1, 2, N)).astype(np.float32)
+    unif = rng.random(T)
+    sched = [1, 0, 0, 1, 0, 0, 0, 0]
+    algo = G.RBPF(G.BF(N), G.KalmanFilter())
+    if apf:
+        algo = G.APF(algo, G.MeanPredictive())
+    st, ll = G.filter(hier, algo, ys, noise=noise, uniforms=unif, schedule=sched, seed=9,
+                      want_ancestors=True, want_means=True, ctx=ctx)
+    ref = O.rbpf_run(rb, N, ys, schedule=sched, noise=noise.astype(np.float64), uniforms=unif, seed=9,
+                     want_ancestors=True, want_margins=True, lookahead=int(apf))
+    bad, boundary = ancestors_match(st.ancestors, ref["ancestors"], ref["margins"], 1e-6)
+    print(f"time-varying RBPF (apf={apf}): ancestor boundary cases {boundary}")
+    assert bad == 0
+    np.testing.assert_allclose(st.ll_steps, ref["ll_steps"], rtol=1e-4, atol=1e-4)
+    np.testing.assert_allclose(st.means, ref["means"], rtol=1e-3, atol=1e-4)
+    np.testing.assert_allclose(st.zmeans, ref["zmeans"], rtol=1e-3, atol=1e-4)
+
+
+def test_nonhomogeneous_rbpf_converges_to_kf(ctx):
+    """N = 2^22 on a time-varying hierarchical model that is jointly linear-Gaussian:
+    the log-evidence within the reference's 1e-3 of the joint time-varying KF."""
+    from helpers import tv_rb_model, tv_rb_oracle_pair
+    rng = np.random.default_rng(1234)
+    T = 4
+    joint, rb = tv_rb_oracle_pair(rng, T, 1, 1, 1)
+    _, ys = O.sample(rng, joint, T)
+    algo = G.RBPF(G.BF(2**22, resampler=G.AlternatingResampler()), G.KalmanFilter())
+    st, ll = G.filter(tv_rb_model(rb), algo, ys, seed=31, ctx=ctx)
+    assert abs(ll - O.kf_filter(joint, ys)[0]) <= 1e-3
+

@@ -454,3 +454,30 @@ def test_rbpf_apf_oracle_converges_to_kf(lookahead):
                    threads=4)
     assert r["resampled"].all()
     assert abs(r["ll"] - kll) < 2e-3
+
+
+@pytest.mark.parametrize("lookahead", [0, 1])
+def test_nonhomogeneous_rbpf_oracle_converges_to_kf(lookahead):
+    """An RBPF on a time-varying hierarchical model (every outer, inner and
+    observation parameter of step t its own, calc_params(., t)) uses step t's
+    parameters: its log-evidence converges to the exact Kalman filter of the
+    time-varying joint model, plain and auxiliary."""
+    _, _, _ = _rb_helpers()
+    from helpers import tv_rb_oracle_pair
+    rng = np.random.default_rng(321)
+    T = 5
+    joint, rb = tv_rb_oracle_pair(rng, T, 1, 2, 1)
+    _, ys = O.sample(rng, joint, T)
+    kll = O.kf_filter(joint, ys)[0]
+    runs = [O.rbpf_run(rb, 100_000, ys, threshold=1.0, seed=s, lookahead=lookahead, threads=4)
+            for s in (3, 4)]
+    assert all(r["resampled"][1:].all() for r in runs)
+    # Monte-Carlo SD of one run's ll here is about 3e-3
+    assert abs(np.mean([r["ll"] for r in runs]) - kll) < 6e-3
+    # a homogeneous model written as per-step copies runs as the homogeneous one
+    h = O.RBModel.time_varying(rb.mu_o, rb.Sigma_o, rb.mu_z, rb.Sigma_z,
+                               [{n: getattr(rb.steps[0], n) for n in O.RBModel.STEP_NAMES}] * T)
+    a = O.rbpf_run(h, 500, ys, threshold=0.5, seed=4)
+    b = O.rbpf_run(rb.steps[0], 500, ys, threshold=0.5, seed=4)
+    assert a["ll"] == b["ll"]
+
