@@ -433,6 +433,15 @@ gf_status gf_csmc_run(gf_ctx* ctx, const gf_lg_model* model, const gf_csmc_confi
                       const double* ys, int32_t chains, int32_t iters, int32_t burnin,
                       int32_t ref_given, const double* noise, const double* uniforms,
                       int32_t memspace, gf_csmc_out* out);
+/* The same for a time-varying model: param_steps = 1 is gf_csmc_run;
+ * param_steps >= T means A, b, Q, H, c, R each hold param_steps per-step blocks
+ * (block t-1 = calc_params(., t), column-major).  Ancestor sampling at step t
+ * and the backward-simulation weight from x_{t-1} to x_t use step t's
+ * transition. */
+gf_status gf_csmc_run_tv(gf_ctx* ctx, const gf_lg_model* model, int32_t param_steps,
+                         const gf_csmc_config* cfg, int32_t T, const double* ys, int32_t chains,
+                         int32_t iters, int32_t burnin, int32_t ref_given, const double* noise,
+                         const double* uniforms, int32_t memspace, gf_csmc_out* out);
 int32_t gf_csmc_max_particles(void);
 
 /* ------------------------------------------------------------------ serving */

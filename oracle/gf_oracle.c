@@ -1416,17 +1416,26 @@ int or_csmc_run(const or_lg_model* m, int N, double threshold, int resampler, in
                 const double* noise, const double* uniforms, uint64_t seed, double* ref,
                 double* traj_out, double* ll_out) {
   const int dx = m->dx, dy = m->dy;
-  double *LQ = calloc((size_t)dx * dx, 8), *LR = calloc((size_t)dy * dy, 8), *L0 = calloc((size_t)dx * dx, 8);
-  int st = OR_OK;
-  if ((st = or_chol_lower(dx, m->Q, LQ)) || (st = or_chol_lower(dy, m->R, LR)) ||
-      (st = or_chol_lower(dx, m->Sigma0, L0))) {
-    free(LQ); free(LR); free(L0);
+  /* factors of every step's model (time-varying: calc_params(., t) for t = 1..T) */
+  const int nb = m->tv ? T : 1;
+  double *LQs = calloc((size_t)nb * dx * dx, 8), *LRs = calloc((size_t)nb * dy * dy, 8);
+  double *tcs = calloc(nb, 8), *ocs = calloc(nb, 8), *L0 = calloc((size_t)dx * dx, 8);
+  int st = or_chol_lower(dx, m->Sigma0, L0);
+  for (int k = 0; k < nb && !st; ++k) {
+    const or_step_params SP = step_params(m, k);
+    double *LQk = LQs + (size_t)k * dx * dx, *LRk = LRs + (size_t)k * dy * dy;
+    if ((st = or_chol_lower(dx, SP.Q, LQk)) || (st = or_chol_lower(dy, SP.R, LRk))) break;
+    double ldq = 0.0, ldr = 0.0;
+    for (int i = 0; i < dx; ++i) ldq += log(LQk[i + i * dx]);
+    for (int i = 0; i < dy; ++i) ldr += log(LRk[i + i * dy]);
+    tcs[k] = -ldq - 0.5 * dx * LOG2PI;
+    ocs[k] = -ldr - 0.5 * dy * LOG2PI;
+  }
+  if (st) {
+    free(LQs); free(LRs); free(tcs); free(ocs); free(L0);
     return st;
   }
-  double ldq = 0.0, ldr = 0.0;
-  for (int i = 0; i < dx; ++i) ldq += log(LQ[i + i * dx]);
-  for (int i = 0; i < dy; ++i) ldr += log(LR[i + i * dy]);
-  const double trans_const = -ldq - 0.5 * dx * LOG2PI, obs_const = -ldr - 0.5 * dy * LOG2PI;
+#define CS_BLK(t) (m->tv ? (t) - 1 : 0) /* block of 1-based step t */
   const cs_rng rng = {noise, uniforms, seed, iters, T, N, dx};
   int fail = 0;
 #pragma omp parallel for num_threads(g_threads) schedule(dynamic) reduction(| : fail)
@@ -1463,9 +1472,13 @@ int or_csmc_run(const or_lg_model* m, int N, double threshold, int resampler, in
         const double lse = mx + log(s1), ess = s1 * s1 / s2;
         const int resamp = refresh == 1 || threshold * (double)N >= ess;
         int as_idx = 0;
+        /* this step's model */
+        const int kb = CS_BLK(t);
+        const or_step_params SP = step_params(m, kb);
+        const double *LQ = LQs + (size_t)kb * dx * dx, *LR = LRs + (size_t)kb * dy * dy;
         if (refresh == 1 && has_ref) {
           for (int i = 0; i < N; ++i)
-            W[i] = LWp[i] + cs_trans_logpdf(dx, m->A, m->b, LQ, trans_const, REF + (size_t)t * dx,
+            W[i] = LWp[i] + cs_trans_logpdf(dx, SP.A, SP.b, LQ, tcs[kb], REF + (size_t)t * dx,
                                             Xp + (size_t)i * dx, r);
           cs_exp_cumsum(W, N);
           as_idx = cs_draw(W, N, cs_uniform(&rng, c, it, t, N));
@@ -1499,22 +1512,22 @@ int or_csmc_run(const or_lg_model* m, int N, double threshold, int resampler, in
             memcpy(xa, Xp + (size_t)AN[i] * dx, sizeof(double) * dx);
             cs_normals(&rng, c, it, t, i, e);
             for (int rr = 0; rr < dx; ++rr) {
-              double s = m->b[rr];
-              for (int k = 0; k < dx; ++k) s += m->A[rr + k * dx] * xa[k];
+              double s = SP.b[rr];
+              for (int k = 0; k < dx; ++k) s += SP.A[rr + k * dx] * xa[k];
               for (int k = 0; k <= rr; ++k) s += LQ[rr + k * dx] * e[k];
               x[rr] = s;
             }
           }
           for (int j = 0; j < dy; ++j) {
-            double s = y[j] - m->c[j];
-            for (int k = 0; k < dx; ++k) s -= m->H[j + k * dy] * x[k];
+            double s = y[j] - SP.c[j];
+            for (int k = 0; k < dx; ++k) s -= SP.H[j + k * dy] * x[k];
             z[j] = s;
           }
           trsv_lower(dy, LR, z);
           double q = 0.0;
           for (int j = 0; j < dy; ++j) q += z[j] * z[j];
           memcpy(Xt + (size_t)i * dx, x, sizeof(double) * dx);
-          LWt[i] = LWP[i] + obs_const - 0.5 * q;
+          LWt[i] = LWP[i] + ocs[kb] - 0.5 * q;
           ANC[(size_t)(t - 1) * N + i] = AN[i];
         }
         double M = -INFINITY, s = 0.0;
@@ -1536,8 +1549,11 @@ int or_csmc_run(const or_lg_model* m, int N, double threshold, int resampler, in
       } else {
         memcpy(REF + (size_t)T * dx, X + ((size_t)T * N + k) * dx, sizeof(double) * dx);
         for (int t = T - 1; t >= 0; --t) {
+          /* the transition from x_t to x_{t+1} is step t+1's */
+          const int kb = CS_BLK(t + 1);
+          const or_step_params SP = step_params(m, kb);
           for (int i = 0; i < N; ++i)
-            W[i] = LW[(size_t)t * N + i] + cs_trans_logpdf(dx, m->A, m->b, LQ, trans_const,
+            W[i] = LW[(size_t)t * N + i] + cs_trans_logpdf(dx, SP.A, SP.b, LQs + (size_t)kb * dx * dx, tcs[kb],
                                                            REF + (size_t)(t + 1) * dx,
                                                            X + ((size_t)t * N + i) * dx, r);
           cs_exp_cumsum(W, N);
@@ -1553,6 +1569,7 @@ int or_csmc_run(const or_lg_model* m, int N, double threshold, int resampler, in
     }
     free(X); free(LW); free(ANC); free(W); free(LWP); free(AN);
   }
-  free(LQ); free(LR); free(L0);
+#undef CS_BLK
+  free(LQs); free(LRs); free(tcs); free(ocs); free(L0);
   return fail ? OR_ARG : OR_OK;
 }

@@ -35,7 +35,9 @@ struct CsmcArgs {
   int dx, dy, N, T, iters, burnin, refresh, resampler, ref_given;
   double threshold, obs_const, trans_const, log_n;
   uint64_t seed;
-  const double* P;      // A | b | LQ | LQi | Ht | mu0 | L0, column-major
+  const double* P;      // A | b | LQ | LQi | Ht | mu0 | L0, column-major (one block per step if pstride)
+  int64_t pstride;      // time-varying model: block of step t at P + (t-1) * pstride; 0: one block
+  const double* consts; // time-varying: [T][2] (transition, observation) log-normalisers; else null
   const double* yt;     // [T][dy] whitened observations L_R^{-1} (y_t - c)
   const double* noise;  // nullable [chains][iters][T+1][N][dx]
   const double* unif;   // nullable [chains][iters][T+1][N+1]
@@ -149,8 +151,9 @@ __device__ __forceinline__ void cs_exp_cumsum(double* W, int N, double* red) {
 
 // log N(xn; A x + b, Q) with Q = LQ LQ^T
 template <int DXP>
-__device__ __forceinline__ double cs_trans_logpdf(const CsmcArgs& a, const double* A, const double* b,
-                                                  const double* LQi, const double* xn, const double* x) {
+__device__ __forceinline__ double cs_trans_logpdf(const CsmcArgs& a, double trans_const, const double* A,
+                                                  const double* b, const double* LQi, const double* xn,
+                                                  const double* x) {
   const int dx = a.dx;
   double r[DXP];
 #pragma unroll
@@ -173,7 +176,7 @@ __device__ __forceinline__ double cs_trans_logpdf(const CsmcArgs& a, const doubl
       if (i < dx) z += LQi[i + k * dx] * r[k];
     q += z * z;
   }
-  return a.trans_const - 0.5 * q;
+  return trans_const - 0.5 * q;
 }
 
 // Up to dx = 4 four 256-thread chains fit on an SM (<= 64 registers).
@@ -187,7 +190,14 @@ __global__ void __launch_bounds__(256, DXP <= 4 ? 4 : 1) csmc_kernel(CsmcArgs a)
   __shared__ double sP[4 * CS_MAXD * CS_MAXD + 2 * CS_MAXD + CS_MAXD * CS_MAXD];
   __shared__ double red[33];
   const int chain = blockIdx.x, tid = threadIdx.x, bd = blockDim.x;
-  for (int e = tid; e < cs_param_count(dx, dy); e += bd) sP[e] = a.P[e];
+  // the model of step t (time-varying: block t-1; every block also holds the prior)
+  auto load_step = [&](int t) {
+    const double* src = a.P + (size_t)(t - 1) * a.pstride;
+    for (int e = tid; e < cs_param_count(dx, dy); e += bd) sP[e] = src[e];
+  };
+  auto trans_const = [&](int t) { return a.consts ? a.consts[2 * (t - 1)] : a.trans_const; };
+  auto obs_const = [&](int t) { return a.consts ? a.consts[2 * (t - 1) + 1] : a.obs_const; };
+  load_step(1);
   const double* A = sP;
   const double* b = A + dx * dx;
   const double* LQ = b + dx;
@@ -232,6 +242,11 @@ __global__ void __launch_bounds__(256, DXP <= 4 ? 4 : 1) csmc_kernel(CsmcArgs a)
     for (int t = 1; t <= T && status == 0; ++t) {
       const double* Xp = X + (size_t)(t - 1) * N * dx;
       const double* LWp = LW + (size_t)(t - 1) * N;
+      if (a.pstride) {  // step t's model (the previous step's readers are past a barrier)
+        __syncthreads();
+        load_step(t);
+        __syncthreads();
+      }
       // LSE and ESS of the weights entering the step (resamplers.jl:179-183)
       double m = -INFINITY;
       for (int i = tid; i < N; i += bd) m = fmax(m, LWp[i]);
@@ -252,7 +267,7 @@ __global__ void __launch_bounds__(256, DXP <= 4 ? 4 : 1) csmc_kernel(CsmcArgs a)
       if (a.refresh == GF_CSMC_ANCESTOR && has_ref) {
         const double* xr = REF + (size_t)t * dx;
         for (int i = tid; i < N; i += bd)
-          W[i] = LWp[i] + cs_trans_logpdf<DXP>(a, A, b, LQi, xr, Xp + (size_t)i * dx);
+          W[i] = LWp[i] + cs_trans_logpdf<DXP>(a, trans_const(t), A, b, LQi, xr, Xp + (size_t)i * dx);
         cs_exp_cumsum(W, N, red);
         as_idx = cs_draw(W, N, cs_uniform(a, chain, it, t, N), red);
       }
@@ -327,7 +342,7 @@ __global__ void __launch_bounds__(256, DXP <= 4 ? 4 : 1) csmc_kernel(CsmcArgs a)
             if (k < dx) r -= Ht[j + k * dy] * x[k];
           q += r * r;
         }
-        const double lw = LWP[i] + a.obs_const - 0.5 * q;
+        const double lw = LWP[i] + obs_const(t) - 0.5 * q;
 #pragma unroll
         for (int d = 0; d < DXP; ++d)
           if (d < dx) Xt[(size_t)i * dx + d] = x[d];
@@ -364,8 +379,14 @@ __global__ void __launch_bounds__(256, DXP <= 4 ? 4 : 1) csmc_kernel(CsmcArgs a)
       __syncthreads();
       for (int t = T - 1; t >= 0; --t) {
         const double* xn = REF + (size_t)(t + 1) * dx;
+        if (a.pstride) {  // the transition from x_t to x_{t+1} is step t+1's
+          __syncthreads();
+          load_step(t + 1);
+          __syncthreads();
+        }
         for (int i = tid; i < N; i += bd)
-          W[i] = LW[(size_t)t * N + i] + cs_trans_logpdf<DXP>(a, A, b, LQi, xn, X + ((size_t)t * N + i) * dx);
+          W[i] = LW[(size_t)t * N + i] +
+                 cs_trans_logpdf<DXP>(a, trans_const(t + 1), A, b, LQi, xn, X + ((size_t)t * N + i) * dx);
         cs_exp_cumsum(W, N, red);
         k = cs_draw(W, N, cs_uniform(a, chain, it, t + 1, N), red);
         if (tid < dx) REF[(size_t)t * dx + tid] = X[((size_t)t * N + k) * dx + tid];
@@ -392,10 +413,10 @@ void launch_csmc(const CsmcArgs& a, int chains, int threads, size_t smem, cudaSt
 
 extern "C" int32_t gf_csmc_max_particles(void) { return CS_MAXN; }
 
-extern "C" gf_status gf_csmc_run(gf_ctx* ctx, const gf_lg_model* m, const gf_csmc_config* cfg, int32_t T,
-                                 const double* ys, int32_t chains, int32_t iters, int32_t burnin,
-                                 int32_t ref_given, const double* noise, const double* uniforms,
-                                 int32_t memspace, gf_csmc_out* out) {
+static gf_status csmc_run_impl(gf_ctx* ctx, const gf_lg_model* m, int32_t param_steps,
+                               const gf_csmc_config* cfg, int32_t T, const double* ys, int32_t chains,
+                               int32_t iters, int32_t burnin, int32_t ref_given, const double* noise,
+                               const double* uniforms, int32_t memspace, gf_csmc_out* out) {
   if (!ctx) return GF_ERR_ARG;
   if (!m || !cfg || !ys || !out || !out->ref) return set_err(ctx, GF_ERR_ARG, "null argument");
   const int dx = m->dx, dy = m->dy, N = cfg->N;
@@ -414,23 +435,13 @@ extern "C" gf_status gf_csmc_run(gf_ctx* ctx, const gf_lg_model* m, const gf_csm
   cudaSetDevice(ctx->device);
   cudaStream_t s = ctx->stream;
 
-  // model factors (FP64, host)
-  std::vector<double> LQ(dx * dx), LQi(dx * dx), LR(dy * dy), LRi(dy * dy), L0(dx * dx), Ht(dy * dx);
-  if (chol_lower(dx, m->Q, LQ.data())) return set_err(ctx, GF_ERR_NOT_PD, "Q is not positive definite");
-  if (chol_lower(dy, m->R, LR.data())) return set_err(ctx, GF_ERR_NOT_PD, "R is not positive definite");
+  const bool tv = param_steps != 1;
+  if (tv && param_steps < T) return set_err(ctx, GF_ERR_ARG, "%d parameter steps for T = %d", param_steps, T);
+  const int nblk = tv ? T : 1;
+  // model factors (FP64, host), one block per step of a time-varying model
+  // (calc_params(dyn, t), calc_params(obs, t)); each block repeats the prior
+  std::vector<double> L0(dx * dx);
   if (chol_lower(dx, m->Sigma0, L0.data())) return set_err(ctx, GF_ERR_NOT_PD, "Sigma0 is not positive definite");
-  tri_inv_lower(dx, LQ.data(), LQi.data());
-  tri_inv_lower(dy, LR.data(), LRi.data());
-  matmul(dy, dy, dx, LRi.data(), m->H, Ht.data());
-  std::vector<double> P;
-  P.reserve(cs_param_count(dx, dy));
-  P.insert(P.end(), m->A, m->A + dx * dx);
-  P.insert(P.end(), m->b, m->b + dx);
-  P.insert(P.end(), LQ.begin(), LQ.end());
-  P.insert(P.end(), LQi.begin(), LQi.end());
-  P.insert(P.end(), Ht.begin(), Ht.end());
-  P.insert(P.end(), m->mu0, m->mu0 + dx);
-  P.insert(P.end(), L0.begin(), L0.end());
   std::vector<double> yh((size_t)T * dy), yt((size_t)T * dy);
   if (memspace == GF_MEM_DEVICE) {
     GF_CHECK_CUDA(ctx, cudaMemcpyAsync(yh.data(), ys, sizeof(double) * yh.size(), cudaMemcpyDeviceToHost, s));
@@ -438,15 +449,41 @@ extern "C" gf_status gf_csmc_run(gf_ctx* ctx, const gf_lg_model* m, const gf_csm
   } else {
     std::copy(ys, ys + yh.size(), yh.begin());
   }
-  for (int t = 0; t < T; ++t)
-    for (int k = 0; k < dy; ++k) {
-      double v = 0.0;
-      for (int j = 0; j <= k; ++j) v += LRi[k + j * dy] * (yh[(size_t)t * dy + j] - m->c[j]);
-      yt[(size_t)t * dy + k] = v;
-    }
+  std::vector<double> P, consts;
+  P.reserve((size_t)nblk * cs_param_count(dx, dy));
   double ldr = 0.0, ldq = 0.0;
-  for (int i = 0; i < dy; ++i) ldr += std::log(LR[i + i * dy]);
-  for (int i = 0; i < dx; ++i) ldq += std::log(LQ[i + i * dx]);
+  for (int k = 0; k < nblk; ++k) {
+    const double *mA = m->A + (size_t)k * dx * dx, *mb = m->b + (size_t)k * dx, *mQ = m->Q + (size_t)k * dx * dx;
+    const double *mH = m->H + (size_t)k * dy * dx, *mc = m->c + (size_t)k * dy, *mR = m->R + (size_t)k * dy * dy;
+    std::vector<double> LQ(dx * dx), LQi(dx * dx), LR(dy * dy), LRi(dy * dy), Ht(dy * dx);
+    if (chol_lower(dx, mQ, LQ.data())) return set_err(ctx, GF_ERR_NOT_PD, "Q of step %d is not positive definite", k + 1);
+    if (chol_lower(dy, mR, LR.data())) return set_err(ctx, GF_ERR_NOT_PD, "R of step %d is not positive definite", k + 1);
+    tri_inv_lower(dx, LQ.data(), LQi.data());
+    tri_inv_lower(dy, LR.data(), LRi.data());
+    matmul(dy, dy, dx, LRi.data(), mH, Ht.data());
+    P.insert(P.end(), mA, mA + dx * dx);
+    P.insert(P.end(), mb, mb + dx);
+    P.insert(P.end(), LQ.begin(), LQ.end());
+    P.insert(P.end(), LQi.begin(), LQi.end());
+    P.insert(P.end(), Ht.begin(), Ht.end());
+    P.insert(P.end(), m->mu0, m->mu0 + dx);
+    P.insert(P.end(), L0.begin(), L0.end());
+    // whitened observations of the steps this block serves
+    for (int t = (tv ? k : 0); t < (tv ? k + 1 : T); ++t)
+      for (int r = 0; r < dy; ++r) {
+        double v = 0.0;
+        for (int j = 0; j <= r; ++j) v += LRi[r + j * dy] * (yh[(size_t)t * dy + j] - mc[j]);
+        yt[(size_t)t * dy + r] = v;
+      }
+    ldr = 0.0;
+    ldq = 0.0;
+    for (int i = 0; i < dy; ++i) ldr += std::log(LR[i + i * dy]);
+    for (int i = 0; i < dx; ++i) ldq += std::log(LQ[i + i * dx]);
+    if (tv) {
+      consts.push_back(-ldq - 0.5 * dx * GF_LOG2PI);
+      consts.push_back(-ldr - 0.5 * dy * GF_LOG2PI);
+    }
+  }
 
   // device buffers
   std::vector<DevBuf> bufs;
@@ -468,7 +505,8 @@ extern "C" gf_status gf_csmc_run(gf_ctx* ctx, const gf_lg_model* m, const gf_csm
   const size_t nz = sizeof(double) * chains * (size_t)iters * steps * N * dx;
   const size_t nu = sizeof(double) * chains * (size_t)iters * steps * (N + 1);
   gf_status st;
-  void *dP, *dyt, *dX, *dLW, *dANC;
+  void *dP, *dyt, *dX, *dLW, *dANC, *dC = nullptr;
+  if (tv && (st = get(sizeof(double) * consts.size(), &dC))) return st;
   if ((st = get(sizeof(double) * P.size(), &dP)) || (st = get(sizeof(double) * yt.size(), &dyt)) ||
       (st = get(sizeof(double) * chains * steps * N * dx, &dX)) ||
       (st = get(sizeof(double) * chains * steps * N, &dLW)) ||
@@ -476,7 +514,10 @@ extern "C" gf_status gf_csmc_run(gf_ctx* ctx, const gf_lg_model* m, const gf_csm
     return st;
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(dP, P.data(), sizeof(double) * P.size(), cudaMemcpyHostToDevice, s));
   GF_CHECK_CUDA(ctx, cudaMemcpyAsync(dyt, yt.data(), sizeof(double) * yt.size(), cudaMemcpyHostToDevice, s));
+  if (dC) GF_CHECK_CUDA(ctx, cudaMemcpyAsync(dC, consts.data(), sizeof(double) * consts.size(), cudaMemcpyHostToDevice, s));
   CsmcArgs a{};
+  a.pstride = tv ? cs_param_count(dx, dy) : 0;
+  a.consts = (const double*)dC;
   a.dx = dx;
   a.dy = dy;
   a.N = N;
@@ -563,3 +604,20 @@ extern "C" gf_status gf_csmc_run(gf_ctx* ctx, const gf_lg_model* m, const gf_csm
 }
 
 }  // namespace gf
+
+using namespace gf;
+
+extern "C" gf_status gf_csmc_run(gf_ctx* ctx, const gf_lg_model* m, const gf_csmc_config* cfg, int32_t T,
+                                 const double* ys, int32_t chains, int32_t iters, int32_t burnin,
+                                 int32_t ref_given, const double* noise, const double* uniforms,
+                                 int32_t memspace, gf_csmc_out* out) {
+  return csmc_run_impl(ctx, m, 1, cfg, T, ys, chains, iters, burnin, ref_given, noise, uniforms, memspace, out);
+}
+
+extern "C" gf_status gf_csmc_run_tv(gf_ctx* ctx, const gf_lg_model* m, int32_t param_steps,
+                                    const gf_csmc_config* cfg, int32_t T, const double* ys, int32_t chains,
+                                    int32_t iters, int32_t burnin, int32_t ref_given, const double* noise,
+                                    const double* uniforms, int32_t memspace, gf_csmc_out* out) {
+  return csmc_run_impl(ctx, m, param_steps, cfg, T, ys, chains, iters, burnin, ref_given, noise, uniforms,
+                       memspace, out);
+}

@@ -39,7 +39,7 @@ EXPORTED = [
     "gf_rng_normals", "gf_sample_ancestors_noalloc", "gf_sample_ancestors_noalloc_max_n",
     "gf_srv_create", "gf_srv_submit", "gf_srv_poll", "gf_srv_drain", "gf_srv_stats",
     "gf_srv_reset_stats", "gf_srv_last_error", "gf_srv_destroy",
-    "gf_csmc_run", "gf_csmc_max_particles", "gf_pf_dense_ancestry", "gf_kf_loglikelihood_grad",
+    "gf_csmc_run", "gf_csmc_run_tv", "gf_csmc_max_particles", "gf_pf_dense_ancestry", "gf_kf_loglikelihood_grad",
     "gf_kf_backward_information", "gf_kf_backward_information_tv",
 ]
 
@@ -204,6 +204,8 @@ def load(path: str | None = None):
         "gf_srv_last_error": (C.c_char_p, [_vp]),
         "gf_srv_destroy": (i32, [_vp]),
         "gf_csmc_run": (i32, [ctxp, C.POINTER(LGModelC), C.POINTER(CsmcConfigC), i32, _vp, i32,
+                              i32, i32, i32, _vp, _vp, i32, C.POINTER(CsmcOutC)]),
+        "gf_csmc_run_tv": (i32, [ctxp, C.POINTER(LGModelC), i32, C.POINTER(CsmcConfigC), i32, _vp, i32,
                               i32, i32, i32, _vp, _vp, i32, C.POINTER(CsmcOutC)]),
         "gf_csmc_max_particles": (i32, []),
         "gf_pf_dense_ancestry": (i32, [ctxp, i32, i64, i32, i32, _vp, _vp, i64, _vp, i32, _vp]),

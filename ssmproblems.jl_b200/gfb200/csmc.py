@@ -93,9 +93,15 @@ def _run(ssm, csmc: ConditionalSMC, observations, *, chains, iters, burnin, ref,
     if un is not None and un.size != chains * iters * (T + 1) * (csmc.pf.N + 1):
         raise ValueError("uniforms must hold [chains][iters][T+1][N+1] values")
     out = L.CsmcOutC(L.ptr(trajs), L.ptr(lls), L.ptr(refs), L.ptr(status))
-    L.check(ctx.h, L.load().gf_csmc_run(ctx.h, C.byref(ssm._c_struct()), C.byref(cfg), T, L.ptr(ys),
-                                        chains, iters, burnin, int(ref is not None), L.ptr(nz),
-                                        L.ptr(un), L.GF_MEM_HOST, C.byref(out)))
+    mc = ssm._c_struct()
+    rest = (chains, iters, burnin, int(ref is not None), L.ptr(nz), L.ptr(un), L.GF_MEM_HOST, C.byref(out))
+    if ssm.is_time_varying():
+        ps = ssm.param_steps()
+        if ps < T:
+            raise ValueError(f"{ps} parameter steps for {T} observations")
+        L.check(ctx.h, L.load().gf_csmc_run_tv(ctx.h, C.byref(mc), ps, C.byref(cfg), T, L.ptr(ys), *rest))
+    else:
+        L.check(ctx.h, L.load().gf_csmc_run(ctx.h, C.byref(mc), C.byref(cfg), T, L.ptr(ys), *rest))
     return trajs, lls, refs
 
 

@@ -126,3 +126,29 @@ def test_csmc_single_sweep_and_errors(ctx):
     _, ys17 = simulate(rng, wide, 3)
     with pytest.raises(G.GFError):
         CS._csmc_sample(wide, csmc, ys17, None, ctx=ctx)
+
+
+@pytest.mark.parametrize("refresh", list(REFRESH))
+def test_nonhomogeneous_csmc_matches_oracle(ctx, refresh):
+    """A time-varying model: every step's transition (in the propagation, the
+    ancestor-sampling and the backward-simulation weights) and observation model
+    are that step's; GPU = FP64 oracle on the same injected randomness."""
+    rng = np.random.default_rng(300 + len(refresh))
+    T, N, chains, iters, burnin, dx, dy = 9, 17, 3, 5, 1, 3, 2
+    om = O.create_nonhomogeneous_linear_gaussian_model(rng, dx, dy, T)
+    As = [O.random_orthogonal(rng, dx) * rng.uniform(0.5, 0.95) for _ in range(T)]
+    om = O.LGModel.time_varying(om.mu0, om.Sigma0, As, om.bs, om.Qs, om.Hs, om.cs, om.Rs)
+    gm = G.create_nonhomogeneous_linear_gaussian_model(om.mu0, om.Sigma0, om.As, om.bs, om.Qs, om.Hs,
+                                                       om.cs, om.Rs)
+    _, ys = O.sample(rng, om, T)
+    noise, unif = _inputs(rng, chains, iters, T, N, dx)
+    ref0 = rng.standard_normal((chains, T + 1, dx)) if refresh != "backward" else None
+    csmc = G.ConditionalSMC(G.BF(N, threshold=0.6, resampler=G.Stratified()), REFRESH[refresh])
+    tr, lls, last = CS.sample(G.CSMCModel(gm, ys), csmc, iters - burnin, burnin=burnin, chains=chains,
+                              initial=ref0, noise=noise, uniforms=unif, ctx=ctx)
+    otr, olls, olast = O.csmc_run(om, N, ys, threshold=0.6, resampler=O.STRATIFIED,
+                                  refresh=REFRESH[refresh].kind, chains=chains, iters=iters,
+                                  burnin=burnin, ref=ref0, noise=noise, uniforms=unif)
+    np.testing.assert_allclose(tr, otr, rtol=1e-9, atol=1e-9)
+    np.testing.assert_allclose(lls, olls, rtol=1e-9, atol=1e-9)
+    np.testing.assert_allclose(last, olast, rtol=1e-9, atol=1e-9)

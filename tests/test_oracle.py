@@ -109,6 +109,24 @@ def test_csmc_oracle_targets_the_smoothing_distribution(refresh):
     np.testing.assert_allclose(l.max() + np.log(np.mean(np.exp(l - l.max()))), -kf_ll, rtol=1e-3)
 
 
+@pytest.mark.parametrize("refresh", [O.CSMC_ANCESTOR, O.CSMC_BACKWARD])
+def test_nonhomogeneous_csmc_oracle_targets_the_smoothing_distribution(refresh):
+    """CSMC on a time-varying model: each step's transition (also in the ancestor
+    and backward-simulation weights) and observation model are that step's, so the
+    sampled trajectories' mean matches the time-varying RTS smoother."""
+    rng = np.random.default_rng(77)
+    T = 8
+    m = O.create_nonhomogeneous_linear_gaussian_model(rng, 1, 1, T)
+    m = O.LGModel.time_varying(m.mu0, m.Sigma0, [np.array([[rng.uniform(0.5, 0.95)]]) for _ in range(T)],
+                               m.bs, m.Qs, m.Hs, m.cs, m.Rs)
+    _, ys = O.sample(rng, m, T)
+    _, mus, _ = O.rts_smooth(m, ys)
+    tr, _, _ = O.csmc_run(m, 10, ys, threshold=0.6, resampler=O.MULTINOMIAL, refresh=refresh,
+                          chains=64, iters=1600, burnin=100, seed=5 + refresh, threads=4)
+    for t in (1, 4, 7):
+        np.testing.assert_allclose(tr[:, :, t + 1, 0].mean(), mus[t, 0], rtol=1e-2, atol=5e-3)
+
+
 def test_csmc_oracle_pins_reference_particle():
     """With NoRefreshment and threshold 0 (no resampling) every particle keeps
     its own lineage, so the sampled trajectory is one particle's path and, when
