@@ -216,11 +216,68 @@ def pf_parity(ctx, model, ys, N, ll_timed, seeds=8, tf_steps=4):
     }
 
 
+def _pf_wide(args, world, rank, local):
+    """The Dx=64, Dy=32 half of the large-PF configuration: N = 2^18, T = 200,
+    FP32 state on the tensor-core propagation; graph replays timed with events,
+    the propagate per launch from eager events for its roofline."""
+    import torch
+    import gfb200 as G
+    from gfb200 import workloads as W
+    from gfb200.plans import PfPlan
+    dev = f"cuda:{local}"
+    torch.cuda.set_device(local)
+    ctx = G.Context(local)
+    N, T, dx, dy, K = 2**18, 200, 64, 32, 3
+    model, ys = W.lgssm_rot(seed=64, dx=dx, dy=dy, T=T)
+    algo = G.BF(N, threshold=0.5)
+    ys_dev = torch.tensor(ys, dtype=torch.float64, device=dev)
+    plan = PfPlan(model, algo, T, seed=3 + rank, ctx=ctx, graph=True)
+    for _ in range(3):
+        plan.run(ys_dev)
+    ctx.synchronize()
+    ext = torch.cuda.ExternalStream(ctx.stream, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        e0.record(ext)
+        for _ in range(K):
+            plan.run(ys_dev)
+        e1.record(ext)
+        e1.synchronize()
+    ms = _max_over_ranks(e0.elapsed_time(e1), world, dev)
+    ll, n_res = float(plan.ll.item()), int(plan.resampled.sum().item())
+    plan.close()
+    eplan = PfPlan(model, algo, T, seed=3 + rank, ctx=ctx, graph=False)
+    prof = _profiled(ctx, lambda: eplan.run(ys_dev), 1, [(0, "propagate"), (1, "resample"),
+                                                         (5, "ancestor_fill")])
+    eplan.close()
+    ctx.close()
+    pms, pn = prof["propagate"]
+    avg = pms / max(pn, 1)
+    bytes_launch = N * (8 * dx + 8)
+    peak, peak_kind = _peaks()
+    return {"metric": "particle-steps/s", "value": N * T * K * world / (ms / 1e3),
+            "unit": "particle-steps/s", "ms_per_step": ms / K,
+            "config": {"workload": f"bootstrap PF, LGSSM Dx={dx} Dy={dy} (A orthogonal*0.95, Q=0.1I, "
+                                   f"H~N(0,1/{dx}), R=0.2I), N=2^18, T={T}, systematic at ESS<0.5N",
+                       "resampled_steps": n_res, "ll": ll, "precision": "FP32 state, FP64 normaliser"},
+            "roofline": {"bound": "hbm", "achieved": bytes_launch / (avg / 1e3) / 1e9, "peak": peak,
+                         "unit": "GB/s", "frac": bytes_launch / (avg / 1e3) / 1e9 / peak,
+                         "kernel": "pf_lg_propagate_tc<64,32> (tcgen05 3xTF32)", "peak_source": peak_kind,
+                         "avg_launch_ms": avg, "bytes_per_launch": bytes_launch},
+            "kernels_ms": {k: v[0] for k, v in prof.items()}, "clocks": clk.summary()}
+
+
 def _secondary(args, world, rank, local):
-    """The other halves of the metric, from the same process: the batched
-    Kalman bank (config 3) and the serving loop at stated request rates."""
+    """The other halves of the metric, from the same process: the Dx=64 half of
+    the large PF, the RBPF (config 4), the batched Kalman bank (config 3) and
+    the serving loop at stated request rates."""
     import copy
-    out = {}
+    out = {"pf_dx64": _pf_wide(args, world, rank, local)}
+    a = copy.copy(args)
+    a.steps, a.warmup, a.no_cpu_baseline = 3, 3, True
+    rb = bench_rbpf(a, world, rank, local)
+    out["rbpf"] = {k: rb[k] for k in ("metric", "value", "unit", "ms_per_step", "config", "e2e",
+                                      "roofline", "clocks")}
     a = copy.copy(args)
     a.steps, a.warmup = 2, 3
     kf = bench_kf(a, world, rank, local, accuracy_sample=32)

@@ -279,9 +279,11 @@ gf_status gf_kf_plan_destroy(gf_kf_plan* plan);
  * copy each 128-particle sub-tile's sorted ancestor range into shared memory
  * with bulk async copies, one sub-tile ahead, instead of per-thread loads),
  * UNITS (PF, tensor-core path: a grid of resident blocks striding over
- * 128-particle units instead of one block per 1024-particle tile). */
+ * 128-particle units instead of one block per 1024-particle tile; the default
+ * for Dx > 32, where it is the faster form), TILES (PF: one block per tile
+ * even where UNITS is the default). */
 enum { GF_PLAN_AUTOTUNE = 1, GF_PLAN_NO_GRAPH = 2, GF_PLAN_PLAIN = 4, GF_PLAN_SIMT = 8, GF_PLAN_NO_FUSE = 16,
-       GF_PLAN_STAGED_GATHER = 32, GF_PLAN_UNITS = 64 };
+       GF_PLAN_STAGED_GATHER = 32, GF_PLAN_UNITS = 64, GF_PLAN_TILES = 128 };
 
 /* -------------------------------------------------------- particle filters */
 /* filter(rng, model, ParticleFilter(N, proposal; threshold, resampler), ys)

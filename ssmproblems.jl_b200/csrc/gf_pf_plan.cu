@@ -180,6 +180,12 @@ static gf_status pf_plan_create_impl(gf_ctx* ctx, const gf_lg_model* m, int32_t 
                                      const gf_pf_config* cfg, int32_t T, int32_t flags, gf_pf_plan** out) {
   if (!ctx || !out) return GF_ERR_ARG;
   *out = nullptr;
+  // the unit grid is the default for the widest states (Dx > 32, FP32 bootstrap):
+  // there one tile block per SM leaves the last wave partly empty and the unit
+  // grid's separate finalise costs less than that wave
+  if (m && cfg && !(flags & (GF_PLAN_TILES | GF_PLAN_STAGED_GATHER | GF_PLAN_SIMT)) && m->dx > 32 &&
+      cfg->precision == GF_PREC_F32 && cfg->proposal == GF_PROP_BOOTSTRAP)
+    flags |= GF_PLAN_UNITS;
   LgJobSetup L;
   gf_status st = lg_job_setup(ctx, m, cfg, T, flags, &L, param_steps);
   if (st) return st;

@@ -23,7 +23,7 @@ GF_PREC_F32, GF_PREC_F64 = 0, 1
 GF_PROP_BOOTSTRAP, GF_PROP_OPTIMAL, GF_PROP_OVERDISPERSED = 0, 1, 2
 GF_ALGO_KF, GF_ALGO_SRKF = 0, 1
 GF_PLAN_AUTOTUNE, GF_PLAN_NO_GRAPH, GF_PLAN_PLAIN, GF_PLAN_SIMT, GF_PLAN_NO_FUSE = 1, 2, 4, 8, 16
-GF_PLAN_STAGED_GATHER, GF_PLAN_UNITS = 32, 64
+GF_PLAN_STAGED_GATHER, GF_PLAN_UNITS, GF_PLAN_TILES = 32, 64, 128
 GF_REQ_KF, GF_REQ_SRKF, GF_REQ_PF, GF_REQ_RBPF = 0, 1, 2, 3
 GF_CSMC_NONE, GF_CSMC_ANCESTOR, GF_CSMC_BACKWARD = 0, 1, 2
 GF_LOOKAHEAD_NONE, GF_LOOKAHEAD_MEAN, GF_LOOKAHEAD_DRAW = 0, 1, 2

@@ -16,7 +16,9 @@ from .filtering import _pf_config
 
 class PfPlan:
     def __init__(self, model, algo, T, *, seed=0, ctx=None, graph=True, want_steps=True,
-                 simt=False, fuse=True, staged_gather=False, units=False):
+                 simt=False, fuse=True, staged_gather=False, units=None):
+        """units: True = the unit-grid tensor-core propagation, False = one block per
+        tile, None = the library's default (the unit grid for Dx > 32)."""
         import torch
         self.ctx = ctx or L.default_context()
         self.model, self.algo, self.T = model, algo, int(T)
@@ -25,7 +27,8 @@ class PfPlan:
         h = C.c_void_p()
         flags = ((0 if graph else L.GF_PLAN_NO_GRAPH) | (L.GF_PLAN_SIMT if simt else 0)
                  | (0 if fuse else L.GF_PLAN_NO_FUSE)
-                 | (L.GF_PLAN_STAGED_GATHER if staged_gather else 0) | (L.GF_PLAN_UNITS if units else 0))
+                 | (L.GF_PLAN_STAGED_GATHER if staged_gather else 0) | (L.GF_PLAN_UNITS if units else 0)
+                 | (L.GF_PLAN_TILES if units is False else 0))
         L.check(self.ctx.h, L.load().gf_pf_plan_create(self.ctx.h, C.byref(self._mc),
                                                        C.byref(self._cfg), self.T, flags,
                                                        C.byref(h)))

@@ -320,7 +320,8 @@ def test_staged_gather_equals_per_thread_gather(ctx, kind, N, threshold):
         assert out[True][3].sum() >= 3
 
 
-@pytest.mark.parametrize("dims,N", [((16, 8), 5000), ((16, 16), 2 ** 16 + 77), ((32, 16), 3000)])
+@pytest.mark.parametrize("dims,N", [((16, 8), 5000), ((16, 16), 2 ** 16 + 77), ((32, 16), 3000),
+                                    ((64, 32), 2 ** 14 + 5)])
 def test_unit_grid_propagation_matches_tile_blocks(ctx, dims, N):
     """The unit-grid tensor-core propagation (resident blocks striding over
     128-particle units, one log-sum-exp partial per unit) computes the same MMA
