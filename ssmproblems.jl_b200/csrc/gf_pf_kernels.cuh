@@ -325,20 +325,42 @@ static __device__ void global_stats(const S& g, const PfJob& J, int nparts, doub
   const int nall = J.ntiles * nparts;
   const size_t ps = part_stride(J);
   const double* __restrict__ part = J.part;
+  // each thread's partials are read in batches of independent loads (one L2
+  // round trip per batch, not per partial); the per-thread order of the sums
+  // is the partial order, as in an unbatched loop
+  const int G = g.size();
+  constexpr int kMaxB = 8, kSumB = 4;
   double m = -INFINITY;
-  for (int bb = g.tid(); bb < nall; bb += g.size()) m = fmax(m, __ldcg(part + bb));
+  for (int b0 = g.tid(); b0 < nall; b0 += kMaxB * G) {
+    double v[kMaxB];
+#pragma unroll
+    for (int k = 0; k < kMaxB; ++k) v[k] = b0 + k * G < nall ? __ldcg(part + b0 + k * G) : -INFINITY;
+#pragma unroll
+    for (int k = 0; k < kMaxB; ++k) m = fmax(m, v[k]);
+  }
   double GM = sync_max(g, m, red);
   double s1 = 0.0, s2 = 0.0;
-  for (int bb = g.tid(); bb < nall; bb += g.size()) {
-    const double* p = part + bb;
-    double mb = __ldcg(p);
-    double ff = 0.0;
-    if (mb > -INFINITY) {
-      ff = exp(mb - GM);
-      s1 += __ldcg(p + ps) * ff;
-      s2 += __ldcg(p + 2 * ps) * ff * ff;
+  for (int b0 = g.tid(); b0 < nall; b0 += kSumB * G) {
+    double mb[kSumB], p1[kSumB], p2[kSumB];
+#pragma unroll
+    for (int k = 0; k < kSumB; ++k) {
+      const int bb = b0 + k * G;
+      const double* p = part + (bb < nall ? bb : 0);
+      mb[k] = bb < nall ? __ldcg(p) : -INFINITY;
+      p1[k] = __ldcg(p + ps);
+      p2[k] = __ldcg(p + 2 * ps);
     }
-    if (ecache) ecache[bb] = ff;
+#pragma unroll
+    for (int k = 0; k < kSumB; ++k) {
+      const int bb = b0 + k * G;
+      double ff = 0.0;
+      if (mb[k] > -INFINITY) {
+        ff = exp(mb[k] - GM);
+        s1 += p1[k] * ff;
+        s2 += p2[k] * ff * ff;
+      }
+      if (ecache && bb < nall) ecache[bb] = ff;
+    }
   }
   *GM_out = GM;
   *GS1_out = sync_sum(g, s1, red);
@@ -363,25 +385,47 @@ static __device__ void write_tile_prefixes(const S& g, const PfJob& J, int npart
   double* __restrict__ tprefix = J.tprefix;
   const int per = (ntiles + g.size() - 1) / g.size();
   const int b0 = min(g.tid() * per, ntiles), b1 = min(b0 + per, ntiles);
-  unsigned long long tot = 0ull;
-  auto tile_fix = [&](int bb) {  // fixed-point normalised weight of tile bb
-    unsigned long long w = 0ull;
-    for (int q = 0; q < nparts; ++q) {
-      const double* p = part + (size_t)bb * nparts + q;
-      const double mb = __ldcg(p);
-      if (mb > -INFINITY) {
-        const double e = ecache ? ecache[(size_t)bb * nparts + q] * inv_gs1 : exp(mb - lse);
-        w += __double2ull_rn(__ldcg(p + ps) * e * kFix);
+  // this thread's tiles own the contiguous partials [q0, q1), nparts per tile,
+  // read in batches of independent loads
+  constexpr int kB = 8;
+  const int q0 = b0 * nparts, q1 = b1 * nparts;
+  auto batch = [&](int j0, unsigned long long (&w)[kB]) {  // fixed-point weights of j0 .. j0+kB-1
+    double mb[kB], p1[kB];
+#pragma unroll
+    for (int k = 0; k < kB; ++k) {
+      const double* p = part + (j0 + k < q1 ? j0 + k : 0);
+      mb[k] = j0 + k < q1 ? __ldcg(p) : -INFINITY;
+      p1[k] = __ldcg(p + ps);
+    }
+#pragma unroll
+    for (int k = 0; k < kB; ++k) {
+      w[k] = 0ull;
+      if (mb[k] > -INFINITY) {
+        const double e = ecache ? ecache[j0 + k] * inv_gs1 : exp(mb[k] - lse);
+        w[k] = __double2ull_rn(p1[k] * e * kFix);
       }
     }
-    return w;
   };
-  for (int bb = b0; bb < b1; ++bb) tot += tile_fix(bb);
+  unsigned long long tot = 0ull;
+  for (int j0 = q0; j0 < q1; j0 += kB) {
+    unsigned long long w[kB];
+    batch(j0, w);
+#pragma unroll
+    for (int k = 0; k < kB; ++k) tot += w[k];
+  }
   unsigned long long all = 0ull;
   unsigned long long run = sync_excl_scan_u64(g, tot, wsum, &all);
-  for (int bb = b0; bb < b1; ++bb) {
-    tprefix[bb] = (double)run * kInvFix;
-    run += tile_fix(bb);
+  for (int j0 = q0; j0 < q1; j0 += kB) {
+    unsigned long long w[kB];
+    batch(j0, w);
+#pragma unroll
+    for (int k = 0; k < kB; ++k) {
+      const int j = j0 + k;
+      if (j < q1) {
+        if ((j - q0) % nparts == 0) tprefix[j / nparts] = (double)run * kInvFix;  // tile start
+        run += w[k];
+      }
+    }
   }
   if (g.tid() == 0) {
     tprefix[ntiles] = (double)all * kInvFix;
