@@ -511,7 +511,8 @@ function csmc_sample(rng::AbstractRNG, model, csmc::ConditionalSMC, observations
     ys = reduce(vcat, [Float64.(collect(y)) for y in observations])
     cfg = Ref(GfCsmcConfig(Int32(pf.N), pf.resampler.threshold, resampler_code(pf.resampler.resampler),
                            refresh_code(csmc.refreshment), rand(rng, UInt64)))
-    return with_lg_model(model) do m
+    # a model not of the homogeneous types runs with one parameter block per step
+    return with_lg_model_steps(model, T) do m, psteps
         dx = Int(m.dx)
         trajs = zeros(dx, T + 1, n, chains)   # the C layout [chains][n][T+1][dx], column-major here
         lls = zeros(n, chains)
@@ -519,11 +520,11 @@ function csmc_sample(rng::AbstractRNG, model, csmc::ConditionalSMC, observations
         status = zeros(Int32, chains)
         GC.@preserve trajs lls ref status ys begin
             out = Ref(GfCsmcOut(pointer(trajs), pointer(lls), pointer(ref), pointer(status)))
-            check(ccall((:gf_csmc_run, libgfb200), Int32,
-                        (Ptr{Cvoid}, Ref{GfLgModel}, Ref{GfCsmcConfig}, Int32, Ptr{Float64}, Int32, Int32,
-                         Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Ref{GfCsmcOut}),
-                        context(), m, cfg, Int32(T), ys, Int32(chains), Int32(burnin + n), Int32(burnin),
-                        isnothing(init) ? 0 : 1, C_NULL, C_NULL, GF_MEM_HOST, out))
+            check(ccall((:gf_csmc_run_tv, libgfb200), Int32,
+                        (Ptr{Cvoid}, Ref{GfLgModel}, Int32, Ref{GfCsmcConfig}, Int32, Ptr{Float64}, Int32,
+                         Int32, Int32, Int32, Ptr{Float64}, Ptr{Float64}, Int32, Ref{GfCsmcOut}),
+                        context(), m, psteps, cfg, Int32(T), ys, Int32(chains), Int32(burnin + n),
+                        Int32(burnin), isnothing(init) ? 0 : 1, C_NULL, C_NULL, GF_MEM_HOST, out))
         end
         return trajs, lls, ref
     end
