@@ -138,14 +138,10 @@ __global__ void pf_dense_ancestry_kernel(int T, int64_t N, int dx, const Real* _
 
 // The step's finalise after pf_lg_propagate_tc_units: one block of 1024
 // threads per job folds the job's unit partials (finish_step, as the last
-// propagate block does in the tile kernels), keeping each partial's
-// exponential in shared memory between the fold and the tile prefixes when
-// they fit (UNITS_ECACHE partials).
+// propagate block does in the tile kernels).
 constexpr int UNITS_FINISH_THREADS = 1024;
-constexpr int UNITS_ECACHE = 16384;
 __global__ void __launch_bounds__(UNITS_FINISH_THREADS) pf_finish_units_kernel(const PfJob* __restrict__ jobs,
                                                                                int njobs) {
-  extern __shared__ double ecache[];
   __shared__ double red[32];
   __shared__ unsigned long long s_wsum[32];
   __shared__ int s_res;
@@ -154,16 +150,11 @@ __global__ void __launch_bounds__(UNITS_FINISH_THREADS) pf_finish_units_kernel(c
   const int t = sc->t + 1;
   if (t > J.T || sc->status != 0) return;
   const bool fresh = sc->resample != 0 || sc->uniform != 0;
-  const bool cache = J.ntiles * TC_SUB <= UNITS_ECACHE;
-  finish_step(BlockSync(), J, t, fresh, TC_SUB, red, s_wsum, &s_res, cache ? ecache : nullptr);
+  finish_step(BlockSync(), J, t, fresh, TC_SUB, red, s_wsum, &s_res);
 }
 
 void launch_finish_units(gf_ctx* ctx, const PfJob* jobs_dev, int njobs) {
-  // the cache's dynamic shared memory (128 KB) needs the opt-in (current device)
-  cudaFuncSetAttribute((const void*)pf_finish_units_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)(sizeof(double) * UNITS_ECACHE));
-  pf_finish_units_kernel<<<njobs, UNITS_FINISH_THREADS, sizeof(double) * UNITS_ECACHE, ctx->stream>>>(jobs_dev,
-                                                                                                   njobs);
+  pf_finish_units_kernel<<<njobs, UNITS_FINISH_THREADS, 0, ctx->stream>>>(jobs_dev, njobs);
 }
 
 void launch_record(gf_ctx* ctx, bool dbl, const PfJob* jobs_dev, int64_t N) {
