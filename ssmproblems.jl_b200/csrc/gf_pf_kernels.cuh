@@ -504,12 +504,15 @@ static __device__ void finish_step(const S& g, const PfJob& J, int t, bool fresh
 // the job finalise the step (finish_step).  A tile may be covered by `nparts`
 // blocks (block `part` of tile `tile`); the partials are then kept per part,
 // folded in part order and summed per tile for the tile prefixes.
+// ecache (nullable): shared memory for one double per partial, which keeps each
+// partial's exponential from the fold for the tile prefixes (one exponential
+// per partial instead of three on the last block's serial path).
 static __device__ void block_finish(const PfJob& J, int tile, int t, bool fresh, LseAcc a,
-                                    double* red, int part = 0, int nparts = 1) {
+                                    double* red, int part = 0, int nparts = 1, double* ecache = nullptr) {
   if (!fold_partials(J, tile, a, red, part, nparts)) return;
   __shared__ unsigned long long s_wsum[32];
   __shared__ int s_res;
-  finish_step(BlockSync(), J, t, fresh, nparts, red, s_wsum, &s_res);
+  finish_step(BlockSync(), J, t, fresh, nparts, red, s_wsum, &s_res, ecache);
 }
 
 // Auxiliary particle filter, last block of the lookahead launch of step t:

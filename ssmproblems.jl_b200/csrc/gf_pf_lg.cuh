@@ -568,7 +568,10 @@ __global__ void __launch_bounds__(TC_THREADS, (TcSmem<DXP, DYP, STAGED>::min_blo
   if (!ok && tid == 0) sc->status = GF_ERR_TIMEOUT;
   if (STAGED && !ok) umma::mbar_wait(&gbar, (uint32_t)((TC_SUB_BLOCK - 1) & 1), TC_WAIT);  // copies in flight
   if (tid < 32) umma::tmem_dealloc(tbase, TL::NCOLS);
-  block_finish(J, tile, t, fresh, acc, red, part, TC_SPLIT);
+  // the operand buffers are free now (every MMA has completed): in the job's
+  // last block they cache the partials' exponentials for the finalise
+  const bool fits = (size_t)J.ntiles * TC_SPLIT * sizeof(double) <= TL::smem_bytes;
+  block_finish(J, tile, t, fresh, acc, red, part, TC_SPLIT, fits ? reinterpret_cast<double*>(smraw) : nullptr);
 }
 
 // The same propagation over 128-particle units instead of whole tiles: a grid
