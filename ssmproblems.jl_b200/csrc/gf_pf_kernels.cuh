@@ -448,27 +448,28 @@ static __device__ void finish_step(const S& g, const PfJob& J, int t, bool fresh
                                    double* ecache = nullptr) {
   PfScalars* const sc = J.sc;
   const bool aux = J.eta != nullptr;
+  // the job's fields and this step's schedule / uniform entries are read before
+  // the fold, so their L2 round trips overlap it (the later stores through sc
+  // and the output pointers may alias the job table and would order each read
+  // after the previous store)
+  const int T = J.T;
+  const int64_t N = J.N;
+  const double threshold = J.threshold, log_n = J.log_n;
+  const int8_t* const schedule = J.schedule;
+  double* const ll_steps = J.ll_steps;
+  double* const ess_steps = J.ess_steps;
+  int8_t* const res_steps = J.res_steps;
+  const double* const unif = J.unif;
+  const uint64_t seed = J.seed;
+  const int sch = (t < T && schedule) ? (int)schedule[t] : -1;
+  const double u_next = (t < T && unif) ? unif[t] : 0.0;
+  const double ll_prev = sc->ll, base_adj = sc->base_adj;
   // fold all partials in a fixed order (deterministic)
   double GM, GS1, GS2;
   global_stats(g, J, nparts, red, &GM, &GS1, &GS2, ecache);
-  const double base = fresh ? J.log_n + sc->base_adj : 0.0;
+  const double base = fresh ? log_n + base_adj : 0.0;
   const double lse = GM + log(GS1);
   if (g.tid() == 0) {
-    // the job's fields are loaded together before the stores through sc and
-    // the output pointers (which may alias the job table) would force each
-    // one after the previous store: one L2 round trip instead of a chain
-    const int T = J.T;
-    const int64_t N = J.N;
-    const double threshold = J.threshold;
-    const int8_t* const schedule = J.schedule;
-    double* const ll_steps = J.ll_steps;
-    double* const ess_steps = J.ess_steps;
-    int8_t* const res_steps = J.res_steps;
-    const double* const unif = J.unif;
-    const uint64_t seed = J.seed;
-    const int sch = (t < T && schedule) ? (int)schedule[t] : -1;
-    const double u_next = (t < T && unif) ? unif[t] : 0.0;
-    const double ll_prev = sc->ll;
     double inc = lse - base;
     double ess = GS1 * GS1 / GS2;
     if (!(lse > -INFINITY) || isnan(lse)) sc->status = GF_ERR_ARG;  // all weights vanished
