@@ -476,7 +476,9 @@ typedef struct {
   const double* ys;         /* host [T][dy]; copied by gf_srv_submit */
   double jitter;            /* KF, SRKF */
   int32_t use_jitter;
-  int32_t reserved;
+  int32_t param_steps;      /* PF: >= T for a time-varying model laid out as for
+                               gf_pf_run_tv; 0 or 1 = homogeneous (KF, SRKF, RBPF:
+                               homogeneous only) */
   /* Optional host destinations, written before the result is reported; they
    * must stay valid until then. */
   double* ll_steps;         /* [T] per-step log-likelihood increments */

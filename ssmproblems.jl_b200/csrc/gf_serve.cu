@@ -114,6 +114,7 @@ enum { REQ_KF = GF_REQ_KF, REQ_SRKF = GF_REQ_SRKF, REQ_PF = GF_REQ_PF, REQ_RBPF 
 struct Req {
   uint64_t id = 0, tag = 0;
   int kind = 0, T = 0;
+  int64_t obs_off = 0;  // PF: offset (doubles) of the per-step constants in the prep buffer
   int dx = 0, dy = 0, mdim = 0;  // mdim: length of the mean result
   int64_t N = 0;
   double jitter = 0.0;
@@ -330,6 +331,8 @@ static gf_status prepare(gf_ctx* ectx, const gf_srv_request* q, Req* r) {
   if (q->T < 1) return set_err(ectx, GF_ERR_ARG, "T must be >= 1");
   if (!q->ys) return set_err(ectx, GF_ERR_ARG, "ys is required");
   r->kind = q->kind;
+  if (q->kind != REQ_PF && q->param_steps > 1)
+    return set_err(ectx, GF_ERR_UNSUPPORTED, "served time-varying models run with the particle filter");
   r->T = q->T;
   r->tag = q->tag;
   r->out_steps = q->ll_steps;
@@ -374,8 +377,12 @@ static gf_status prepare(gf_ctx* ectx, const gf_srv_request* q, Req* r) {
   if (q->kind == REQ_PF) {
     if (!q->lg) return set_err(ectx, GF_ERR_ARG, "PF request needs lg");
     r->lg.reset(new LgJobSetup);
-    gf_status st = lg_job_setup(ectx, q->lg, &cfg, r->T, 0, r->lg.get());
+    gf_status st = lg_job_setup(ectx, q->lg, &cfg, r->T, 0, r->lg.get(), q->param_steps > 1 ? q->param_steps : 1);
     if (st) return st;
+    // a time-varying model's per-step observation and proposal constants ride at
+    // the end of the observation-prep buffer
+    r->obs_off = (int64_t)r->lg->pp.size();
+    r->lg->pp.insert(r->lg->pp.end(), r->lg->obs_consts.begin(), r->lg->obs_consts.end());
     r->dx = q->lg->dx;
     r->dy = q->lg->dy;
     r->mdim = r->dx;
@@ -497,6 +504,8 @@ gf_status gf_srv::start_pf(Req* r) {
   J.ys = (const double*)D(r->d_ys);
   J.ll_steps = r->out_steps ? (double*)D(r->d_steps) : nullptr;
   J.means_out = r->out_mean ? (double*)D(r->d_means) : nullptr;
+  if (r->kind == REQ_PF)
+    J.obs_consts = r->lg->obs_consts.empty() ? nullptr : (const double*)D(r->d_pp) + r->obs_off;
   r->job = J;
   r->job_dev = (PfJob*)D(r->d_job);
   // staging

@@ -105,7 +105,7 @@ class SrvConfigC(C.Structure):
 class SrvRequestC(C.Structure):
     _fields_ = [("kind", C.c_int32), ("T", C.c_int32), ("lg", C.POINTER(LGModelC)),
                 ("rb", C.POINTER(RBModelC)), ("pf", C.POINTER(PFConfigC)), ("ys", _dp),
-                ("jitter", C.c_double), ("use_jitter", C.c_int32), ("reserved", C.c_int32),
+                ("jitter", C.c_double), ("use_jitter", C.c_int32), ("param_steps", C.c_int32),
                 ("ll_steps", _dp), ("mean", _dp), ("cov", _dp), ("tag", C.c_uint64)]
 
 

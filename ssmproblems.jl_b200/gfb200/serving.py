@@ -62,6 +62,7 @@ class Server:
             mc = model._c_struct()
             keep["mc"] = mc
             req.lg = C.pointer(mc)
+            req.param_steps = model.param_steps() if model.is_time_varying() else 1
             req.jitter = float(algo.jitter or 0.0)
             req.use_jitter = int(algo.jitter is not None)
             dx, dy, mdim = model.dx, model.dy, model.dx
@@ -84,6 +85,7 @@ class Server:
             mc = model._c_struct()
             keep["mc"] = mc
             req.lg = C.pointer(mc)
+            req.param_steps = model.param_steps() if model.is_time_varying() else 1
             dy, mdim = model.dy, model.dx
             T = ys.size // dy
             cfg, sched, _ = _pf_config(algo, T, seed, schedule)

@@ -162,3 +162,36 @@ def test_invalid_request_rejected_at_submit(ctx):
         with pytest.raises(G.GFError) as e:
             srv.submit(m, G.KF(), rng.standard_normal((5, 2)))
         assert e.value.code == L.GF_ERR_DIM
+
+
+def test_served_time_varying_pf_matches_standalone(ctx):
+    """A particle filter on a time-varying model, served in a mix with homogeneous
+    ones, returns exactly what the standalone gf_pf_run_tv call returns; a
+    time-varying Kalman request is refused at submit (homogeneous only)."""
+    import oracle as O
+    rng = np.random.default_rng(8)
+    reqs = []
+    for dx, dy, T, N in [(2, 2, 30, 5000), (4, 3, 50, 3000), (16, 8, 20, 8192)]:
+        om = O.create_nonhomogeneous_linear_gaussian_model(rng, dx, dy, T)
+        As = [O.random_orthogonal(rng, dx) * rng.uniform(0.5, 0.95) for _ in range(T)]
+        om = O.LGModel.time_varying(om.mu0, om.Sigma0, As, om.bs, om.Qs, om.Hs, om.cs, om.Rs)
+        gm = G.create_nonhomogeneous_linear_gaussian_model(om.mu0, om.Sigma0, om.As, om.bs, om.Qs,
+                                                           om.Hs, om.cs, om.Rs)
+        reqs.append((gm, G.BF(N, threshold=0.6), O.sample(rng, om, T)[1], 40 + dx))
+    m, ys = W.lgssm_1d(seed=5, T=40)
+    reqs.append((m, G.BF(4096, threshold=0.5), ys, 9))
+    with G.Server(hbm_budget_bytes=1 << 30, host_budget_bytes=128 << 20, pf_chunk=8) as srv:
+        for k, (gm, algo, ys, seed) in enumerate(reqs):
+            srv.submit(gm, algo, ys, seed=seed, tag=k, want_steps=True, want_mean=True)
+        with pytest.raises(Exception):
+            srv.submit(reqs[0][0], G.KalmanFilter(), reqs[0][2])
+        srv.drain(timeout_ms=60000)
+        got = {r["tag"]: r for r in srv.poll(max_results=64)}
+    assert len(got) == len(reqs)
+    for k, (gm, algo, ys, seed) in enumerate(reqs):
+        r = got[k]
+        assert r["status"] == 0, (k, r)
+        ll, steps, mean, _ = _standalone(ctx, "bf", gm, algo, ys, seed)
+        assert r["ll"] == ll, (k, r["ll"], ll)
+        np.testing.assert_array_equal(r["ll_steps"], steps)
+        np.testing.assert_array_equal(r["mean"], mean)
